@@ -1,0 +1,86 @@
+/*
+ * oracle.h — CPU restatement of compute-vp9's reconstruction, used ONLY as
+ * the checker by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg. Nothing in the product links or calls it.
+ *
+ * Two arithmetic profiles:
+ *   REFCPU — src/decoder/vp9_reconstruct.c:13-370 plus the reference-pool and
+ *            output handling of src/decoder/vp9_decoder.c:209-247. Pinned
+ *            against the reference compiled from source (oracle/_ref) and the
+ *            committed golden hashes in tests/golden/.
+ *   SPEC   — the arithmetic of shaders/vp9_idct.comp.glsl, vp9_mc.comp.glsl,
+ *            vp9_intra_pred.comp.glsl, vp9_loopfilter.comp.glsl and
+ *            vp9_nv12_pack.comp.glsl, applied block by block in parse order,
+ *            with chroma MC and the all-plane residual written from the VP9
+ *            design. The shaders cannot run here (no graphics stack), so this
+ *            profile's parity is unpinned except where it coincides with the
+ *            REFCPU loop filter.
+ */
+#ifndef CVP9_ORACLE_H
+#define CVP9_ORACLE_H
+
+#include "cvp9_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORACLE_REFCPU = 0, ORACLE_SPEC = 1 };
+
+/* A frame owned by the oracle: I420, stride = width (vp9_frame.c:8-34). */
+typedef struct {
+    uint32_t width, height, stride_y, stride_uv;
+    uint8_t *y, *u, *v;
+} oracle_frame_t;
+
+/* REFCPU: whole-frame reconstruction. refs[i] may be NULL or have NULL planes
+ * (the "reference missing" path). out is (re)allocated and filled. */
+int  oracle_refcpu_reconstruct(const vp9_parsed_frame_t *pf,
+                               const oracle_frame_t *const refs[8],
+                               oracle_frame_t *out);
+
+/* SPEC: whole-frame reconstruction from the pool slots (8). */
+int  oracle_spec_reconstruct(const vp9_parsed_frame_t *pf,
+                             const oracle_frame_t *const pool[8],
+                             oracle_frame_t *out);
+
+void oracle_frame_free(oracle_frame_t *f);
+
+/* ── Stage-level entry points (unit tests) ─────────────────────────────── */
+
+/* REFCPU float64 inverse DCT of raw coefficients (vp9_reconstruct.c:13-60). */
+void oracle_refcpu_idct2d(const int16_t *in, int16_t *out, int n);
+
+/* SPEC integer inverse DCT with dequantisation (vp9_idct.comp.glsl:654-789):
+ * returns the rounded residual (before the add/clamp). */
+void oracle_spec_idct2d(const int16_t *in, int32_t *out, int n, int q_dc, int q_ac);
+
+/* Loop filter in place on a luma plane: REFCPU (level 0 = off) or SPEC
+ * (threshold floored at 1, always on). */
+void oracle_loopfilter(uint8_t *y, uint32_t w, uint32_t h, uint32_t stride,
+                       int level, int sharpness, int profile);
+
+/* I420 -> NV12 (vp9_nv12_pack.comp.glsl:33-59); dst holds w*h + 2*cw*ch bytes. */
+void oracle_nv12_pack(const uint8_t *i420, uint8_t *dst, uint32_t w, uint32_t h);
+
+/* ── Stream harness: recon + reference pool + delivery ─────────────────── */
+
+typedef struct oracle_stream oracle_stream_t;
+
+oracle_stream_t *oracle_stream_create(int profile);
+void             oracle_stream_destroy(oracle_stream_t *s);
+
+/* Reconstruct one frame and apply the profile's pool update. The decoded
+ * I420 frame (w*h + 2*cw*ch bytes) is copied to out_i420 if non-NULL. */
+int              oracle_stream_decode(oracle_stream_t *s, const vp9_parsed_frame_t *pf,
+                                      uint8_t *out_i420);
+
+/* 8-bit DC/AC quantiser lookups (src/decoder/vp9_dequant.h:12-75). */
+int oracle_dc_quant(int qindex);
+int oracle_ac_quant(int qindex);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVP9_ORACLE_H */
