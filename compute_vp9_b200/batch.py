@@ -1,0 +1,146 @@
+"""ctypes binding of the multi-stream engine (include/cvp9_batch.h)."""
+import ctypes as C
+
+import numpy as np
+
+from .cvp9_ctypes import CVP9_OK, ERR_NAMES, FrameInfo, ParsedFrame, i420_size
+
+DEVICE_INPUTS = 1
+NO_OUTPUT = 2
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("arith", C.c_int), ("hbm_budget", C.c_uint64),
+                ("max_streams", C.c_int), ("use_graphs", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("step_ms", C.c_float), ("kernels_ms", C.c_float), ("h2d_ms", C.c_float),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("reserved_bytes", C.c_uint64), ("open_streams", C.c_int),
+                ("graph_replays", C.c_int), ("kernel_launches", C.c_uint32),
+                ("scan_ms", C.c_float), ("recon_ms", C.c_float), ("filter_ms", C.c_float)]
+
+
+def _bind(lib):
+    vp = C.c_void_p
+    lib.cvp9_batch_create.argtypes = [C.POINTER(BatchConfig), C.POINTER(vp)]
+    lib.cvp9_batch_destroy.argtypes = [vp]
+    lib.cvp9_batch_destroy.restype = None
+    lib.cvp9_batch_stream_bytes.argtypes = [C.c_uint32, C.c_uint32]
+    lib.cvp9_batch_stream_bytes.restype = C.c_uint64
+    lib.cvp9_batch_open_stream.argtypes = [vp, C.c_uint32, C.c_uint32]
+    lib.cvp9_batch_close_stream.argtypes = [vp, C.c_int]
+    lib.cvp9_batch_submit.argtypes = [vp, C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(C.POINTER(ParsedFrame)), C.POINTER(C.c_int64),
+                                      C.c_uint32]
+    lib.cvp9_batch_wait.argtypes = [vp]
+    lib.cvp9_batch_poll.argtypes = [vp]
+    lib.cvp9_batch_get_frame.argtypes = [vp, C.c_int, C.POINTER(FrameInfo)]
+    lib.cvp9_batch_stats.argtypes = [vp, C.POINTER(BatchStats)]
+    lib.cvp9_batch_last_error.argtypes = [vp]
+    lib.cvp9_batch_last_error.restype = C.c_char_p
+    lib.cvp9_batch_timer_start.argtypes = [vp]
+    lib.cvp9_batch_timer_stop.argtypes = [vp, C.POINTER(C.c_float)]
+    lib.cvp9_batch_last_seq.argtypes = [vp]
+    lib.cvp9_batch_last_seq.restype = C.c_uint64
+    lib.cvp9_batch_step_latency.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double)]
+
+
+class BatchError(RuntimeError):
+    def __init__(self, code, what, detail=""):
+        self.code = code
+        super().__init__("%s: %s (%d) %s" % (what, ERR_NAMES.get(code, "?"), code, detail))
+
+
+class Batch:
+    """Engine handle. Streams are admitted by HBM budget (open_stream returns
+    None when the budget is full); step() reconstructs one frame per listed
+    stream in one launch chain."""
+
+    def __init__(self, device=-1, arith=-1, hbm_budget=0, max_streams=0, use_graphs=1):
+        from . import cuda_lib
+        self._lib = cuda_lib()
+        self._h = C.c_void_p()
+        cfg = BatchConfig(device, arith, hbm_budget, max_streams, use_graphs)
+        rc = self._lib.cvp9_batch_create(C.byref(cfg), C.byref(self._h))
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_create")
+
+    def stream_bytes(self, w, h):
+        return int(self._lib.cvp9_batch_stream_bytes(w, h))
+
+    def open_stream(self, w, h):
+        sid = self._lib.cvp9_batch_open_stream(self._h, w, h)
+        return sid if sid >= 0 else None
+
+    def close_stream(self, sid):
+        rc = self._lib.cvp9_batch_close_stream(self._h, sid)
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_close_stream", self.last_error())
+
+    def submit(self, sids, pfs, pts=None, flags=0):
+        n = len(sids)
+        arr_s = (C.c_int * n)(*sids)
+        arr_p = (C.POINTER(ParsedFrame) * n)(*pfs)
+        arr_t = (C.c_int64 * n)(*(pts if pts is not None else [0] * n))
+        rc = self._lib.cvp9_batch_submit(self._h, n, arr_s, arr_p, arr_t, flags)
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_submit", self.last_error())
+
+    def wait(self):
+        return self._lib.cvp9_batch_wait(self._h)
+
+    def poll(self):
+        return self._lib.cvp9_batch_poll(self._h)
+
+    def get_frame(self, sid):
+        info = FrameInfo()
+        rc = self._lib.cvp9_batch_get_frame(self._h, sid, C.byref(info))
+        return rc, info
+
+    def get_frame_array(self, sid):
+        rc, info = self.get_frame(sid)
+        if rc != CVP9_OK:
+            return rc, None
+        n = i420_size(info.width, info.height)
+        return rc, np.ctypeslib.as_array(info.plane_y, shape=(n,)).copy()
+
+    def stats(self):
+        st = BatchStats()
+        self._lib.cvp9_batch_stats(self._h, C.byref(st))
+        return st
+
+    def last_error(self):
+        return self._lib.cvp9_batch_last_error(self._h).decode()
+
+    def timer_start(self):
+        rc = self._lib.cvp9_batch_timer_start(self._h)
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_timer_start", self.last_error())
+
+    def timer_stop(self):
+        ms = C.c_float()
+        rc = self._lib.cvp9_batch_timer_stop(self._h, C.byref(ms))
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_timer_stop", self.last_error())
+        return ms.value
+
+    def last_seq(self):
+        return int(self._lib.cvp9_batch_last_seq(self._h))
+
+    def step_latency_ms(self, seq):
+        ms = C.c_double()
+        rc = self._lib.cvp9_batch_step_latency(self._h, seq, C.byref(ms))
+        return ms.value if rc == CVP9_OK else None
+
+    def close(self):
+        if self._h:
+            self._lib.cvp9_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,122 @@
+/*
+ * backend_common.c — device setup, DCT basis, ticket order, job geometry.
+ * Compiled with -ffp-contract=off so the basis matches the reference's
+ * separately rounded float64 arithmetic.
+ */
+#include "backend_common.h"
+#include "recon_launch.h"
+#include "vp9_tables.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+static const int16_t k_dc_q[256] = CVP9_QTABLE_DC_INIT;
+static const int16_t k_ac_q[256] = CVP9_QTABLE_AC_INIT;
+
+int cvp9_dc_q(int q) { return k_dc_q[CVP9_QINDEX_CLAMP(q)]; }
+int cvp9_ac_q(int q) { return k_ac_q[CVP9_QINDEX_CLAMP(q)]; }
+
+void cvp9_build_dct_basis(double *out)
+{
+    int base = 0;
+    for (int n = 4; n <= 32; n *= 2) {
+        double scale_zero = sqrt(1.0 / n);
+        double scale_other = sqrt(2.0 / n);
+        for (int i = 0; i < n; i++) {
+            double scale = (i == 0) ? scale_zero : scale_other;
+            for (int j = 0; j < n; j++)
+                out[base + i * n + j] = scale * cos(((2.0 * j + 1.0) * i * 3.141592653589793) / (2.0 * n));
+        }
+        base += n * n;
+    }
+}
+
+#define MAX_DEVICES 64
+static pthread_mutex_t g_setup_lock = PTHREAD_MUTEX_INITIALIZER;
+static int g_setup_done[MAX_DEVICES];
+static int g_ctas[MAX_DEVICES][2];
+
+int cvp9_device_setup(int device)
+{
+    if (device < 0 || device >= MAX_DEVICES) return -1;
+    if (cudaSetDevice(device) != cudaSuccess) return -1;
+    pthread_mutex_lock(&g_setup_lock);
+    int rc = 0;
+    if (!g_setup_done[device]) {
+        double basis[16 + 64 + 256 + 1024];
+        cvp9_build_dct_basis(basis);
+        if (cvp9k_upload_dct_basis(basis, 16 + 64 + 256 + 1024) != 0 || cvp9k_configure() != 0) {
+            rc = -1;
+        } else {
+            g_ctas[device][0] = cvp9k_recon_ctas_per_sm(CVP9_ARITH_REFCPU);
+            g_ctas[device][1] = cvp9k_recon_ctas_per_sm(CVP9_ARITH_SPEC);
+            g_setup_done[device] = 1;
+        }
+    }
+    pthread_mutex_unlock(&g_setup_lock);
+    return rc;
+}
+
+int cvp9_recon_ctas_per_sm(int device, int arith)
+{
+    if (device < 0 || device >= MAX_DEVICES) return 1;
+    int v = g_ctas[device][arith == CVP9_ARITH_SPEC ? 1 : 0];
+    return v > 0 ? v : 1;
+}
+
+int cvp9_tickets_on_diagonal(int sb_cols, int sb_rows, int job, int d, uint32_t *out)
+{
+    int n = 0;
+    int r0 = d - (sb_cols - 1);
+    if (r0 < 0) r0 = 0;
+    int r1 = d < sb_rows - 1 ? d : sb_rows - 1;
+    for (int r = r0; r <= r1; r++) {
+        int c = d - r;
+        out[n++] = ((uint32_t)job << 20) | (uint32_t)(r * sb_cols + c);
+    }
+    return n;
+}
+
+int cvp9_env_device(void)
+{
+    const char *e = getenv("CVP9_CUDA_DEVICE");
+    return e && *e ? atoi(e) : 0;
+}
+
+int cvp9_env_arith(void)
+{
+    const char *e = getenv("CVP9_ARITH");
+    if (e && (strcmp(e, "spec") == 0 || strcmp(e, "SPEC") == 0)) return CVP9_ARITH_SPEC;
+    return CVP9_ARITH_REFCPU;
+}
+
+void cvp9_job_geometry(cvp9_job_t *job, const vp9_parsed_frame_t *pf)
+{
+    int W = (int)pf->hdr.width, H = (int)pf->hdr.height;
+    job->W = W;
+    job->H = H;
+    job->CW = (W + 1) / 2;
+    job->CH = (H + 1) / 2;
+    job->sb_cols = (W + 63) / 64;
+    job->sb_rows = (H + 63) / 64;
+    job->mi_cols = (W + 7) / 8;
+    job->mi_rows = (H + 7) / 8;
+    job->num_blocks = pf->num_blocks;
+    job->num_coeffs = pf->num_coeffs;
+    job->q_dc = cvp9_dc_q(pf->hdr.base_qindex);
+    job->q_ac = cvp9_ac_q(pf->hdr.base_qindex);
+    job->lf_level = pf->hdr.filter_level;
+    job->lf_sharpness = pf->hdr.sharpness_level;
+    for (int i = 0; i < 3; i++) job->ref_slot_of[i] = pf->hdr.ref_frame_idx[i] & 7;
+    job->lf_tiled = (uint8_t)((W % 8) != 1 && (H % 8) != 1);
+}
+
+double cvp9_now(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}

@@ -1,0 +1,813 @@
+/*
+ * batch.c — multi-stream reconstruction engine (include/cvp9_batch.h).
+ *
+ * Three CUDA streams: inputs go up on `hs`, kernels run on `cs`, outputs
+ * come down on `ds`, so step n+1's upload and step n-1's download overlap
+ * step n's kernels. Two step slots hold the per-step staging (pinned
+ * inputs, device inputs, job table, SB scratch, tickets, statuses, cached
+ * graph); a slot is reused only after the step that last used it is done.
+ *
+ * Per stream the engine keeps the reference pool on the device (up to 12
+ * frame buffers; refs are pointer swaps) and its SB done flags, whose epoch
+ * advances every frame so they never need clearing.
+ */
+#include "cvp9_batch.h"
+#include "backend_common.h"
+#include "recon_launch.h"
+
+#include <cuda_runtime_api.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#define BSLOTS 2
+#define MAXF 12
+#define WAIT_LIMIT_S 60.0
+#define ALIGN_UP(x, a) (((x) + (a) - 1) / (a) * (a))
+#define LAT_RING 4096
+
+typedef struct {
+    uint8_t *dev;
+    size_t   cap;
+    int32_t  w, h;
+    int      users;
+    uint64_t d2h_seq;          /* last step whose download reads this frame */
+} bframe_t;
+
+typedef struct {
+    int       open;
+    int32_t   W, H;
+    int       n_sb;
+    uint32_t *d_sb_done;
+    uint32_t  epoch;
+    bframe_t  f[MAXF];
+    int       ref_slot[8];
+    uint64_t  reserved;
+    uint8_t  *h_out[2];
+    size_t    h_out_cap[2];
+    int32_t   out_w[2], out_h[2];
+    int64_t   out_pts[2];
+    uint64_t  out_seq[2];
+    int       latest;           /* output buffer of the newest step, -1 none */
+    uint64_t  last_seq;         /* newest step that included this stream     */
+    uint32_t  last_status;
+} bstream_t;
+
+struct cvp9_batch;
+typedef struct { struct cvp9_batch *b; uint64_t seq; } lat_arg_t;
+
+typedef struct {
+    uint64_t        seq;
+    int             busy;
+    lat_arg_t       lat_arg;     /* completion-callback argument of this slot */
+    cudaEvent_t     ev_start, ev_h2d, ev_k0, ev_k1, ev_end;
+    cudaEvent_t     ev_kern[4];
+    uint8_t        *h_in;   size_t h_in_cap;
+    uint8_t        *d_in;   size_t d_in_cap;
+    cvp9_job_t     *h_jobs; cvp9_job_t *d_jobs; int jobs_cap;
+    uint32_t       *d_sb_range; size_t sb_cap;      /* uint32 entries */
+    uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status */
+    uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
+    cudaGraphExec_t graph; uint64_t graph_key;
+    int             n;
+    int            *sids;  int sids_cap;
+    uint64_t        h2d_bytes, d2h_bytes;
+    uint32_t        launches;
+} bslot_t;
+
+struct cvp9_batch {
+    int          device, arith, use_graphs, max_streams;
+    uint64_t     budget, reserved;
+    cudaStream_t cs, hs, ds;
+    bstream_t   *st;
+    int          nst;
+    bslot_t      slot[BSLOTS];
+    uint64_t     seq;        /* steps submitted */
+    uint64_t     done_seq;   /* every step <= done_seq is complete */
+    int          graph_replays;
+    int          resident_ctas;
+    cudaEvent_t  ev_t0, ev_t1;
+    /* host-clock submit and completion time of recent steps */
+    double       lat_submit[LAT_RING];
+    volatile double lat_done[LAT_RING];
+    uint64_t     lat_seq[LAT_RING];
+    cvp9_batch_stats_t last;
+    char         err[192];
+};
+
+static cvp9_err_t bfail(cvp9_batch_t *b, cudaError_t e, const char *what)
+{
+    snprintf(b->err, sizeof(b->err), "%s: %s", what, cudaGetErrorString(e));
+    return CVP9_ERR_GPU;
+}
+
+#define BCK(call, what) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return bfail(b, e_, what); } while (0)
+
+static size_t frame_bytes(int32_t w, int32_t h)
+{
+    return (size_t)w * h + 2 * (size_t)((w + 1) / 2) * ((h + 1) / 2);
+}
+
+uint64_t cvp9_batch_stream_bytes(uint32_t w, uint32_t h)
+{
+    /* reference frames (LAST, GOLDEN, ALTREF, a stale key frame), the frame
+     * being written, one whose download is in flight; SB flags; per-step
+     * inputs at the dense coefficient size (2 bytes per sample) x 2 slots */
+    uint64_t fb = frame_bytes((int32_t)w, (int32_t)h);
+    uint64_t nsb = (uint64_t)((w + 63) / 64) * ((h + 63) / 64);
+    return 6 * fb + nsb * 20 + 2 * (2 * fb + (uint64_t)((w + 7) / 8) * ((h + 7) / 8) * 32);
+}
+
+cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
+{
+    if (!out) return CVP9_ERR_INVALID_DATA;
+    *out = NULL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return CVP9_ERR_NO_BACKEND;
+    cvp9_batch_t *b = calloc(1, sizeof(*b));
+    if (!b) return CVP9_ERR_NOMEM;
+    b->device = (cfg && cfg->device >= 0) ? cfg->device : cvp9_env_device();
+    b->arith = (cfg && cfg->arith >= 0) ? (cfg->arith ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU) : cvp9_env_arith();
+    b->budget = (cfg && cfg->hbm_budget) ? cfg->hbm_budget : 150ull * 1000 * 1000 * 1000;
+    b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
+    b->use_graphs = cfg ? cfg->use_graphs : 1;
+    if (b->device >= ndev || cvp9_device_setup(b->device) != 0) { free(b); return CVP9_ERR_NO_BACKEND; }
+    b->st = calloc((size_t)b->max_streams, sizeof(bstream_t));
+    if (!b->st) { free(b); return CVP9_ERR_NOMEM; }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->resident_ctas = sms * cvp9_recon_ctas_per_sm(b->device, b->arith);
+    if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->hs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->ds, cudaStreamNonBlocking) != cudaSuccess) {
+        cvp9_batch_destroy(b);
+        return CVP9_ERR_GPU;
+    }
+    for (int i = 0; i < BSLOTS; i++) {
+        bslot_t *s = &b->slot[i];
+        if (cudaEventCreate(&s->ev_start) != cudaSuccess || cudaEventCreate(&s->ev_h2d) != cudaSuccess ||
+            cudaEventCreate(&s->ev_k0) != cudaSuccess || cudaEventCreate(&s->ev_k1) != cudaSuccess ||
+            cudaEventCreate(&s->ev_end) != cudaSuccess || cudaEventCreate(&s->ev_kern[0]) != cudaSuccess ||
+            cudaEventCreate(&s->ev_kern[1]) != cudaSuccess || cudaEventCreate(&s->ev_kern[2]) != cudaSuccess ||
+            cudaEventCreate(&s->ev_kern[3]) != cudaSuccess) {
+            cvp9_batch_destroy(b);
+            return CVP9_ERR_GPU;
+        }
+    }
+    if (cudaEventCreate(&b->ev_t0) != cudaSuccess || cudaEventCreate(&b->ev_t1) != cudaSuccess) {
+        cvp9_batch_destroy(b);
+        return CVP9_ERR_GPU;
+    }
+    *out = b;
+    return CVP9_OK;
+}
+
+static void free_stream(bstream_t *s)
+{
+    for (int i = 0; i < MAXF; i++) cudaFree(s->f[i].dev);
+    cudaFree(s->d_sb_done);
+    cudaFreeHost(s->h_out[0]);
+    cudaFreeHost(s->h_out[1]);
+    memset(s, 0, sizeof(*s));
+}
+
+void cvp9_batch_destroy(cvp9_batch_t *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->cs) cudaStreamSynchronize(b->cs);
+    if (b->hs) cudaStreamSynchronize(b->hs);
+    if (b->ds) cudaStreamSynchronize(b->ds);
+    for (int i = 0; i < BSLOTS; i++) {
+        bslot_t *s = &b->slot[i];
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        if (s->ev_start) cudaEventDestroy(s->ev_start);
+        if (s->ev_h2d) cudaEventDestroy(s->ev_h2d);
+        if (s->ev_k0) cudaEventDestroy(s->ev_k0);
+        if (s->ev_k1) cudaEventDestroy(s->ev_k1);
+        if (s->ev_end) cudaEventDestroy(s->ev_end);
+        for (int k = 0; k < 4; k++) if (s->ev_kern[k]) cudaEventDestroy(s->ev_kern[k]);
+        cudaFreeHost(s->h_in);
+        cudaFree(s->d_in);
+        cudaFreeHost(s->h_jobs);
+        cudaFree(s->d_jobs);
+        cudaFree(s->d_sb_range);
+        cudaFree(s->d_misc);
+        cudaFreeHost(s->h_misc);
+        cudaFree(s->d_tickets);
+        free(s->sids);
+    }
+    if (b->st)
+        for (int i = 0; i < b->max_streams; i++)
+            if (b->st[i].open) free_stream(&b->st[i]);
+    free(b->st);
+    if (b->ev_t0) cudaEventDestroy(b->ev_t0);
+    if (b->ev_t1) cudaEventDestroy(b->ev_t1);
+    if (b->cs) cudaStreamDestroy(b->cs);
+    if (b->hs) cudaStreamDestroy(b->hs);
+    if (b->ds) cudaStreamDestroy(b->ds);
+    free(b);
+}
+
+int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
+{
+    if (!b || w == 0 || h == 0 || w > 65535 || h > 65535) return CVP9_ERR_INVALID_DATA;
+    uint64_t need = cvp9_batch_stream_bytes(w, h);
+    if (b->reserved + need > b->budget) return CVP9_ERR_NOMEM;
+    int sid = -1;
+    for (int i = 0; i < b->max_streams; i++)
+        if (!b->st[i].open) { sid = i; break; }
+    if (sid < 0) return CVP9_ERR_NOMEM;
+    bstream_t *s = &b->st[sid];
+    memset(s, 0, sizeof(*s));
+    s->W = (int32_t)w;
+    s->H = (int32_t)h;
+    s->n_sb = (int)(((w + 63) / 64) * ((h + 63) / 64));
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaMalloc((void **)&s->d_sb_done, (size_t)s->n_sb * 4) != cudaSuccess ||
+        cudaMemset(s->d_sb_done, 0, (size_t)s->n_sb * 4) != cudaSuccess) {
+        free_stream(s);
+        return CVP9_ERR_NOMEM;
+    }
+    for (int i = 0; i < 8; i++) s->ref_slot[i] = -1;
+    s->latest = -1;
+    s->reserved = need;
+    s->open = 1;
+    b->reserved += need;
+    if (sid + 1 > b->nst) b->nst = sid + 1;
+    return sid;
+}
+
+static int stream_busy(cvp9_batch_t *b, const bstream_t *s)
+{
+    return s->last_seq > b->done_seq;
+}
+
+static cvp9_err_t wait_slot(cvp9_batch_t *b, bslot_t *s);
+
+cvp9_err_t cvp9_batch_close_stream(cvp9_batch_t *b, int sid)
+{
+    if (!b || sid < 0 || sid >= b->max_streams || !b->st[sid].open) return CVP9_ERR_INVALID_DATA;
+    bstream_t *s = &b->st[sid];
+    if (stream_busy(b, s)) {
+        cvp9_err_t e = cvp9_batch_wait(b);
+        if (e == CVP9_ERR_GPU) return e;
+    }
+    b->reserved -= s->reserved;
+    free_stream(s);
+    return CVP9_OK;
+}
+
+static cvp9_err_t grow_dev(cvp9_batch_t *b, void **p, size_t *cap, size_t need)
+{
+    if (*cap >= need) return CVP9_OK;
+    cudaFree(*p);
+    *p = NULL;
+    *cap = 0;
+    size_t n = need + need / 4 + 4096;
+    BCK(cudaMalloc(p, n), "device staging");
+    *cap = n;
+    return CVP9_OK;
+}
+
+static cvp9_err_t grow_host(cvp9_batch_t *b, void **p, size_t *cap, size_t need)
+{
+    if (*cap >= need) return CVP9_OK;
+    cudaFreeHost(*p);
+    *p = NULL;
+    *cap = 0;
+    size_t n = need + need / 4 + 4096;
+    BCK(cudaMallocHost(p, n), "pinned staging");
+    *cap = n;
+    return CVP9_OK;
+}
+
+/* A frame buffer of stream s with no reference user; if its last download
+ * may still be running, the compute stream waits for it. */
+static int acquire_frame(cvp9_batch_t *b, bstream_t *s)
+{
+    size_t need = frame_bytes(s->W, s->H);
+    int pick = -1;
+    for (int i = 0; i < MAXF; i++) {
+        if (s->f[i].users) continue;
+        if (s->f[i].dev && s->f[i].cap >= need) { pick = i; break; }
+        if (pick < 0) pick = i;
+    }
+    if (pick < 0) return -1;
+    bframe_t *f = &s->f[pick];
+    if (f->d2h_seq > b->done_seq) {
+        /* only the previous step can still be downloading it */
+        bslot_t *o = &b->slot[f->d2h_seq % BSLOTS];
+        if (o->seq == f->d2h_seq) cudaStreamWaitEvent(b->cs, o->ev_end, 0);
+    }
+    if (!f->dev || f->cap < need) {
+        if (f->dev) { cudaDeviceSynchronize(); cudaFree(f->dev); }
+        f->dev = NULL;
+        f->cap = 0;
+        if (cudaMalloc((void **)&f->dev, need) != cudaSuccess) return -1;
+        f->cap = need;
+    }
+    f->w = s->W;
+    f->h = s->H;
+    return pick;
+}
+
+static void set_ref(bstream_t *s, int slot, int frame)
+{
+    if (s->ref_slot[slot] >= 0) s->f[s->ref_slot[slot]].users--;
+    s->ref_slot[slot] = frame;
+    if (frame >= 0) s->f[frame].users++;
+}
+
+static uint64_t mix64(uint64_t h, uint64_t v)
+{
+    h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    return h * 0xBF58476D1CE4E5B9ull;
+}
+
+static void complete_slot(cvp9_batch_t *b, bslot_t *s)
+{
+    float t = 0.f, k = 0.f, u = 0.f;
+    cudaEventElapsedTime(&t, s->ev_start, s->ev_end);
+    cudaEventElapsedTime(&k, s->ev_k0, s->ev_k1);
+    cudaEventElapsedTime(&u, s->ev_start, s->ev_h2d);
+    b->last.step_ms = t;
+    b->last.kernels_ms = k;
+    b->last.h2d_ms = u;
+    b->last.h2d_bytes = s->h2d_bytes;
+    b->last.d2h_bytes = s->d2h_bytes;
+    b->last.kernel_launches = s->launches;
+    float a = 0.f, r = 0.f, f = 0.f;
+    cudaEventElapsedTime(&a, s->ev_kern[0], s->ev_kern[1]);
+    cudaEventElapsedTime(&r, s->ev_kern[1], s->ev_kern[2]);
+    cudaEventElapsedTime(&f, s->ev_kern[2], s->ev_kern[3]);
+    b->last.scan_ms = a;
+    b->last.recon_ms = r;
+    b->last.filter_ms = f;
+    for (int i = 0; i < s->n; i++) {
+        bstream_t *st = &b->st[s->sids[i]];
+        if (st->open && st->last_seq == s->seq) st->last_status = s->h_misc[1 + i];
+    }
+    if (s->seq > b->done_seq) b->done_seq = s->seq;
+    s->busy = 0;
+}
+
+static cvp9_err_t wait_slot(cvp9_batch_t *b, bslot_t *s)
+{
+    if (!s->busy) return CVP9_OK;
+    double t0 = cvp9_now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(s->ev_end);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return bfail(b, e, "step completion");
+        if (cvp9_now() - t0 > WAIT_LIMIT_S) {
+            snprintf(b->err, sizeof(b->err), "step did not complete within %.0f s", WAIT_LIMIT_S);
+            return CVP9_ERR_GPU;
+        }
+        struct timespec ts = { 0, 20000 };
+        nanosleep(&ts, NULL);
+    }
+    complete_slot(b, s);
+    return CVP9_OK;
+}
+
+static int is_pinned(const void *p)
+{
+    struct cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static void CUDART_CB step_done_cb(void *p)
+{
+    lat_arg_t *a = (lat_arg_t *)p;
+    a->b->lat_done[a->seq % LAT_RING] = cvp9_now();
+}
+
+cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
+                             const vp9_parsed_frame_t *const *pfs, const int64_t *pts, uint32_t flags)
+{
+    if (!b || n <= 0 || !sids || !pfs) return CVP9_ERR_INVALID_DATA;
+    if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
+    const int dev_in = (flags & CVP9_BATCH_DEVICE_INPUTS) != 0;
+    const int want_out = !(flags & CVP9_BATCH_NO_OUTPUT);
+
+    /* validate */
+    for (int i = 0; i < n; i++) {
+        int sid = sids[i];
+        if (sid < 0 || sid >= b->max_streams || !b->st[sid].open || !pfs[i]) return CVP9_ERR_INVALID_DATA;
+        const vp9_parsed_frame_t *pf = pfs[i];
+        if ((int32_t)pf->hdr.width != b->st[sid].W || (int32_t)pf->hdr.height != b->st[sid].H)
+            return CVP9_ERR_INVALID_DATA;
+        if ((pf->num_blocks && !pf->blocks) || (pf->num_coeffs && !pf->coeffs)) return CVP9_ERR_INVALID_DATA;
+        for (int j = 0; j < i; j++) if (sids[j] == sid) return CVP9_ERR_INVALID_DATA;
+    }
+
+    const uint64_t seq = b->seq + 1;
+    bslot_t *s = &b->slot[seq % BSLOTS];
+    cvp9_err_t err = wait_slot(b, s);
+    if (err != CVP9_OK) return err;
+    b->lat_submit[seq % LAT_RING] = cvp9_now();
+
+    /* sizes */
+    size_t in_bytes = 0, n_sb = 0;
+    int max_blocks = 0, max_mi = 0, lf_tx = 0, lf_ty = 0, flat_w = 0, flat_h = 0, flat_nv = 0;
+    int maxd = 0;
+    uint64_t key = mix64(0, (uint64_t)n);
+    for (int i = 0; i < n; i++) {
+        const vp9_parsed_frame_t *pf = pfs[i];
+        bstream_t *st = &b->st[sids[i]];
+        if (!dev_in) {
+            in_bytes += ALIGN_UP((size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t), 256);
+            in_bytes += ALIGN_UP((size_t)pf->num_coeffs * sizeof(int16_t), 256);
+        }
+        n_sb += (size_t)st->n_sb;
+        if ((int)pf->num_blocks > max_blocks) max_blocks = (int)pf->num_blocks;
+        int mi = ((st->W + 7) / 8) * ((st->H + 7) / 8);
+        if (mi > max_mi) max_mi = mi;
+        int tiled = (st->W % 8) != 1 && (st->H % 8) != 1;
+        if (tiled) {
+            int tx = (st->W + 4 + 63) / 64, ty = (st->H + 4 + 63) / 64;
+            if (tx > lf_tx) lf_tx = tx;
+            if (ty > lf_ty) lf_ty = ty;
+        } else {
+            if (st->W > flat_w) flat_w = st->W;
+            if (st->H > flat_h) flat_h = st->H;
+        }
+        int d = (st->W + 63) / 64 + (st->H + 63) / 64 - 1;
+        if (d > maxd) maxd = d;
+        key = mix64(key, ((uint64_t)st->W << 32) | (uint64_t)st->H);
+    }
+
+    /* per-slot buffers */
+    if (!dev_in && in_bytes) {
+        if ((err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes)) ||
+            (err = grow_dev(b, (void **)&s->d_in, &s->d_in_cap, in_bytes)))
+            return err;
+    }
+    if (s->jobs_cap < n) {
+        cudaFreeHost(s->h_jobs);
+        cudaFree(s->d_jobs);
+        s->h_jobs = NULL; s->d_jobs = NULL; s->jobs_cap = 0;
+        BCK(cudaMallocHost((void **)&s->h_jobs, (size_t)n * sizeof(cvp9_job_t)), "job table");
+        BCK(cudaMalloc((void **)&s->d_jobs, (size_t)n * sizeof(cvp9_job_t)), "job table");
+        s->jobs_cap = n;
+    }
+    if (s->misc_cap < n + 1) {
+        cudaFree(s->d_misc);
+        cudaFreeHost(s->h_misc);
+        s->d_misc = NULL; s->h_misc = NULL; s->misc_cap = 0;
+        BCK(cudaMalloc((void **)&s->d_misc, (size_t)(n + 1) * 4), "status words");
+        BCK(cudaMallocHost((void **)&s->h_misc, (size_t)(n + 1) * 4), "status words");
+        s->misc_cap = n + 1;
+    }
+    if ((err = grow_dev(b, (void **)&s->d_sb_range, &s->sb_cap, n_sb * 16))) return err;
+    if (s->sids_cap < n) {
+        free(s->sids);
+        s->sids = malloc((size_t)n * sizeof(int));
+        if (!s->sids) return CVP9_ERR_NOMEM;
+        s->sids_cap = n;
+    }
+
+    /* tickets: SB-diagonal order, streams interleaved on each diagonal */
+    if (s->tickets_key != key || !s->d_tickets) {
+        size_t need = n_sb * 4;
+        if ((err = grow_dev(b, (void **)&s->d_tickets, &s->tickets_cap, need))) return err;
+        uint32_t *t = malloc(need ? need : 4);
+        if (!t) return CVP9_ERR_NOMEM;
+        uint32_t cnt = 0;
+        for (int d = 0; d < maxd; d++)
+            for (int i = 0; i < n; i++) {
+                bstream_t *st = &b->st[sids[i]];
+                cnt += (uint32_t)cvp9_tickets_on_diagonal((st->W + 63) / 64, (st->H + 63) / 64, i, d, t + cnt);
+            }
+        cudaError_t e = cudaMemcpy(s->d_tickets, t, (size_t)cnt * 4, cudaMemcpyHostToDevice);
+        free(t);
+        if (e != cudaSuccess) return bfail(b, e, "tickets");
+        s->n_tickets = cnt;
+        s->tickets_key = key;
+    }
+
+    /* inputs: bulk copy of everything staged, then direct DMA of pinned arrays */
+    s->h2d_bytes = 0;
+    BCK(cudaEventRecord(s->ev_start, b->hs), "event");
+    size_t off = 0;
+    const uint8_t *dev_blocks[256], *dev_coeffs[256];
+    const uint8_t **dbp = n <= 256 ? dev_blocks : malloc((size_t)n * sizeof(void *));
+    const uint8_t **dcp = n <= 256 ? dev_coeffs : malloc((size_t)n * sizeof(void *));
+    if (!dbp || !dcp) return CVP9_ERR_NOMEM;
+    struct { const void *src; size_t off, n; } direct[512];
+    int ndirect = 0;
+    for (int i = 0; i < n; i++) {
+        const vp9_parsed_frame_t *pf = pfs[i];
+        if (dev_in) {
+            dbp[i] = (const uint8_t *)pf->blocks;
+            dcp[i] = (const uint8_t *)pf->coeffs;
+            continue;
+        }
+        size_t nbb = (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t);
+        size_t ncb = (size_t)pf->num_coeffs * sizeof(int16_t);
+        const void *srcs[2] = { pf->blocks, pf->coeffs };
+        size_t lens[2] = { nbb, ncb };
+        for (int k = 0; k < 2; k++) {
+            if (lens[k]) {
+                if (ndirect < 512 && is_pinned(srcs[k])) {
+                    direct[ndirect].src = srcs[k];
+                    direct[ndirect].off = off;
+                    direct[ndirect].n = lens[k];
+                    ndirect++;
+                } else {
+                    memcpy(s->h_in + off, srcs[k], lens[k]);
+                }
+            }
+            (k == 0 ? dbp : dcp)[i] = s->d_in + off;
+            off += ALIGN_UP(lens[k], 256);
+        }
+    }
+    if (!dev_in && off) {
+        /* staged ranges go up in one copy; direct copies land afterwards */
+        int any_staged = ndirect < 2 * n;
+        if (any_staged) {
+            BCK(cudaMemcpyAsync(s->d_in, s->h_in, off, cudaMemcpyHostToDevice, b->hs), "upload inputs");
+            s->h2d_bytes += off;
+        }
+        for (int k = 0; k < ndirect; k++) {
+            BCK(cudaMemcpyAsync(s->d_in + direct[k].off, direct[k].src, direct[k].n,
+                                cudaMemcpyHostToDevice, b->hs), "upload pinned inputs");
+            if (!any_staged) s->h2d_bytes += direct[k].n;
+        }
+    }
+
+    /* jobs, outputs, reference pools */
+    uint32_t sb_base = 0;
+    int out_frame[1024];
+    int *ofr = n <= 1024 ? out_frame : malloc((size_t)n * sizeof(int));
+    if (!ofr) return CVP9_ERR_NOMEM;
+    for (int i = 0; i < n; i++) {
+        const vp9_parsed_frame_t *pf = pfs[i];
+        bstream_t *st = &b->st[sids[i]];
+        int of = acquire_frame(b, st);
+        if (of < 0) {
+            if (ofr != out_frame) free(ofr);
+            return bfail(b, cudaErrorMemoryAllocation, "frame pool");
+        }
+        ofr[i] = of;
+        cvp9_job_t *job = &s->h_jobs[i];
+        memset(job, 0, sizeof(*job));
+        cvp9_job_geometry(job, pf);
+        job->blocks = (const vp9_macroblock_info_t *)dbp[i];
+        job->coeffs = (const int16_t *)dcp[i];
+        job->out = st->f[of].dev;
+        job->nv12 = NULL;
+        for (int r = 0; r < 8; r++) {
+            int f = st->ref_slot[r];
+            if (f >= 0) {
+                job->ref[r].plane = st->f[f].dev;
+                job->ref[r].w = st->f[f].w;
+                job->ref[r].h = st->f[f].h;
+            }
+        }
+        job->epoch = ++st->epoch;
+        job->sb_range = s->d_sb_range + 4 * (size_t)sb_base;
+        job->sb_done = st->d_sb_done;
+        job->status = s->d_misc + 1 + i;
+        sb_base += (uint32_t)st->n_sb;
+        s->sids[i] = sids[i];
+    }
+    if (dbp != dev_blocks) free(dbp);
+    if (dcp != dev_coeffs) free(dcp);
+    BCK(cudaMemcpyAsync(s->d_jobs, s->h_jobs, (size_t)n * sizeof(cvp9_job_t), cudaMemcpyHostToDevice, b->hs),
+        "upload jobs");
+    s->h2d_bytes += (size_t)n * sizeof(cvp9_job_t);
+    BCK(cudaEventRecord(s->ev_h2d, b->hs), "event");
+
+    /* kernels */
+    BCK(cudaStreamWaitEvent(b->cs, s->ev_h2d, 0), "wait inputs");
+    BCK(cudaEventRecord(s->ev_k0, b->cs), "event");
+    cvp9k_launch_t L;
+    memset(&L, 0, sizeof(L));
+    L.jobs = s->d_jobs;
+    L.njobs = n;
+    L.arith = b->arith;
+    L.max_blocks = max_blocks;
+    L.scan_ctas = (max_mi + 255) / 256;
+    L.tickets = s->d_tickets;
+    L.n_tickets = s->n_tickets;
+    L.ticket_counter = s->d_misc;
+    L.recon_ctas = (int)s->n_tickets < b->resident_ctas ? (int)s->n_tickets : b->resident_ctas;
+    L.lf_tiles_x = lf_tx;
+    L.lf_tiles_y = lf_ty;
+    L.flat_lf_max_w = flat_w;
+    L.flat_lf_max_h = flat_h;
+    L.flat_nv12 = flat_nv;
+    for (int k = 0; k < 4; k++) L.ev[k] = s->ev_kern[k];
+    uint64_t gkey = mix64(mix64(mix64(key, (uint64_t)(uintptr_t)s->d_jobs), (uint64_t)(uintptr_t)s->d_sb_range),
+                          mix64((uint64_t)(uintptr_t)s->d_misc, (uint64_t)(uintptr_t)s->d_tickets));
+    gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
+    s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + (lf_tx > 0) + (flat_w > 0 ? 2 : 0));
+    if (b->use_graphs) {
+        if (!s->graph || s->graph_key != gkey) {
+            if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = NULL; }
+            cudaGraph_t g;
+            BCK(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal), "graph capture");
+            cudaMemsetAsync(s->d_sb_range, 0, n_sb * 16, b->cs);
+            cudaMemsetAsync(s->d_misc, 0, (size_t)(n + 1) * 4, b->cs);
+            int lrc = cvp9k_launch_frame(&L, b->cs);
+            cudaError_t ce = cudaStreamEndCapture(b->cs, &g);
+            if (lrc != 0 || ce != cudaSuccess) {
+                if (ce == cudaSuccess) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return bfail(b, lrc != 0 ? (cudaError_t)lrc : ce, "graph capture");
+            }
+            ce = cudaGraphInstantiate(&s->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) { s->graph = NULL; return bfail(b, ce, "graph instantiate"); }
+            s->graph_key = gkey;
+        } else {
+            b->graph_replays++;
+        }
+        BCK(cudaGraphLaunch(s->graph, b->cs), "graph launch");
+    } else {
+        BCK(cudaMemsetAsync(s->d_sb_range, 0, n_sb * 16, b->cs), "clear sb_range");
+        BCK(cudaMemsetAsync(s->d_misc, 0, (size_t)(n + 1) * 4, b->cs), "clear status");
+        int lrc = cvp9k_launch_frame(&L, b->cs);
+        if (lrc != 0) return bfail(b, (cudaError_t)lrc, "launch");
+    }
+    BCK(cudaEventRecord(s->ev_k1, b->cs), "event");
+
+    /* downloads */
+    BCK(cudaStreamWaitEvent(b->ds, s->ev_k1, 0), "wait kernels");
+    s->d2h_bytes = 0;
+    for (int i = 0; i < n; i++) {
+        bstream_t *st = &b->st[sids[i]];
+        if (want_out) {
+            int par = st->latest < 0 ? 0 : (st->latest ^ 1);
+            size_t fb = frame_bytes(st->W, st->H);
+            if ((err = grow_host(b, (void **)&st->h_out[par], &st->h_out_cap[par], fb))) {
+                if (ofr != out_frame) free(ofr);
+                return err;
+            }
+            BCK(cudaMemcpyAsync(st->h_out[par], st->f[ofr[i]].dev, fb, cudaMemcpyDeviceToHost, b->ds), "download");
+            s->d2h_bytes += fb;
+            st->f[ofr[i]].d2h_seq = seq;
+            st->out_w[par] = st->W;
+            st->out_h[par] = st->H;
+            st->out_pts[par] = pts ? pts[i] : 0;
+            st->out_seq[par] = seq;
+            st->latest = par;
+        }
+        st->last_seq = seq;
+        /* pool update, as the per-stream backend does */
+        const vp9_parsed_frame_t *pf = pfs[i];
+        if (b->arith == CVP9_ARITH_SPEC) {
+            unsigned refresh = pf->hdr.refresh_frame_flags ? pf->hdr.refresh_frame_flags : 0x01u;
+            for (int r = 0; r < 8; r++) if (refresh & (1u << r)) set_ref(st, r, ofr[i]);
+        } else if (pf->hdr.frame_type == VP9_FRAME_KEY) {
+            for (int r = 0; r < 8; r++) set_ref(st, r, ofr[i]);
+        } else {
+            set_ref(st, 0, ofr[i]);
+        }
+    }
+    if (ofr != out_frame) free(ofr);
+    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
+    s->d2h_bytes += (size_t)(n + 1) * 4;
+    /* the callback runs before ev_end completes, so a slot's argument is
+     * free again once the slot's step is waited for */
+    s->lat_arg.b = b;
+    s->lat_arg.seq = seq;
+    b->lat_seq[seq % LAT_RING] = seq;
+    b->lat_done[seq % LAT_RING] = 0.0;
+    BCK(cudaLaunchHostFunc(b->ds, step_done_cb, &s->lat_arg), "completion callback");
+    BCK(cudaEventRecord(s->ev_end, b->ds), "event");
+
+    s->seq = seq;
+    s->n = n;
+    s->busy = 1;
+    b->seq = seq;
+    return CVP9_OK;
+}
+
+cvp9_err_t cvp9_batch_wait(cvp9_batch_t *b)
+{
+    if (!b) return CVP9_ERR_INVALID_DATA;
+    cvp9_err_t first = CVP9_OK;
+    for (uint64_t q = b->done_seq + 1; q <= b->seq; q++) {
+        bslot_t *s = &b->slot[q % BSLOTS];
+        if (s->seq != q) continue;
+        cvp9_err_t e = wait_slot(b, s);
+        if (e != CVP9_OK) return e;
+        for (int i = 0; i < s->n && first == CVP9_OK; i++) {
+            uint32_t stt = s->h_misc[1 + i];
+            if (stt & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) first = CVP9_ERR_INVALID_DATA;
+            else if (stt & CVP9_JOB_TIMEOUT) first = CVP9_ERR_GPU;
+        }
+    }
+    b->done_seq = b->seq;
+    return first;
+}
+
+int cvp9_batch_poll(cvp9_batch_t *b)
+{
+    if (!b) return CVP9_ERR_INVALID_DATA;
+    for (uint64_t q = b->done_seq + 1; q <= b->seq; q++) {
+        bslot_t *s = &b->slot[q % BSLOTS];
+        if (s->seq != q || !s->busy) continue;
+        cudaError_t e = cudaEventQuery(s->ev_end);
+        if (e == cudaErrorNotReady) return 0;
+        if (e != cudaSuccess) return CVP9_ERR_GPU;
+        complete_slot(b, s);
+    }
+    b->done_seq = b->seq;
+    return 1;
+}
+
+cvp9_err_t cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *info)
+{
+    if (!b || !info || sid < 0 || sid >= b->max_streams || !b->st[sid].open) return CVP9_ERR_INVALID_DATA;
+    bstream_t *st = &b->st[sid];
+    if (st->latest < 0) return CVP9_ERR_UNSUPPORTED;
+    int par = st->latest;
+    if (st->out_seq[par] > b->done_seq) {
+        bslot_t *s = &b->slot[st->out_seq[par] % BSLOTS];
+        if (s->busy && s->seq == st->out_seq[par]) {
+            cudaError_t e = cudaEventQuery(s->ev_end);
+            if (e == cudaErrorNotReady) return CVP9_ERR_AGAIN;
+            if (e != cudaSuccess) return bfail(b, e, "step completion");
+            complete_slot(b, s);
+        }
+    }
+    if (st->last_status & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) return CVP9_ERR_INVALID_DATA;
+    if (st->last_status & CVP9_JOB_TIMEOUT) return CVP9_ERR_GPU;
+    uint32_t w = (uint32_t)st->out_w[par], h = (uint32_t)st->out_h[par];
+    uint32_t cw = (w + 1) / 2, ch = (h + 1) / 2;
+    info->width = w;
+    info->height = h;
+    info->stride_y = w;
+    info->stride_uv = cw;
+    info->plane_y = st->h_out[par];
+    info->plane_u = st->h_out[par] + (size_t)w * h;
+    info->plane_v = st->h_out[par] + (size_t)w * h + (size_t)cw * ch;
+    info->pts = st->out_pts[par];
+    return CVP9_OK;
+}
+
+cvp9_err_t cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *out)
+{
+    if (!b || !out) return CVP9_ERR_INVALID_DATA;
+    *out = b->last;
+    out->reserved_bytes = b->reserved;
+    int open = 0;
+    for (int i = 0; i < b->nst; i++) open += b->st[i].open;
+    out->open_streams = open;
+    out->graph_replays = b->graph_replays;
+    return CVP9_OK;
+}
+
+const char *cvp9_batch_last_error(cvp9_batch_t *b)
+{
+    return b ? b->err : "";
+}
+
+cvp9_err_t cvp9_batch_timer_start(cvp9_batch_t *b)
+{
+    if (!b) return CVP9_ERR_INVALID_DATA;
+    if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
+    /* the next step's upload (hs) starts after this event */
+    BCK(cudaEventRecord(b->ev_t0, b->hs), "timer");
+    return CVP9_OK;
+}
+
+cvp9_err_t cvp9_batch_timer_stop(cvp9_batch_t *b, float *ms)
+{
+    if (!b || !ms) return CVP9_ERR_INVALID_DATA;
+    if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
+    /* ds holds the last step's download, which follows its kernels */
+    BCK(cudaEventRecord(b->ev_t1, b->ds), "timer");
+    double t0 = cvp9_now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(b->ev_t1);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return bfail(b, e, "timer");
+        if (cvp9_now() - t0 > WAIT_LIMIT_S) return CVP9_ERR_GPU;
+        struct timespec ts = { 0, 20000 };
+        nanosleep(&ts, NULL);
+    }
+    BCK(cudaEventElapsedTime(ms, b->ev_t0, b->ev_t1), "timer");
+    return CVP9_OK;
+}
+
+uint64_t cvp9_batch_last_seq(cvp9_batch_t *b)
+{
+    return b ? b->seq : 0;
+}
+
+cvp9_err_t cvp9_batch_step_latency(cvp9_batch_t *b, uint64_t seq, double *ms)
+{
+    if (!b || !ms || seq == 0 || seq > b->seq || b->seq - seq >= LAT_RING) return CVP9_ERR_INVALID_DATA;
+    if (b->lat_seq[seq % LAT_RING] != seq) return CVP9_ERR_INVALID_DATA;
+    double d = b->lat_done[seq % LAT_RING];
+    if (d == 0.0) return CVP9_ERR_AGAIN;
+    *ms = 1000.0 * (d - b->lat_submit[seq % LAT_RING]);
+    return CVP9_OK;
+}

@@ -1,0 +1,1374 @@
+/*
+ * recon.cu — VP9 reconstruction kernels for sm_100a.
+ *
+ * Three launches per batch of frames (one frame from each of J streams):
+ *
+ *   k_scan_blocks   one thread per block: superblock (SB) membership, the
+ *                   contiguous block range of every SB, layout checks.
+ *   k_recon<A>      one CTA per SB ticket, tickets handed out in
+ *                   SB-diagonal order across all streams of the batch. A CTA
+ *                   builds its SB's dependency levels in shared memory, waits
+ *                   (bounded) for the left / above / above-left SBs only when
+ *                   the SB holds intra blocks, then runs the levels:
+ *                   prediction + first transform pass, barrier, second pass +
+ *                   residual add, barrier. The SB tile (with a one-pixel
+ *                   halo) lives in shared memory; the finished tile is
+ *                   written once and the SB's done flag released.
+ *   k_loopfilter<A> the 4-tap deblock on 64x64 luma tiles shifted by 4 px so
+ *                   every filter tap of every 8-px edge falls inside one tile
+ *                   (horizontal pass then vertical pass, in place), with the
+ *                   NV12 pack fused into the same tile pass.
+ *
+ * Arithmetic profiles (template A):
+ *   CVP9_ARITH_REFCPU reproduces src/decoder/vp9_reconstruct.c:194-370
+ *     bit for bit: float64 inverse DCT of the raw coefficients with the
+ *     host-built basis (separately rounded products and sums, k ascending),
+ *     bilinear MC, the CPU's 127 edge rules, luma-only residual.
+ *   CVP9_ARITH_SPEC reproduces the shader arithmetic: dequantised integer
+ *     butterflies (vp9_idct.comp.glsl), regular 8-tap MC (vp9_mc.comp.glsl)
+ *     on luma and chroma, intra with the shader's availability rules
+ *     (vp9_intra_pred.comp.glsl), the residual of every TX of every plane.
+ *
+ * No tensor cores: every sample is integer-exact and nothing here is a dense
+ * contraction; the kernels are bound by memory traffic and dependency
+ * latency.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "recon_job.h"
+#include "vp9_tables.h"
+#include "recon_launch.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxBlocks = 256;      /* 4x4 cells in a 64x64 SB */
+constexpr int kYPitch = 72;          /* luma tile row pitch; x = 0 at byte 4 */
+constexpr int kCPitch = 40;          /* chroma tile row pitch; x = 0 at byte 4 */
+constexpr int kTempPitch = 65;       /* doubles per REFCPU temp row */
+constexpr int kStagePerWarp = 768;   /* bytes of MC staging per warp */
+constexpr long long kSpinLimit = 1ll << 20;   /* ~0.25 s of polling */
+
+__constant__ double c_dct[16 + 64 + 256 + 1024];      /* N = 4, 8, 16, 32 */
+__constant__ int c_subpel[16][8] = CVP9_SUBPEL_REGULAR_INIT;
+
+__device__ __forceinline__ const double *dct_basis(int txl)
+{
+    return c_dct + (txl == 0 ? 0 : txl == 1 ? 16 : txl == 2 ? 80 : 336);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* ── 32-bit wrap-around integer for the shader butterflies ───────────────── */
+struct wi {
+    int v;
+    __device__ __forceinline__ wi() : v(0) {}
+    __device__ __forceinline__ wi(int x) : v(x) {}
+};
+__device__ __forceinline__ wi operator+(wi a, wi b) { return wi((int)((unsigned)a.v + (unsigned)b.v)); }
+__device__ __forceinline__ wi operator-(wi a, wi b) { return wi((int)((unsigned)a.v - (unsigned)b.v)); }
+__device__ __forceinline__ wi operator-(wi a) { return wi((int)(0u - (unsigned)a.v)); }
+__device__ __forceinline__ wi operator*(wi a, int k) { return wi((int)((unsigned)a.v * (unsigned)k)); }
+__device__ __forceinline__ wi RS(wi x) { return wi(((int)((unsigned)x.v + 8192u)) >> 14); }
+
+/* cos(k*pi/64) in Q14 */
+enum : int {
+    K1 = 16364, K2 = 16305, K3 = 16207, K4 = 16069, K5 = 15893, K6 = 15679,
+    K7 = 15426, K8 = 15137, K9 = 14811, K10 = 14449, K11 = 14053, K12 = 13623,
+    K13 = 13160, K14 = 12665, K15 = 12140, K16 = 11585, K17 = 11003, K18 = 10394,
+    K19 = 9760, K20 = 9102, K21 = 8423, K22 = 7723, K23 = 7005, K24 = 6270,
+    K25 = 5520, K26 = 4756, K27 = 3981, K28 = 3196, K29 = 2404, K30 = 1606,
+    K31 = 804
+};
+
+/* 1-D inverse DCTs, in place on x[0..N). Same stage structure and rounding
+ * as vp9_idct.comp.glsl:47-649. */
+__device__ __forceinline__ void idct4(wi *x)
+{
+    wi s0 = RS((x[0] + x[2]) * K16), s1 = RS((x[0] - x[2]) * K16);
+    wi s2 = RS(x[1] * K24 - x[3] * K8), s3 = RS(x[1] * K8 + x[3] * K24);
+    x[0] = s0 + s3; x[1] = s1 + s2; x[2] = s1 - s2; x[3] = s0 - s3;
+}
+
+__device__ __forceinline__ void idct8(wi *x)
+{
+    wi a[8], b[8];
+    a[0] = x[0]; a[1] = x[2]; a[2] = x[4]; a[3] = x[6];
+    a[4] = RS(x[1] * K28 - x[7] * K4); a[7] = RS(x[1] * K4 + x[7] * K28);
+    a[5] = RS(x[5] * K12 - x[3] * K20); a[6] = RS(x[5] * K20 + x[3] * K12);
+    b[0] = RS((a[0] + a[2]) * K16); b[1] = RS((a[0] - a[2]) * K16);
+    b[2] = RS(a[1] * K24 - a[3] * K8); b[3] = RS(a[1] * K8 + a[3] * K24);
+    b[4] = a[4] + a[5]; b[5] = a[4] - a[5]; b[6] = -a[6] + a[7]; b[7] = a[6] + a[7];
+    a[0] = b[0] + b[3]; a[1] = b[1] + b[2]; a[2] = b[1] - b[2]; a[3] = b[0] - b[3];
+    a[4] = b[4]; a[5] = RS((b[6] - b[5]) * K16); a[6] = RS((b[5] + b[6]) * K16); a[7] = b[7];
+#pragma unroll
+    for (int i = 0; i < 4; i++) { x[i] = a[i] + a[7 - i]; x[7 - i] = a[i] - a[7 - i]; }
+}
+
+__device__ __forceinline__ void idct16(wi *x)
+{
+    wi a[16], b[16];
+    a[0] = x[0]; a[1] = x[8]; a[2] = x[4]; a[3] = x[12]; a[4] = x[2]; a[5] = x[10];
+    a[6] = x[6]; a[7] = x[14]; a[8] = x[1]; a[9] = x[9]; a[10] = x[5]; a[11] = x[13];
+    a[12] = x[3]; a[13] = x[11]; a[14] = x[7]; a[15] = x[15];
+#pragma unroll
+    for (int i = 0; i < 8; i++) b[i] = a[i];
+    b[8] = RS(a[8] * K30 - a[15] * K2);   b[15] = RS(a[8] * K2 + a[15] * K30);
+    b[9] = RS(a[9] * K14 - a[14] * K18);  b[14] = RS(a[9] * K18 + a[14] * K14);
+    b[10] = RS(a[10] * K22 - a[13] * K10); b[13] = RS(a[10] * K10 + a[13] * K22);
+    b[11] = RS(a[11] * K6 - a[12] * K26);  b[12] = RS(a[11] * K26 + a[12] * K6);
+#pragma unroll
+    for (int i = 0; i < 4; i++) a[i] = b[i];
+    a[4] = RS(b[4] * K28 - b[7] * K4); a[7] = RS(b[4] * K4 + b[7] * K28);
+    a[5] = RS(b[5] * K12 - b[6] * K20); a[6] = RS(b[5] * K20 + b[6] * K12);
+    a[8] = b[8] + b[9]; a[9] = b[8] - b[9]; a[10] = -b[10] + b[11]; a[11] = b[10] + b[11];
+    a[12] = b[12] + b[13]; a[13] = b[12] - b[13]; a[14] = -b[14] + b[15]; a[15] = b[14] + b[15];
+    b[0] = RS((a[0] + a[1]) * K16); b[1] = RS((a[0] - a[1]) * K16);
+    b[2] = RS(a[2] * K24 - a[3] * K8); b[3] = RS(a[2] * K8 + a[3] * K24);
+    b[4] = a[4] + a[5]; b[5] = a[4] - a[5]; b[6] = -a[6] + a[7]; b[7] = a[6] + a[7];
+    b[8] = a[8]; b[15] = a[15];
+    b[9] = RS(-a[9] * K8 + a[14] * K24);   b[14] = RS(a[9] * K24 + a[14] * K8);
+    b[10] = RS(-a[10] * K24 - a[13] * K8); b[13] = RS(-a[10] * K8 + a[13] * K24);
+    b[11] = a[11]; b[12] = a[12];
+    a[0] = b[0] + b[3]; a[1] = b[1] + b[2]; a[2] = b[1] - b[2]; a[3] = b[0] - b[3];
+    a[4] = b[4]; a[5] = RS((b[6] - b[5]) * K16); a[6] = RS((b[5] + b[6]) * K16); a[7] = b[7];
+    a[8] = b[8] + b[11]; a[9] = b[9] + b[10]; a[10] = b[9] - b[10]; a[11] = b[8] - b[11];
+    a[12] = -b[12] + b[15]; a[13] = -b[13] + b[14]; a[14] = b[13] + b[14]; a[15] = b[12] + b[15];
+#pragma unroll
+    for (int i = 0; i < 4; i++) { b[i] = a[i] + a[7 - i]; b[7 - i] = a[i] - a[7 - i]; }
+    b[8] = a[8]; b[9] = a[9];
+    b[10] = RS((-a[10] + a[13]) * K16); b[13] = RS((a[10] + a[13]) * K16);
+    b[11] = RS((-a[11] + a[12]) * K16); b[12] = RS((a[11] + a[12]) * K16);
+    b[14] = a[14]; b[15] = a[15];
+#pragma unroll
+    for (int i = 0; i < 8; i++) { x[i] = b[i] + b[15 - i]; x[15 - i] = b[i] - b[15 - i]; }
+}
+
+__device__ __forceinline__ void idct32(wi *x)
+{
+    wi a[32], b[32];
+    a[0] = x[0]; a[1] = x[16]; a[2] = x[8]; a[3] = x[24]; a[4] = x[4]; a[5] = x[20];
+    a[6] = x[12]; a[7] = x[28]; a[8] = x[2]; a[9] = x[18]; a[10] = x[10]; a[11] = x[26];
+    a[12] = x[6]; a[13] = x[22]; a[14] = x[14]; a[15] = x[30];
+    a[16] = RS(x[1] * K31 - x[31] * K1);  a[31] = RS(x[1] * K1 + x[31] * K31);
+    a[17] = RS(x[17] * K15 - x[15] * K17); a[30] = RS(x[17] * K17 + x[15] * K15);
+    a[18] = RS(x[9] * K23 - x[23] * K9);  a[29] = RS(x[9] * K9 + x[23] * K23);
+    a[19] = RS(x[25] * K7 - x[7] * K25);  a[28] = RS(x[25] * K25 + x[7] * K7);
+    a[20] = RS(x[5] * K27 - x[27] * K5);  a[27] = RS(x[5] * K5 + x[27] * K27);
+    a[21] = RS(x[21] * K11 - x[11] * K21); a[26] = RS(x[21] * K21 + x[11] * K11);
+    a[22] = RS(x[13] * K19 - x[19] * K13); a[25] = RS(x[13] * K13 + x[19] * K19);
+    a[23] = RS(x[29] * K3 - x[3] * K29);  a[24] = RS(x[29] * K29 + x[3] * K3);
+    /* stage 2 */
+#pragma unroll
+    for (int i = 0; i < 8; i++) b[i] = a[i];
+    b[8] = RS(a[8] * K30 - a[15] * K2);   b[15] = RS(a[8] * K2 + a[15] * K30);
+    b[9] = RS(a[9] * K14 - a[14] * K18);  b[14] = RS(a[9] * K18 + a[14] * K14);
+    b[10] = RS(a[10] * K22 - a[13] * K10); b[13] = RS(a[10] * K10 + a[13] * K22);
+    b[11] = RS(a[11] * K6 - a[12] * K26);  b[12] = RS(a[11] * K26 + a[12] * K6);
+#pragma unroll
+    for (int i = 16; i < 32; i += 4) {
+        b[i] = a[i] + a[i + 1]; b[i + 1] = a[i] - a[i + 1];
+        b[i + 2] = -a[i + 2] + a[i + 3]; b[i + 3] = a[i + 2] + a[i + 3];
+    }
+    /* stage 3 */
+#pragma unroll
+    for (int i = 0; i < 4; i++) a[i] = b[i];
+    a[4] = RS(b[4] * K28 - b[7] * K4); a[7] = RS(b[4] * K4 + b[7] * K28);
+    a[5] = RS(b[5] * K12 - b[6] * K20); a[6] = RS(b[5] * K20 + b[6] * K12);
+#pragma unroll
+    for (int i = 8; i < 16; i += 4) {
+        a[i] = b[i] + b[i + 1]; a[i + 1] = b[i] - b[i + 1];
+        a[i + 2] = -b[i + 2] + b[i + 3]; a[i + 3] = b[i + 2] + b[i + 3];
+    }
+    a[16] = b[16]; a[31] = b[31];
+    a[17] = RS(-b[17] * K4 + b[30] * K28);  a[30] = RS(b[17] * K28 + b[30] * K4);
+    a[18] = RS(-b[18] * K28 - b[29] * K4);  a[29] = RS(-b[18] * K4 + b[29] * K28);
+    a[19] = b[19]; a[20] = b[20];
+    a[21] = RS(-b[21] * K20 + b[26] * K12); a[26] = RS(b[21] * K12 + b[26] * K20);
+    a[22] = RS(-b[22] * K12 - b[25] * K20); a[25] = RS(-b[22] * K20 + b[25] * K12);
+    a[23] = b[23]; a[24] = b[24]; a[27] = b[27]; a[28] = b[28];
+    /* stage 4 */
+    b[0] = RS((a[0] + a[1]) * K16); b[1] = RS((a[0] - a[1]) * K16);
+    b[2] = RS(a[2] * K24 - a[3] * K8); b[3] = RS(a[2] * K8 + a[3] * K24);
+    b[4] = a[4] + a[5]; b[5] = a[4] - a[5]; b[6] = -a[6] + a[7]; b[7] = a[6] + a[7];
+    b[8] = a[8]; b[15] = a[15];
+    b[9] = RS(-a[9] * K8 + a[14] * K24);   b[14] = RS(a[9] * K24 + a[14] * K8);
+    b[10] = RS(-a[10] * K24 - a[13] * K8); b[13] = RS(-a[10] * K8 + a[13] * K24);
+    b[11] = a[11]; b[12] = a[12];
+#pragma unroll
+    for (int i = 16; i < 32; i += 8) {
+        b[i] = a[i] + a[i + 3]; b[i + 1] = a[i + 1] + a[i + 2];
+        b[i + 2] = a[i + 1] - a[i + 2]; b[i + 3] = a[i] - a[i + 3];
+        b[i + 4] = -a[i + 4] + a[i + 7]; b[i + 5] = -a[i + 5] + a[i + 6];
+        b[i + 6] = a[i + 5] + a[i + 6]; b[i + 7] = a[i + 4] + a[i + 7];
+    }
+    /* stage 5 */
+    a[0] = b[0] + b[3]; a[1] = b[1] + b[2]; a[2] = b[1] - b[2]; a[3] = b[0] - b[3];
+    a[4] = b[4]; a[5] = RS((b[6] - b[5]) * K16); a[6] = RS((b[5] + b[6]) * K16); a[7] = b[7];
+    a[8] = b[8] + b[11]; a[9] = b[9] + b[10]; a[10] = b[9] - b[10]; a[11] = b[8] - b[11];
+    a[12] = -b[12] + b[15]; a[13] = -b[13] + b[14]; a[14] = b[13] + b[14]; a[15] = b[12] + b[15];
+    a[16] = b[16]; a[17] = b[17];
+    a[18] = RS(-b[18] * K8 + b[29] * K24);  a[29] = RS(b[18] * K24 + b[29] * K8);
+    a[19] = RS(-b[19] * K8 + b[28] * K24);  a[28] = RS(b[19] * K24 + b[28] * K8);
+    a[20] = RS(-b[20] * K24 - b[27] * K8);  a[27] = RS(-b[20] * K8 + b[27] * K24);
+    a[21] = RS(-b[21] * K24 - b[26] * K8);  a[26] = RS(-b[21] * K8 + b[26] * K24);
+    a[22] = b[22]; a[23] = b[23]; a[24] = b[24]; a[25] = b[25]; a[30] = b[30]; a[31] = b[31];
+    /* stage 6 */
+#pragma unroll
+    for (int i = 0; i < 4; i++) { b[i] = a[i] + a[7 - i]; b[7 - i] = a[i] - a[7 - i]; }
+    b[8] = a[8]; b[9] = a[9];
+    b[10] = RS((-a[10] + a[13]) * K16); b[13] = RS((a[10] + a[13]) * K16);
+    b[11] = RS((-a[11] + a[12]) * K16); b[12] = RS((a[11] + a[12]) * K16);
+    b[14] = a[14]; b[15] = a[15];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        b[16 + i] = a[16 + i] + a[23 - i]; b[23 - i] = a[16 + i] - a[23 - i];
+        b[24 + i] = -a[24 + i] + a[31 - i]; b[31 - i] = a[24 + i] + a[31 - i];
+    }
+    /* stage 7 */
+#pragma unroll
+    for (int i = 0; i < 8; i++) { a[i] = b[i] + b[15 - i]; a[15 - i] = b[i] - b[15 - i]; }
+#pragma unroll
+    for (int i = 16; i < 20; i++) a[i] = b[i];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        a[20 + i] = RS((-b[20 + i] + b[27 - i]) * K16);
+        a[27 - i] = RS((b[20 + i] + b[27 - i]) * K16);
+    }
+#pragma unroll
+    for (int i = 28; i < 32; i++) a[i] = b[i];
+    /* output */
+#pragma unroll
+    for (int i = 0; i < 16; i++) { x[i] = a[i] + a[31 - i]; x[31 - i] = a[i] - a[31 - i]; }
+}
+
+/* ── Shared-memory layout of one reconstruction CTA ─────────────────────── */
+
+struct BlkS {
+    uint8_t  x, y;          /* local luma position in the SB               */
+    uint8_t  w, h;          /* coded size                                  */
+    uint8_t  cw, ch;        /* size clamped to the frame                   */
+    uint8_t  txl;           /* luma tx_size 0..3                           */
+    uint8_t  flags;         /* 1 intra, 2 skip                             */
+    uint8_t  ymode, uvmode;
+    uint8_t  ref0;
+    uint8_t  ptxl[3];       /* residual TX log2-4 per plane                */
+    uint8_t  pnx[3];        /* residual TXs per row per plane              */
+    uint8_t  pad;
+    uint16_t pnt[3];        /* residual TX count per plane                 */
+    int16_t  mvx, mvy;
+    uint32_t coeff;
+};
+
+struct ReconSmem {
+    union {
+        double  d[64 * kTempPitch];              /* REFCPU first-pass output    */
+        int32_t i[64 * 64 + 2 * 32 * 32];        /* SPEC column-pass output     */
+    } temp;
+    uint8_t  ty[65 * kYPitch];                   /* luma tile, row 0 = halo     */
+    uint8_t  tu[33 * kCPitch];
+    uint8_t  tv[33 * kCPitch];
+    BlkS     blk[kMaxBlocks];
+    unsigned long long lvl_cnt[kMaxBlocks + 1];
+    uint32_t txmask[256 + 64 + 64];              /* per-TX column-nonzero bits  */
+    uint16_t cell[256];                          /* owner block + 1 per 4x4     */
+    uint16_t lvl[kMaxBlocks];
+    uint16_t order[kMaxBlocks];
+    uint16_t chunk_off[kMaxBlocks + 1];
+    uint16_t item_off[kMaxBlocks + 1];
+    uint16_t base_blk[kMaxBlocks + 1];
+    uint16_t base_chunk[kMaxBlocks + 1];
+    uint16_t base_item[kMaxBlocks + 1];
+    uint8_t  stage[kWarps][kStagePerWarp];
+    int      ticket;
+    int      nlev;
+    int      nb;
+};
+
+__device__ __forceinline__ uint8_t &TY(ReconSmem &s, int x, int y) { return s.ty[(y + 1) * kYPitch + x + 4]; }
+__device__ __forceinline__ uint8_t &TC(ReconSmem &s, int p, int x, int y)
+{
+    return (p == 1 ? s.tu : s.tv)[(y + 1) * kCPitch + x + 4];
+}
+
+__device__ __forceinline__ int max_tx_for(int w, int h)
+{
+    int m = w < h ? w : h;
+    return m >= 32 ? 3 : (m >= 16 ? 2 : (m >= 8 ? 1 : 0));
+}
+
+/* Residual TX layout of one block (plane TX size, TXs per row, TX count).
+ * REFCPU: luma only, counts from the frame-clamped size
+ * (vp9_reconstruct.c:336-347). SPEC: every plane in the tile parser's layout
+ * (vp9_kf_tile.c:320-396): coded area clipped at the MI-aligned frame edge. */
+template <int A>
+__device__ void residual_layout(BlkS &b, const cvp9_job_t &job, int gx, int gy)
+{
+    b.pnt[0] = b.pnt[1] = b.pnt[2] = 0;
+    b.pnx[0] = b.pnx[1] = b.pnx[2] = 0;
+    b.ptxl[0] = b.ptxl[1] = b.ptxl[2] = 0;
+    if (b.flags & 2) return;
+    if (A == CVP9_ARITH_REFCPU) {
+        int n = 4 << b.txl;
+        int nx = b.cw / n, ny = b.ch / n;
+        b.ptxl[0] = b.txl;
+        b.pnx[0] = (uint8_t)nx;
+        b.pnt[0] = (uint16_t)(nx * ny);
+    } else {
+        int sub8 = b.w < 8 || b.h < 8;
+        int ew = sub8 ? 8 : b.w, eh = sub8 ? 8 : b.h;
+        int mi_col = gx >> 3, mi_row = gy >> 3;
+        for (int p = 0; p < 3; p++) {
+            int ss = p > 0;
+            int pw = ss ? ew / 2 : ew, ph = ss ? eh / 2 : eh;
+            pw = pw < 4 ? 4 : pw;
+            ph = ph < 4 ? 4 : ph;
+            int tx = b.txl;
+            if (ss) { int mt = max_tx_for(pw, ph); tx = sub8 ? 0 : (tx > mt ? mt : tx); }
+            int t4 = 1 << tx;
+            int o4x = (mi_col * 2) >> ss, o4y = (mi_row * 2) >> ss;
+            int mw = pw / 4, mh = ph / 4;
+            int lim_w = ((job.mi_cols * 2) >> ss) - o4x, lim_h = ((job.mi_rows * 2) >> ss) - o4y;
+            if (mw > lim_w) mw = lim_w;
+            if (mh > lim_h) mh = lim_h;
+            int nx = mw > 0 ? (mw + t4 - 1) / t4 : 0;
+            int ny = mh > 0 ? (mh + t4 - 1) / t4 : 0;
+            b.ptxl[p] = (uint8_t)tx;
+            b.pnx[p] = (uint8_t)nx;
+            b.pnt[p] = (uint16_t)(nx * ny);
+        }
+    }
+}
+
+__device__ __forceinline__ int block_items(const BlkS &b)
+{
+    return b.pnt[0] * (4 << b.ptxl[0]) + b.pnt[1] * (4 << b.ptxl[1]) + b.pnt[2] * (4 << b.ptxl[2]);
+}
+
+__device__ __forceinline__ int block_chunks(const BlkS &b)
+{
+    return ((b.cw + 7) >> 3) * ((b.ch + 7) >> 3);
+}
+
+/* ── Prediction of one 8x8 luma chunk (+ its 4x4 chroma) by one warp ───── */
+
+template <int A>
+__device__ void predict_intra_chunk(ReconSmem &s, const BlkS &b, int gbx, int gby,
+                                    int lx0, int ly0, int lw, int lh,
+                                    int cx0, int cy0, int clw, int clh, int lane)
+{
+    const int fill = A == CVP9_ARITH_REFCPU ? 127 : 128;
+    /* luma */
+    {
+        int has_a = gby > 0, has_l = gbx > 0;
+        int dc = 128;
+        if (b.ymode == 0) {
+            unsigned sa = 0, sl = 0;
+            for (int i = lane; i < b.cw; i += 32) sa += has_a ? TY(s, b.x + i, b.y - 1) : (unsigned)fill;
+            for (int i = lane; i < b.ch; i += 32) sl += has_l ? TY(s, b.x - 1, b.y + i) : (unsigned)fill;
+            sa = __reduce_add_sync(0xffffffffu, sa);
+            sl = __reduce_add_sync(0xffffffffu, sl);
+            if (A == CVP9_ARITH_REFCPU) {
+                unsigned n = b.cw + b.ch;
+                dc = (int)((sa + sl + (n >> 1)) / n);
+            } else {
+                if (has_a && has_l) dc = (int)((sa + sl + (unsigned)(b.cw + b.ch) / 2) / (unsigned)(b.cw + b.ch));
+                else if (has_a) dc = (int)((sa + (unsigned)b.cw / 2) / (unsigned)b.cw);
+                else if (has_l) dc = (int)((sl + (unsigned)b.ch / 2) / (unsigned)b.ch);
+            }
+        }
+        int tl = (has_a && has_l) ? TY(s, b.x - 1, b.y - 1) : fill;
+        for (int idx = lane; idx < 64; idx += 32) {
+            int r = idx >> 3, c = idx & 7;
+            if (r >= lh || c >= lw) continue;
+            int X = lx0 + c, Y = ly0 + r;
+            int av = has_a ? TY(s, X, b.y - 1) : fill;
+            int lv = has_l ? TY(s, b.x - 1, Y) : fill;
+            int v;
+            if (A == CVP9_ARITH_REFCPU) {
+                v = b.ymode == 0 ? dc : b.ymode == 1 ? av : b.ymode == 2 ? lv : clampi(av + lv - tl, 0, 255);
+            } else {
+                v = b.ymode == 0 ? dc : b.ymode == 2 ? lv : b.ymode == 9 ? clampi(av + lv - tl, 0, 255) : av;
+            }
+            TY(s, X, Y) = (uint8_t)v;
+        }
+    }
+    /* chroma: both planes, uv_mode */
+    {
+        int gcx = gbx >> 1, gcy = gby >> 1;
+        int bcx = b.x >> 1, bcy = b.y >> 1;
+        int cbw = (b.cw + 1) >> 1, cbh = (b.ch + 1) >> 1;
+        int has_a = gcy > 0, has_l = gcx > 0;
+        int dcs[2] = { 128, 128 };
+        if (b.uvmode == 0) {
+#pragma unroll
+            for (int p = 1; p <= 2; p++) {
+                unsigned sa = 0, sl = 0;
+                for (int i = lane; i < cbw; i += 32) sa += has_a ? TC(s, p, bcx + i, bcy - 1) : (unsigned)fill;
+                for (int i = lane; i < cbh; i += 32) sl += has_l ? TC(s, p, bcx - 1, bcy + i) : (unsigned)fill;
+                sa = __reduce_add_sync(0xffffffffu, sa);
+                sl = __reduce_add_sync(0xffffffffu, sl);
+                int dc = 128;
+                if (A == CVP9_ARITH_REFCPU) {
+                    unsigned n = cbw + cbh;
+                    dc = (int)((sa + sl + (n >> 1)) / n);
+                } else {
+                    if (has_a && has_l) dc = (int)((sa + sl + (unsigned)(cbw + cbh) / 2) / (unsigned)(cbw + cbh));
+                    else if (has_a) dc = (int)((sa + (unsigned)cbw / 2) / (unsigned)cbw);
+                    else if (has_l) dc = (int)((sl + (unsigned)cbh / 2) / (unsigned)cbh);
+                }
+                dcs[p - 1] = dc;
+            }
+        }
+        int p = 1 + (lane >> 4);
+        int r = (lane >> 2) & 3, c = lane & 3;
+        if (r < clh && c < clw) {
+            int X = cx0 + c, Y = cy0 + r;
+            int av = has_a ? TC(s, p, X, bcy - 1) : fill;
+            int lv = has_l ? TC(s, p, bcx - 1, Y) : fill;
+            int tl = (has_a && has_l) ? TC(s, p, bcx - 1, bcy - 1) : fill;
+            int m = b.uvmode, v;
+            int dc = p == 1 ? dcs[0] : dcs[1];
+            if (A == CVP9_ARITH_REFCPU) {
+                v = m == 0 ? dc : m == 1 ? av : m == 2 ? lv : clampi(av + lv - tl, 0, 255);
+            } else {
+                v = m == 0 ? dc : m == 2 ? lv : m == 9 ? clampi(av + lv - tl, 0, 255) : av;
+            }
+            TC(s, p, X, Y) = (uint8_t)v;
+        }
+    }
+}
+
+/* Stage a (sw x sh) window of a reference plane starting at (x0, y0), every
+ * sample clamped into [0, pw-1] x [0, ph-1], into st (row pitch sp). */
+__device__ __forceinline__ void stage_window(uint8_t *st, int sp, const uint8_t *__restrict__ plane,
+                                             int stride, int pw, int ph, int x0, int y0,
+                                             int sw, int sh, int lane)
+{
+    int xm = pw > 0 ? pw - 1 : 0, ym = ph > 0 ? ph - 1 : 0;
+    for (int i = lane; i < sw * sh; i += 32) {
+        int sy = i / sw, sx = i - sy * sw;
+        int yy = clampi(y0 + sy, 0, ym), xx = clampi(x0 + sx, 0, xm);
+        st[sy * sp + sx] = __ldg(plane + (size_t)yy * stride + xx);
+    }
+}
+
+/* REFCPU bilinear of one region from a staged (w+1) x (h+1) window. */
+__device__ __forceinline__ int bilin(const uint8_t *st, int sp, int r, int c, int fx, int fy)
+{
+    unsigned a = st[r * sp + c], b = st[r * sp + c + 1];
+    unsigned d = st[(r + 1) * sp + c], e = st[(r + 1) * sp + c + 1];
+    unsigned top = (a * (8 - fx) + b * fx + 4) >> 3;
+    unsigned bot = (d * (8 - fx) + e * fx + 4) >> 3;
+    return (int)((top * (8 - fy) + bot * fy + 4) >> 3);
+}
+
+template <int A>
+__device__ void predict_inter_chunk(ReconSmem &s, const cvp9_job_t &job, const BlkS &b,
+                                    int sbx, int sby, int lx0, int ly0, int lw, int lh,
+                                    int cx0, int cy0, int clw, int clh, int warp, int lane)
+{
+    const cvp9_ref_t *R;
+    if (A == CVP9_ARITH_REFCPU) {
+        int slot = (int)b.ref0 - 1;
+        R = (slot >= 0 && slot < 8) ? &job.ref[slot] : nullptr;
+    } else {
+        int sel = clampi((int)b.ref0 - 1, 0, 2);
+        R = &job.ref[job.ref_slot_of[sel] & 7];
+    }
+    const uint8_t *rp = R ? R->plane : nullptr;
+    if (!rp) {
+        const int fill = A == CVP9_ARITH_REFCPU ? 127 : 128;
+        for (int idx = lane; idx < 64; idx += 32) {
+            int r = idx >> 3, c = idx & 7;
+            if (r < lh && c < lw) TY(s, lx0 + c, ly0 + r) = (uint8_t)fill;
+        }
+        int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
+        if (r < clh && c < clw) TC(s, p, cx0 + c, cy0 + r) = (uint8_t)fill;
+        return;
+    }
+    const int rw = R->w, rh = R->h;
+    const int rcs = (rw + 1) >> 1;                       /* chroma stride */
+    const uint8_t *ru = rp + (size_t)rw * rh;
+    const uint8_t *rv = ru + (size_t)rcs * ((rh + 1) >> 1);
+    uint8_t *st = s.stage[warp];
+    const int mvx = b.mvx, mvy = b.mvy;
+
+    if (A == CVP9_ARITH_REFCPU) {
+        /* luma: 9x9 window, pitch 16 */
+        int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
+        int fx = px8 & 7, fy = py8 & 7;
+        stage_window(st, 16, rp, rw, rw, rh, px8 >> 3, py8 >> 3, lw + 1, lh + 1, lane);
+        /* chroma: MV halved toward zero, extent = floor half of the ref size */
+        int cmx = mvx / 2, cmy = mvy / 2;
+        int gcx = (sbx >> 1) + cx0, gcy = (sby >> 1) + cy0;
+        int cpx8 = gcx * 8 + cmx, cpy8 = gcy * 8 + cmy;
+        int cfx = cpx8 & 7, cfy = cpy8 & 7;
+        stage_window(st + 160, 8, ru, rcs, rw >> 1, rh >> 1, cpx8 >> 3, cpy8 >> 3, clw + 1, clh + 1, lane);
+        stage_window(st + 208, 8, rv, rcs, rw >> 1, rh >> 1, cpx8 >> 3, cpy8 >> 3, clw + 1, clh + 1, lane);
+        __syncwarp();
+        for (int idx = lane; idx < 64; idx += 32) {
+            int r = idx >> 3, c = idx & 7;
+            if (r < lh && c < lw) TY(s, lx0 + c, ly0 + r) = (uint8_t)bilin(st, 16, r, c, fx, fy);
+        }
+        int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
+        if (r < clh && c < clw)
+            TC(s, p, cx0 + c, cy0 + r) = (uint8_t)bilin(st + (p == 1 ? 160 : 208), 8, r, c, cfx, cfy);
+        __syncwarp();
+    } else {
+        /* luma: (lw+7) x (lh+7) window at pitch 16; H pass into 15 x 8 */
+        int bx = sbx + lx0 + (mvx >> 3), by = sby + ly0 + (mvy >> 3);
+        int fx = (mvx & 7) << 1, fy = (mvy & 7) << 1;
+        int gcx = (sbx >> 1) + cx0, gcy = (sby >> 1) + cy0;
+        int cbx = gcx + (mvx >> 4), cby = gcy + (mvy >> 4);
+        int cfx = mvx & 15, cfy = mvy & 15;
+        int cw2 = (rw + 1) >> 1, ch2 = (rh + 1) >> 1;
+        uint8_t *sy_ = st;              /* 15 x 16 */
+        uint8_t *hy = st + 240;         /* 15 x 8  */
+        uint8_t *su = st + 360;         /* 11 x 12 */
+        uint8_t *sv = st + 492;         /* 11 x 12 */
+        uint8_t *hu = st + 624;         /* 11 x 4  */
+        uint8_t *hv = st + 668;         /* 11 x 4  */
+        stage_window(sy_, 16, rp, rw, rw, rh, bx - 3, by - 3, lw + 7, lh + 7, lane);
+        stage_window(su, 12, ru, rcs, cw2, ch2, cbx - 3, cby - 3, clw + 7, clh + 7, lane);
+        stage_window(sv, 12, rv, rcs, cw2, ch2, cbx - 3, cby - 3, clw + 7, clh + 7, lane);
+        __syncwarp();
+        /* horizontal pass (rounded, clipped to 8 bits) */
+        for (int i = lane; i < (lh + 7) * lw; i += 32) {
+            int r = i / lw, c = i - r * lw;
+            int acc = 0;
+#pragma unroll
+            for (int t = 0; t < 8; t++) acc += c_subpel[fx][t] * sy_[r * 16 + c + t];
+            hy[r * 8 + c] = (uint8_t)clampi((acc + 64) >> 7, 0, 255);
+        }
+        for (int i = lane; i < 2 * (clh + 7) * clw; i += 32) {
+            int pl = i >= (clh + 7) * clw;
+            int j = pl ? i - (clh + 7) * clw : i;
+            int r = j / clw, c = j - r * clw;
+            const uint8_t *src = pl ? sv : su;
+            int acc = 0;
+#pragma unroll
+            for (int t = 0; t < 8; t++) acc += c_subpel[cfx][t] * src[r * 12 + c + t];
+            (pl ? hv : hu)[r * 4 + c] = (uint8_t)clampi((acc + 64) >> 7, 0, 255);
+        }
+        __syncwarp();
+        for (int idx = lane; idx < 64; idx += 32) {
+            int r = idx >> 3, c = idx & 7;
+            if (r >= lh || c >= lw) continue;
+            int v;
+            if (fx == 0 && fy == 0) {
+                v = sy_[(r + 3) * 16 + c + 3];
+            } else {
+                int acc = 0;
+#pragma unroll
+                for (int t = 0; t < 8; t++) acc += c_subpel[fy][t] * hy[(r + t) * 8 + c];
+                v = clampi((acc + 64) >> 7, 0, 255);
+            }
+            TY(s, lx0 + c, ly0 + r) = (uint8_t)v;
+        }
+        {
+            int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
+            if (r < clh && c < clw) {
+                int v;
+                if (cfx == 0 && cfy == 0) {
+                    v = (p == 1 ? su : sv)[(r + 3) * 12 + c + 3];
+                } else {
+                    const uint8_t *h = p == 1 ? hu : hv;
+                    int acc = 0;
+#pragma unroll
+                    for (int t = 0; t < 8; t++) acc += c_subpel[cfy][t] * h[(r + t) * 4 + c];
+                    v = clampi((acc + 64) >> 7, 0, 255);
+                }
+                TC(s, p, cx0 + c, cy0 + r) = (uint8_t)v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+/* ── Residual: one item = one TX column (pass 1) or one TX row (pass 2) ── */
+
+struct TxRef {
+    int plane, txl, n;
+    int px0, py0;      /* TX origin in the SB tile of its plane */
+    uint64_t coeff;    /* first coefficient of the TX            */
+    int mask_idx;
+};
+
+__device__ __forceinline__ TxRef locate_item(const BlkS &b, int item, int *lane_idx)
+{
+    TxRef t;
+    uint64_t off = b.coeff;
+    int p = 0;
+    for (; p < 2; p++) {
+        int cnt = b.pnt[p] * (4 << b.ptxl[p]);
+        if (item < cnt) break;
+        item -= cnt;
+        off += (uint64_t)b.pnt[p] * (uint64_t)(16 << (2 * b.ptxl[p]));
+    }
+    int txl = b.ptxl[p], n = 4 << txl;
+    int tx = item >> (2 + txl);
+    *lane_idx = item & (n - 1);
+    int nx = b.pnx[p];
+    int tx_x = tx % nx, tx_y = tx / nx;
+    t.plane = p;
+    t.txl = txl;
+    t.n = n;
+    int ox = p ? (b.x >> 1) : b.x, oy = p ? (b.y >> 1) : b.y;
+    t.px0 = ox + tx_x * n;
+    t.py0 = oy + tx_y * n;
+    t.coeff = off + (uint64_t)tx * (uint64_t)(n * n);
+    t.mask_idx = p == 0 ? (t.py0 >> 2) * 16 + (t.px0 >> 2)
+                        : 256 + (p - 1) * 64 + (t.py0 >> 2) * 8 + (t.px0 >> 2);
+    return t;
+}
+
+/* REFCPU pass 1: T[:, j] = M^T X[:, j] over the nonzero X[k][j], k ascending
+ * (vp9_reconstruct.c:31-40). Skipped zero terms add +-0 to a sum that is
+ * never -0, so the result is bit-identical to the full sum. */
+template <int N>
+__device__ __forceinline__ void refcpu_col(ReconSmem &s, const int16_t *__restrict__ X, int j,
+                                           int px0, int py0, int mask_idx, const double *M)
+{
+    double acc[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) acc[i] = 0.0;
+    bool any = false;
+#pragma unroll 1
+    for (int k = 0; k < N; k++) {
+        int x = __ldg(X + k * N + j);
+        if (x == 0) continue;
+        any = true;
+        double xd = (double)x;
+#pragma unroll
+        for (int i = 0; i < N; i++) acc[i] = __dadd_rn(acc[i], __dmul_rn(M[k * N + i], xd));
+    }
+    if (!any) return;
+#pragma unroll
+    for (int i = 0; i < N; i++) s.temp.d[(py0 + i) * kTempPitch + px0 + j] = acc[i];
+    atomicOr(&s.txmask[mask_idx], 1u << j);
+}
+
+/* REFCPU pass 2: O[i, :] = T[i, :] M over the nonzero columns, round half
+ * away from zero, saturate to int16, add and clamp (:42-59, :351-360). */
+template <int N>
+__device__ __forceinline__ void refcpu_row(ReconSmem &s, int i, int px0, int py0, unsigned mask,
+                                           const double *M)
+{
+    double acc[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) acc[j] = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < N; k++) {
+        if (!((mask >> k) & 1u)) continue;
+        double t = s.temp.d[(py0 + i) * kTempPitch + px0 + k];
+#pragma unroll
+        for (int j = 0; j < N; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, M[k * N + j]));
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        double v = acc[j];
+        int r = __double2int_rz(__dadd_rn(v, v >= 0.0 ? 0.5 : -0.5));
+        r = clampi(r, -32768, 32767);
+        uint8_t &px = TY(s, px0 + j, py0 + i);
+        px = (uint8_t)clampi((int)px + r, 0, 255);
+    }
+}
+
+__device__ __forceinline__ void idct_n(wi *x, int n)
+{
+    if (n == 4) idct4(x);
+    else if (n == 8) idct8(x);
+    else if (n == 16) idct16(x);
+    else idct32(x);
+}
+
+__device__ __forceinline__ int32_t *spec_temp(ReconSmem &s, int plane, int x, int y)
+{
+    if (plane == 0) return &s.temp.i[y * 64 + x];
+    return &s.temp.i[4096 + (plane - 1) * 1024 + y * 32 + x];
+}
+
+/* SPEC pass 1: dequantise column j (DC step at [0][0] only) and run the
+ * 1-D transform down the column (vp9_idct.comp.glsl:666-679). */
+template <int N>
+__device__ __forceinline__ void spec_col(ReconSmem &s, const int16_t *__restrict__ X, int j,
+                                         const TxRef &t, int q_dc, int q_ac)
+{
+    wi v[N];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        int c = __ldg(X + k * N + j);
+        any |= c != 0;
+        v[k] = wi(c) * ((k == 0 && j == 0) ? q_dc : q_ac);
+    }
+    if (any) {
+        idct_n(v, N);
+        atomicOr(&s.txmask[t.mask_idx], 1u);
+    }
+#pragma unroll
+    for (int k = 0; k < N; k++) *spec_temp(s, t.plane, t.px0 + j, t.py0 + k) = any ? v[k].v : 0;
+}
+
+/* SPEC pass 2: row transform, final rounding shift 4/5/6/6, add and clamp;
+ * samples outside the frame are left alone (tile write-back clips them). */
+template <int N>
+__device__ __forceinline__ void spec_row(ReconSmem &s, int i, const TxRef &t)
+{
+    wi v[N];
+#pragma unroll
+    for (int k = 0; k < N; k++) v[k] = wi(*spec_temp(s, t.plane, t.px0 + k, t.py0 + i));
+    idct_n(v, N);
+    const int sh = N == 4 ? 4 : (N == 8 ? 5 : 6);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        int r = ((int)((unsigned)v[j].v + (1u << (sh - 1)))) >> sh;
+        uint8_t &px = t.plane == 0 ? TY(s, t.px0 + j, t.py0 + i) : TC(s, t.plane, t.px0 + j, t.py0 + i);
+        px = (uint8_t)clampi((int)px + r, 0, 255);
+    }
+}
+
+/* ── Synchronisation helpers ────────────────────────────────────────────── */
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+/* Bounded wait until flag == epoch; returns false on timeout. */
+__device__ bool wait_flag(const unsigned *flag, unsigned epoch)
+{
+    for (long long it = 0; it < kSpinLimit; it++) {
+        if (ld_acquire(flag) == epoch) return true;
+        __nanosleep(it < 64 ? 32 : 256);
+    }
+    return false;
+}
+
+} /* namespace */
+
+/* ── Kernels ─────────────────────────────────────────────────────────────── */
+
+/* Per block: SB membership and the contiguous range of each SB. The
+ * per-frame scratch (sb_range, status) is zeroed before this launch. */
+__global__ void __launch_bounds__(256) k_scan_blocks(const cvp9_job_t *__restrict__ jobs)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    const vp9_macroblock_info_t *B = job.blocks;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < job.num_blocks; i += gridDim.x * blockDim.x) {
+    auto sb_of = [&](uint32_t k, bool *ok) -> int {
+        vp9_macroblock_info_t b = B[k];
+        int x = b.x, y = b.y, w = b.width, h = b.height;
+        bool good = x < job.W && y < job.H && w >= 4 && h >= 4 && w <= 64 && h <= 64 &&
+                    !(x & 3) && !(y & 3) && !(w & 3) && !(h & 3) &&
+                    (x & 63) + w <= 64 && (y & 63) + h <= 64 && b.tx_size <= 3;
+        *ok = good;
+        return (y >> 6) * job.sb_cols + (x >> 6);
+    };
+    bool ok;
+    int sb = sb_of(i, &ok);
+    if (!ok) { atomicOr(job.status, (unsigned)CVP9_JOB_BAD_BLOCK); continue; }
+    bool okp = true, okn = true;
+    int prev = i > 0 ? sb_of(i - 1, &okp) : -1;
+    int next = i + 1 < job.num_blocks ? sb_of(i + 1, &okn) : -1;
+    uint32_t *r = job.sb_range + 4 * sb;
+    if (prev != sb) { r[0] = i; atomicAdd(&r[2], 1u); }
+    if (next != sb) r[1] = i + 1;
+    }
+}
+
+template <int A>
+__global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict__ jobs,
+                                                   const uint32_t *__restrict__ tickets,
+                                                   uint32_t n_tickets, uint32_t *ticket_counter)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ReconSmem &s = *reinterpret_cast<ReconSmem *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s.ticket = (int)atomicAdd(ticket_counter, 1u);
+        __syncthreads();
+        const int ticket = s.ticket;
+        if (ticket >= (int)n_tickets) return;
+        const uint32_t code = tickets[ticket];
+        const cvp9_job_t &job = jobs[code >> 20];
+        const int sb = (int)(code & 0xFFFFFu);
+        const int sbr = sb / job.sb_cols, sbc = sb - sbr * job.sb_cols;
+        const int sbx = sbc * 64, sby = sbr * 64;
+        const uint32_t *rg = job.sb_range + 4 * sb;
+        const uint32_t start = rg[0], end = rg[1], groups = rg[2];
+        const bool layout_bad = (*(volatile uint32_t *)job.status & CVP9_JOB_BAD_BLOCK) != 0;
+        bool bad = groups > 1 || end < start || end > job.num_blocks ||
+                   (groups && end - start > (uint32_t)kMaxBlocks);
+        int nb = (groups && !bad && !layout_bad) ? (int)(end - start) : 0;
+
+        /* reset per-SB state, tile = 128 */
+        for (int i = tid; i < 65 * kYPitch; i += kThreads) s.ty[i] = 128;
+        for (int i = tid; i < 33 * kCPitch; i += kThreads) { s.tu[i] = 128; s.tv[i] = 128; }
+        for (int i = tid; i < 256 + 128; i += kThreads) s.txmask[i] = 0;
+        for (int i = tid; i < 256; i += kThreads) s.cell[i] = 0;
+        for (int i = tid; i <= kMaxBlocks; i += kThreads) s.lvl_cnt[i] = 0ull;
+        if (tid == 0) { s.nlev = 1; s.nb = nb; }
+        __syncthreads();
+
+        /* 1. load and re-check blocks (a block must sit inside this SB,
+         * 4-aligned, 4..64 px, tx_size <= 3; sub-8x8 blocks on the 8x8 MI
+         * grid), then mark the 4x4 cells each one covers */
+        bool my_intra = false, overlap = false, my_bad = false;
+        BlkS mb;
+        int nch = 0, nit = 0;
+        if (tid < nb) {
+            vp9_macroblock_info_t g = job.blocks[start + tid];
+            int lx = (int)g.x - sbx, ly = (int)g.y - sby;
+            my_bad = lx < 0 || ly < 0 || (lx & 3) || (ly & 3) || (g.width & 3) || (g.height & 3) ||
+                     g.width < 4 || g.height < 4 || lx + g.width > 64 || ly + g.height > 64 ||
+                     g.x >= job.W || g.y >= job.H || g.tx_size > 3 ||
+                     ((g.width < 8 || g.height < 8) && ((lx & 7) || (ly & 7)));
+            if (my_bad) { lx = 0; ly = 0; g.width = 4; g.height = 4; g.tx_size = 0; }
+            mb.x = (uint8_t)lx;
+            mb.y = (uint8_t)ly;
+            mb.w = g.width;
+            mb.h = g.height;
+            int cw = g.width, ch = g.height;
+            if (g.x + cw > job.W) cw = job.W - g.x;
+            if (g.y + ch > job.H) ch = job.H - g.y;
+            mb.cw = (uint8_t)cw;
+            mb.ch = (uint8_t)ch;
+            mb.txl = g.tx_size;
+            mb.flags = (uint8_t)((g.is_intra ? 1 : 0) | (g.skip ? 2 : 0));
+            mb.ymode = g.y_mode;
+            mb.uvmode = g.uv_mode;
+            mb.ref0 = g.ref_frame[0];
+            mb.mvx = g.mv[0][0];
+            mb.mvy = g.mv[0][1];
+            mb.coeff = g.coeff_offset;
+            residual_layout<A>(mb, job, g.x, g.y);
+            s.blk[tid] = mb;
+            my_intra = g.is_intra != 0;
+            nch = block_chunks(mb);
+            nit = block_items(mb);
+        }
+        if (__syncthreads_or(my_bad)) {
+            /* leave the tile at 128 and flag the frame */
+            if (tid == 0) atomicOr(job.status, (unsigned)CVP9_JOB_BAD_BLOCK);
+            nb = 0;
+            my_intra = false;
+            if (tid == 0) s.nb = 0;
+        }
+        if (tid < nb) {
+            /* cells a block writes: its prediction area; under SPEC a
+             * sub-8x8 block's residual spans the whole 8x8 MI
+             * (vp9_kf_tile.c:327-330), so it owns that area too */
+            int ow = mb.cw, oh = mb.ch;
+            if (A == CVP9_ARITH_SPEC && (mb.w < 8 || mb.h < 8)) {
+                ow = min(8, job.W - (sbx + mb.x));
+                oh = min(8, job.H - (sby + mb.y));
+            }
+            int c0x = mb.x >> 2, c0y = mb.y >> 2;
+            int c1x = (mb.x + ow - 1) >> 2, c1y = (mb.y + oh - 1) >> 2;
+            for (int cy = c0y; cy <= c1y; cy++)
+                for (int cx = c0x; cx <= c1x; cx++)
+                    if (atomicCAS(&s.cell[cy * 16 + cx], (uint16_t)0, (uint16_t)(tid + 1)) != 0) overlap = true;
+        }
+        const int any_intra = __syncthreads_or(my_intra);
+        const int any_overlap = __syncthreads_or(overlap);
+
+        /* 2. dependency levels. An intra block depends on the blocks that own
+         * its above row, left column and above-left corner inside the SB. */
+        bool seq = any_overlap != 0;
+        int deps[33];
+        int ndeps = 0;
+        if (any_intra && !seq) {
+            bool late = false;
+            if (tid < nb && my_intra) {
+                const BlkS &b = s.blk[tid];
+                int c0x = b.x >> 2, c0y = b.y >> 2;
+                int c1x = (b.x + b.cw - 1) >> 2, c1y = (b.y + b.ch - 1) >> 2;
+                auto add = [&](int cx, int cy) {
+                    int o = s.cell[cy * 16 + cx];
+                    if (!o) return;
+                    o -= 1;
+                    if (o >= tid) { late = true; return; }
+                    for (int k = 0; k < ndeps; k++) if (deps[k] == o) return;
+                    if (ndeps < 33) deps[ndeps++] = o;
+                };
+                if (c0y > 0) for (int cx = c0x; cx <= c1x; cx++) add(cx, c0y - 1);
+                if (c0x > 0) for (int cy = c0y; cy <= c1y; cy++) add(c0x - 1, cy);
+                if (c0x > 0 && c0y > 0) add(c0x - 1, c0y - 1);
+            }
+            seq = __syncthreads_or(late) != 0;
+        }
+        if (tid < kMaxBlocks) s.lvl[tid] = 0;
+        __syncthreads();
+        if (seq) {
+            if (tid < nb) s.lvl[tid] = (uint16_t)tid;
+        } else if (any_intra) {
+            volatile uint16_t *vl = s.lvl;
+            for (;;) {
+                bool changed = false;
+                if (tid < nb && ndeps) {
+                    int L = 0;
+                    for (int k = 0; k < ndeps; k++) { int v = vl[deps[k]] + 1; L = v > L ? v : L; }
+                    if (L != vl[tid]) { vl[tid] = (uint16_t)L; changed = true; }
+                }
+                if (!__syncthreads_or(changed)) break;
+            }
+        }
+        __syncthreads();
+
+        /* 3. counting sort by level; each level's blocks, chunks and items
+         * get contiguous ranges (one packed 64-bit atomic keeps the three
+         * offsets of a block consistent with each other) */
+        unsigned long long old = 0;
+        int my_lvl = 0;
+        if (tid < nb) {
+            my_lvl = s.lvl[tid];
+            atomicMax(&s.nlev, my_lvl + 1);
+            old = atomicAdd(&s.lvl_cnt[my_lvl], (1ull << 40) | ((unsigned long long)nch << 20) |
+                                                    (unsigned long long)nit);
+        }
+        __syncthreads();
+        const int nlev = s.nlev;
+        if (warp == 0) {
+            /* exclusive scan over levels, 8 levels per lane */
+            int per = (nlev + 31) / 32;
+            int b0 = lane * per;
+            unsigned sb_ = 0, sc = 0, si = 0;
+            for (int l = b0; l < b0 + per && l < nlev; l++) {
+                unsigned long long v = s.lvl_cnt[l];
+                sb_ += (unsigned)(v >> 40); sc += (unsigned)((v >> 20) & 0xFFFFF); si += (unsigned)(v & 0xFFFFF);
+            }
+            unsigned xb = sb_, xc = sc, xi = si;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned yb = __shfl_up_sync(0xffffffffu, xb, o);
+                unsigned yc = __shfl_up_sync(0xffffffffu, xc, o);
+                unsigned yi = __shfl_up_sync(0xffffffffu, xi, o);
+                if (lane >= o) { xb += yb; xc += yc; xi += yi; }
+            }
+            unsigned eb = xb - sb_, ec = xc - sc, ei = xi - si;
+            for (int l = b0; l < b0 + per && l < nlev; l++) {
+                s.base_blk[l] = (uint16_t)eb; s.base_chunk[l] = (uint16_t)ec; s.base_item[l] = (uint16_t)ei;
+                unsigned long long v = s.lvl_cnt[l];
+                eb += (unsigned)(v >> 40); ec += (unsigned)((v >> 20) & 0xFFFFF); ei += (unsigned)(v & 0xFFFFF);
+            }
+            if (lane == 31) { s.base_blk[nlev] = (uint16_t)eb; s.base_chunk[nlev] = (uint16_t)ec; s.base_item[nlev] = (uint16_t)ei; }
+        }
+        __syncthreads();
+        if (tid < nb) {
+            int p = s.base_blk[my_lvl] + (int)(old >> 40);
+            s.order[p] = (uint16_t)tid;
+            s.chunk_off[p] = (uint16_t)(s.base_chunk[my_lvl] + (int)((old >> 20) & 0xFFFFF));
+            s.item_off[p] = (uint16_t)(s.base_item[my_lvl] + (int)(old & 0xFFFFF));
+        }
+        if (tid == 0 && nb > 0) { s.chunk_off[nb] = s.base_chunk[nlev]; s.item_off[nb] = s.base_item[nlev]; }
+
+        /* 4. wait for the neighbour SBs when intra blocks read their edges */
+        if (any_intra) {
+            if (tid == 0) {
+                bool ok = true;
+                if (sbc > 0) ok &= wait_flag(job.sb_done + sb - 1, job.epoch);
+                if (sbr > 0) ok &= wait_flag(job.sb_done + sb - job.sb_cols, job.epoch);
+                if (sbr > 0 && sbc > 0) ok &= wait_flag(job.sb_done + sb - job.sb_cols - 1, job.epoch);
+                if (!ok) atomicOr(job.status, (unsigned)CVP9_JOB_TIMEOUT);
+            }
+            __syncthreads();
+            /* halo: row above (x = -1..63) and column to the left */
+            const uint8_t *Y = job.out;
+            const uint8_t *U = job.out + (size_t)job.W * job.H;
+            const uint8_t *V = U + (size_t)job.CW * job.CH;
+            if (sby > 0) {
+                for (int i = tid - 1; i < 64; i += kThreads) {
+                    int gx = sbx + i;
+                    if (gx >= 0 && gx < job.W) TY(s, i, -1) = Y[(size_t)(sby - 1) * job.W + gx];
+                }
+                for (int i = tid - 1; i < 32; i += kThreads) {
+                    int gx = (sbx >> 1) + i;
+                    if (gx >= 0 && gx < job.CW) {
+                        TC(s, 1, i, -1) = U[(size_t)((sby >> 1) - 1) * job.CW + gx];
+                        TC(s, 2, i, -1) = V[(size_t)((sby >> 1) - 1) * job.CW + gx];
+                    }
+                }
+            }
+            if (sbx > 0) {
+                for (int i = tid; i < 64; i += kThreads) {
+                    int gy = sby + i;
+                    if (gy < job.H) TY(s, -1, i) = Y[(size_t)gy * job.W + sbx - 1];
+                }
+                for (int i = tid; i < 32; i += kThreads) {
+                    int gy = (sby >> 1) + i;
+                    if (gy < job.CH) {
+                        TC(s, 1, -1, i) = U[(size_t)gy * job.CW + (sbx >> 1) - 1];
+                        TC(s, 2, -1, i) = V[(size_t)gy * job.CW + (sbx >> 1) - 1];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        /* 5. levels */
+        for (int L = 0; L < nlev && nb > 0; L++) {
+            const int pb0 = s.base_blk[L], pb1 = s.base_blk[L + 1];
+            /* phase P: prediction, warp per 8x8 chunk */
+            for (int chk = s.base_chunk[L] + warp; chk < s.base_chunk[L + 1]; chk += kWarps) {
+                int lo = pb0, hi = pb1 - 1;
+                while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.chunk_off[mid] <= chk) lo = mid; else hi = mid - 1; }
+                const BlkS &b = s.blk[s.order[lo]];
+                int c = chk - s.chunk_off[lo];
+                int nx = (b.cw + 7) >> 3;
+                int ccy = c / nx, ccx = c - ccy * nx;
+                int lx0 = b.x + ccx * 8, ly0 = b.y + ccy * 8;
+                int lw = min(8, b.cw - ccx * 8), lh = min(8, b.ch - ccy * 8);
+                int cbw = (b.cw + 1) >> 1, cbh = (b.ch + 1) >> 1;
+                int cx0 = (b.x >> 1) + ccx * 4, cy0 = (b.y >> 1) + ccy * 4;
+                int clw = min(4, cbw - ccx * 4), clh = min(4, cbh - ccy * 4);
+                if (b.flags & 1)
+                    predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, lx0, ly0, lw, lh, cx0, cy0, clw, clh, lane);
+                else
+                    predict_inter_chunk<A>(s, job, b, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh, warp, lane);
+            }
+            /* phase P': first transform pass, thread per TX column */
+            for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
+                int lo = pb0, hi = pb1 - 1;
+                while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.item_off[mid] <= it) lo = mid; else hi = mid - 1; }
+                const BlkS &b = s.blk[s.order[lo]];
+                int j;
+                TxRef t = locate_item(b, it - s.item_off[lo], &j);
+                if (t.coeff + (uint64_t)(t.n * t.n) > (uint64_t)job.num_coeffs) continue;
+                const int16_t *X = job.coeffs + t.coeff;
+                if (A == CVP9_ARITH_REFCPU) {
+                    const double *M = dct_basis(t.txl);
+                    switch (t.txl) {
+                    case 0: refcpu_col<4>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+                    case 1: refcpu_col<8>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+                    case 2: refcpu_col<16>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+                    default: refcpu_col<32>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+                    }
+                } else {
+                    switch (t.txl) {
+                    case 0: spec_col<4>(s, X, j, t, job.q_dc, job.q_ac); break;
+                    case 1: spec_col<8>(s, X, j, t, job.q_dc, job.q_ac); break;
+                    case 2: spec_col<16>(s, X, j, t, job.q_dc, job.q_ac); break;
+                    default: spec_col<32>(s, X, j, t, job.q_dc, job.q_ac); break;
+                    }
+                }
+            }
+            __syncthreads();
+            /* phase Q: second pass + residual add, thread per TX row */
+            for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
+                int lo = pb0, hi = pb1 - 1;
+                while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.item_off[mid] <= it) lo = mid; else hi = mid - 1; }
+                const BlkS &b = s.blk[s.order[lo]];
+                int i;
+                TxRef t = locate_item(b, it - s.item_off[lo], &i);
+                unsigned mask = s.txmask[t.mask_idx];
+                if (!mask) continue;
+                if (A == CVP9_ARITH_REFCPU) {
+                    const double *M = dct_basis(t.txl);
+                    switch (t.txl) {
+                    case 0: refcpu_row<4>(s, i, t.px0, t.py0, mask, M); break;
+                    case 1: refcpu_row<8>(s, i, t.px0, t.py0, mask, M); break;
+                    case 2: refcpu_row<16>(s, i, t.px0, t.py0, mask, M); break;
+                    default: refcpu_row<32>(s, i, t.px0, t.py0, mask, M); break;
+                    }
+                } else {
+                    switch (t.txl) {
+                    case 0: spec_row<4>(s, i, t); break;
+                    case 1: spec_row<8>(s, i, t); break;
+                    case 2: spec_row<16>(s, i, t); break;
+                    default: spec_row<32>(s, i, t); break;
+                    }
+                }
+            }
+            __syncthreads();
+            if (seq) {
+                /* overlapping blocks may reuse a TX position at a later level */
+                for (int i = tid; i < 256 + 128; i += kThreads) s.txmask[i] = 0;
+                __syncthreads();
+            }
+        }
+
+        /* 6. write the tile (clipped to the frame) and release the SB */
+        {
+            const int vw = min(64, job.W - sbx), vh = min(64, job.H - sby);
+            uint8_t *Y = job.out;
+            if ((job.W & 3) == 0) {
+                for (int i = tid; i < vh * 16; i += kThreads) {
+                    int r = i >> 4, c4 = (i & 15) * 4;
+                    if (c4 >= vw) continue;
+                    *reinterpret_cast<uint32_t *>(Y + (size_t)(sby + r) * job.W + sbx + c4) =
+                        *reinterpret_cast<const uint32_t *>(&TY(s, c4, r));
+                }
+            } else {
+                for (int i = tid; i < vh * 64; i += kThreads) {
+                    int r = i >> 6, c = i & 63;
+                    if (c < vw) Y[(size_t)(sby + r) * job.W + sbx + c] = TY(s, c, r);
+                }
+            }
+            const int cvw = min(32, job.CW - (sbx >> 1)), cvh = min(32, job.CH - (sby >> 1));
+            uint8_t *U = job.out + (size_t)job.W * job.H;
+            uint8_t *V = U + (size_t)job.CW * job.CH;
+            for (int i = tid; i < 2 * cvh * 32; i += kThreads) {
+                int p = i >= cvh * 32;
+                int k = p ? i - cvh * 32 : i;
+                int r = k >> 5, c = k & 31;
+                if (c >= cvw) continue;
+                (p ? V : U)[(size_t)((sby >> 1) + r) * job.CW + (sbx >> 1) + c] = TC(s, 1 + p, c, r);
+            }
+        }
+        if (tid == 0 && bad)
+            atomicOr(job.status, (unsigned)CVP9_JOB_BAD_ORDER |
+                                 ((groups && end >= start && end - start > (uint32_t)kMaxBlocks) ? (unsigned)CVP9_JOB_TOO_MANY : 0u));
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(job.sb_done + sb, job.epoch);
+        }
+    }
+}
+
+/* ── Loop filter ─────────────────────────────────────────────────────────── */
+
+__device__ __forceinline__ void filter4(uint8_t *p1, uint8_t *p0, uint8_t *q0, uint8_t *q1, int thr)
+{
+    int P1 = *p1, P0 = *p0, Q0 = *q0, Q1 = *q1;
+    int d0 = P0 - Q0, d1 = P1 - Q1;
+    if ((d0 < 0 ? -d0 : d0) * 2 + (d1 < 0 ? -d1 : d1) / 2 > thr) return;
+    int delta = clampi((3 * (Q0 - P0) + 4) >> 3, -thr, thr);
+    *p0 = (uint8_t)clampi(P0 + delta, 0, 255);
+    *q0 = (uint8_t)clampi(Q0 - delta, 0, 255);
+    *p1 = (uint8_t)clampi(P1 + delta / 2, 0, 255);
+    *q1 = (uint8_t)clampi(Q1 - delta / 2, 0, 255);
+}
+
+__device__ __forceinline__ int lf_threshold(int level, int sharp)
+{
+    int t = level;
+    if (sharp > 0) {
+        t >>= (sharp > 4) ? 2 : 1;
+        if (t > 9 - sharp) t = 9 - sharp;
+    }
+    return t < 1 ? 1 : t;
+}
+
+/* Tile (tx, ty) covers luma [64tx-4, 64tx+60) x [64ty-4, 64ty+60): every tap
+ * of every 8-px edge (rows/cols e-2..e+1) lies in one tile, so the
+ * horizontal pass then the vertical pass run tile-locally and in place with
+ * the same result as the frame-wide passes (vp9_reconstruct.c:146-190).
+ * Requires W and H not of the form 8k+1 (lf_tiled). */
+template <int A>
+__global__ void __launch_bounds__(256) k_loopfilter(const cvp9_job_t *__restrict__ jobs)
+{
+    __shared__ __align__(16) uint8_t t[64 * 68];
+    const cvp9_job_t &job = jobs[blockIdx.z];
+    const int tx = blockIdx.x, ty = blockIdx.y;
+    const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
+    if (!job.lf_tiled || x0 >= job.W || y0 >= job.H) return;
+    const bool filt = !(A == CVP9_ARITH_REFCPU && job.lf_level == 0);
+    if (!filt && !job.nv12) return;
+    const int tid = threadIdx.x;
+    const int xa = max(x0, 0), xb = min(x0 + 64, job.W);
+    const int ya = max(y0, 0), yb = min(y0 + 64, job.H);
+    uint8_t *Y = job.out;
+    const int W = job.W;
+    /* tile byte (x - x0, y - y0) at t[(y - y0) * 68 + (x - x0)] */
+    for (int i = tid; i < (yb - ya) * 64; i += 256) {
+        int r = i >> 6, c = i & 63;
+        int gx = xa + c;
+        if (gx < xb) t[(ya - y0 + r) * 68 + (gx - x0)] = Y[(size_t)(ya + r) * W + gx];
+    }
+    __syncthreads();
+    if (filt) {
+        const int thr = lf_threshold(job.lf_level, job.lf_sharpness);
+        /* horizontal edges e = y0 + 4 + 8k */
+        for (int i = tid; i < 8 * 64; i += 256) {
+            int k = i >> 6, c = i & 63;
+            int e = y0 + 4 + 8 * k, gx = x0 + c;
+            if (e < 8 || e >= job.H || gx < xa || gx >= xb) continue;
+            int r = e - y0;
+            filter4(&t[(r - 2) * 68 + c], &t[(r - 1) * 68 + c], &t[r * 68 + c], &t[(r + 1) * 68 + c], thr);
+        }
+        __syncthreads();
+        for (int i = tid; i < 8 * 64; i += 256) {
+            int k = i >> 6, r = i & 63;
+            int e = x0 + 4 + 8 * k, gy = y0 + r;
+            if (e < 8 || e >= job.W || gy < ya || gy >= yb) continue;
+            int c = e - x0;
+            uint8_t *row = &t[r * 68];
+            filter4(&row[c - 2], &row[c - 1], &row[c], &row[c + 1], thr);
+        }
+        __syncthreads();
+        for (int i = tid; i < (yb - ya) * 64; i += 256) {
+            int r = i >> 6, c = i & 63;
+            int gx = xa + c;
+            if (gx < xb) Y[(size_t)(ya + r) * W + gx] = t[(ya - y0 + r) * 68 + (gx - x0)];
+        }
+    }
+    if (job.nv12) {
+        uint8_t *D = job.nv12;
+        for (int i = tid; i < (yb - ya) * 64; i += 256) {
+            int r = i >> 6, c = i & 63;
+            int gx = xa + c;
+            if (gx < xb) D[(size_t)(ya + r) * W + gx] = t[(ya - y0 + r) * 68 + (gx - x0)];
+        }
+        /* chroma [32tx-2, 32tx+30) x [32ty-2, 32ty+30) interleaved */
+        const int cxa = max(tx * 32 - 2, 0), cxb = min(tx * 32 + 30, job.CW);
+        const int cya = max(ty * 32 - 2, 0), cyb = min(ty * 32 + 30, job.CH);
+        const uint8_t *U = job.out + (size_t)W * job.H;
+        const uint8_t *V = U + (size_t)job.CW * job.CH;
+        uint8_t *UV = D + (size_t)W * job.H;
+        for (int i = tid; i < (cyb - cya) * 32; i += 256) {
+            int r = i >> 5, c = i & 31;
+            int gx = cxa + c, gy = cya + r;
+            if (gx >= cxb) continue;
+            size_t so = (size_t)gy * job.CW + gx;
+            size_t d = (size_t)gy * 2 * job.CW + 2 * gx;
+            UV[d] = U[so];
+            UV[d + 1] = V[so];
+        }
+    }
+}
+
+/* Frame-wide loop filter for widths/heights of the form 8k+1, with the
+ * reference's flat addressing (vertical edges at the last column read the
+ * next row's first sample) and out-of-plane accesses skipped. */
+__global__ void k_lf_flat_h(const cvp9_job_t *__restrict__ jobs, int refcpu)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    if (job.lf_tiled || (refcpu && job.lf_level == 0)) return;
+    int thr = lf_threshold(job.lf_level, job.lf_sharpness);
+    int nedge = job.H > 8 ? (job.H - 1) / 8 : 0;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nedge * job.W) return;
+    int e = 8 * (int)(i / job.W + 1), x = (int)(i % job.W);
+    if (e + 1 >= job.H) return;
+    uint8_t *Y = job.out;
+    size_t S = (size_t)job.W;
+    filter4(Y + (e - 2) * S + x, Y + (e - 1) * S + x, Y + e * S + x, Y + (e + 1) * S + x, thr);
+}
+
+__global__ void k_lf_flat_v(const cvp9_job_t *__restrict__ jobs, int refcpu)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    if (job.lf_tiled || (refcpu && job.lf_level == 0)) return;
+    int thr = lf_threshold(job.lf_level, job.lf_sharpness);
+    int nedge = job.W > 8 ? (job.W - 1) / 8 : 0;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nedge * job.H) return;
+    int e = 8 * (int)(i / job.H + 1), r = (int)(i % job.H);
+    uint8_t *Y = job.out;
+    size_t S = (size_t)job.W, plane = S * job.H;
+    size_t base = (size_t)r * S + e;
+    if (base + 1 >= plane) return;
+    filter4(Y + base - 2, Y + base - 1, Y + base, Y + base + 1, thr);
+}
+
+__global__ void k_nv12_pack(const cvp9_job_t *__restrict__ jobs)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    if (job.lf_tiled || !job.nv12) return;
+    size_t ny = (size_t)job.W * job.H, nc = (size_t)job.CW * job.CH;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ny) job.nv12[i] = job.out[i];
+    if (i < nc) {
+        size_t gy = i / job.CW, gx = i % job.CW;
+        job.nv12[ny + gy * 2 * job.CW + 2 * gx] = job.out[ny + i];
+        job.nv12[ny + gy * 2 * job.CW + 2 * gx + 1] = job.out[ny + nc + i];
+    }
+}
+
+/* ── C-ABI launch shims ─────────────────────────────────────────────────── */
+
+extern "C" {
+
+size_t cvp9k_recon_smem_bytes(void) { return sizeof(ReconSmem); }
+
+int cvp9k_upload_dct_basis(const double *basis, int count)
+{
+    if (count != 16 + 64 + 256 + 1024) return -1;
+    return cudaMemcpyToSymbol(c_dct, basis, sizeof(double) * (size_t)count) == cudaSuccess ? 0 : -1;
+}
+
+int cvp9k_configure(void)
+{
+    size_t smem = sizeof(ReconSmem);
+    if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_REFCPU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+    if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+    return 0;
+}
+
+int cvp9k_recon_ctas_per_sm(int arith)
+{
+    int n = 0;
+    cudaError_t e = arith == CVP9_ARITH_SPEC
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_recon<CVP9_ARITH_SPEC>, kThreads, sizeof(ReconSmem))
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_recon<CVP9_ARITH_REFCPU>, kThreads, sizeof(ReconSmem));
+    return e == cudaSuccess ? n : -1;
+}
+
+/* Timing events become event-record nodes when the stream is being captured. */
+static cudaError_t mark(cudaEvent_t ev, cudaStream_t st, bool capturing)
+{
+    if (!ev) return cudaSuccess;
+    return capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
+}
+
+int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
+{
+    if (!L || L->njobs <= 0) return (int)cudaErrorInvalidValue;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return (int)e;
+    const bool capturing = cap == cudaStreamCaptureStatusActive;
+    if ((e = mark(L->ev[0], st, capturing)) != cudaSuccess) return (int)e;
+    if (L->max_blocks > 0 || L->scan_ctas > 0) {
+        int gx = L->scan_ctas > 0 ? L->scan_ctas : (L->max_blocks + 255) / 256;
+        dim3 g((unsigned)gx, (unsigned)L->njobs);
+        k_scan_blocks<<<g, 256, 0, st>>>(L->jobs);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    if ((e = mark(L->ev[1], st, capturing)) != cudaSuccess) return (int)e;
+    if (L->n_tickets > 0) {
+        int grid = L->recon_ctas > 0 ? L->recon_ctas : (int)L->n_tickets;
+        if (grid > (int)L->n_tickets) grid = (int)L->n_tickets;
+        size_t smem = sizeof(ReconSmem);
+        if (L->arith == CVP9_ARITH_SPEC)
+            k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter);
+        else
+            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    if ((e = mark(L->ev[2], st, capturing)) != cudaSuccess) return (int)e;
+    if (L->lf_tiles_x > 0 && L->lf_tiles_y > 0) {
+        dim3 g((unsigned)L->lf_tiles_x, (unsigned)L->lf_tiles_y, (unsigned)L->njobs);
+        if (L->arith == CVP9_ARITH_SPEC) k_loopfilter<CVP9_ARITH_SPEC><<<g, 256, 0, st>>>(L->jobs);
+        else k_loopfilter<CVP9_ARITH_REFCPU><<<g, 256, 0, st>>>(L->jobs);
+    }
+    if (L->flat_lf_max_w > 0) {
+        long long nh = (long long)((L->flat_lf_max_h + 7) / 8) * L->flat_lf_max_w;
+        long long nv = (long long)((L->flat_lf_max_w + 7) / 8) * L->flat_lf_max_h;
+        int refcpu = L->arith == CVP9_ARITH_REFCPU;
+        k_lf_flat_h<<<dim3((unsigned)((nh + 255) / 256), (unsigned)L->njobs), 256, 0, st>>>(L->jobs, refcpu);
+        k_lf_flat_v<<<dim3((unsigned)((nv + 255) / 256), (unsigned)L->njobs), 256, 0, st>>>(L->jobs, refcpu);
+        if (L->flat_nv12) {
+            long long n = (long long)L->flat_lf_max_w * L->flat_lf_max_h;
+            k_nv12_pack<<<dim3((unsigned)((n + 255) / 256), (unsigned)L->njobs), 256, 0, st>>>(L->jobs);
+        }
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    return (int)mark(L->ev[3], st, capturing);
+}
+
+} /* extern "C" */

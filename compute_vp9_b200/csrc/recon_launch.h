@@ -1,0 +1,46 @@
+/*
+ * recon_launch.h — C-ABI launch shims exported by recon.cu (internal: the
+ * public entry points are in include/cuda_backend.h and include/cvp9_batch.h).
+ */
+#ifndef CVP9_RECON_LAUNCH_H
+#define CVP9_RECON_LAUNCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+#include "recon_job.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One batch step: J jobs (one frame each) through scan -> recon -> filter. */
+typedef struct {
+    const cvp9_job_t *jobs;        /* device array of njobs descriptors          */
+    int              njobs;
+    int              arith;        /* CVP9_ARITH_*                               */
+    int              max_blocks;   /* largest num_blocks over the jobs           */
+    int              scan_ctas;    /* >0: fixed scan grid (grid-stride), else from max_blocks */
+    const uint32_t  *tickets;      /* device: (job << 20 | sb) in SB-diagonal order */
+    uint32_t         n_tickets;
+    uint32_t        *ticket_counter;  /* device, zeroed before the launch        */
+    int              recon_ctas;   /* grid of the persistent recon kernel        */
+    int              lf_tiles_x, lf_tiles_y;   /* tiled filter grid (max over jobs) */
+    int              flat_lf_max_w, flat_lf_max_h; /* >0: run the frame-wide filter */
+    int              flat_nv12;
+    cudaEvent_t      ev[4];        /* optional: before scan, recon, filter; after */
+} cvp9k_launch_t;
+
+size_t cvp9k_recon_smem_bytes(void);
+int    cvp9k_upload_dct_basis(const double *basis, int count);
+int    cvp9k_configure(void);
+int    cvp9k_recon_ctas_per_sm(int arith);
+/* Enqueue the chain on `stream`; returns the cudaError_t of the first
+ * failing call (0 on success). */
+int    cvp9k_launch_frame(const cvp9k_launch_t *launch, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVP9_RECON_LAUNCH_H */

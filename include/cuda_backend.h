@@ -1,0 +1,88 @@
+/*
+ * cuda_backend.h — CUDA reconstruction backend for compute-vp9 (B200,
+ * sm_100a). Drop-in for the Vulkan backend: the eight entry points below
+ * have the signatures and return-code contract of
+ * src/backend/vulkan/vulkan_backend.h:141-163 and are called from the same
+ * places in src/decoder/vp9_decoder.c (init 110-119, decode 203-207 and
+ * 448-452, get 256-259, dmabuf 286-293, export 295-317, render target
+ * 319-325, destroy 131-134). INTEGRATION.md shows the patch.
+ *
+ * Contract (mirrors the Vulkan backend):
+ *  - cuda_decode_frame copies everything it needs out of *pf before it
+ *    returns (the caller reuses the parsed frame), enqueues the frame and
+ *    returns CVP9_OK; CVP9_ERR_AGAIN when all CVP9_CUDA_INFLIGHT slots hold
+ *    undelivered frames.
+ *  - cuda_get_frame(wait=0) returns CVP9_ERR_AGAIN while the oldest frame is
+ *    still on the GPU unless every slot is busy, in which case it blocks;
+ *    wait=1 always blocks. CVP9_ERR_UNSUPPORTED when nothing is queued.
+ *    Frames come back in submission order. Plane pointers point into
+ *    backend-owned pinned memory and stay valid until that slot is reused,
+ *    i.e. for at least the next CVP9_CUDA_INFLIGHT-1 decodes.
+ *  - Errors found on the device (invalid block layout, an expired bounded
+ *    wait) are reported by the cuda_get_frame call that delivers the frame:
+ *    CVP9_ERR_INVALID_DATA or CVP9_ERR_GPU.
+ *  - cuda_get_frame_dmabuf returns CVP9_ERR_UNSUPPORTED (no DMA-BUF export
+ *    on a headless compute box). cuda_export_buffer_alloc returns a
+ *    host-mapped pinned buffer (fd = -1, mapped = host pointer) that the GPU
+ *    writes directly; cuda_set_render_target arms it as the one-shot NV12
+ *    target of the next decode.
+ *
+ * Arithmetic: CVP9_CUDA_ARITH_REFCPU (default) reproduces the library's CPU
+ * reconstruction (src/decoder/vp9_reconstruct.c) and reference-pool rules
+ * (src/decoder/vp9_decoder.c:224-231) bit for bit; CVP9_CUDA_ARITH_SPEC runs
+ * the shader arithmetic (integer butterflies with dequantisation, 8-tap MC
+ * on all planes, shader intra rules) with the Vulkan pool rules
+ * (refresh_frame_flags, ref_frame_idx). The environment variable
+ * CVP9_ARITH=refcpu|spec picks the profile for cuda_backend_init;
+ * CVP9_CUDA_DEVICE picks the GPU.
+ */
+#ifndef CVP9_CUDA_BACKEND_H
+#define CVP9_CUDA_BACKEND_H
+
+#include "cvp9_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CVP9_CUDA_INFLIGHT 3
+
+typedef enum {
+    CVP9_CUDA_ARITH_REFCPU = 0,
+    CVP9_CUDA_ARITH_SPEC   = 1,
+} cvp9_cuda_arith_t;
+
+typedef struct {
+    int device;     /* CUDA ordinal; -1: $CVP9_CUDA_DEVICE or 0        */
+    int arith;      /* cvp9_cuda_arith_t; -1: $CVP9_ARITH or REFCPU     */
+} cuda_backend_options_t;
+
+/* ── Drop-in entry points (vulkan_backend.h:141-163) ────────────────────── */
+
+cvp9_err_t cuda_backend_init(void **ctx);
+void       cuda_backend_destroy(void *ctx);
+cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pts);
+cvp9_err_t cuda_get_frame(void *ctx, cvp9_frame_info_t *info, int wait);
+cvp9_err_t cuda_get_frame_dmabuf(void *ctx, cvp9_dmabuf_frame_t *out);
+cvp9_err_t cuda_export_buffer_alloc(void *ctx, uint64_t size, cvp9_export_buffer_t *out);
+void       cuda_export_buffer_free(void *ctx, cvp9_export_buffer_t *buf);
+cvp9_err_t cuda_set_render_target(void *ctx, const cvp9_export_buffer_t *target);
+
+/* ── Additions beside the drop-in set ───────────────────────────────────── */
+
+/* init with explicit options (NULL = defaults above) */
+cvp9_err_t cuda_backend_init_ex(void **ctx, const cuda_backend_options_t *opt);
+
+/* Device timing of the most recently delivered frame: milliseconds from the
+ * start of its input upload to the end of its output copy, and of the GPU
+ * kernels alone. */
+cvp9_err_t cuda_backend_last_timing(void *ctx, float *total_ms, float *kernels_ms);
+
+/* Text of the last CUDA error seen by this context ("" if none). */
+const char *cuda_backend_last_error(void *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVP9_CUDA_BACKEND_H */

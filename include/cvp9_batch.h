@@ -1,0 +1,116 @@
+/*
+ * cvp9_batch.h — multi-stream reconstruction engine (added beside the
+ * drop-in backend; no counterpart in the reference, which decodes one
+ * stream per context, src/decoder/vp9_decoder.c:21-46).
+ *
+ * One step reconstructs one frame of each listed stream through a single
+ * launch chain (block scan, SB-diagonal wavefront recon across all streams,
+ * loop filter + NV12), optionally replayed from a CUDA graph per shape
+ * bucket. Every stream keeps its reference pool on the device. Streams are
+ * admitted against an HBM budget. The arithmetic per stream is exactly the
+ * per-stream backend's (include/cuda_backend.h): a frame decodes to the same
+ * bytes alone or inside any batch.
+ *
+ * Lifetime rules:
+ *  - host inputs: parsed frames are read during cvp9_batch_submit; arrays in
+ *    page-locked memory (cudaHostAlloc / cudaHostRegister) are DMA'd directly
+ *    and must stay unchanged until the step completes (cvp9_batch_wait or
+ *    cvp9_batch_poll returning 1); other arrays are copied before submit
+ *    returns.
+ *  - CVP9_BATCH_DEVICE_INPUTS: pf->blocks and pf->coeffs are device pointers
+ *    on the engine's GPU, read by the step's kernels.
+ *  - outputs: cvp9_batch_get_frame returns pinned host planes of the
+ *    stream's most recent completed frame, valid until that stream's second
+ *    next step completes. With CVP9_BATCH_NO_OUTPUT the frame stays on the
+ *    device only (it still becomes the stream's reference).
+ */
+#ifndef CVP9_BATCH_H
+#define CVP9_BATCH_H
+
+#include "cvp9_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cvp9_batch cvp9_batch_t;
+
+typedef struct {
+    int      device;         /* CUDA ordinal; -1: $CVP9_CUDA_DEVICE or 0         */
+    int      arith;          /* 0 REFCPU, 1 SPEC; -1: $CVP9_ARITH or REFCPU       */
+    uint64_t hbm_budget;     /* bytes of stream state to admit; 0: 150 GB         */
+    int      max_streams;    /* 0: 1024                                          */
+    int      use_graphs;     /* replay the kernel chain from per-bucket graphs    */
+} cvp9_batch_config_t;
+
+enum {
+    CVP9_BATCH_DEVICE_INPUTS = 1u << 0,
+    CVP9_BATCH_NO_OUTPUT     = 1u << 1,
+};
+
+typedef struct {
+    float    step_ms;        /* device time of the last completed step          */
+    float    kernels_ms;     /* its scan + recon + filter kernels                */
+    float    h2d_ms;         /* its input upload                                 */
+    uint64_t h2d_bytes;      /* bytes uploaded by that step                      */
+    uint64_t d2h_bytes;      /* bytes downloaded by that step                    */
+    uint64_t reserved_bytes; /* HBM reserved by the open streams                 */
+    int      open_streams;
+    int      graph_replays;  /* steps launched from a cached graph (cumulative)  */
+    uint32_t kernel_launches;/* kernels launched by that step                    */
+    float    scan_ms;        /* per-kernel device times of that step             */
+    float    recon_ms;
+    float    filter_ms;
+} cvp9_batch_stats_t;
+
+cvp9_err_t  cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out);
+void        cvp9_batch_destroy(cvp9_batch_t *b);
+
+/* HBM the engine reserves for one stream of this size (admission unit). */
+uint64_t    cvp9_batch_stream_bytes(uint32_t width, uint32_t height);
+
+/* Admit a stream: returns its id (>= 0), or CVP9_ERR_NOMEM when the HBM
+ * budget or the stream limit would be exceeded (retry after a close). */
+int         cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t width, uint32_t height);
+cvp9_err_t  cvp9_batch_close_stream(cvp9_batch_t *b, int sid);
+
+/* Enqueue one step: frame pfs[i] for stream sids[i] (each stream at most
+ * once). Returns once inputs are staged; up to two steps are in flight. */
+cvp9_err_t  cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
+                              const vp9_parsed_frame_t *const *pfs, const int64_t *pts,
+                              uint32_t flags);
+
+/* Block (bounded) until every submitted step is complete. Returns the first
+ * per-stream error of those steps (CVP9_ERR_INVALID_DATA for a rejected
+ * block layout, CVP9_ERR_GPU for an expired device wait), else CVP9_OK. */
+cvp9_err_t  cvp9_batch_wait(cvp9_batch_t *b);
+
+/* 1 if every submitted step is complete, 0 if not, <0 on error. */
+int         cvp9_batch_poll(cvp9_batch_t *b);
+
+/* Latest completed frame of a stream (CVP9_ERR_AGAIN if its last step is
+ * still running, CVP9_ERR_UNSUPPORTED if it has none on the host). */
+cvp9_err_t  cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *info);
+
+cvp9_err_t  cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *st);
+
+/* Device timer over whole steps: start records an event ahead of the next
+ * step's upload; stop records one after the last submitted step's download,
+ * waits for it (bounded) and returns the elapsed device milliseconds. */
+cvp9_err_t  cvp9_batch_timer_start(cvp9_batch_t *b);
+cvp9_err_t  cvp9_batch_timer_stop(cvp9_batch_t *b, float *ms);
+const char *cvp9_batch_last_error(cvp9_batch_t *b);
+
+/* Sequence number of the most recently submitted step (steps count from 1). */
+uint64_t    cvp9_batch_last_seq(cvp9_batch_t *b);
+
+/* Host-clock latency of step `seq`: from cvp9_batch_submit to its outputs
+ * landing in host memory (CVP9_ERR_AGAIN while it runs; the most recent
+ * 4096 steps are kept). */
+cvp9_err_t  cvp9_batch_step_latency(cvp9_batch_t *b, uint64_t seq, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVP9_BATCH_H */

@@ -1,0 +1,154 @@
+"""ctypes wrapper of the CPU checkers. TEST INFRASTRUCTURE ONLY: imported by
+tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, never by the
+product package.
+
+    OracleStream(profile)   the restatement in oracle/*.c (REFCPU or SPEC)
+    RefStream()             the reference's own vp9_reconstruct_frame compiled
+                            from its sources (oracle/_ref), REFCPU only
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libvp9ref.so")
+
+REFCPU = 0
+SPEC = 1
+
+_orc = None
+_ref = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def oracle_lib():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_LIB):
+            build()
+        from compute_vp9_b200.cvp9_ctypes import ParsedFrame
+        lib = C.CDLL(ORACLE_LIB)
+        lib.oracle_stream_create.argtypes = [C.c_int]
+        lib.oracle_stream_create.restype = C.c_void_p
+        lib.oracle_stream_destroy.argtypes = [C.c_void_p]
+        lib.oracle_stream_destroy.restype = None
+        lib.oracle_stream_decode.argtypes = [C.c_void_p, C.POINTER(ParsedFrame), C.c_void_p]
+        lib.oracle_refcpu_idct2d.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        lib.oracle_refcpu_idct2d.restype = None
+        lib.oracle_spec_idct2d.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+        lib.oracle_spec_idct2d.restype = None
+        lib.oracle_loopfilter.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_int, C.c_int, C.c_int]
+        lib.oracle_loopfilter.restype = None
+        lib.oracle_nv12_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]
+        lib.oracle_nv12_pack.restype = None
+        lib.oracle_dc_quant.argtypes = [C.c_int]
+        lib.oracle_ac_quant.argtypes = [C.c_int]
+        _orc = lib
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError("oracle/_ref not built (needs the reference sources)")
+        from compute_vp9_b200.cvp9_ctypes import ParsedFrame
+        lib = C.CDLL(REF_LIB)
+        lib.ref_stream_create.restype = C.c_void_p
+        lib.ref_stream_destroy.argtypes = [C.c_void_p]
+        lib.ref_stream_destroy.restype = None
+        lib.ref_stream_decode.argtypes = [C.c_void_p, C.POINTER(ParsedFrame), C.c_void_p]
+        lib.ref_layout.argtypes = [C.c_void_p, C.c_int]
+        _ref = lib
+    return _ref
+
+
+def _i420_size(w, h):
+    return w * h + 2 * ((w + 1) // 2) * ((h + 1) // 2)
+
+
+class OracleStream:
+    """Restated reconstruction + reference pool for one stream."""
+
+    def __init__(self, profile=REFCPU):
+        self._lib = oracle_lib()
+        self._h = self._lib.oracle_stream_create(profile)
+
+    def decode(self, pf):
+        w, h = pf.contents.hdr.width, pf.contents.hdr.height
+        out = np.empty(_i420_size(w, h), np.uint8)
+        if not self._lib.oracle_stream_decode(self._h, pf, out.ctypes.data):
+            raise RuntimeError("oracle decode failed")
+        return out
+
+    def close(self):
+        if self._h:
+            self._lib.oracle_stream_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class RefStream:
+    """The reference's compiled CPU reconstruction + its pool rules."""
+
+    def __init__(self):
+        self._lib = ref_lib()
+        self._h = self._lib.ref_stream_create()
+
+    def decode(self, pf):
+        w, h = pf.contents.hdr.width, pf.contents.hdr.height
+        out = np.empty(_i420_size(w, h), np.uint8)
+        if not self._lib.ref_stream_decode(self._h, pf, out.ctypes.data):
+            raise RuntimeError("reference decode failed")
+        return out
+
+    def close(self):
+        if self._h:
+            self._lib.ref_stream_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def refcpu_idct2d(coeffs):
+    n = coeffs.shape[0]
+    x = np.ascontiguousarray(coeffs, np.int16)
+    out = np.empty((n, n), np.int16)
+    oracle_lib().oracle_refcpu_idct2d(x.ctypes.data, out.ctypes.data, n)
+    return out
+
+
+def spec_idct2d(coeffs, q_dc, q_ac):
+    n = coeffs.shape[0]
+    x = np.ascontiguousarray(coeffs, np.int16)
+    out = np.empty((n, n), np.int32)
+    oracle_lib().oracle_spec_idct2d(x.ctypes.data, out.ctypes.data, n, q_dc, q_ac)
+    return out
+
+
+def loopfilter(plane, level, sharpness, profile):
+    p = np.ascontiguousarray(plane, np.uint8).copy()
+    h, w = p.shape
+    oracle_lib().oracle_loopfilter(p.ctypes.data, w, h, w, level, sharpness, profile)
+    return p
+
+
+def nv12_pack(i420, w, h):
+    src = np.ascontiguousarray(i420, np.uint8)
+    dst = np.empty(_i420_size(w, h), np.uint8)
+    oracle_lib().oracle_nv12_pack(src.ctypes.data, dst.ctypes.data, w, h)
+    return dst

@@ -1,0 +1,105 @@
+"""Multi-stream engine: every stream of a mixed-resolution batch decodes to the
+oracle's bytes, and the same frames decode identically alone and in the mix
+(with and without graph replay, with host and device-resident inputs)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from compute_vp9_b200 import CVP9_OK, Synth, synth_config
+from compute_vp9_b200.batch import DEVICE_INPUTS, Batch
+from oracle.oracle_py import REFCPU, SPEC, OracleStream
+
+pytestmark = pytest.mark.gpu
+
+MIX = [
+    (1, 320, 192, {}),
+    (2, 352, 288, {"gop": 3}),
+    (2, 200, 120, {"gop": 2, "min_bsize": 4, "skip_prob": 0.2, "intra_in_inter": 0.3}),
+    (1, 257, 129, {"intra_in_inter": 0.1}),
+    (2, 640, 360, {"gop": 4, "log2_tile_cols": 1}),
+]
+
+
+def decode_mix(profile, streams, frames, graphs=1, order=None, seeds=None):
+    eng = Batch(arith=profile, use_graphs=graphs)
+    seeds = seeds or [10 + i for i in range(len(streams))]
+    syns = [Synth(synth_config(p, w, h, seed=seeds[i], **ov)) for i, (p, w, h, ov) in enumerate(streams)]
+    sids = [eng.open_stream(w, h) for (_, w, h, _) in streams]
+    assert all(s is not None for s in sids)
+    outs = [[] for _ in streams]
+    for f in range(frames):
+        idx = order(f) if order else list(range(len(streams)))
+        eng.submit([sids[i] for i in idx], [syns[i].frame(f) for i in idx], [f] * len(idx))
+        assert eng.wait() == CVP9_OK, eng.last_error()
+        for i in idx:
+            rc, arr = eng.get_frame_array(sids[i])
+            assert rc == CVP9_OK, (rc, eng.last_error())
+            outs[i].append(arr)
+    eng.close()
+    return outs
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_batch_matches_oracle(profile):
+    outs = decode_mix(profile, MIX, 4)
+    for i, (p, w, h, ov) in enumerate(MIX):
+        syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
+        orc = OracleStream(profile)
+        for f in range(4):
+            want = orc.decode(syn.frame(f))
+            assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_alone_equals_in_mix(profile):
+    mixed = decode_mix(profile, MIX, 3, graphs=1)
+    for i in range(len(MIX)):
+        alone = decode_mix(profile, [MIX[i]], 3, graphs=0, seeds=[10 + i])
+        for f in range(3):
+            assert np.array_equal(alone[0][f], mixed[i][f]), "stream %d frame %d" % (i, f)
+
+
+def test_device_inputs_and_pipelining():
+    """Two steps in flight, parsed frames already on the device."""
+    import torch
+    p, w, h, ov = 1, 256, 192, {}
+    syn = Synth(synth_config(p, w, h, seed=5, **ov))
+    from compute_vp9_b200 import ParsedFrame, BlockInfo
+    keep = []
+    pfs = []
+    for f in range(5):
+        src = syn.frame(f).contents
+        nb, nc = src.num_blocks, src.num_coeffs
+        bt = torch.from_numpy(np.ctypeslib.as_array(C.cast(src.blocks, C.POINTER(C.c_uint8)),
+                                                    shape=(nb * 32,)).copy()).cuda()
+        ct = torch.from_numpy(np.ctypeslib.as_array(src.coeffs, shape=(nc,)).copy()).cuda()
+        d = ParsedFrame()
+        C.memmove(C.byref(d), C.byref(src), C.sizeof(ParsedFrame))
+        d.blocks = C.cast(C.c_void_p(bt.data_ptr()), C.POINTER(BlockInfo))
+        d.coeffs = C.cast(C.c_void_p(ct.data_ptr()), C.POINTER(C.c_int16))
+        keep += [bt, ct]
+        pfs.append(d)
+    torch.cuda.synchronize()
+    eng = Batch(arith=REFCPU)
+    sid = eng.open_stream(w, h)
+    for f in range(5):
+        eng.submit([sid], [C.pointer(pfs[f])], [f], DEVICE_INPUTS)
+    assert eng.wait() == CVP9_OK, eng.last_error()
+    rc, got = eng.get_frame_array(sid)
+    assert rc == CVP9_OK
+    orc = OracleStream(REFCPU)
+    syn2 = Synth(synth_config(p, w, h, seed=5, **ov))
+    for f in range(5):
+        want = orc.decode(syn2.frame(f))
+    assert np.array_equal(got, want)
+    eng.close()
+
+
+def test_admission_budget():
+    eng = Batch(arith=REFCPU, hbm_budget=3 * Batch(arith=REFCPU).stream_bytes(1920, 1080))
+    ids = [eng.open_stream(1920, 1080) for _ in range(4)]
+    assert ids[:3] == [0, 1, 2] and ids[3] is None
+    eng.close_stream(1)
+    assert eng.open_stream(1920, 1080) == 1
+    eng.close()
