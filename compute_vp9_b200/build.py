@@ -21,7 +21,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_C = ["backend_common.c", "cuda_backend.c", "batch.c"]
-CUDA_SRC = ["recon.cu"]
+CUDA_SRC = ["recon.cu", "recon_static.cu"]
 
 
 def _run(cmd):

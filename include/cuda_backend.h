@@ -81,6 +81,33 @@ cvp9_err_t cuda_backend_last_timing(void *ctx, float *total_ms, float *kernels_m
 /* Text of the last CUDA error seen by this context ("" if none). */
 const char *cuda_backend_last_error(void *ctx);
 
+/* ── Allocation-free reconstruction of one frame ────────────────────────── *
+ * No counterpart in the reference. For callers that must not allocate GPU
+ * memory while decoding — a media framework or inference server that owns
+ * all device memory through its own pools, or a real-time thread where
+ * cudaMalloc/cudaFree could stall on device-wide synchronisation. The caller
+ * owns every buffer: pf->blocks and pf->coeffs are DEVICE pointers,
+ * ref_planes[i] are device I420 frames (NULL = empty slot) of size
+ * ref_width[i] x ref_height[i], out_i420 receives the frame
+ * (W*H + 2*ceil(W/2)*ceil(H/2) bytes), status_dev (optional, device) receives
+ * the CVP9_JOB_* status word. Work is enqueued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream); nothing is allocated or freed.
+ * The kernels' scratch is a fixed ~200 KB __device__ array in the library:
+ *  - frames above CVP9_NOALLOC_MAX_SB superblocks (7680x4320) are rejected
+ *    with CVP9_ERR_INVALID_DATA and a message on stderr;
+ *  - every GPU the library is used on keeps that array until process exit;
+ *  - all calls share it, so calls that overlap on the GPU race: serialise
+ *    them on one stream;
+ *  - the first call on a device performs that device's one-time set-up,
+ *    so make it before any stream capture. */
+#define CVP9_NOALLOC_MAX_SB 8160
+cvp9_err_t cuda_reconstruct_noalloc(const vp9_parsed_frame_t *pf,
+                                    const uint8_t *const ref_planes[8],
+                                    const uint32_t ref_width[8],
+                                    const uint32_t ref_height[8],
+                                    uint8_t *out_i420, int arith,
+                                    uint32_t *status_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
