@@ -62,7 +62,9 @@ def step_frame(t):
 
 # ── distributed plumbing ─────────────────────────────────────────────────────
 
-def dist_setup():
+def dist_setup(backend=None):
+    """One process per GPU (torchrun env). NCCL when CUDA is present, gloo
+    otherwise; used only for barriers and the max-over-ranks of the timings."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -70,8 +72,11 @@ def dist_setup():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
@@ -86,9 +91,15 @@ def allreduce_max(ws, v):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(v)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_seeds(rank, streams):
+    """Stream seeds of a rank: ranks decode disjoint sets of streams."""
+    return list(range(rank * streams, (rank + 1) * streams))
 
 
 # ── workload ─────────────────────────────────────────────────────────────────
@@ -98,7 +109,7 @@ class Workload:
     optional device copy. pfs_host[s][f] / pfs_dev[s][f] are ParsedFrame
     structs whose arrays live in those arenas."""
 
-    def __init__(self, streams, w, h, device_copy=True):
+    def __init__(self, streams, w, h, device_copy=True, seeds=None):
         import numpy as np
         import torch
         from compute_vp9_b200 import ParsedFrame, Synth, synth_config
@@ -106,8 +117,9 @@ class Workload:
         t0 = time.time()
         # pass 1: generate and measure
         frames = []
+        seeds = seeds if seeds is not None else list(range(streams))
         for s in range(streams):
-            syn = Synth(synth_config(1, w, h, seed=s))
+            syn = Synth(synth_config(1, w, h, seed=seeds[s]))
             per = []
             for f in range(DISTINCT):
                 pf = syn.frame(f).contents
@@ -379,7 +391,7 @@ def read_peaks():
 
 def read_traffic():
     """Per-launch DRAM bytes of the recon kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_recon_refcpu_1080p_x64.md")
+    p = os.path.join(ROOT, "profiles", "k_recon_refcpu_1080p_x32.md")
     try:
         with open(p) as f:
             for line in f:
@@ -457,7 +469,8 @@ def main():
     os.environ.setdefault("CVP9_CUDA_DEVICE", str(local))
     from compute_vp9_b200 import ARITH_REFCPU, ARITH_SPEC
     arith = ARITH_SPEC if args.arith == "spec" else ARITH_REFCPU
-    wl = Workload(args.streams, args.width, args.height, device_copy=True)
+    wl = Workload(args.streams, args.width, args.height, device_copy=True,
+                  seeds=rank_seeds(rank, args.streams))
     px_step = wl.S * wl.w * wl.h
 
     clocks = ClockSampler(int(os.environ.get("CVP9_NVSMI_INDEX", str(local))))

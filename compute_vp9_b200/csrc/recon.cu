@@ -44,11 +44,15 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxBlocks = 256;      /* 4x4 cells in a 64x64 SB */
+constexpr int kMaxBlocks = 128;      /* blocks per SB (the tile parser emits at most 64) */
+constexpr int kCoefStage = 6144;     /* int16 coefficients staged per SB (64x64 luma + chroma) */
+constexpr int kMaxItems = 1536;      /* TX columns per SB: 4x4 TXs on all three planes */
 constexpr int kYPitch = 72;          /* luma tile row pitch; x = 0 at byte 4 */
 constexpr int kCPitch = 40;          /* chroma tile row pitch; x = 0 at byte 4 */
 constexpr int kTempPitch = 65;       /* doubles per REFCPU temp row */
 constexpr int kStagePerWarp = 768;   /* bytes of MC staging per warp */
+constexpr int kTyBytes = (65 * kYPitch + 15) / 16 * 16;
+constexpr int kTcBytes = (33 * kCPitch + 15) / 16 * 16;
 constexpr long long kSpinLimit = 1ll << 20;   /* ~0.25 s of polling */
 
 __constant__ double c_dct[16 + 64 + 256 + 1024];      /* N = 4, 8, 16, 32 */
@@ -60,6 +64,17 @@ __device__ __forceinline__ const double *dct_basis(int txl)
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* ── Asynchronous global -> shared copies (16 bytes, both sides aligned) ── */
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 
 /* ── 32-bit wrap-around integer for the shader butterflies ───────────────── */
 struct wi {
@@ -267,9 +282,12 @@ struct ReconSmem {
         double  d[64 * kTempPitch];              /* REFCPU first-pass output    */
         int32_t i[64 * 64 + 2 * 32 * 32];        /* SPEC column-pass output     */
     } temp;
-    uint8_t  ty[65 * kYPitch];                   /* luma tile, row 0 = halo     */
-    uint8_t  tu[33 * kCPitch];
-    uint8_t  tv[33 * kCPitch];
+    /* tiles, contiguous and 16-byte sized so they fill with vector stores */
+    uint8_t  ty[kTyBytes];                       /* luma tile, row 0 = halo     */
+    uint8_t  tu[kTcBytes];
+    uint8_t  tv[kTcBytes];
+    int16_t  coef[kCoefStage];                   /* the SB's coefficient span   */
+    cvp9_job_t jc;                               /* this ticket's job           */
     BlkS     blk[kMaxBlocks];
     unsigned long long lvl_cnt[kMaxBlocks + 1];
     uint32_t txmask[256 + 64 + 64];              /* per-TX column-nonzero bits  */
@@ -281,7 +299,11 @@ struct ReconSmem {
     uint16_t base_blk[kMaxBlocks + 1];
     uint16_t base_chunk[kMaxBlocks + 1];
     uint16_t base_item[kMaxBlocks + 1];
-    uint8_t  stage[kWarps][kStagePerWarp];
+    uint8_t  chunk_blk[256];                     /* chunk -> block position     */
+    uint8_t  item_blk[kMaxItems];                /* TX column/row -> position   */
+    alignas(16) uint8_t stage[kWarps][kStagePerWarp];
+    int      scan_tmp[2 * kWarps];
+    unsigned c_lo, c_hi;                         /* coefficient span of the SB  */
     int      ticket;
     int      nlev;
     int      nb;
@@ -448,76 +470,157 @@ __device__ __forceinline__ void stage_window(uint8_t *st, int sp, const uint8_t 
                                              int sw, int sh, int lane)
 {
     int xm = pw > 0 ? pw - 1 : 0, ym = ph > 0 ? ph - 1 : 0;
-    for (int i = lane; i < sw * sh; i += 32) {
-        int sy = i / sw, sx = i - sy * sw;
-        int yy = clampi(y0 + sy, 0, ym), xx = clampi(x0 + sx, 0, xm);
+    const int sx = lane & 15;                 /* windows are at most 16 wide */
+    if (sx >= sw) return;
+    const int xx = clampi(x0 + sx, 0, xm);
+    for (int sy = lane >> 4; sy < sh; sy += 2) {
+        int yy = clampi(y0 + sy, 0, ym);
         st[sy * sp + sx] = __ldg(plane + (size_t)yy * stride + xx);
     }
 }
 
-/* REFCPU bilinear of one region from a staged (w+1) x (h+1) window. */
-__device__ __forceinline__ int bilin(const uint8_t *st, int sp, int r, int c, int fx, int fy)
+/* Geometry of one chunk's REFCPU bilinear prediction: integer positions and
+ * fractions of the luma and chroma windows (vp9_reconstruct.c:94-131,
+ * :313-327) and whether each window can be staged with aligned 16-byte
+ * copies (inside its plane, rows 16-byte aligned). */
+struct McGeo {
+    const uint8_t *rp, *ru, *rv;
+    int rw, rh, rcs;
+    int ix, iy, fx, fy, cix, ciy, cfx, cfy, la, ca;
+    bool lfast, cfast;
+};
+
+__device__ __forceinline__ bool refcpu_geo(const ReconSmem &s, const BlkS &b, int sbx, int sby,
+                                           int lx0, int ly0, int lw, int lh, int cx0, int cy0,
+                                           int clw, int clh, McGeo &g)
 {
-    unsigned a = st[r * sp + c], b = st[r * sp + c + 1];
-    unsigned d = st[(r + 1) * sp + c], e = st[(r + 1) * sp + c + 1];
-    unsigned top = (a * (8 - fx) + b * fx + 4) >> 3;
-    unsigned bot = (d * (8 - fx) + e * fx + 4) >> 3;
-    return (int)((top * (8 - fy) + bot * fy + 4) >> 3);
+    const int slot = (int)b.ref0 - 1;
+    if (slot < 0 || slot >= 8 || !s.jc.ref[slot].plane) return false;
+    const cvp9_ref_t &R = s.jc.ref[slot];
+    g.rp = R.plane;
+    g.rw = R.w;
+    g.rh = R.h;
+    g.rcs = (g.rw + 1) >> 1;
+    g.ru = g.rp + (size_t)g.rw * g.rh;
+    g.rv = g.ru + (size_t)g.rcs * ((g.rh + 1) >> 1);
+    const int px8 = (sbx + lx0) * 8 + b.mvx, py8 = (sby + ly0) * 8 + b.mvy;
+    g.ix = px8 >> 3; g.iy = py8 >> 3; g.fx = px8 & 7; g.fy = py8 & 7;
+    const int cmx = b.mvx / 2, cmy = b.mvy / 2;            /* halves toward zero */
+    const int cpx8 = ((sbx >> 1) + cx0) * 8 + cmx, cpy8 = ((sby >> 1) + cy0) * 8 + cmy;
+    g.cix = cpx8 >> 3; g.ciy = cpy8 >> 3; g.cfx = cpx8 & 7; g.cfy = cpy8 & 7;
+    const int crw = g.rw >> 1, crh = g.rh >> 1;            /* floor half of the ref size */
+    const bool aligned = !(g.rw & 15) && !(g.rcs & 15) && !((uintptr_t)g.rp & 15) &&
+                         !((uintptr_t)g.ru & 15) && !((uintptr_t)g.rv & 15);
+    g.lfast = aligned && g.ix >= 0 && g.iy >= 0 && g.ix + lw < g.rw && g.iy + lh < g.rh;
+    g.cfast = aligned && g.cix >= 0 && g.ciy >= 0 && g.cix + clw < crw && g.ciy + clh < crh;
+    g.la = g.ix & ~15;
+    g.ca = g.cix & ~15;
+    return true;
 }
 
-template <int A>
-__device__ void predict_inter_chunk(ReconSmem &s, const cvp9_job_t &job, const BlkS &b,
-                                    int sbx, int sby, int lx0, int ly0, int lw, int lh,
-                                    int cx0, int cy0, int clw, int clh, int warp, int lane)
+/* Stage layout of one chunk (608 bytes): luma rows at 32-byte pitch, then U
+ * and V rows. Rows needing bytes past the first 16 take a second copy. */
+constexpr int kChunkStage = 608;
+
+__device__ __forceinline__ void refcpu_issue(uint8_t *st, const McGeo &g, int lw, int lh,
+                                             int clw, int clh, int lane)
 {
-    const cvp9_ref_t *R;
-    if (A == CVP9_ARITH_REFCPU) {
-        int slot = (int)b.ref0 - 1;
-        R = (slot >= 0 && slot < 8) ? &job.ref[slot] : nullptr;
-    } else {
-        int sel = clampi((int)b.ref0 - 1, 0, 2);
-        R = &job.ref[job.ref_slot_of[sel] & 7];
+    if (g.lfast) {
+        const int row = lane >> 1, half = lane & 1;
+        if (row <= lh && (half == 0 || (g.ix - g.la) + lw >= 16))
+            cp_async16(st + row * 32 + half * 16, g.rp + (size_t)(g.iy + row) * g.rw + g.la + half * 16);
     }
-    const uint8_t *rp = R ? R->plane : nullptr;
-    if (!rp) {
-        const int fill = A == CVP9_ARITH_REFCPU ? 127 : 128;
-        for (int idx = lane; idx < 64; idx += 32) {
-            int r = idx >> 3, c = idx & 7;
-            if (r < lh && c < lw) TY(s, lx0 + c, ly0 + r) = (uint8_t)fill;
+    if (g.cfast) {
+        const int pl = lane >> 4, row = (lane & 15) >> 1, half = lane & 1;
+        if (row <= clh && (half == 0 || (g.cix - g.ca) + clw >= 16))
+            cp_async16(st + 288 + pl * 160 + row * 32 + half * 16,
+                       (pl ? g.rv : g.ru) + (size_t)(g.ciy + row) * g.rcs + g.ca + half * 16);
+    }
+}
+
+/* Bilinear with a per-sample clamp into the reference (vp9_reconstruct.c:
+ * 105-128): from the staged window on the fast path, else from clamped
+ * byte reads. */
+__device__ __forceinline__ void refcpu_compute(ReconSmem &s, const uint8_t *st, const McGeo &g,
+                                               int lx0, int ly0, int lw, int lh,
+                                               int cx0, int cy0, int clw, int clh, int lane)
+{
+    {
+        const int r = lane >> 2, c = (lane & 3) * 2;
+        if (r < lh && c < lw) {
+            unsigned a0, a1, a2, b0, b1, b2;
+            if (g.lfast) {
+                const uint8_t *s0 = st + r * 32 + (g.ix - g.la) + c, *s1 = s0 + 32;
+                a0 = s0[0]; a1 = s0[1]; a2 = s0[2];
+                b0 = s1[0]; b1 = s1[1]; b2 = s1[2];
+            } else {
+                int y0 = clampi(g.iy + r, 0, g.rh - 1), y1 = clampi(g.iy + r + 1, 0, g.rh - 1);
+                int xa = clampi(g.ix + c, 0, g.rw - 1), xb = clampi(g.ix + c + 1, 0, g.rw - 1);
+                int xc = clampi(g.ix + c + 2, 0, g.rw - 1);
+                const uint8_t *r0 = g.rp + (size_t)y0 * g.rw, *r1 = g.rp + (size_t)y1 * g.rw;
+                a0 = __ldg(r0 + xa); a1 = __ldg(r0 + xb); a2 = __ldg(r0 + xc);
+                b0 = __ldg(r1 + xa); b1 = __ldg(r1 + xb); b2 = __ldg(r1 + xc);
+            }
+            const unsigned wx = 8 - g.fx, wy = 8 - g.fy;
+            unsigned t0 = (a0 * wx + a1 * g.fx + 4) >> 3, u0 = (b0 * wx + b1 * g.fx + 4) >> 3;
+            TY(s, lx0 + c, ly0 + r) = (uint8_t)((t0 * wy + u0 * g.fy + 4) >> 3);
+            if (c + 1 < lw) {
+                unsigned t1 = (a1 * wx + a2 * g.fx + 4) >> 3, u1 = (b1 * wx + b2 * g.fx + 4) >> 3;
+                TY(s, lx0 + c + 1, ly0 + r) = (uint8_t)((t1 * wy + u1 * g.fy + 4) >> 3);
+            }
         }
-        int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
-        if (r < clh && c < clw) TC(s, p, cx0 + c, cy0 + r) = (uint8_t)fill;
-        return;
     }
-    const int rw = R->w, rh = R->h;
-    const int rcs = (rw + 1) >> 1;                       /* chroma stride */
+    {
+        const int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
+        if (r < clh && c < clw) {
+            unsigned a0, a1, b0, b1;
+            if (g.cfast) {
+                const uint8_t *s0 = st + 288 + (p - 1) * 160 + r * 32 + (g.cix - g.ca) + c, *s1 = s0 + 32;
+                a0 = s0[0]; a1 = s0[1]; b0 = s1[0]; b1 = s1[1];
+            } else {
+                const int crw = g.rw >> 1, crh = g.rh >> 1;
+                int xm = crw > 0 ? crw - 1 : 0, ym = crh > 0 ? crh - 1 : 0;
+                const uint8_t *pl = p == 1 ? g.ru : g.rv;
+                int y0 = clampi(g.ciy + r, 0, ym), y1 = clampi(g.ciy + r + 1, 0, ym);
+                int xa = clampi(g.cix + c, 0, xm), xb = clampi(g.cix + c + 1, 0, xm);
+                a0 = __ldg(pl + (size_t)y0 * g.rcs + xa); a1 = __ldg(pl + (size_t)y0 * g.rcs + xb);
+                b0 = __ldg(pl + (size_t)y1 * g.rcs + xa); b1 = __ldg(pl + (size_t)y1 * g.rcs + xb);
+            }
+            unsigned t0 = (a0 * (8 - g.cfx) + a1 * g.cfx + 4) >> 3, u0 = (b0 * (8 - g.cfx) + b1 * g.cfx + 4) >> 3;
+            TC(s, p, cx0 + c, cy0 + r) = (uint8_t)((t0 * (8 - g.cfy) + u0 * g.cfy + 4) >> 3);
+        }
+    }
+}
+
+/* A reference that is absent predicts as a flat value (127 REFCPU, 128 SPEC). */
+__device__ __forceinline__ void fill_chunk(ReconSmem &s, int v, int lx0, int ly0, int lw, int lh,
+                                          int cx0, int cy0, int clw, int clh, int lane)
+{
+    for (int idx = lane; idx < 64; idx += 32) {
+        int r = idx >> 3, c = idx & 7;
+        if (r < lh && c < lw) TY(s, lx0 + c, ly0 + r) = (uint8_t)v;
+    }
+    int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
+    if (r < clh && c < clw) TC(s, p, cx0 + c, cy0 + r) = (uint8_t)v;
+}
+
+/* SPEC inter prediction of one chunk: regular 8-tap on luma (even phases of
+ * the 1/8-pel MV) and chroma (1/16 chroma pel), every fetch clamped into the
+ * reference plane, horizontal pass rounded and clipped to 8 bits before the
+ * vertical pass (vp9_mc.comp.glsl:61-110). */
+__device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
+                                 int lx0, int ly0, int lw, int lh,
+                                 int cx0, int cy0, int clw, int clh, int warp, int lane)
+{
+    const cvp9_ref_t &R = s.jc.ref[s.jc.ref_slot_of[clampi((int)b.ref0 - 1, 0, 2)] & 7];
+    const uint8_t *rp = R.plane;
+    if (!rp) { fill_chunk(s, 128, lx0, ly0, lw, lh, cx0, cy0, clw, clh, lane); return; }
+    const int rw = R.w, rh = R.h;
+    const int rcs = (rw + 1) >> 1;
     const uint8_t *ru = rp + (size_t)rw * rh;
     const uint8_t *rv = ru + (size_t)rcs * ((rh + 1) >> 1);
     uint8_t *st = s.stage[warp];
     const int mvx = b.mvx, mvy = b.mvy;
-
-    if (A == CVP9_ARITH_REFCPU) {
-        /* luma: 9x9 window, pitch 16 */
-        int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
-        int fx = px8 & 7, fy = py8 & 7;
-        stage_window(st, 16, rp, rw, rw, rh, px8 >> 3, py8 >> 3, lw + 1, lh + 1, lane);
-        /* chroma: MV halved toward zero, extent = floor half of the ref size */
-        int cmx = mvx / 2, cmy = mvy / 2;
-        int gcx = (sbx >> 1) + cx0, gcy = (sby >> 1) + cy0;
-        int cpx8 = gcx * 8 + cmx, cpy8 = gcy * 8 + cmy;
-        int cfx = cpx8 & 7, cfy = cpy8 & 7;
-        stage_window(st + 160, 8, ru, rcs, rw >> 1, rh >> 1, cpx8 >> 3, cpy8 >> 3, clw + 1, clh + 1, lane);
-        stage_window(st + 208, 8, rv, rcs, rw >> 1, rh >> 1, cpx8 >> 3, cpy8 >> 3, clw + 1, clh + 1, lane);
-        __syncwarp();
-        for (int idx = lane; idx < 64; idx += 32) {
-            int r = idx >> 3, c = idx & 7;
-            if (r < lh && c < lw) TY(s, lx0 + c, ly0 + r) = (uint8_t)bilin(st, 16, r, c, fx, fy);
-        }
-        int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
-        if (r < clh && c < clw)
-            TC(s, p, cx0 + c, cy0 + r) = (uint8_t)bilin(st + (p == 1 ? 160 : 208), 8, r, c, cfx, cfy);
-        __syncwarp();
-    } else {
         /* luma: (lw+7) x (lh+7) window at pitch 16; H pass into 15 x 8 */
         int bx = sbx + lx0 + (mvx >> 3), by = sby + ly0 + (mvy >> 3);
         int fx = (mvx & 7) << 1, fy = (mvy & 7) << 1;
@@ -585,7 +688,6 @@ __device__ void predict_inter_chunk(ReconSmem &s, const cvp9_job_t &job, const B
             }
         }
         __syncwarp();
-    }
 }
 
 /* ── Residual: one item = one TX column (pass 1) or one TX row (pass 2) ── */
@@ -629,23 +731,23 @@ __device__ __forceinline__ TxRef locate_item(const BlkS &b, int item, int *lane_
  * (vp9_reconstruct.c:31-40). Skipped zero terms add +-0 to a sum that is
  * never -0, so the result is bit-identical to the full sum. */
 template <int N>
-__device__ __forceinline__ void refcpu_col(ReconSmem &s, const int16_t *__restrict__ X, int j,
+__device__ __forceinline__ void refcpu_col(ReconSmem &s, const int16_t *X, int j,
                                            int px0, int py0, int mask_idx, const double *M)
 {
+    unsigned nzm = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) nzm |= (X[k * N + j] != 0 ? 1u : 0u) << k;
+    if (!nzm) return;
     double acc[N];
 #pragma unroll
     for (int i = 0; i < N; i++) acc[i] = 0.0;
-    bool any = false;
-#pragma unroll 1
-    for (int k = 0; k < N; k++) {
-        int x = __ldg(X + k * N + j);
-        if (x == 0) continue;
-        any = true;
-        double xd = (double)x;
+    while (nzm) {
+        const int k = __ffs(nzm) - 1;
+        nzm &= nzm - 1;
+        const double xd = (double)X[k * N + j];
 #pragma unroll
         for (int i = 0; i < N; i++) acc[i] = __dadd_rn(acc[i], __dmul_rn(M[k * N + i], xd));
     }
-    if (!any) return;
 #pragma unroll
     for (int i = 0; i < N; i++) s.temp.d[(py0 + i) * kTempPitch + px0 + j] = acc[i];
     atomicOr(&s.txmask[mask_idx], 1u << j);
@@ -660,9 +762,9 @@ __device__ __forceinline__ void refcpu_row(ReconSmem &s, int i, int px0, int py0
     double acc[N];
 #pragma unroll
     for (int j = 0; j < N; j++) acc[j] = 0.0;
-#pragma unroll 1
-    for (int k = 0; k < N; k++) {
-        if (!((mask >> k) & 1u)) continue;
+    while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1;
         double t = s.temp.d[(py0 + i) * kTempPitch + px0 + k];
 #pragma unroll
         for (int j = 0; j < N; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, M[k * N + j]));
@@ -694,14 +796,14 @@ __device__ __forceinline__ int32_t *spec_temp(ReconSmem &s, int plane, int x, in
 /* SPEC pass 1: dequantise column j (DC step at [0][0] only) and run the
  * 1-D transform down the column (vp9_idct.comp.glsl:666-679). */
 template <int N>
-__device__ __forceinline__ void spec_col(ReconSmem &s, const int16_t *__restrict__ X, int j,
+__device__ __forceinline__ void spec_col(ReconSmem &s, const int16_t *X, int j,
                                          const TxRef &t, int q_dc, int q_ac)
 {
     wi v[N];
     bool any = false;
 #pragma unroll
     for (int k = 0; k < N; k++) {
-        int c = __ldg(X + k * N + j);
+        int c = X[k * N + j];
         any |= c != 0;
         v[k] = wi(c) * ((k == 0 && j == 0) ? q_dc : q_ac);
     }
@@ -755,6 +857,113 @@ __device__ bool wait_flag(const unsigned *flag, unsigned epoch)
     return false;
 }
 
+__device__ __forceinline__ void pf_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
+
+/* Prefetch into L2 the rows of a reference window (clamped like the
+ * prediction reads) — first and last 128-byte line of each row. */
+__device__ __forceinline__ void pf_window(const uint8_t *plane, int stride, int pw, int ph,
+                                          int x0, int y0, int w, int h)
+{
+    int xm = pw > 0 ? pw - 1 : 0, ym = ph > 0 ? ph - 1 : 0;
+    int xa = clampi(x0, 0, xm), xb = clampi(x0 + w - 1, 0, xm);
+    for (int r = 0; r < h; r++) {
+        const uint8_t *row = plane + (size_t)clampi(y0 + r, 0, ym) * stride;
+        pf_l2(row + xa);
+        if ((xb >> 7) != (xa >> 7)) pf_l2(row + xb);
+    }
+}
+
+/* One thread per block, right after the descriptors are read: pull the
+ * block's reference windows towards L2 so the prediction phase finds them
+ * there. Addresses are clamped into the buffers exactly as the later reads
+ * are. */
+template <int A>
+__device__ void prefetch_block(const BlkS &b, const cvp9_job_t &job, int sbx, int sby)
+{
+    if (b.flags & 1) return;
+    const cvp9_ref_t *R;
+    if (A == CVP9_ARITH_REFCPU) {
+        int slot = (int)b.ref0 - 1;
+        R = (slot >= 0 && slot < 8) ? &job.ref[slot] : nullptr;
+    } else {
+        R = &job.ref[job.ref_slot_of[clampi((int)b.ref0 - 1, 0, 2)] & 7];
+    }
+    if (!R || !R->plane) return;
+    const int rw = R->w, rh = R->h, rcs = (rw + 1) >> 1;
+    const uint8_t *ru = R->plane + (size_t)rw * rh;
+    const uint8_t *rv = ru + (size_t)rcs * ((rh + 1) >> 1);
+    const int gx = sbx + b.x, gy = sby + b.y, cbw = (b.cw + 1) >> 1, cbh = (b.ch + 1) >> 1;
+    if (A == CVP9_ARITH_REFCPU) {
+        int px8 = gx * 8 + b.mvx, py8 = gy * 8 + b.mvy;
+        pf_window(R->plane, rw, rw, rh, px8 >> 3, py8 >> 3, b.cw + 1, b.ch + 1);
+        int cx8 = (gx >> 1) * 8 + b.mvx / 2, cy8 = (gy >> 1) * 8 + b.mvy / 2;
+        pf_window(ru, rcs, rw >> 1, rh >> 1, cx8 >> 3, cy8 >> 3, cbw + 1, cbh + 1);
+        pf_window(rv, rcs, rw >> 1, rh >> 1, cx8 >> 3, cy8 >> 3, cbw + 1, cbh + 1);
+    } else {
+        pf_window(R->plane, rw, rw, rh, gx + (b.mvx >> 3) - 3, gy + (b.mvy >> 3) - 3, b.cw + 7, b.ch + 7);
+        int cx = (gx >> 1) + (b.mvx >> 4) - 3, cy = (gy >> 1) + (b.mvy >> 4) - 3;
+        pf_window(ru, rcs, rcs, (rh + 1) >> 1, cx, cy, cbw + 7, cbh + 7);
+        pf_window(rv, rcs, rcs, (rh + 1) >> 1, cx, cy, cbw + 7, cbh + 7);
+    }
+}
+
+/* Exclusive prefix sums of two per-thread counts over the CTA (thread order).
+ * Returns the totals; uses s_tmp[2 * kWarps]. Must be called by all threads. */
+__device__ __forceinline__ void cta_scan2(int a, int b, int *ea, int *eb, int *ta, int *tb, int *s_tmp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int xa = a, xb = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int ya = __shfl_up_sync(0xffffffffu, xa, o), yb = __shfl_up_sync(0xffffffffu, xb, o);
+        if (lane >= o) { xa += ya; xb += yb; }
+    }
+    if (lane == 31) { s_tmp[warp] = xa; s_tmp[kWarps + warp] = xb; }
+    __syncthreads();
+    int pa = 0, pb = 0, sa = 0, sb = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) {
+        int va = s_tmp[w], vb = s_tmp[kWarps + w];
+        if (w < warp) { pa += va; pb += vb; }
+        sa += va; sb += vb;
+    }
+    *ea = pa + xa - a;
+    *eb = pb + xb - b;
+    *ta = sa;
+    *tb = sb;
+}
+
+/* Position and extent of chunk `chk` (level order): an 8x8 luma region of
+ * its block clipped to the frame, and the matching 4x4 chroma region. */
+struct ChunkP {
+    const BlkS *b;
+    int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
+};
+
+__device__ __forceinline__ ChunkP chunk_params(const ReconSmem &s, int chk)
+{
+    ChunkP c;
+    const int lo = s.chunk_blk[chk];
+    const BlkS &b = s.blk[s.order[lo]];
+    c.b = &b;
+    const int k = chk - s.chunk_off[lo];
+    const int nx = (b.cw + 7) >> 3;
+    const int ccy = k / nx, ccx = k - ccy * nx;
+    c.lx0 = b.x + ccx * 8;
+    c.ly0 = b.y + ccy * 8;
+    c.lw = min(8, b.cw - ccx * 8);
+    c.lh = min(8, b.ch - ccy * 8);
+    const int cbw = (b.cw + 1) >> 1, cbh = (b.ch + 1) >> 1;
+    c.cx0 = (b.x >> 1) + ccx * 4;
+    c.cy0 = (b.y >> 1) + ccy * 4;
+    c.clw = min(4, cbw - ccx * 4);
+    c.clh = min(4, cbh - ccy * 4);
+    return c;
+}
+
 } /* namespace */
 
 /* ── Kernels ─────────────────────────────────────────────────────────────── */
@@ -788,13 +997,14 @@ __global__ void __launch_bounds__(256) k_scan_blocks(const cvp9_job_t *__restric
 }
 
 template <int A>
-__global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restrict__ jobs,
                                                    const uint32_t *__restrict__ tickets,
                                                    uint32_t n_tickets, uint32_t *ticket_counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ReconSmem &s = *reinterpret_cast<ReconSmem *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const cvp9_job_t &job = s.jc;     /* valid after the reset barrier */
 
     for (;;) {
         __syncthreads();
@@ -803,24 +1013,34 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
         const int ticket = s.ticket;
         if (ticket >= (int)n_tickets) return;
         const uint32_t code = tickets[ticket];
-        const cvp9_job_t &job = jobs[code >> 20];
+        const cvp9_job_t *gj = jobs + (code >> 20);
+        {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(gj);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&s.jc);
+            for (int i = tid; i < (int)(sizeof(cvp9_job_t) / 4); i += kThreads) dst[i] = src[i];
+        }
         const int sb = (int)(code & 0xFFFFFu);
-        const int sbr = sb / job.sb_cols, sbc = sb - sbr * job.sb_cols;
+        const int g_sb_cols = gj->sb_cols;
+        const int sbr = sb / g_sb_cols, sbc = sb - sbr * g_sb_cols;
         const int sbx = sbc * 64, sby = sbr * 64;
-        const uint32_t *rg = job.sb_range + 4 * sb;
+        const uint32_t *rg = gj->sb_range + 4 * sb;
         const uint32_t start = rg[0], end = rg[1], groups = rg[2];
-        const bool layout_bad = (*(volatile uint32_t *)job.status & CVP9_JOB_BAD_BLOCK) != 0;
-        bool bad = groups > 1 || end < start || end > job.num_blocks ||
+        const uint32_t g_nblocks = gj->num_blocks;
+        const bool layout_bad = (*(volatile uint32_t *)gj->status & CVP9_JOB_BAD_BLOCK) != 0;
+        bool bad = groups > 1 || end < start || end > g_nblocks ||
                    (groups && end - start > (uint32_t)kMaxBlocks);
         int nb = (groups && !bad && !layout_bad) ? (int)(end - start) : 0;
 
         /* reset per-SB state, tile = 128 */
-        for (int i = tid; i < 65 * kYPitch; i += kThreads) s.ty[i] = 128;
-        for (int i = tid; i < 33 * kCPitch; i += kThreads) { s.tu[i] = 128; s.tv[i] = 128; }
+        {
+            uint4 *t4 = reinterpret_cast<uint4 *>(s.ty);
+            const uint4 fill = make_uint4(0x80808080u, 0x80808080u, 0x80808080u, 0x80808080u);
+            for (int i = tid; i < (kTyBytes + 2 * kTcBytes) / 16; i += kThreads) t4[i] = fill;
+        }
         for (int i = tid; i < 256 + 128; i += kThreads) s.txmask[i] = 0;
         for (int i = tid; i < 256; i += kThreads) s.cell[i] = 0;
         for (int i = tid; i <= kMaxBlocks; i += kThreads) s.lvl_cnt[i] = 0ull;
-        if (tid == 0) { s.nlev = 1; s.nb = nb; }
+        if (tid == 0) { s.nlev = 1; s.nb = nb; s.c_lo = 0xFFFFFFFFu; s.c_hi = 0u; }
         __syncthreads();
 
         /* 1. load and re-check blocks (a block must sit inside this SB,
@@ -867,6 +1087,21 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
             my_intra = false;
             if (tid == 0) s.nb = 0;
         }
+        if (tid < nb) prefetch_block<A>(mb, job, sbx, sby);
+        {
+            /* span of coefficients the residual pass reads */
+            unsigned lo = 0xFFFFFFFFu, hi = 0u;
+            if (tid < nb) {
+                uint64_t n = 0;
+#pragma unroll
+                for (int q = 0; q < 3; q++) n += (uint64_t)mb.pnt[q] * (uint64_t)(16 << (2 * mb.ptxl[q]));
+                uint64_t e = (uint64_t)mb.coeff + n;
+                if (n) { lo = mb.coeff; hi = e > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)e; }
+            }
+            lo = __reduce_min_sync(0xffffffffu, lo);
+            hi = __reduce_max_sync(0xffffffffu, hi);
+            if (lane == 0) { atomicMin(&s.c_lo, lo); atomicMax(&s.c_hi, hi); }
+        }
         if (tid < nb) {
             /* cells a block writes: its prediction area; under SPEC a
              * sub-8x8 block's residual spans the whole 8x8 MI
@@ -884,6 +1119,21 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
         }
         const int any_intra = __syncthreads_or(my_intra);
         const int any_overlap = __syncthreads_or(overlap);
+
+        /* stage the SB's coefficient span in shared memory with 16-byte loads
+         * (issued now, stored after the dependency analysis) */
+        const unsigned c_lo = s.c_lo, c_hi = s.c_hi;
+        const unsigned c_base = c_lo & ~7u;
+        const bool staged = c_hi > c_lo && c_hi <= job.num_coeffs && c_hi - c_base <= (unsigned)kCoefStage;
+        const bool c_vec = !((uintptr_t)job.coeffs & 15);
+        constexpr int kStageIt = kCoefStage / 8 / kThreads;
+#pragma unroll
+        for (int k = 0; k < kStageIt; k++) {
+            unsigned e = c_base + 8u * (unsigned)(tid + k * kThreads);
+            if (staged && c_vec && e < c_hi && e + 8 <= job.num_coeffs)
+                cp_async16(&s.coef[e - c_base], job.coeffs + e);
+        }
+        cp_async_commit();
 
         /* 2. dependency levels. An intra block depends on the blocks that own
          * its above row, left column and above-left corner inside the SB. */
@@ -928,9 +1178,27 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
         }
         __syncthreads();
 
-        /* 3. counting sort by level; each level's blocks, chunks and items
-         * get contiguous ranges (one packed 64-bit atomic keeps the three
-         * offsets of a block consistent with each other) */
+        /* 3. order blocks by level. One level (no intra dependency inside the
+         * SB): list order, offsets from a CTA-wide prefix sum. Otherwise a
+         * counting sort: each level's blocks, chunks and items get contiguous
+         * ranges (one packed 64-bit atomic keeps a block's three offsets
+         * consistent with each other). */
+        if (!any_intra && !seq) {
+            int ec, ei, tc, ti;
+            cta_scan2(tid < nb ? nch : 0, tid < nb ? nit : 0, &ec, &ei, &tc, &ti, s.scan_tmp);
+            if (tid < nb) {
+                s.order[tid] = (uint16_t)tid;
+                s.chunk_off[tid] = (uint16_t)ec;
+                s.item_off[tid] = (uint16_t)ei;
+            }
+            if (tid == 0) {
+                s.nlev = 1;
+                s.base_blk[0] = 0; s.base_blk[1] = (uint16_t)nb;
+                s.base_chunk[0] = 0; s.base_chunk[1] = (uint16_t)tc;
+                s.base_item[0] = 0; s.base_item[1] = (uint16_t)ti;
+                if (nb > 0) { s.chunk_off[nb] = (uint16_t)tc; s.item_off[nb] = (uint16_t)ti; }
+            }
+        } else {
         unsigned long long old = 0;
         int my_lvl = 0;
         if (tid < nb) {
@@ -940,13 +1208,13 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
                                                     (unsigned long long)nit);
         }
         __syncthreads();
-        const int nlev = s.nlev;
+        const int nlev_s = s.nlev;
         if (warp == 0) {
             /* exclusive scan over levels, 8 levels per lane */
-            int per = (nlev + 31) / 32;
+            int per = (nlev_s + 31) / 32;
             int b0 = lane * per;
             unsigned sb_ = 0, sc = 0, si = 0;
-            for (int l = b0; l < b0 + per && l < nlev; l++) {
+            for (int l = b0; l < b0 + per && l < nlev_s; l++) {
                 unsigned long long v = s.lvl_cnt[l];
                 sb_ += (unsigned)(v >> 40); sc += (unsigned)((v >> 20) & 0xFFFFF); si += (unsigned)(v & 0xFFFFF);
             }
@@ -959,12 +1227,12 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
                 if (lane >= o) { xb += yb; xc += yc; xi += yi; }
             }
             unsigned eb = xb - sb_, ec = xc - sc, ei = xi - si;
-            for (int l = b0; l < b0 + per && l < nlev; l++) {
+            for (int l = b0; l < b0 + per && l < nlev_s; l++) {
                 s.base_blk[l] = (uint16_t)eb; s.base_chunk[l] = (uint16_t)ec; s.base_item[l] = (uint16_t)ei;
                 unsigned long long v = s.lvl_cnt[l];
                 eb += (unsigned)(v >> 40); ec += (unsigned)((v >> 20) & 0xFFFFF); ei += (unsigned)(v & 0xFFFFF);
             }
-            if (lane == 31) { s.base_blk[nlev] = (uint16_t)eb; s.base_chunk[nlev] = (uint16_t)ec; s.base_item[nlev] = (uint16_t)ei; }
+            if (lane == 31) { s.base_blk[nlev_s] = (uint16_t)eb; s.base_chunk[nlev_s] = (uint16_t)ec; s.base_item[nlev_s] = (uint16_t)ei; }
         }
         __syncthreads();
         if (tid < nb) {
@@ -973,7 +1241,24 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
             s.chunk_off[p] = (uint16_t)(s.base_chunk[my_lvl] + (int)((old >> 20) & 0xFFFFF));
             s.item_off[p] = (uint16_t)(s.base_item[my_lvl] + (int)(old & 0xFFFFF));
         }
-        if (tid == 0 && nb > 0) { s.chunk_off[nb] = s.base_chunk[nlev]; s.item_off[nb] = s.base_item[nlev]; }
+        if (tid == 0 && nb > 0) { s.chunk_off[nb] = s.base_chunk[nlev_s]; s.item_off[nb] = s.base_item[nlev_s]; }
+        }
+        __syncthreads();
+        const int nlev = s.nlev;
+#pragma unroll
+        for (int k = 0; k < kStageIt; k++) {
+            unsigned e = c_base + 8u * (unsigned)(tid + k * kThreads);
+            if (!staged || e >= c_hi) continue;
+            if (!(c_vec && e + 8 <= job.num_coeffs))
+                for (unsigned q = e; q < e + 8 && q < c_hi; q++) s.coef[q - c_base] = job.coeffs[q];
+        }
+        /* chunk -> block and TX item -> block maps, a warp per block */
+        for (int p = warp; p < nb; p += kWarps) {
+            int c0 = s.chunk_off[p], c1 = s.chunk_off[p + 1];
+            for (int c = c0 + lane; c < c1; c += 32) s.chunk_blk[c] = (uint8_t)p;
+            int i0 = s.item_off[p], i1 = s.item_off[p + 1];
+            for (int i = i0 + lane; i < i1 && i < kMaxItems; i += 32) s.item_blk[i] = (uint8_t)p;
+        }
 
         /* 4. wait for the neighbour SBs when intra blocks read their edges */
         if (any_intra) {
@@ -1020,34 +1305,67 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
 
         /* 5. levels */
         for (int L = 0; L < nlev && nb > 0; L++) {
-            const int pb0 = s.base_blk[L], pb1 = s.base_blk[L + 1];
-            /* phase P: prediction, warp per 8x8 chunk */
-            for (int chk = s.base_chunk[L] + warp; chk < s.base_chunk[L + 1]; chk += kWarps) {
-                int lo = pb0, hi = pb1 - 1;
-                while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.chunk_off[mid] <= chk) lo = mid; else hi = mid - 1; }
-                const BlkS &b = s.blk[s.order[lo]];
-                int c = chk - s.chunk_off[lo];
-                int nx = (b.cw + 7) >> 3;
-                int ccy = c / nx, ccx = c - ccy * nx;
-                int lx0 = b.x + ccx * 8, ly0 = b.y + ccy * 8;
-                int lw = min(8, b.cw - ccx * 8), lh = min(8, b.ch - ccy * 8);
-                int cbw = (b.cw + 1) >> 1, cbh = (b.ch + 1) >> 1;
-                int cx0 = (b.x >> 1) + ccx * 4, cy0 = (b.y >> 1) + ccy * 4;
-                int clw = min(4, cbw - ccx * 4), clh = min(4, cbh - ccy * 4);
-                if (b.flags & 1)
-                    predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, lx0, ly0, lw, lh, cx0, cy0, clw, clh, lane);
-                else
-                    predict_inter_chunk<A>(s, job, b, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh, warp, lane);
+            /* phase P: prediction, warp per 8x8 chunk. REFCPU stages the
+             * windows of up to kRound chunks per warp with async copies into
+             * the (idle) transform buffer, waits once, then computes them. */
+            const int chk0 = s.base_chunk[L], chk1 = s.base_chunk[L + 1];
+            if (A == CVP9_ARITH_REFCPU) {
+                constexpr int kRound = 4;
+                uint8_t *wst = reinterpret_cast<uint8_t *>(s.temp.d) + warp * (kRound * kChunkStage);
+                for (int base = chk0 + warp; base < chk1; base += kRound * kWarps) {
+#pragma unroll
+                    for (int q = 0; q < kRound; q++) {
+                        const int chk = base + q * kWarps;
+                        if (chk >= chk1) break;
+                        ChunkP c = chunk_params(s, chk);
+                        McGeo g;
+                        if (!(c.b->flags & 1) &&
+                            refcpu_geo(s, *c.b, sbx, sby, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, g))
+                            refcpu_issue(wst + q * kChunkStage, g, c.lw, c.lh, c.clw, c.clh, lane);
+                    }
+                    cp_async_commit();
+                    cp_async_wait_all();
+                    __syncwarp();
+#pragma unroll
+                    for (int q = 0; q < kRound; q++) {
+                        const int chk = base + q * kWarps;
+                        if (chk >= chk1) break;
+                        ChunkP c = chunk_params(s, chk);
+                        const BlkS &b = *c.b;
+                        McGeo g;
+                        if (b.flags & 1)
+                            predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, c.lx0, c.ly0, c.lw, c.lh,
+                                                   c.cx0, c.cy0, c.clw, c.clh, lane);
+                        else if (refcpu_geo(s, b, sbx, sby, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, g))
+                            refcpu_compute(s, wst + q * kChunkStage, g, c.lx0, c.ly0, c.lw, c.lh,
+                                           c.cx0, c.cy0, c.clw, c.clh, lane);
+                        else
+                            fill_chunk(s, 127, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, lane);
+                    }
+                    __syncwarp();
+                }
+            } else {
+                for (int chk = chk0 + warp; chk < chk1; chk += kWarps) {
+                    ChunkP c = chunk_params(s, chk);
+                    const BlkS &b = *c.b;
+                    if (b.flags & 1)
+                        predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, c.lx0, c.ly0, c.lw, c.lh,
+                                               c.cx0, c.cy0, c.clw, c.clh, lane);
+                    else
+                        spec_inter_chunk(s, b, sbx, sby, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0,
+                                         c.clw, c.clh, warp, lane);
+                }
             }
+            cp_async_wait_all();     /* the SB's coefficient span */
+            __syncthreads();
             /* phase P': first transform pass, thread per TX column */
             for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
-                int lo = pb0, hi = pb1 - 1;
-                while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.item_off[mid] <= it) lo = mid; else hi = mid - 1; }
+                const int lo = s.item_blk[it];
                 const BlkS &b = s.blk[s.order[lo]];
                 int j;
                 TxRef t = locate_item(b, it - s.item_off[lo], &j);
                 if (t.coeff + (uint64_t)(t.n * t.n) > (uint64_t)job.num_coeffs) continue;
-                const int16_t *X = job.coeffs + t.coeff;
+                const int16_t *X = staged ? s.coef + (t.coeff - c_base) : job.coeffs + t.coeff;
                 if (A == CVP9_ARITH_REFCPU) {
                     const double *M = dct_basis(t.txl);
                     switch (t.txl) {
@@ -1068,8 +1386,7 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
             __syncthreads();
             /* phase Q: second pass + residual add, thread per TX row */
             for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
-                int lo = pb0, hi = pb1 - 1;
-                while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.item_off[mid] <= it) lo = mid; else hi = mid - 1; }
+                const int lo = s.item_blk[it];
                 const BlkS &b = s.blk[s.order[lo]];
                 int i;
                 TxRef t = locate_item(b, it - s.item_off[lo], &i);
@@ -1120,6 +1437,16 @@ __global__ void __launch_bounds__(kThreads) k_recon(const cvp9_job_t *__restrict
             const int cvw = min(32, job.CW - (sbx >> 1)), cvh = min(32, job.CH - (sby >> 1));
             uint8_t *U = job.out + (size_t)job.W * job.H;
             uint8_t *V = U + (size_t)job.CW * job.CH;
+            if ((job.CW & 3) == 0 && ((size_t)job.W * job.H & 3) == 0) {
+                for (int i = tid; i < 2 * cvh * 8; i += kThreads) {
+                    int p = i >= cvh * 8;
+                    int k = p ? i - cvh * 8 : i;
+                    int r = k >> 3, c4 = (k & 7) * 4;
+                    if (c4 >= cvw) continue;
+                    *reinterpret_cast<uint32_t *>((p ? V : U) + (size_t)((sby >> 1) + r) * job.CW + (sbx >> 1) + c4) =
+                        *reinterpret_cast<const uint32_t *>(&TC(s, 1 + p, c4, r));
+                }
+            } else
             for (int i = tid; i < 2 * cvh * 32; i += kThreads) {
                 int p = i >= cvh * 32;
                 int k = p ? i - cvh * 32 : i;
@@ -1306,6 +1633,9 @@ int cvp9k_configure(void)
     size_t smem = sizeof(ReconSmem);
     if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_REFCPU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
     if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+    /* all of the unified L1/shared storage as shared memory: three CTAs per SM */
+    cudaFuncSetAttribute(k_recon<CVP9_ARITH_REFCPU>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_recon<CVP9_ARITH_SPEC>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return 0;
 }
 

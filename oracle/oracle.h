@@ -48,6 +48,9 @@ void oracle_frame_free(oracle_frame_t *f);
 
 /* ── Stage-level entry points (unit tests) ─────────────────────────────── */
 
+/* REFCPU float64 DCT basis for N = 4, 8, 16, 32 concatenated (1360 doubles). */
+void oracle_refcpu_basis(double *out);
+
 /* REFCPU float64 inverse DCT of raw coefficients (vp9_reconstruct.c:13-60). */
 void oracle_refcpu_idct2d(const int16_t *in, int16_t *out, int n);
 

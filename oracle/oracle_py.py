@@ -48,6 +48,8 @@ def oracle_lib():
         lib.oracle_loopfilter.restype = None
         lib.oracle_nv12_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]
         lib.oracle_nv12_pack.restype = None
+        lib.oracle_refcpu_basis.argtypes = [C.c_void_p]
+        lib.oracle_refcpu_basis.restype = None
         lib.oracle_dc_quant.argtypes = [C.c_int]
         lib.oracle_ac_quant.argtypes = [C.c_int]
         _orc = lib
@@ -122,6 +124,12 @@ class RefStream:
 
     def __del__(self):
         self.close()
+
+
+def refcpu_basis():
+    out = np.empty(16 + 64 + 256 + 1024, np.float64)
+    oracle_lib().oracle_refcpu_basis(out.ctypes.data)
+    return out
 
 
 def refcpu_idct2d(coeffs):

@@ -55,6 +55,18 @@ static void dct_basis(double M[32][32], int n)
     }
 }
 
+void oracle_refcpu_basis(double *out)
+{
+    double M[32][32];
+    int base = 0;
+    for (int n = 4; n <= 32; n *= 2) {
+        dct_basis(M, n);
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) out[base + i * n + j] = M[i][j];
+        base += n * n;
+    }
+}
+
 void oracle_refcpu_idct2d(const int16_t *in, int16_t *out, int n)
 {
     double M[32][32], T[32][32];

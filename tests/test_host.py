@@ -1,0 +1,98 @@
+"""CPU: the C ABI library loads and exports every function include/*.h
+declares; boundary layouts and tables equal the reference's; host-side
+logic (DCT basis, wavefront ticket order) is correct. No GPU calls."""
+import ctypes as C
+import hashlib
+import json
+import os
+import re
+
+import numpy as np
+
+import compute_vp9_b200 as P
+from compute_vp9_b200.cvp9_ctypes import layout_offsets
+from oracle import oracle_py as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def _declared_functions(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\([^;{]*\)\s*;", text, flags=re.M)
+    return [n for n in names if not n.startswith("if")]
+
+
+def test_library_exports_every_declared_function():
+    lib = P.cuda_lib()
+    declared = _declared_functions("cuda_backend.h") + _declared_functions("cvp9_batch.h")
+    assert "cuda_decode_frame" in declared and "cvp9_batch_submit" in declared
+    assert "cuda_reconstruct_noalloc" in declared
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(P.EXPORTED_SYMBOLS) <= set(declared)
+
+
+def test_synth_library_exports():
+    lib = P.synth_lib()
+    for n in _declared_functions("cvp9_synth.h"):
+        assert hasattr(lib, n), n
+
+
+def test_struct_layout_matches_reference():
+    want = json.load(open(os.path.join(GOLD, "layout.json")))["offsets"]
+    assert layout_offsets() == want
+
+
+def test_tables_match_reference():
+    want = json.load(open(os.path.join(GOLD, "tables.json")))
+    lib = O.oracle_lib()
+    dc = np.array([lib.oracle_dc_quant(q) for q in range(256)], np.int32)
+    ac = np.array([lib.oracle_ac_quant(q) for q in range(256)], np.int32)
+    assert hashlib.sha256(dc.tobytes()).hexdigest() == want["dc_q_sha256"]
+    assert hashlib.sha256(ac.tobytes()).hexdigest() == want["ac_q_sha256"]
+    text = open(os.path.join(ROOT, "compute_vp9_b200", "csrc", "vp9_tables.h")).read()
+    body = text[text.index("CVP9_SUBPEL_REGULAR_INIT") + len("CVP9_SUBPEL_REGULAR_INIT"):]
+    body = body[:body.index("#define CVP9_QINDEX_CLAMP")]
+    taps = [int(x) for x in re.findall(r"-?\d+", body)]
+    assert len(taps) == 128
+    assert hashlib.sha256(np.array(taps, np.int32).reshape(16, 8).tobytes()).hexdigest() == \
+        want["subpel_regular_sha256"]
+
+
+def test_dct_basis_identical_to_oracle():
+    lib = P.cuda_lib()
+    lib.cvp9_build_dct_basis.argtypes = [C.c_void_p]
+    lib.cvp9_build_dct_basis.restype = None
+    mine = np.empty(1360, np.float64)
+    lib.cvp9_build_dct_basis(mine.ctypes.data)
+    assert np.array_equal(mine.view(np.uint64), O.refcpu_basis().view(np.uint64))
+
+
+def test_wavefront_ticket_order():
+    lib = P.cuda_lib()
+    lib.cvp9_tickets_on_diagonal.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    for cols, rows in [(30, 17), (1, 1), (5, 1), (1, 7), (20, 12)]:
+        out = (C.c_uint32 * (cols * rows))()
+        n = 0
+        order = []
+        for d in range(cols + rows - 1):
+            buf = (C.c_uint32 * (cols * rows))()
+            k = lib.cvp9_tickets_on_diagonal(cols, rows, 3, d, buf)
+            order += [buf[i] for i in range(k)]
+        assert len(order) == cols * rows
+        assert all(t >> 20 == 3 for t in order)
+        pos = {t & 0xFFFFF: i for i, t in enumerate(order)}
+        assert sorted(pos) == list(range(cols * rows))
+        for sb, i in pos.items():
+            r, c = divmod(sb, cols)
+            for dr, dc in ((0, -1), (-1, 0), (-1, -1)):
+                if r + dr >= 0 and c + dc >= 0:
+                    assert pos[(r + dr) * cols + c + dc] < i   # dependencies come first
+
+
+def test_job_struct_is_word_copyable():
+    # the recon kernel copies the job descriptor into shared memory as 32-bit words
+    text = open(os.path.join(ROOT, "compute_vp9_b200", "csrc", "recon_job.h")).read()
+    assert "cvp9_ref_t ref[8]" in text
