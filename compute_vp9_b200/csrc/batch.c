@@ -52,6 +52,7 @@ typedef struct {
     int       latest;           /* output buffer of the newest step, -1 none */
     uint64_t  last_seq;         /* newest step that included this stream     */
     uint32_t  last_status;
+    int       sb_cap;           /* capacity of d_sb_done (SBs)               */
 } bstream_t;
 
 struct cvp9_batch;
@@ -62,6 +63,7 @@ typedef struct {
     int             busy;
     lat_arg_t       lat_arg;     /* completion-callback argument of this slot */
     cudaEvent_t     ev_start, ev_h2d, ev_k0, ev_k1, ev_end;
+    cudaEvent_t     ev_cb;       /* after the completion callback: slot reuse waits on it */
     cudaEvent_t     ev_kern[4];
     uint8_t        *h_in;   size_t h_in_cap;
     uint8_t        *d_in;   size_t d_in_cap;
@@ -69,6 +71,7 @@ typedef struct {
     uint32_t       *d_sb_range; size_t sb_cap;      /* uint32 entries */
     uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status */
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
+    uint32_t       *h_tickets; size_t h_tickets_cap;
     cudaGraphExec_t graph; uint64_t graph_key;
     int             n;
     int            *sids;  int sids_cap;
@@ -138,6 +141,15 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     b->resident_ctas = sms * cvp9_recon_ctas_per_sm(b->device, b->arith);
+    {
+        /* frame buffers come from the stream-ordered pool: keep freed memory
+         * cached there instead of returning it at every synchronisation */
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, b->device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->hs, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->ds, cudaStreamNonBlocking) != cudaSuccess) {
@@ -150,7 +162,7 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
             cudaEventCreate(&s->ev_k0) != cudaSuccess || cudaEventCreate(&s->ev_k1) != cudaSuccess ||
             cudaEventCreate(&s->ev_end) != cudaSuccess || cudaEventCreate(&s->ev_kern[0]) != cudaSuccess ||
             cudaEventCreate(&s->ev_kern[1]) != cudaSuccess || cudaEventCreate(&s->ev_kern[2]) != cudaSuccess ||
-            cudaEventCreate(&s->ev_kern[3]) != cudaSuccess) {
+            cudaEventCreate(&s->ev_kern[3]) != cudaSuccess || cudaEventCreate(&s->ev_cb) != cudaSuccess) {
             cvp9_batch_destroy(b);
             return CVP9_ERR_GPU;
         }
@@ -187,6 +199,7 @@ void cvp9_batch_destroy(cvp9_batch_t *b)
         if (s->ev_k0) cudaEventDestroy(s->ev_k0);
         if (s->ev_k1) cudaEventDestroy(s->ev_k1);
         if (s->ev_end) cudaEventDestroy(s->ev_end);
+        if (s->ev_cb) cudaEventDestroy(s->ev_cb);
         for (int k = 0; k < 4; k++) if (s->ev_kern[k]) cudaEventDestroy(s->ev_kern[k]);
         cudaFreeHost(s->h_in);
         cudaFree(s->d_in);
@@ -196,11 +209,12 @@ void cvp9_batch_destroy(cvp9_batch_t *b)
         cudaFree(s->d_misc);
         cudaFreeHost(s->h_misc);
         cudaFree(s->d_tickets);
+        cudaFreeHost(s->h_tickets);
         free(s->sids);
     }
     if (b->st)
         for (int i = 0; i < b->max_streams; i++)
-            if (b->st[i].open) free_stream(&b->st[i]);
+            free_stream(&b->st[i]);
     free(b->st);
     if (b->ev_t0) cudaEventDestroy(b->ev_t0);
     if (b->ev_t1) cudaEventDestroy(b->ev_t1);
@@ -215,21 +229,46 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
     if (!b || w == 0 || h == 0 || w > 65535 || h > 65535) return CVP9_ERR_INVALID_DATA;
     uint64_t need = cvp9_batch_stream_bytes(w, h);
     if (b->reserved + need > b->budget) return CVP9_ERR_NOMEM;
-    int sid = -1;
-    for (int i = 0; i < b->max_streams; i++)
-        if (!b->st[i].open) { sid = i; break; }
-    if (sid < 0) return CVP9_ERR_NOMEM;
+    /* prefer a closed slot whose device buffers can be reused as they are
+     * (no cudaMalloc/cudaFree, which would synchronise the device) */
+    int sid = -1, fresh = -1;
+    const int n_sb = (int)(((w + 63) / 64) * ((h + 63) / 64));
+    for (int i = 0; i < b->max_streams; i++) {
+        bstream_t *c = &b->st[i];
+        if (c->open) continue;
+        if (c->d_sb_done && c->sb_cap >= n_sb && c->f[0].cap >= frame_bytes((int32_t)w, (int32_t)h)) { sid = i; break; }
+        if (fresh < 0 && !c->d_sb_done) fresh = i;
+    }
+    if (sid < 0) sid = fresh;
+    if (sid < 0) {   /* every free slot holds buffers of another size: recycle one */
+        for (int i = 0; i < b->max_streams; i++) if (!b->st[i].open) { sid = i; break; }
+        if (sid < 0) return CVP9_ERR_NOMEM;
+        free_stream(&b->st[sid]);
+    }
     bstream_t *s = &b->st[sid];
-    memset(s, 0, sizeof(*s));
-    s->W = (int32_t)w;
-    s->H = (int32_t)h;
-    s->n_sb = (int)(((w + 63) / 64) * ((h + 63) / 64));
-    if (cudaSetDevice(b->device) != cudaSuccess ||
-        cudaMalloc((void **)&s->d_sb_done, (size_t)s->n_sb * 4) != cudaSuccess ||
-        cudaMemset(s->d_sb_done, 0, (size_t)s->n_sb * 4) != cudaSuccess) {
+    if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
+    if (!s->d_sb_done || s->sb_cap < n_sb) {
+        cudaFree(s->d_sb_done);
+        s->d_sb_done = NULL;
+        if (cudaMalloc((void **)&s->d_sb_done, (size_t)n_sb * 4) != cudaSuccess) {
+            free_stream(s);
+            return CVP9_ERR_NOMEM;
+        }
+        s->sb_cap = n_sb;
+    }
+    /* flags are compared against a per-stream epoch: start from zero */
+    if (cudaMemsetAsync(s->d_sb_done, 0, (size_t)n_sb * 4, b->cs) != cudaSuccess) {
         free_stream(s);
         return CVP9_ERR_NOMEM;
     }
+    s->W = (int32_t)w;
+    s->H = (int32_t)h;
+    s->n_sb = n_sb;
+    s->epoch = 0;
+    for (int i = 0; i < MAXF; i++) { s->f[i].users = 0; s->f[i].d2h_seq = 0; }
+    s->latest = -1;
+    s->last_seq = 0;
+    s->last_status = 0;
     for (int i = 0; i < 8; i++) s->ref_slot[i] = -1;
     s->latest = -1;
     s->reserved = need;
@@ -255,7 +294,11 @@ cvp9_err_t cvp9_batch_close_stream(cvp9_batch_t *b, int sid)
         if (e == CVP9_ERR_GPU) return e;
     }
     b->reserved -= s->reserved;
-    free_stream(s);
+    /* keep the device buffers for the next admitted stream */
+    s->open = 0;
+    s->reserved = 0;
+    for (int i = 0; i < 8; i++) s->ref_slot[i] = -1;
+    for (int i = 0; i < MAXF; i++) s->f[i].users = 0;
     return CVP9_OK;
 }
 
@@ -302,10 +345,12 @@ static int acquire_frame(cvp9_batch_t *b, bstream_t *s)
         if (o->seq == f->d2h_seq) cudaStreamWaitEvent(b->cs, o->ev_end, 0);
     }
     if (!f->dev || f->cap < need) {
-        if (f->dev) { cudaDeviceSynchronize(); cudaFree(f->dev); }
+        /* stream-ordered: the old buffer is released after the work already
+         * queued on the compute stream, without a device-wide sync */
+        if (f->dev) cudaFreeAsync(f->dev, b->cs);
         f->dev = NULL;
         f->cap = 0;
-        if (cudaMalloc((void **)&f->dev, need) != cudaSuccess) return -1;
+        if (cudaMallocAsync((void **)&f->dev, need, b->cs) != cudaSuccess) return -1;
         f->cap = need;
     }
     f->w = s->W;
@@ -358,7 +403,7 @@ static cvp9_err_t wait_slot(cvp9_batch_t *b, bslot_t *s)
     if (!s->busy) return CVP9_OK;
     double t0 = cvp9_now();
     for (;;) {
-        cudaError_t e = cudaEventQuery(s->ev_end);
+        cudaError_t e = cudaEventQuery(s->ev_cb);
         if (e == cudaSuccess) break;
         if (e != cudaErrorNotReady) return bfail(b, e, "step completion");
         if (cvp9_now() - t0 > WAIT_LIMIT_S) {
@@ -474,16 +519,15 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     if (s->tickets_key != key || !s->d_tickets) {
         size_t need = n_sb * 4;
         if ((err = grow_dev(b, (void **)&s->d_tickets, &s->tickets_cap, need))) return err;
-        uint32_t *t = malloc(need ? need : 4);
-        if (!t) return CVP9_ERR_NOMEM;
+        if ((err = grow_host(b, (void **)&s->h_tickets, &s->h_tickets_cap, need ? need : 4))) return err;
+        uint32_t *t = s->h_tickets;
         uint32_t cnt = 0;
         for (int d = 0; d < maxd; d++)
             for (int i = 0; i < n; i++) {
                 bstream_t *st = &b->st[sids[i]];
                 cnt += (uint32_t)cvp9_tickets_on_diagonal((st->W + 63) / 64, (st->H + 63) / 64, i, d, t + cnt);
             }
-        cudaError_t e = cudaMemcpy(s->d_tickets, t, (size_t)cnt * 4, cudaMemcpyHostToDevice);
-        free(t);
+        cudaError_t e = cudaMemcpyAsync(s->d_tickets, t, (size_t)cnt * 4, cudaMemcpyHostToDevice, b->hs);
         if (e != cudaSuccess) return bfail(b, e, "tickets");
         s->n_tickets = cnt;
         s->tickets_key = key;
@@ -672,14 +716,16 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     if (ofr != out_frame) free(ofr);
     BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
     s->d2h_bytes += (size_t)(n + 1) * 4;
-    /* the callback runs before ev_end completes, so a slot's argument is
-     * free again once the slot's step is waited for */
+    /* ev_end, then the completion callback (so a stamped step is complete
+     * for every other query), then ev_cb, which slot reuse waits on so the
+     * callback's argument is never overwritten while pending */
+    BCK(cudaEventRecord(s->ev_end, b->ds), "event");
     s->lat_arg.b = b;
     s->lat_arg.seq = seq;
     b->lat_seq[seq % LAT_RING] = seq;
     b->lat_done[seq % LAT_RING] = 0.0;
     BCK(cudaLaunchHostFunc(b->ds, step_done_cb, &s->lat_arg), "completion callback");
-    BCK(cudaEventRecord(s->ev_end, b->ds), "event");
+    BCK(cudaEventRecord(s->ev_cb, b->ds), "event");
 
     s->seq = seq;
     s->n = n;
@@ -713,7 +759,7 @@ int cvp9_batch_poll(cvp9_batch_t *b)
     for (uint64_t q = b->done_seq + 1; q <= b->seq; q++) {
         bslot_t *s = &b->slot[q % BSLOTS];
         if (s->seq != q || !s->busy) continue;
-        cudaError_t e = cudaEventQuery(s->ev_end);
+        cudaError_t e = cudaEventQuery(s->ev_cb);
         if (e == cudaErrorNotReady) return 0;
         if (e != cudaSuccess) return CVP9_ERR_GPU;
         complete_slot(b, s);
@@ -731,10 +777,13 @@ cvp9_err_t cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *inf
     if (st->out_seq[par] > b->done_seq) {
         bslot_t *s = &b->slot[st->out_seq[par] % BSLOTS];
         if (s->busy && s->seq == st->out_seq[par]) {
+            /* the frame and the status words have landed once ev_end is done */
             cudaError_t e = cudaEventQuery(s->ev_end);
             if (e == cudaErrorNotReady) return CVP9_ERR_AGAIN;
             if (e != cudaSuccess) return bfail(b, e, "step completion");
-            complete_slot(b, s);
+            for (int i = 0; i < s->n; i++)
+                if (s->sids[i] == sid) st->last_status = s->h_misc[1 + i];
+            if (cudaEventQuery(s->ev_cb) == cudaSuccess) complete_slot(b, s);
         }
     }
     if (st->last_status & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) return CVP9_ERR_INVALID_DATA;

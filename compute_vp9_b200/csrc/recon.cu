@@ -65,6 +65,13 @@ __device__ __forceinline__ const double *dct_basis(int txl)
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+/* t / d for 0 <= t < 4096 and 1 <= d <= 16 without an integer divide:
+ * (t * ceil(2^16 / d)) >> 16 is exact in that range. */
+__device__ __forceinline__ int div_small(int t, int d)
+{
+    return (int)(((unsigned)t * ((65536u + (unsigned)d - 1u) / (unsigned)d)) >> 16);
+}
+
 /* ── Asynchronous global -> shared copies (16 bytes, both sides aligned) ── */
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -538,6 +545,115 @@ __device__ __forceinline__ void refcpu_issue(uint8_t *st, const McGeo &g, int lw
     }
 }
 
+/* Lane-group variants: 8 lanes per chunk (k = lane & 7). Issue: the group's
+ * lanes share the chunk's window copies. Compute: lane k produces luma row k
+ * (up to 8 samples) and, for k < 4 / k >= 4, row k&3 of U / V. */
+__device__ __forceinline__ void refcpu_issue8(uint8_t *st, const McGeo &g, int lw, int lh,
+                                              int clw, int clh, int k)
+{
+    if (g.lfast) {
+        const int two = (g.ix - g.la) + lw >= 16;
+        for (int j = k; j < 2 * (lh + 1); j += 8) {
+            const int row = j >> 1, half = j & 1;
+            if (half == 0 || two)
+                cp_async16(st + row * 32 + half * 16, g.rp + (size_t)(g.iy + row) * g.rw + g.la + half * 16);
+        }
+    }
+    if (g.cfast) {
+        const int two = (g.cix - g.ca) + clw >= 16;
+        const int per = 2 * (clh + 1);
+        for (int j = k; j < 2 * per; j += 8) {
+            const int pl = j >= per, jj = j - pl * per, row = jj >> 1, half = jj & 1;
+            if (half == 0 || two)
+                cp_async16(st + 288 + pl * 160 + row * 32 + half * 16,
+                           (pl ? g.rv : g.ru) + (size_t)(g.ciy + row) * g.rcs + g.ca + half * 16);
+        }
+    }
+}
+
+/* nine consecutive bytes of a staged row starting at byte `off`, from three
+ * aligned 32-bit shared-memory words */
+__device__ __forceinline__ void row9(const uint8_t *row, int off, unsigned v[9])
+{
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(row) + (off >> 2);
+    const unsigned sh = 8u * (unsigned)(off & 3);
+    const unsigned w0 = w[0], w1 = w[1], w2 = w[2];
+    const unsigned lo = __funnelshift_r(w0, w1, sh), mid = __funnelshift_r(w1, w2, sh), hi = w2 >> sh;
+#pragma unroll
+    for (int i = 0; i < 4; i++) { v[i] = (lo >> (8 * i)) & 0xffu; v[4 + i] = (mid >> (8 * i)) & 0xffu; }
+    v[8] = hi & 0xffu;
+}
+
+__device__ __forceinline__ void refcpu_compute8(ReconSmem &s, const uint8_t *st, const McGeo &g,
+                                                int lx0, int ly0, int lw, int lh,
+                                                int cx0, int cy0, int clw, int clh, int k)
+{
+    if (k < lh) {
+        unsigned a[9], b[9];
+        if (g.lfast) {
+            row9(st + k * 32, g.ix - g.la, a);
+            row9(st + (k + 1) * 32, g.ix - g.la, b);
+        } else {
+            const int y0 = clampi(g.iy + k, 0, g.rh - 1), y1 = clampi(g.iy + k + 1, 0, g.rh - 1);
+            const uint8_t *r0 = g.rp + (size_t)y0 * g.rw, *r1 = g.rp + (size_t)y1 * g.rw;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                const int x = clampi(g.ix + c, 0, g.rw - 1);
+                a[c] = __ldg(r0 + x);
+                b[c] = __ldg(r1 + x);
+            }
+        }
+        const unsigned wx = 8 - g.fx, wy = 8 - g.fy;
+        unsigned out[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const unsigned t = (a[c] * wx + a[c + 1] * g.fx + 4) >> 3;
+            const unsigned u = (b[c] * wx + b[c + 1] * g.fx + 4) >> 3;
+            out[c] = (t * wy + u * g.fy + 4) >> 3;
+        }
+        uint8_t *d = &TY(s, lx0, ly0 + k);
+        if (lw == 8) {
+            uint32_t *d4 = reinterpret_cast<uint32_t *>(d);
+            d4[0] = out[0] | out[1] << 8 | out[2] << 16 | out[3] << 24;
+            d4[1] = out[4] | out[5] << 8 | out[6] << 16 | out[7] << 24;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; c++) if (c < lw) d[c] = (uint8_t)out[c];
+        }
+    }
+    {
+        const int p = 1 + (k >> 2), r = k & 3;
+        if (r < clh) {
+            unsigned a[5], b[5];
+            if (g.cfast) {
+                const uint8_t *s0 = st + 288 + (p - 1) * 160 + r * 32 + (g.cix - g.ca), *s1 = s0 + 32;
+#pragma unroll
+                for (int c = 0; c < 5; c++) { a[c] = s0[c]; b[c] = s1[c]; }
+            } else {
+                const int crw = g.rw >> 1, crh = g.rh >> 1;
+                const int xm = crw > 0 ? crw - 1 : 0, ym = crh > 0 ? crh - 1 : 0;
+                const uint8_t *pl = p == 1 ? g.ru : g.rv;
+                const uint8_t *r0 = pl + (size_t)clampi(g.ciy + r, 0, ym) * g.rcs;
+                const uint8_t *r1 = pl + (size_t)clampi(g.ciy + r + 1, 0, ym) * g.rcs;
+#pragma unroll
+                for (int c = 0; c < 5; c++) {
+                    const int x = clampi(g.cix + c, 0, xm);
+                    a[c] = __ldg(r0 + x);
+                    b[c] = __ldg(r1 + x);
+                }
+            }
+            uint8_t *d = &TC(s, p, cx0, cy0 + r);
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (c >= clw) break;
+                const unsigned t = (a[c] * (8 - g.cfx) + a[c + 1] * g.cfx + 4) >> 3;
+                const unsigned u = (b[c] * (8 - g.cfx) + b[c + 1] * g.cfx + 4) >> 3;
+                d[c] = (uint8_t)((t * (8 - g.cfy) + u * g.cfy + 4) >> 3);
+            }
+        }
+    }
+}
+
 /* Bilinear with a per-sample clamp into the reference (vp9_reconstruct.c:
  * 105-128): from the staged window on the fast path, else from clamped
  * byte reads. */
@@ -590,6 +706,18 @@ __device__ __forceinline__ void refcpu_compute(ReconSmem &s, const uint8_t *st, 
             TC(s, p, cx0 + c, cy0 + r) = (uint8_t)((t0 * (8 - g.cfy) + u0 * g.cfy + 4) >> 3);
         }
     }
+}
+
+/* Lane-group flat fill (missing reference): lane k fills luma row k and one
+ * chroma row, like refcpu_compute8. */
+__device__ __forceinline__ void refcpu_fill8(ReconSmem &s, int v, int lx0, int ly0, int lw, int lh,
+                                             int cx0, int cy0, int clw, int clh, int k)
+{
+    if (k < lh)
+        for (int c = 0; c < lw; c++) TY(s, lx0 + c, ly0 + k) = (uint8_t)v;
+    const int p = 1 + (k >> 2), r = k & 3;
+    if (r < clh)
+        for (int c = 0; c < clw; c++) TC(s, p, cx0 + c, cy0 + r) = (uint8_t)v;
 }
 
 /* A reference that is absent predicts as a flat value (127 REFCPU, 128 SPEC). */
@@ -714,7 +842,7 @@ __device__ __forceinline__ TxRef locate_item(const BlkS &b, int item, int *lane_
     int tx = item >> (2 + txl);
     *lane_idx = item & (n - 1);
     int nx = b.pnx[p];
-    int tx_x = tx % nx, tx_y = tx / nx;
+    int tx_y = nx == 1 ? tx : div_small(tx, nx), tx_x = tx - tx_y * nx;
     t.plane = p;
     t.txl = txl;
     t.n = n;
@@ -951,7 +1079,7 @@ __device__ __forceinline__ ChunkP chunk_params(const ReconSmem &s, int chk)
     c.b = &b;
     const int k = chk - s.chunk_off[lo];
     const int nx = (b.cw + 7) >> 3;
-    const int ccy = k / nx, ccx = k - ccy * nx;
+    const int ccy = nx == 1 ? k : div_small(k, nx), ccx = k - ccy * nx;
     c.lx0 = b.x + ccx * 8;
     c.ly0 = b.y + ccy * 8;
     c.lw = min(8, b.cw - ccx * 8);
@@ -1312,35 +1440,41 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
             if (A == CVP9_ARITH_REFCPU) {
                 constexpr int kRound = 4;
                 uint8_t *wst = reinterpret_cast<uint8_t *>(s.temp.d) + warp * (kRound * kChunkStage);
+                const int q = lane >> 3, k = lane & 7;
                 for (int base = chk0 + warp; base < chk1; base += kRound * kWarps) {
-#pragma unroll
-                    for (int q = 0; q < kRound; q++) {
-                        const int chk = base + q * kWarps;
-                        if (chk >= chk1) break;
-                        ChunkP c = chunk_params(s, chk);
-                        McGeo g;
-                        if (!(c.b->flags & 1) &&
-                            refcpu_geo(s, *c.b, sbx, sby, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, g))
-                            refcpu_issue(wst + q * kChunkStage, g, c.lw, c.lh, c.clw, c.clh, lane);
+                    /* lane group q works on chunk base + q * kWarps */
+                    const int chk = base + q * kWarps;
+                    const bool have = chk < chk1;
+                    ChunkP c;
+                    McGeo g;
+                    bool inter = false, has_ref = false;
+                    if (have) {
+                        c = chunk_params(s, chk);
+                        inter = !(c.b->flags & 1);
+                        if (inter) {
+                            has_ref = refcpu_geo(s, *c.b, sbx, sby, c.lx0, c.ly0, c.lw, c.lh,
+                                                 c.cx0, c.cy0, c.clw, c.clh, g);
+                            if (has_ref) refcpu_issue8(wst + q * kChunkStage, g, c.lw, c.lh, c.clw, c.clh, k);
+                        }
                     }
                     cp_async_commit();
                     cp_async_wait_all();
                     __syncwarp();
-#pragma unroll
-                    for (int q = 0; q < kRound; q++) {
-                        const int chk = base + q * kWarps;
-                        if (chk >= chk1) break;
-                        ChunkP c = chunk_params(s, chk);
-                        const BlkS &b = *c.b;
-                        McGeo g;
-                        if (b.flags & 1)
-                            predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, c.lx0, c.ly0, c.lw, c.lh,
-                                                   c.cx0, c.cy0, c.clw, c.clh, lane);
-                        else if (refcpu_geo(s, b, sbx, sby, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, g))
-                            refcpu_compute(s, wst + q * kChunkStage, g, c.lx0, c.ly0, c.lw, c.lh,
-                                           c.cx0, c.cy0, c.clw, c.clh, lane);
+                    if (have && inter) {
+                        if (has_ref)
+                            refcpu_compute8(s, wst + q * kChunkStage, g, c.lx0, c.ly0, c.lw, c.lh,
+                                            c.cx0, c.cy0, c.clw, c.clh, k);
                         else
-                            fill_chunk(s, 127, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, lane);
+                            refcpu_fill8(s, 127, c.lx0, c.ly0, c.lw, c.lh, c.cx0, c.cy0, c.clw, c.clh, k);
+                    }
+                    /* intra chunks of this round, one at a time with the whole warp */
+                    const unsigned intra_mask = __ballot_sync(0xffffffffu, have && !inter && k == 0);
+                    for (unsigned m = intra_mask; m; m &= m - 1) {
+                        const int qq = (__ffs(m) - 1) >> 3;
+                        ChunkP ci = chunk_params(s, base + qq * kWarps);
+                        const BlkS &bi = *ci.b;
+                        predict_intra_chunk<A>(s, bi, sbx + bi.x, sby + bi.y, ci.lx0, ci.ly0, ci.lw, ci.lh,
+                                               ci.cx0, ci.cy0, ci.clw, ci.clh, lane);
                     }
                     __syncwarp();
                 }

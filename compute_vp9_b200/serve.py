@@ -1,0 +1,249 @@
+"""Continuous-batching serving loop over the multi-stream engine.
+
+    python -m compute_vp9_b200.serve [--streams 256] [--rate 2] [--speed 20]
+
+Streams arrive as a Poisson process; each carries `frames` frames paced at
+`fps`. A stream is admitted when the engine's HBM budget has room
+(cvp9_batch_open_stream); otherwise it waits in the admission queue and is
+admitted as soon as a finished stream frees its reservation. Every loop
+iteration gathers the frames that are due from all admitted streams — new
+arrivals join the very next step — and reconstructs them in one engine step;
+up to two steps are in flight, so frames that become due while the GPU works
+go into the next step. Latency of a frame = time its reconstructed planes
+reach host memory minus the time it became due. `speed` compresses the
+arrival and pacing schedule (20 = twenty times faster than real time) so a
+run fits in seconds; the GPU work per frame is unchanged.
+
+Resolution mix, GOP and content follow the serving workload: 640x360,
+1280x720, 1920x1080 and 3840x2160 streams in ratio 4:3:2:1, 8-bit 4:2:0,
+GOP 60 with config-1 content. Parsed frames come from a pre-generated pool
+per resolution (pinned host memory), cycled per stream; each stream keeps its
+own reference pool on the device.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import random
+import statistics
+import sys
+import time
+
+import numpy as np
+
+from . import BlockInfo, CVP9_OK, ParsedFrame, Synth, synth_config
+from .batch import Batch
+
+SIZES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+WEIGHTS = [4, 3, 2, 1]
+
+
+class FramePool:
+    """Distinct parsed frames per resolution in one pinned arena; frame 0 of
+    each pool entry is a key frame, the rest inter (GOP handled by index)."""
+
+    def __init__(self, sizes, distinct=8, gop=60, seed=0):
+        import torch
+        self.frames = {}
+        arrays = []
+        for (w, h) in sizes:
+            syn = Synth(synth_config(1, w, h, seed=seed + w, gop=gop))
+            per = []
+            for f in range(distinct):
+                p = syn.frame(f).contents
+                blocks = np.ctypeslib.as_array(C.cast(p.blocks, C.POINTER(C.c_uint8)),
+                                               shape=(p.num_blocks * 32,)).copy()
+                coeffs = np.ctypeslib.as_array(p.coeffs, shape=(p.num_coeffs,)).copy()
+                hdr = ParsedFrame()
+                C.memmove(C.byref(hdr), C.byref(p), C.sizeof(ParsedFrame))
+                per.append((hdr, blocks, coeffs))
+                arrays += [blocks, coeffs.view(np.uint8)]
+            syn.close()
+            self.frames[(w, h)] = per
+        total = sum((a.nbytes + 255) // 256 * 256 for a in arrays)
+        self.arena = torch.empty(total, dtype=torch.uint8, pin_memory=torch.cuda.is_available())
+        view = self.arena.numpy()
+        base = self.arena.data_ptr()
+        off = 0
+        self.pf = {}
+        for key, per in self.frames.items():
+            lst = []
+            for hdr, blocks, coeffs in per:
+                ob = off
+                view[ob:ob + blocks.nbytes] = blocks
+                off += (blocks.nbytes + 255) // 256 * 256
+                oc = off
+                view[oc:oc + coeffs.nbytes] = coeffs.view(np.uint8)
+                off += (coeffs.nbytes + 255) // 256 * 256
+                pf = ParsedFrame()
+                C.memmove(C.byref(pf), C.byref(hdr), C.sizeof(ParsedFrame))
+                pf.blocks = C.cast(C.c_void_p(base + ob), C.POINTER(BlockInfo))
+                pf.coeffs = C.cast(C.c_void_p(base + oc), C.POINTER(C.c_int16))
+                lst.append(pf)
+            self.pf[key] = lst
+        self.distinct = distinct
+        self.gop = gop
+
+    def frame(self, size, index):
+        """Parsed frame for frame `index` of a stream: key frames at GOP
+        boundaries, inter frames cycling through the pool."""
+        lst = self.pf[size]
+        if index % self.gop == 0:
+            return lst[0]
+        return lst[1 + (index - 1) % (self.distinct - 1)]
+
+
+class Stream:
+    def __init__(self, sid_req, size, arrival, frames, fps):
+        self.req = sid_req
+        self.size = size
+        self.arrival = arrival
+        self.frames = frames
+        self.fps = fps
+        self.sid = None
+        self.admit_time = None
+        self.next_frame = 0
+        self.done_frames = 0
+
+    def due(self, i):
+        base = self.admit_time if self.admit_time is not None else self.arrival
+        return base + i / self.fps
+
+
+def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=20.0, hbm_budget=150e9,
+        arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None):
+    """Serve a Poisson arrival of `streams` streams; returns a summary dict.
+    verify_hook(stream_req, frame_index, planes) receives every delivered
+    frame (used by the tests to check bit-exactness in the mix)."""
+    rng = random.Random(seed)
+    sizes = sizes or SIZES
+    weights = weights or WEIGHTS
+    pool = pool or FramePool(sizes)
+    # the set of streams changes from step to step, so kernels are launched
+    # directly rather than replayed from per-shape graphs
+    eng = Batch(arith=arith, hbm_budget=int(hbm_budget), use_graphs=0)
+    # schedule in scaled time
+    t = 0.0
+    pending = []
+    for i in range(streams):
+        t += rng.expovariate(rate) / speed
+        size = rng.choices(sizes, weights)[0]
+        pending.append(Stream(i, size, t, frames, fps * speed))
+    waiting = []          # arrived, not admitted (HBM budget)
+    active = []
+    inflight = []         # (seq, [(stream, frame_index, due_time)])
+    lat = []
+    px = 0
+    steps = 0
+    batch_sizes = []
+    rejected = 0
+    t0 = time.perf_counter()
+
+    def now():
+        return time.perf_counter() - t0
+
+    def reap(block):
+        """Deliver finished steps in order; a step is finished once the
+        engine's completion callback stamped it (host time at which its
+        frames landed in host memory)."""
+        nonlocal px
+        while inflight:
+            seq, items, t_sub = inflight[0]
+            ms = eng.step_latency_ms(seq)
+            if ms is None:
+                if not block:
+                    return
+                if eng.poll() < 0:
+                    raise RuntimeError("step failed: %s" % eng.last_error())
+                time.sleep(0.0001)
+                continue
+            tdone = t_sub + ms / 1000.0
+            for st, fi, due in items:
+                lat.append(1000.0 * (tdone - due))
+                px += st.size[0] * st.size[1]
+                st.done_frames += 1
+                if verify_hook is not None:
+                    rc, arr = eng.get_frame_array(st.sid)
+                    verify_hook(st.req, fi, arr if rc == CVP9_OK else None)
+                if st.done_frames == st.frames:
+                    eng.close_stream(st.sid)
+                    st.sid = None
+            inflight.pop(0)
+            active[:] = [s for s in active if s.done_frames < s.frames]
+            block = False
+
+    while pending or waiting or active or inflight:
+        tn = now()
+        while pending and pending[0].arrival <= tn:
+            waiting.append(pending.pop(0))
+        # admission by HBM budget, first come first served
+        still = []
+        for st in waiting:
+            sid = eng.open_stream(*st.size)
+            if sid is None:
+                still.append(st)
+                rejected += 1
+                continue
+            st.sid = sid
+            st.admit_time = max(st.arrival, tn)
+            active.append(st)
+        waiting = still
+        # gather due frames (one per stream per step)
+        busy = {id(st) for _, items, _ in inflight for st, _, _ in items}
+        ready = [st for st in active if st.next_frame < st.frames and st.due(st.next_frame) <= tn
+                 and id(st) not in busy]
+        if ready and len(inflight) < 2:
+            ready = ready[:max_batch]
+            items = [(st, st.next_frame, st.due(st.next_frame)) for st in ready]
+            t_sub = now()
+            eng.submit([st.sid for st in ready], [C.pointer(pool.frame(st.size, st.next_frame)) for st in ready],
+                       [st.next_frame for st in ready])
+            for st in ready:
+                st.next_frame += 1
+            inflight.append((eng.last_seq(), items, t_sub))
+            steps += 1
+            batch_sizes.append(len(ready))
+            continue
+        if inflight:
+            reap(block=len(inflight) >= 2 or not ready and not pending and not waiting)
+            continue
+        # idle until the next due frame or arrival
+        nxt = [st.due(st.next_frame) for st in active if st.next_frame < st.frames]
+        if pending:
+            nxt.append(pending[0].arrival)
+        if nxt:
+            time.sleep(max(0.0, min(nxt) - now()))
+    wall = now()
+    eng.close()
+    lat.sort()
+    return {
+        "sizes": [list(x) for x in sizes], "weights": list(weights),
+        "streams": streams, "frames_per_stream": frames, "speed": speed,
+        "frames": len(lat), "steps": steps,
+        "mean_batch": statistics.mean(batch_sizes) if batch_sizes else 0,
+        "max_batch": max(batch_sizes) if batch_sizes else 0,
+        "admission_waits": rejected,
+        "p50_ms": lat[len(lat) // 2] if lat else None,
+        "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None,
+        "wall_s": wall, "mpx_per_s": px / wall / 1e6 if wall > 0 else None,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--streams", type=int, default=256)
+    ap.add_argument("--rate", type=float, default=2.0, help="stream arrivals per second (real time)")
+    ap.add_argument("--frames", type=int, default=120)
+    ap.add_argument("--fps", type=float, default=30.0)
+    ap.add_argument("--speed", type=float, default=20.0)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec"])
+    a = ap.parse_args()
+    out = run(a.streams, a.rate, a.frames, a.fps, a.speed, a.budget_gb * 1e9,
+              1 if a.arith == "spec" else 0)
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

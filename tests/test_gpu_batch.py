@@ -101,5 +101,6 @@ def test_admission_budget():
     ids = [eng.open_stream(1920, 1080) for _ in range(4)]
     assert ids[:3] == [0, 1, 2] and ids[3] is None
     eng.close_stream(1)
-    assert eng.open_stream(1920, 1080) == 1
+    assert eng.open_stream(1920, 1080) is not None     # the freed reservation admits one more
+    assert eng.open_stream(1920, 1080) is None
     eng.close()

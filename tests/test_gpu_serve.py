@@ -1,0 +1,49 @@
+"""Continuous-batching serving loop: streams arrive while others decode,
+are admitted by HBM budget, join the next step, and every delivered frame is
+byte-identical to the same stream decoded alone by the oracle."""
+import numpy as np
+import pytest
+
+from compute_vp9_b200 import serve
+from oracle.oracle_py import REFCPU, SPEC, OracleStream
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(192, 128), (256, 144), (320, 192)]
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_served_frames_match_alone(profile):
+    pool = serve.FramePool(SIZES, distinct=4, gop=5)
+    expect = {}
+    seen = []
+
+    def hook(req, fi, arr):
+        assert arr is not None, "frame not delivered"
+        seen.append((req, fi))
+        o = expect.setdefault(req, {"stream": OracleStream(profile), "size": None, "next": 0})
+        assert fi == o["next"], "frames delivered out of order"
+        o["next"] += 1
+        size = sizes_of[req]
+        want = o["stream"].decode(__import__("ctypes").pointer(pool.frame(size, fi)))
+        assert np.array_equal(arr, want), "stream %d frame %d" % (req, fi)
+
+    # admission: a budget for about three streams at a time forces queueing
+    from compute_vp9_b200.batch import Batch
+    budget = 3 * Batch(arith=profile).stream_bytes(320, 192)
+    sizes_of = {}
+    orig = serve.Stream.__init__
+
+    def capture(self, req, size, *a):
+        orig(self, req, size, *a)
+        sizes_of[req] = size
+    serve.Stream.__init__ = capture
+    try:
+        out = serve.run(streams=8, rate=400.0, frames=7, fps=100.0, speed=1.0, hbm_budget=budget,
+                        arith=profile, seed=3, pool=pool, verify_hook=hook, sizes=SIZES, weights=[1, 1, 1])
+    finally:
+        serve.Stream.__init__ = orig
+    assert out["frames"] == 8 * 7 and len(seen) == 8 * 7
+    assert out["admission_waits"] > 0           # the budget made streams wait
+    assert out["max_batch"] > 1                 # frames of several streams shared a step
+    assert out["p99_ms"] is not None
