@@ -10,10 +10,17 @@
  * Per stream the engine keeps the reference pool on the device (up to 12
  * frame buffers; refs are pointer swaps) and its SB done flags, whose epoch
  * advances every frame so they never need clearing.
+ *
+ * Nothing on the submit or admission path calls the driver's allocator:
+ * device and pinned host buffers are carved from two chunked arenas
+ * (arena.h). A stream's buffers are released when a closed slot is recycled
+ * (its last step is complete by then) and a step slot's when they are
+ * outgrown (after the slot's previous step completed).
  */
 #include "cvp9_batch.h"
 #include "backend_common.h"
 #include "recon_launch.h"
+#include "arena.h"
 
 #include <cuda_runtime_api.h>
 #include <stdio.h>
@@ -72,6 +79,7 @@ typedef struct {
     uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status */
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
     uint32_t       *h_tickets; size_t h_tickets_cap;
+    size_t          h_jobs_bytes, d_jobs_bytes, h_misc_bytes, d_misc_bytes;
     cudaGraphExec_t graph; uint64_t graph_key;
     int             n;
     int            *sids;  int sids_cap;
@@ -96,6 +104,8 @@ struct cvp9_batch {
     volatile double lat_done[LAT_RING];
     uint64_t     lat_seq[LAT_RING];
     cvp9_batch_stats_t last;
+    arena_t      dev;        /* device buffers: frames, flags, step inputs      */
+    arena_t      pin;        /* pinned host buffers: downloads, job tables      */
     char         err[192];
 };
 
@@ -142,13 +152,20 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     b->resident_ctas = sms * cvp9_recon_ctas_per_sm(b->device, b->arith);
     {
-        /* frame buffers come from the stream-ordered pool: keep freed memory
-         * cached there instead of returning it at every synchronisation */
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, b->device) == cudaSuccess) {
-            uint64_t keep = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        /* chunk sizes scale with the budget: 2 GB device / 256 MB pinned at
+         * the 150 GB default; the first chunk of each is taken now */
+        uint64_t dc = b->budget / 64, hc = b->budget / 512;
+        b->dev.host = 0;
+        b->dev.chunk_min = dc < (64ull << 20) ? (64ull << 20) : dc > (2ull << 30) ? (2ull << 30) : dc;
+        b->pin.host = 1;
+        b->pin.chunk_min = hc < (16ull << 20) ? (16ull << 20) : hc > (256ull << 20) ? (256ull << 20) : hc;
+        void *p0 = arena_alloc(&b->dev, 1), *p1 = arena_alloc(&b->pin, 1);
+        if (!p0 || !p1) {
+            cvp9_batch_destroy(b);
+            return CVP9_ERR_NOMEM;
         }
+        arena_free(&b->dev, p0, 1);
+        arena_free(&b->pin, p1, 1);
     }
     if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->hs, cudaStreamNonBlocking) != cudaSuccess ||
@@ -175,12 +192,13 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     return CVP9_OK;
 }
 
-static void free_stream(bstream_t *s)
+/* Release a stream slot's buffers (its last step is complete). */
+static void free_stream(cvp9_batch_t *b, bstream_t *s)
 {
-    for (int i = 0; i < MAXF; i++) cudaFree(s->f[i].dev);
-    cudaFree(s->d_sb_done);
-    cudaFreeHost(s->h_out[0]);
-    cudaFreeHost(s->h_out[1]);
+    for (int i = 0; i < MAXF; i++) arena_free(&b->dev, s->f[i].dev, s->f[i].cap);
+    arena_free(&b->dev, s->d_sb_done, (size_t)s->sb_cap * 4);
+    arena_free(&b->pin, s->h_out[0], s->h_out_cap[0]);
+    arena_free(&b->pin, s->h_out[1], s->h_out_cap[1]);
     memset(s, 0, sizeof(*s));
 }
 
@@ -201,20 +219,12 @@ void cvp9_batch_destroy(cvp9_batch_t *b)
         if (s->ev_end) cudaEventDestroy(s->ev_end);
         if (s->ev_cb) cudaEventDestroy(s->ev_cb);
         for (int k = 0; k < 4; k++) if (s->ev_kern[k]) cudaEventDestroy(s->ev_kern[k]);
-        cudaFreeHost(s->h_in);
-        cudaFree(s->d_in);
-        cudaFreeHost(s->h_jobs);
-        cudaFree(s->d_jobs);
-        cudaFree(s->d_sb_range);
-        cudaFree(s->d_misc);
-        cudaFreeHost(s->h_misc);
-        cudaFree(s->d_tickets);
-        cudaFreeHost(s->h_tickets);
         free(s->sids);
     }
-    if (b->st)
-        for (int i = 0; i < b->max_streams; i++)
-            free_stream(&b->st[i]);
+    /* every stream and slot buffer lives in the arenas; the streams were
+     * synchronised above */
+    arena_destroy(&b->dev);
+    arena_destroy(&b->pin);
     free(b->st);
     if (b->ev_t0) cudaEventDestroy(b->ev_t0);
     if (b->ev_t1) cudaEventDestroy(b->ev_t1);
@@ -229,37 +239,61 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
     if (!b || w == 0 || h == 0 || w > 65535 || h > 65535) return CVP9_ERR_INVALID_DATA;
     uint64_t need = cvp9_batch_stream_bytes(w, h);
     if (b->reserved + need > b->budget) return CVP9_ERR_NOMEM;
-    /* prefer a closed slot whose device buffers can be reused as they are
-     * (no cudaMalloc/cudaFree, which would synchronise the device) */
+    /* prefer a closed slot whose buffers can be reused as they are */
     int sid = -1, fresh = -1;
     const int n_sb = (int)(((w + 63) / 64) * ((h + 63) / 64));
+    const size_t fb_need = frame_bytes((int32_t)w, (int32_t)h);
     for (int i = 0; i < b->max_streams; i++) {
         bstream_t *c = &b->st[i];
         if (c->open) continue;
-        if (c->d_sb_done && c->sb_cap >= n_sb && c->f[0].cap >= frame_bytes((int32_t)w, (int32_t)h)) { sid = i; break; }
+        /* smallest closed slot whose buffers fit */
+        if (c->d_sb_done && c->sb_cap >= n_sb && c->h_out_cap[0] >= fb_need &&
+            (sid < 0 || c->sb_cap < b->st[sid].sb_cap)) sid = i;
         if (fresh < 0 && !c->d_sb_done) fresh = i;
     }
     if (sid < 0) sid = fresh;
     if (sid < 0) {   /* every free slot holds buffers of another size: recycle one */
         for (int i = 0; i < b->max_streams; i++) if (!b->st[i].open) { sid = i; break; }
         if (sid < 0) return CVP9_ERR_NOMEM;
-        free_stream(&b->st[sid]);
+        free_stream(b, &b->st[sid]);
     }
     bstream_t *s = &b->st[sid];
     if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
+    /* frames too small for this stream are released now, while idle, so
+     * that acquire_frame only ever fills empty entries */
+    for (int i = 0; i < MAXF; i++)
+        if (s->f[i].dev && s->f[i].cap < fb_need) {
+            arena_free(&b->dev, s->f[i].dev, s->f[i].cap);
+            s->f[i].dev = NULL;
+            s->f[i].cap = 0;
+        }
     if (!s->d_sb_done || s->sb_cap < n_sb) {
-        cudaFree(s->d_sb_done);
-        s->d_sb_done = NULL;
-        if (cudaMalloc((void **)&s->d_sb_done, (size_t)n_sb * 4) != cudaSuccess) {
-            free_stream(s);
+        arena_free(&b->dev, s->d_sb_done, (size_t)s->sb_cap * 4);
+        s->d_sb_done = (uint32_t *)arena_alloc(&b->dev, (size_t)n_sb * 4);
+        s->sb_cap = s->d_sb_done ? n_sb : 0;
+        if (!s->d_sb_done) {
+            free_stream(b, s);
             return CVP9_ERR_NOMEM;
         }
-        s->sb_cap = n_sb;
     }
     /* flags are compared against a per-stream epoch: start from zero */
     if (cudaMemsetAsync(s->d_sb_done, 0, (size_t)n_sb * 4, b->cs) != cudaSuccess) {
-        free_stream(s);
+        free_stream(b, s);
         return CVP9_ERR_NOMEM;
+    }
+    /* both download buffers now, so no pinned allocation happens per step */
+    {
+        size_t fb = frame_bytes((int32_t)w, (int32_t)h);
+        for (int k = 0; k < 2; k++) {
+            if (s->h_out_cap[k] >= fb) continue;
+            arena_free(&b->pin, s->h_out[k], s->h_out_cap[k]);
+            s->h_out[k] = (uint8_t *)arena_alloc(&b->pin, fb);
+            s->h_out_cap[k] = s->h_out[k] ? fb : 0;
+            if (!s->h_out[k]) {
+                free_stream(b, s);
+                return CVP9_ERR_NOMEM;
+            }
+        }
     }
     s->W = (int32_t)w;
     s->H = (int32_t)h;
@@ -289,8 +323,12 @@ cvp9_err_t cvp9_batch_close_stream(cvp9_batch_t *b, int sid)
 {
     if (!b || sid < 0 || sid >= b->max_streams || !b->st[sid].open) return CVP9_ERR_INVALID_DATA;
     bstream_t *s = &b->st[sid];
-    if (stream_busy(b, s)) {
-        cvp9_err_t e = cvp9_batch_wait(b);
+    /* wait for the steps up to this stream's last one only; later steps
+     * keep running */
+    for (uint64_t q = b->done_seq + 1; stream_busy(b, s) && q <= s->last_seq; q++) {
+        bslot_t *o = &b->slot[q % BSLOTS];
+        if (o->seq != q) continue;
+        cvp9_err_t e = wait_slot(b, o);
         if (e == CVP9_ERR_GPU) return e;
     }
     b->reserved -= s->reserved;
@@ -302,27 +340,23 @@ cvp9_err_t cvp9_batch_close_stream(cvp9_batch_t *b, int sid)
     return CVP9_OK;
 }
 
+/* Per-slot buffers grow with 50% headroom; the slot's previous step is
+ * complete when they do, so the old range is idle. */
 static cvp9_err_t grow_dev(cvp9_batch_t *b, void **p, size_t *cap, size_t need)
 {
-    if (*cap >= need) return CVP9_OK;
-    cudaFree(*p);
-    *p = NULL;
-    *cap = 0;
-    size_t n = need + need / 4 + 4096;
-    BCK(cudaMalloc(p, n), "device staging");
-    *cap = n;
+    if (arena_grow(&b->dev, p, cap, need) != 0) {
+        snprintf(b->err, sizeof(b->err), "device arena: no memory for %zu bytes", need);
+        return CVP9_ERR_NOMEM;
+    }
     return CVP9_OK;
 }
 
 static cvp9_err_t grow_host(cvp9_batch_t *b, void **p, size_t *cap, size_t need)
 {
-    if (*cap >= need) return CVP9_OK;
-    cudaFreeHost(*p);
-    *p = NULL;
-    *cap = 0;
-    size_t n = need + need / 4 + 4096;
-    BCK(cudaMallocHost(p, n), "pinned staging");
-    *cap = n;
+    if (arena_grow(&b->pin, p, cap, need) != 0) {
+        snprintf(b->err, sizeof(b->err), "pinned arena: no memory for %zu bytes", need);
+        return CVP9_ERR_NOMEM;
+    }
     return CVP9_OK;
 }
 
@@ -344,13 +378,10 @@ static int acquire_frame(cvp9_batch_t *b, bstream_t *s)
         bslot_t *o = &b->slot[f->d2h_seq % BSLOTS];
         if (o->seq == f->d2h_seq) cudaStreamWaitEvent(b->cs, o->ev_end, 0);
     }
-    if (!f->dev || f->cap < need) {
-        /* stream-ordered: the old buffer is released after the work already
-         * queued on the compute stream, without a device-wide sync */
-        if (f->dev) cudaFreeAsync(f->dev, b->cs);
-        f->dev = NULL;
-        f->cap = 0;
-        if (cudaMallocAsync((void **)&f->dev, need, b->cs) != cudaSuccess) return -1;
+    if (!f->dev) {
+        /* open_stream released every entry smaller than this stream's frames */
+        f->dev = (uint8_t *)arena_alloc(&b->dev, need);
+        if (!f->dev) return -1;
         f->cap = need;
     }
     f->w = s->W;
@@ -485,27 +516,33 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         key = mix64(key, ((uint64_t)st->W << 32) | (uint64_t)st->H);
     }
 
-    /* per-slot buffers */
+    /* per-slot buffers; pinned staging only when some array is pageable */
     if (!dev_in && in_bytes) {
-        if ((err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes)) ||
+        int staged = 0;
+        for (int i = 0; i < n && !staged; i++)
+            staged = (pfs[i]->num_blocks && !is_pinned(pfs[i]->blocks)) ||
+                     (pfs[i]->num_coeffs && !is_pinned(pfs[i]->coeffs));
+        if ((staged && (err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes))) ||
             (err = grow_dev(b, (void **)&s->d_in, &s->d_in_cap, in_bytes)))
             return err;
     }
     if (s->jobs_cap < n) {
-        cudaFreeHost(s->h_jobs);
-        cudaFree(s->d_jobs);
-        s->h_jobs = NULL; s->d_jobs = NULL; s->jobs_cap = 0;
-        BCK(cudaMallocHost((void **)&s->h_jobs, (size_t)n * sizeof(cvp9_job_t)), "job table");
-        BCK(cudaMalloc((void **)&s->d_jobs, (size_t)n * sizeof(cvp9_job_t)), "job table");
-        s->jobs_cap = n;
+        /* sized for every admitted stream at once, so this happens at most
+         * a few times */
+        int cap = n > b->nst ? n : b->nst;
+        s->jobs_cap = 0;
+        if ((err = grow_host(b, (void **)&s->h_jobs, &s->h_jobs_bytes, (size_t)cap * sizeof(cvp9_job_t))) ||
+            (err = grow_dev(b, (void **)&s->d_jobs, &s->d_jobs_bytes, (size_t)cap * sizeof(cvp9_job_t))))
+            return err;
+        s->jobs_cap = cap;
     }
     if (s->misc_cap < n + 1) {
-        cudaFree(s->d_misc);
-        cudaFreeHost(s->h_misc);
-        s->d_misc = NULL; s->h_misc = NULL; s->misc_cap = 0;
-        BCK(cudaMalloc((void **)&s->d_misc, (size_t)(n + 1) * 4), "status words");
-        BCK(cudaMallocHost((void **)&s->h_misc, (size_t)(n + 1) * 4), "status words");
-        s->misc_cap = n + 1;
+        int cap = (n > b->nst ? n : b->nst) + 1;
+        s->misc_cap = 0;
+        if ((err = grow_host(b, (void **)&s->h_misc, &s->h_misc_bytes, (size_t)cap * 4)) ||
+            (err = grow_dev(b, (void **)&s->d_misc, &s->d_misc_bytes, (size_t)cap * 4)))
+            return err;
+        s->misc_cap = cap;
     }
     if ((err = grow_dev(b, (void **)&s->d_sb_range, &s->sb_cap, n_sb * 16))) return err;
     if (s->sids_cap < n) {
@@ -541,8 +578,11 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     const uint8_t **dbp = n <= 256 ? dev_blocks : malloc((size_t)n * sizeof(void *));
     const uint8_t **dcp = n <= 256 ? dev_coeffs : malloc((size_t)n * sizeof(void *));
     if (!dbp || !dcp) return CVP9_ERR_NOMEM;
-    struct { const void *src; size_t off, n; } direct[512];
-    int ndirect = 0;
+    typedef struct { const void *src; size_t off, n; } direct_t;
+    direct_t direct_local[512];
+    direct_t *direct = n <= 256 ? direct_local : malloc((size_t)2 * n * sizeof(direct_t));
+    if (!direct) return CVP9_ERR_NOMEM;
+    int ndirect = 0, any_staged = 0;
     for (int i = 0; i < n; i++) {
         const vp9_parsed_frame_t *pf = pfs[i];
         if (dev_in) {
@@ -556,31 +596,39 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         size_t lens[2] = { nbb, ncb };
         for (int k = 0; k < 2; k++) {
             if (lens[k]) {
-                if (ndirect < 512 && is_pinned(srcs[k])) {
+                if (is_pinned(srcs[k])) {
                     direct[ndirect].src = srcs[k];
                     direct[ndirect].off = off;
                     direct[ndirect].n = lens[k];
                     ndirect++;
                 } else {
+                    /* h_in was sized above because a pageable array exists */
                     memcpy(s->h_in + off, srcs[k], lens[k]);
+                    any_staged = 1;
                 }
             }
             (k == 0 ? dbp : dcp)[i] = s->d_in + off;
             off += ALIGN_UP(lens[k], 256);
         }
     }
+    cudaError_t ue = cudaSuccess;
     if (!dev_in && off) {
         /* staged ranges go up in one copy; direct copies land afterwards */
-        int any_staged = ndirect < 2 * n;
         if (any_staged) {
-            BCK(cudaMemcpyAsync(s->d_in, s->h_in, off, cudaMemcpyHostToDevice, b->hs), "upload inputs");
+            ue = cudaMemcpyAsync(s->d_in, s->h_in, off, cudaMemcpyHostToDevice, b->hs);
             s->h2d_bytes += off;
         }
-        for (int k = 0; k < ndirect; k++) {
-            BCK(cudaMemcpyAsync(s->d_in + direct[k].off, direct[k].src, direct[k].n,
-                                cudaMemcpyHostToDevice, b->hs), "upload pinned inputs");
+        for (int k = 0; k < ndirect && ue == cudaSuccess; k++) {
+            ue = cudaMemcpyAsync(s->d_in + direct[k].off, direct[k].src, direct[k].n,
+                                 cudaMemcpyHostToDevice, b->hs);
             if (!any_staged) s->h2d_bytes += direct[k].n;
         }
+    }
+    if (direct != direct_local) free(direct);
+    if (ue != cudaSuccess) {
+        if (dbp != dev_blocks) free(dbp);
+        if (dcp != dev_coeffs) free(dcp);
+        return bfail(b, ue, "upload inputs");
     }
 
     /* jobs, outputs, reference pools */

@@ -112,10 +112,13 @@ class Stream:
 
 
 def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=20.0, hbm_budget=150e9,
-        arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None):
+        arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None,
+        trace=None):
     """Serve a Poisson arrival of `streams` streams; returns a summary dict.
     verify_hook(stream_req, frame_index, planes) receives every delivered
-    frame (used by the tests to check bit-exactness in the mix)."""
+    frame (used by the tests to check bit-exactness in the mix). If `trace` is
+    a list, one tuple (stream, width, height, frame_index, due_s, submit_s,
+    done_s, step_seq, step_frames) per delivered frame is appended to it."""
     rng = random.Random(seed)
     sizes = sizes or SIZES
     weights = weights or WEIGHTS
@@ -161,6 +164,8 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=20.0, hbm_budget=150e
             tdone = t_sub + ms / 1000.0
             for st, fi, due in items:
                 lat.append(1000.0 * (tdone - due))
+                if trace is not None:
+                    trace.append((st.req, st.size[0], st.size[1], fi, due, t_sub, tdone, seq, len(items)))
                 px += st.size[0] * st.size[1]
                 st.done_frames += 1
                 if verify_hook is not None:
