@@ -86,6 +86,13 @@ int cvp9_env_device(void)
     return e && *e ? atoi(e) : 0;
 }
 
+int cvp9_env_inter_fast(void)
+{
+    const char *e = getenv("CVP9_INTER_FAST");
+    if (e && (*e == '0' || *e == '1' || *e == '2') && !e[1]) return *e - '0';
+    return 1;
+}
+
 int cvp9_env_arith(void)
 {
     const char *e = getenv("CVP9_ARITH");

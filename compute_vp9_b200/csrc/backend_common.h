@@ -35,9 +35,12 @@ int cvp9_tickets_on_diagonal(int sb_cols, int sb_rows, int job, int d, uint32_t 
 int cvp9_dc_q(int qindex);
 int cvp9_ac_q(int qindex);
 
-/* Environment knobs: $CVP9_CUDA_DEVICE, $CVP9_ARITH (refcpu|spec). */
+/* Environment knobs: $CVP9_CUDA_DEVICE, $CVP9_ARITH (refcpu|spec),
+ * $CVP9_INTER_FAST (warp-per-superblock inter path: 0 off, 1 the
+ * 96-register kernel, 2 the 80-register kernel; default 1). */
 int cvp9_env_device(void);
 int cvp9_env_arith(void);
+int cvp9_env_inter_fast(void);
 
 /* Fill the frame-geometry and parameter fields of a job from a parsed
  * frame (inputs, output, refs and scratch pointers are set by the caller). */

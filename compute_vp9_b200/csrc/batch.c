@@ -79,6 +79,7 @@ typedef struct {
     uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status */
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
     uint32_t       *h_tickets; size_t h_tickets_cap;
+    uint32_t       *d_fast; size_t fast_cap;    /* inter fast path: flags, tickets, count */
     size_t          h_jobs_bytes, d_jobs_bytes, h_misc_bytes, d_misc_bytes;
     cudaGraphExec_t graph; uint64_t graph_key;
     int             n;
@@ -88,7 +89,7 @@ typedef struct {
 } bslot_t;
 
 struct cvp9_batch {
-    int          device, arith, use_graphs, max_streams;
+    int          device, arith, use_graphs, max_streams, inter_fast;
     uint64_t     budget, reserved;
     cudaStream_t cs, hs, ds;
     bstream_t   *st;
@@ -145,6 +146,7 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     b->budget = (cfg && cfg->hbm_budget) ? cfg->hbm_budget : 150ull * 1000 * 1000 * 1000;
     b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
     b->use_graphs = cfg ? cfg->use_graphs : 1;
+    b->inter_fast = cvp9_env_inter_fast();
     if (b->device >= ndev || cvp9_device_setup(b->device) != 0) { free(b); return CVP9_ERR_NO_BACKEND; }
     b->st = calloc((size_t)b->max_streams, sizeof(bstream_t));
     if (!b->st) { free(b); return CVP9_ERR_NOMEM; }
@@ -545,6 +547,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         s->misc_cap = cap;
     }
     if ((err = grow_dev(b, (void **)&s->d_sb_range, &s->sb_cap, n_sb * 16))) return err;
+    if ((err = grow_dev(b, (void **)&s->d_fast, &s->fast_cap, (2 * n_sb + 1) * 4))) return err;
     if (s->sids_cap < n) {
         free(s->sids);
         s->sids = malloc((size_t)n * sizeof(int));
@@ -688,6 +691,12 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     L.n_tickets = s->n_tickets;
     L.ticket_counter = s->d_misc;
     L.recon_ctas = (int)s->n_tickets < b->resident_ctas ? (int)s->n_tickets : b->resident_ctas;
+    if (b->inter_fast) {
+        L.general = s->d_fast;
+        L.general_tickets = s->d_fast + s->n_tickets;
+        L.n_general = s->d_fast + 2 * (size_t)s->n_tickets;
+        L.inter_variant = b->inter_fast;
+    }
     L.lf_tiles_x = lf_tx;
     L.lf_tiles_y = lf_ty;
     L.flat_lf_max_w = flat_w;
@@ -697,7 +706,9 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     uint64_t gkey = mix64(mix64(mix64(key, (uint64_t)(uintptr_t)s->d_jobs), (uint64_t)(uintptr_t)s->d_sb_range),
                           mix64((uint64_t)(uintptr_t)s->d_misc, (uint64_t)(uintptr_t)s->d_tickets));
     gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
-    s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + (lf_tx > 0) + (flat_w > 0 ? 2 : 0));
+    gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
+    s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + (lf_tx > 0) + (flat_w > 0 ? 2 : 0) +
+                             (L.general && b->arith == CVP9_ARITH_REFCPU ? 2 : 0));
     if (b->use_graphs) {
         if (!s->graph || s->graph_key != gkey) {
             if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = NULL; }

@@ -64,6 +64,8 @@ typedef struct {
     uint32_t    *d_sb_done;            /* n_sb                          */
     uint32_t    *d_misc;               /* [0] status, [1] ticket counter */
     uint32_t    *d_tickets;
+    uint32_t    *d_fast;               /* inter fast path: general flags, tickets, count */
+    int          inter_fast;
     uint32_t     n_tickets;
     int          recon_ctas;
     slot_t       slots[CVP9_CUDA_INFLIGHT];
@@ -104,7 +106,8 @@ static void free_geometry(cuctx_t *c)
     cudaFree(c->d_sb_range);
     cudaFree(c->d_sb_done);
     cudaFree(c->d_tickets);
-    c->d_sb_range = c->d_sb_done = c->d_tickets = NULL;
+    cudaFree(c->d_fast);
+    c->d_sb_range = c->d_sb_done = c->d_tickets = c->d_fast = NULL;
     c->n_tickets = 0;
 }
 
@@ -119,6 +122,7 @@ cvp9_err_t cuda_backend_init_ex(void **out, const cuda_backend_options_t *opt)
     c->device = (opt && opt->device >= 0) ? opt->device : cvp9_env_device();
     c->arith = (opt && opt->arith >= 0) ? (opt->arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU)
                                         : cvp9_env_arith();
+    c->inter_fast = cvp9_env_inter_fast();
     if (c->device >= dev_count || cvp9_device_setup(c->device) != 0) { free(c); return CVP9_ERR_NO_BACKEND; }
     for (int i = 0; i < 8; i++) c->ref_slot[i] = -1;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -177,6 +181,7 @@ static cvp9_err_t set_geometry(cuctx_t *c, int32_t W, int32_t H)
     CK(cudaMalloc((void **)&c->d_sb_done, (size_t)c->n_sb * 4), "alloc sb_done");
     CK(cudaMemset(c->d_sb_done, 0, (size_t)c->n_sb * 4), "clear sb_done");
     CK(cudaMalloc((void **)&c->d_tickets, (size_t)c->n_sb * 4), "alloc tickets");
+    CK(cudaMalloc((void **)&c->d_fast, (size_t)(2 * c->n_sb + 1) * 4), "alloc fast-path scratch");
     uint32_t *t = malloc((size_t)c->n_sb * 4);
     if (!t) return CVP9_ERR_NOMEM;
     uint32_t n = 0;
@@ -324,6 +329,12 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     L.n_tickets = c->n_tickets;
     L.ticket_counter = c->d_misc + 1;
     L.recon_ctas = c->recon_ctas;
+    if (c->inter_fast) {
+        L.general = c->d_fast;
+        L.general_tickets = c->d_fast + c->n_sb;
+        L.n_general = c->d_fast + 2 * c->n_sb;
+        L.inter_variant = c->inter_fast;
+    }
     if (job->lf_tiled) {
         L.lf_tiles_x = (W + 4 + 63) / 64;
         L.lf_tiles_y = (H + 4 + 63) / 64;

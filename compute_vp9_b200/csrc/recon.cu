@@ -34,6 +34,7 @@
  * latency.
  */
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "recon_job.h"
@@ -1127,8 +1128,11 @@ __global__ void __launch_bounds__(256) k_scan_blocks(const cvp9_job_t *__restric
 template <int A>
 __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restrict__ jobs,
                                                    const uint32_t *__restrict__ tickets,
-                                                   uint32_t n_tickets, uint32_t *ticket_counter)
+                                                   uint32_t n_tickets, uint32_t *ticket_counter,
+                                                   const uint32_t *__restrict__ n_dev)
 {
+    /* with the inter fast path the general ticket count is known on the device */
+    if (n_dev) n_tickets = *n_dev;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ReconSmem &s = *reinterpret_cast<ReconSmem *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1600,6 +1604,690 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
     }
 }
 
+/* ── Inter-only superblocks: one warp per SB ─────────────────────────────
+ *
+ * Most superblocks of an inter frame hold inter blocks only; nothing in them
+ * depends on another superblock of the same frame. k_inter gives each such
+ * SB to one warp, which predicts and adds the residual in a per-warp tile
+ * and writes the tile once, with no CTA barriers and no dependency analysis.
+ * An SB the warp cannot take (an intra block, a block outside the supported
+ * domain, overlapping blocks, uncovered 4x4 cells, more than 64 blocks) is
+ * marked general and left to k_recon, which k_compact feeds with the general
+ * tickets in their original SB-diagonal order. k_inter releases the done
+ * flag of every SB it finishes, so general SBs that wait on a neighbour see
+ * it done. The arithmetic is the REFCPU profile of k_recon, term for term. */
+
+namespace {
+
+constexpr int kFastWarps = 4;                     /* SBs per CTA */
+
+/* One block, 12 bytes. geo: x/4 | y/4 << 4 | clamped cw << 8 | ch << 15 |
+ * reference slot << 22 (15: none) | tx_size << 26 | skip << 28. */
+struct FastBlk {
+    uint32_t geo;
+    uint32_t mv;      /* mv[0]: col in the low half, row in the high half (1/8 pel) */
+    uint32_t coeff;   /* first coefficient of the block */
+};
+
+__device__ __forceinline__ int fb_x(const FastBlk &b) { return (int)(b.geo & 0xfu) << 2; }
+__device__ __forceinline__ int fb_y(const FastBlk &b) { return (int)((b.geo >> 4) & 0xfu) << 2; }
+__device__ __forceinline__ int fb_cw(const FastBlk &b) { return (int)((b.geo >> 8) & 0x7fu); }
+__device__ __forceinline__ int fb_ch(const FastBlk &b) { return (int)((b.geo >> 15) & 0x7fu); }
+__device__ __forceinline__ int fb_slot(const FastBlk &b) { return (int)((b.geo >> 22) & 0xfu); }
+__device__ __forceinline__ int fb_txl(const FastBlk &b) { return (int)((b.geo >> 26) & 3u); }
+__device__ __forceinline__ bool fb_skip(const FastBlk &b) { return (b.geo >> 28) & 1u; }
+
+struct __align__(16) FastSmem {                   /* one per warp; 16-byte vector access */
+    uint8_t  ty[64 * 64];                         /* luma tile, pitch 64 */
+    uint8_t  tu[32 * 32];
+    uint8_t  tv[32 * 32];
+    union {
+        int16_t  coef[1024];                      /* residual: coefficients of the TXs in flight */
+        uint32_t cells[8];                        /* set-up: 4x4-cell occupancy, 2 cell rows per word */
+    };
+    FastBlk  blk[64];
+    union {
+        struct {                                  /* prediction */
+            uint16_t choff[65];                   /* first chunk of each block */
+            uint8_t  chblk[128];                  /* chunk -> block */
+        };
+        struct {                                  /* residual, per TX size */
+            uint16_t txoff[65];                   /* first TX of each block */
+            uint8_t  txblk[256];                  /* TX -> block */
+        };
+    };
+};
+
+/* The basis again in global memory: lane-varying reads are served by L1
+ * instead of being serialised by the constant cache. */
+__device__ double g_dct[16 + 64 + 256 + 1024];
+
+static_assert(sizeof(FastSmem) % 16 == 0, "per-warp tiles must stay 16-byte aligned");
+static_assert(sizeof(FastSmem) * kFastWarps + 1024 <= 233472 / 6, "six CTAs of k_inter per SM");
+static_assert(offsetof(FastSmem, coef) % 16 == 0 && offsetof(FastSmem, tu) % 16 == 0 &&
+              offsetof(FastSmem, tv) % 16 == 0, "vector-accessed members must be 16-byte aligned");
+
+__device__ __forceinline__ int warp_incl_scan(int x, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+/* Bytes r[0..8] of a row at p, as r0..r3 / r4..r7 / r8 in three words,
+ * from aligned word reads (callers keep the aligned span inside the buffer). */
+__device__ __forceinline__ void ld9w(const uint8_t *p, uint32_t &lo, uint32_t &mid, uint32_t &hi)
+{
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    const unsigned sh = 8u * (unsigned)(a & 3);
+    const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+    lo = __funnelshift_r(w0, w1, sh);
+    mid = __funnelshift_r(w1, w2, sh);
+    hi = w2 >> sh;
+}
+
+/* The same nine bytes with every sample clamped into [0, pw-1] x [0, ph-1]. */
+__device__ __forceinline__ void ld9c(const uint8_t *plane, int pw, int ph, int x0, int y,
+                                     uint32_t &lo, uint32_t &mid, uint32_t &hi)
+{
+    const uint8_t *row = plane + (size_t)clampi(y, 0, ph - 1) * pw;
+    uint32_t v[3] = { 0, 0, 0 };
+#pragma unroll
+    for (int x = 0; x < 9; x++) v[x >> 2] |= (uint32_t)__ldg(row + clampi(x0 + x, 0, pw - 1)) << (8 * (x & 3));
+    lo = v[0]; mid = v[1]; hi = v[2];
+}
+
+__device__ __forceinline__ void ld5w(const uint8_t *p, uint32_t &lo, uint32_t &hi)
+{
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    const unsigned sh = 8u * (unsigned)(a & 3);
+    const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1);
+    lo = __funnelshift_r(w0, w1, sh);
+    hi = w1 >> sh;
+}
+
+/* five chroma bytes, clamped into [0, cw-1] x [0, ch-1] (cw, ch may be 0) */
+__device__ __forceinline__ void ld5c(const uint8_t *plane, int stride, int cw, int ch, int x0, int y,
+                                     uint32_t &lo, uint32_t &hi)
+{
+    const int xm = cw > 0 ? cw - 1 : 0, ym = ch > 0 ? ch - 1 : 0;
+    const uint8_t *row = plane + (size_t)clampi(y, 0, ym) * stride;
+    uint32_t v[2] = { 0, 0 };
+#pragma unroll
+    for (int x = 0; x < 5; x++) v[x >> 2] |= (uint32_t)__ldg(row + clampi(x0 + x, 0, xm)) << (8 * (x & 3));
+    lo = v[0]; hi = v[1];
+}
+
+/* Two-stage bilinear of vp9_reconstruct.c:105-128 on two samples at once:
+ * (a (8-f) + b f + 4) >> 3 per 16-bit field; every intermediate is below
+ * 2^11, so fields never carry into each other. */
+__device__ __forceinline__ uint32_t bil2(uint32_t a, uint32_t b, uint32_t wa, uint32_t wb)
+{
+    return ((a * wa + b * wb + 0x00040004u) >> 3) & 0x00ff00ffu;
+}
+
+/* Eight luma samples of one row from rows r (lo0 mid0 hi0) and r+1. */
+__device__ __forceinline__ void bilinear8(uint32_t lo0, uint32_t mid0, uint32_t hi0,
+                                          uint32_t lo1, uint32_t mid1, uint32_t hi1,
+                                          int fx, int fy, uint32_t &o0, uint32_t &o1)
+{
+    const uint32_t wx = 8u - (uint32_t)fx, ux = (uint32_t)fx, wy = 8u - (uint32_t)fy, uy = (uint32_t)fy;
+    /* fields (r[2k], r[2k+1]) and (r[2k+1], r[2k+2]) */
+    const uint32_t s0 = __funnelshift_r(lo0, mid0, 8), t0 = __funnelshift_r(mid0, hi0, 8);
+    const uint32_t s1 = __funnelshift_r(lo1, mid1, 8), t1 = __funnelshift_r(mid1, hi1, 8);
+    const uint32_t h00 = bil2(__byte_perm(lo0, 0, 0x4140), __byte_perm(s0, 0, 0x4140), wx, ux);
+    const uint32_t h01 = bil2(__byte_perm(lo0, 0, 0x4342), __byte_perm(s0, 0, 0x4342), wx, ux);
+    const uint32_t h02 = bil2(__byte_perm(mid0, 0, 0x4140), __byte_perm(t0, 0, 0x4140), wx, ux);
+    const uint32_t h03 = bil2(__byte_perm(mid0, 0, 0x4342), __byte_perm(t0, 0, 0x4342), wx, ux);
+    const uint32_t h10 = bil2(__byte_perm(lo1, 0, 0x4140), __byte_perm(s1, 0, 0x4140), wx, ux);
+    const uint32_t h11 = bil2(__byte_perm(lo1, 0, 0x4342), __byte_perm(s1, 0, 0x4342), wx, ux);
+    const uint32_t h12 = bil2(__byte_perm(mid1, 0, 0x4140), __byte_perm(t1, 0, 0x4140), wx, ux);
+    const uint32_t h13 = bil2(__byte_perm(mid1, 0, 0x4342), __byte_perm(t1, 0, 0x4342), wx, ux);
+    const uint32_t v0 = bil2(h00, h10, wy, uy), v1 = bil2(h01, h11, wy, uy);
+    const uint32_t v2 = bil2(h02, h12, wy, uy), v3 = bil2(h03, h13, wy, uy);
+    o0 = __byte_perm(v0, v1, 0x6420);
+    o1 = __byte_perm(v2, v3, 0x6420);
+}
+
+/* Four chroma samples from rows r (lo0 hi0: bytes 0..4) and r+1. */
+__device__ __forceinline__ uint32_t bilinear4(uint32_t lo0, uint32_t hi0, uint32_t lo1, uint32_t hi1,
+                                              int fx, int fy)
+{
+    const uint32_t wx = 8u - (uint32_t)fx, ux = (uint32_t)fx, wy = 8u - (uint32_t)fy, uy = (uint32_t)fy;
+    const uint32_t s0 = __funnelshift_r(lo0, hi0, 8), s1 = __funnelshift_r(lo1, hi1, 8);
+    const uint32_t h00 = bil2(__byte_perm(lo0, 0, 0x4140), __byte_perm(s0, 0, 0x4140), wx, ux);
+    const uint32_t h01 = bil2(__byte_perm(lo0, 0, 0x4342), __byte_perm(s0, 0, 0x4342), wx, ux);
+    const uint32_t h10 = bil2(__byte_perm(lo1, 0, 0x4140), __byte_perm(s1, 0, 0x4140), wx, ux);
+    const uint32_t h11 = bil2(__byte_perm(lo1, 0, 0x4342), __byte_perm(s1, 0, 0x4342), wx, ux);
+    return __byte_perm(bil2(h00, h10, wy, uy), bil2(h01, h11, wy, uy), 0x6420);
+}
+
+/* One lane's share of a prediction pass, split so that a warp can issue the
+ * reads of two passes before computing either. */
+struct FastLuma {
+    uint8_t *d;
+    int lw, fx, fy;
+    bool act, ref;
+    uint32_t lo0, mid0, hi0, lo1, mid1, hi1;
+};
+
+struct FastChroma {
+    uint8_t *d;
+    int clw, fx, fy;
+    bool act, ref;
+    uint32_t lo0, hi0, lo1, hi1;
+};
+
+/* Chunk k of block b: its 8x8 luma and 4x4 chroma regions (clipped). */
+__device__ __forceinline__ void fast_chunk(const FastSmem &w, int c, FastBlk &fb, int &lx0, int &ly0, int &lw,
+                                           int &lh, int &cx0, int &cy0, int &clw, int &clh)
+{
+    const int b = w.chblk[c];
+    fb = w.blk[b];
+    const int bx = fb_x(fb), by = fb_y(fb), cw = fb_cw(fb), ch = fb_ch(fb);
+    const int k = c - w.choff[b];
+    const int nx = (cw + 7) >> 3;
+    const int ccy = nx == 1 ? k : div_small(k, nx), ccx = k - ccy * nx;
+    lx0 = bx + ccx * 8;
+    ly0 = by + ccy * 8;
+    lw = min(8, cw - ccx * 8);
+    lh = min(8, ch - ccy * 8);
+    cx0 = (bx >> 1) + ccx * 4;
+    cy0 = (by >> 1) + ccy * 4;
+    clw = min(4, ((cw + 1) >> 1) - ccx * 4);
+    clh = min(4, ((ch + 1) >> 1) - ccy * 4);
+}
+
+__device__ __forceinline__ FastLuma fast_luma_issue(FastSmem &w, const cvp9_job_t &job, int c, int kk,
+                                                   int nchunks, int sbx, int sby)
+{
+    FastLuma J;
+    J.act = false;
+    J.ref = false;
+    if (c >= nchunks) return J;
+    FastBlk fb;
+    int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
+    fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
+    if (kk >= lh) return J;
+    J.act = true;
+    J.d = w.ty + (ly0 + kk) * 64 + lx0;
+    J.lw = lw;
+    const int slot = fb_slot(fb);
+    if (slot >= 8) return J;
+    const cvp9_ref_t &R = job.ref[slot];
+    const uint8_t *rp = R.plane;
+    if (!rp) return J;
+    J.ref = true;
+    const int rw = R.w, rh = R.h;
+    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+    const int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
+    const int ix = px8 >> 3, iy = py8 >> 3;
+    J.fx = px8 & 7;
+    J.fy = py8 & 7;
+    const int y0 = iy + kk;
+    if (ix >= 0 && ix + lw < rw && y0 >= 0 && y0 + 1 < rh) {
+        /* luma rows are followed by the chroma planes: the word reads past
+         * a row end stay inside the frame */
+        ld9w(rp + (size_t)y0 * rw + ix, J.lo0, J.mid0, J.hi0);
+        ld9w(rp + (size_t)(y0 + 1) * rw + ix, J.lo1, J.mid1, J.hi1);
+    } else {
+        ld9c(rp, rw, rh, ix, y0, J.lo0, J.mid0, J.hi0);
+        ld9c(rp, rw, rh, ix, y0 + 1, J.lo1, J.mid1, J.hi1);
+    }
+    return J;
+}
+
+__device__ __forceinline__ void fast_luma_finish(const FastLuma &J)
+{
+    if (!J.act) return;
+    uint32_t o0 = 0x7f7f7f7fu, o1 = 0x7f7f7f7fu;     /* missing reference: 127 */
+    if (J.ref) bilinear8(J.lo0, J.mid0, J.hi0, J.lo1, J.mid1, J.hi1, J.fx, J.fy, o0, o1);
+    if (J.lw == 8) {
+        reinterpret_cast<uint32_t *>(J.d)[0] = o0;
+        reinterpret_cast<uint32_t *>(J.d)[1] = o1;
+    } else {
+#pragma unroll
+        for (int x = 0; x < 8; x++) if (x < J.lw) J.d[x] = (uint8_t)((x < 4 ? o0 : o1) >> (8 * (x & 3)));
+    }
+}
+
+__device__ __forceinline__ FastChroma fast_chroma_issue(FastSmem &w, const cvp9_job_t &job, int c, int p, int r,
+                                                       int nchunks, int sbx, int sby)
+{
+    FastChroma J;
+    J.act = false;
+    J.ref = false;
+    if (c >= nchunks) return J;
+    FastBlk fb;
+    int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
+    fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
+    if (r >= clh || clw <= 0) return J;
+    J.act = true;
+    J.d = (p ? w.tv : w.tu) + (cy0 + r) * 32 + cx0;
+    J.clw = clw;
+    const int slot = fb_slot(fb);
+    if (slot >= 8) return J;
+    const cvp9_ref_t &R = job.ref[slot];
+    const uint8_t *rp = R.plane;
+    if (!rp) return J;
+    J.ref = true;
+    const int rw = R.w, rh = R.h;
+    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+    const int rcs = (rw + 1) >> 1, crw = rw >> 1, crh = rh >> 1;
+    const uint8_t *pl = rp + (size_t)rw * rh + (p ? (size_t)rcs * ((rh + 1) >> 1) : 0);
+    const int cmx = mvx / 2, cmy = mvy / 2;          /* halves toward zero */
+    const int cpx8 = ((sbx >> 1) + cx0) * 8 + cmx, cpy8 = ((sby >> 1) + cy0) * 8 + cmy;
+    const int cix = cpx8 >> 3, ciy = cpy8 >> 3;
+    J.fx = cpx8 & 7;
+    J.fy = cpy8 & 7;
+    const int y0 = ciy + r;
+    if (cix >= 0 && cix + clw < crw && y0 >= 0 && y0 + 2 < crh) {
+        /* a further chroma row exists below: word reads stay inside */
+        ld5w(pl + (size_t)y0 * rcs + cix, J.lo0, J.hi0);
+        ld5w(pl + (size_t)(y0 + 1) * rcs + cix, J.lo1, J.hi1);
+    } else {
+        ld5c(pl, rcs, crw, crh, cix, y0, J.lo0, J.hi0);
+        ld5c(pl, rcs, crw, crh, cix, y0 + 1, J.lo1, J.hi1);
+    }
+    return J;
+}
+
+__device__ __forceinline__ void fast_chroma_finish(const FastChroma &J)
+{
+    if (!J.act) return;
+    const uint32_t o = J.ref ? bilinear4(J.lo0, J.hi0, J.lo1, J.hi1, J.fx, J.fy) : 0x7f7f7f7fu;
+    if (J.clw == 4 && !((uintptr_t)J.d & 3)) {
+        *reinterpret_cast<uint32_t *>(J.d) = o;
+    } else {
+#pragma unroll
+        for (int x = 0; x < 4; x++) if (x < J.clw) J.d[x] = (uint8_t)(o >> (8 * x));
+    }
+}
+
+/* Where the q-th TX of size N in the SB sits; `ok` is false past the last
+ * TX or when the TX's coefficients run past the array. */
+template <int N>
+__device__ __forceinline__ const int16_t *fast_tx_locate(const FastSmem &w, const cvp9_job_t &job, int q, int ntx,
+                                                        int i, int &px0, int &py0, bool &ok)
+{
+    ok = false;
+    px0 = py0 = 0;
+    if (q >= ntx) return nullptr;
+    const int b = w.txblk[q];
+    const FastBlk fb = w.blk[b];
+    const int bx = fb_x(fb), by = fb_y(fb), cw = fb_cw(fb);
+    const int nx = cw / N;
+    const int tq = q - w.txoff[b];
+    const int tyy = nx == 1 ? tq : tq / nx, txx = tq - tyy * nx;
+    px0 = bx + txx * N;
+    py0 = by + tyy * N;
+    const uint64_t c0 = (uint64_t)fb.coeff + (uint64_t)tq * (N * N);
+    if (c0 + N * N > (uint64_t)job.num_coeffs) return nullptr;
+    ok = true;
+    return job.coeffs + c0 + (uint64_t)i * N;
+}
+
+/* one TX row (N int16) into registers, widest loads the alignment allows */
+template <int N>
+__device__ __forceinline__ void fast_row_load(uint32_t (&v)[N / 2], const int16_t *src)
+{
+    const uintptr_t a = (uintptr_t)src;
+    if (N >= 8 && !(a & 15)) {
+#pragma unroll
+        for (int k = 0; k < N / 8; k++) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(src) + k);
+            v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
+        }
+    } else if (!(a & 3)) {
+#pragma unroll
+        for (int k = 0; k < N / 2; k++) v[k] = __ldg(reinterpret_cast<const uint32_t *>(src) + k);
+    } else {
+#pragma unroll
+        for (int k = 0; k < N / 2; k++)
+            v[k] = (uint32_t)(uint16_t)__ldg(src + 2 * k) | (uint32_t)(uint16_t)__ldg(src + 2 * k + 1) << 16;
+    }
+}
+
+/* REFCPU residual of every luma TX of size N in the SB. 32/N TXs at a time,
+ * lane = (TX, row i). A lane forms T[i][k] = sum_l M[l][i] X[l][k] (l
+ * ascending) for each nonzero column k and accumulates O[i][j] += T[i][k]
+ * M[k][j] (k ascending) — the two passes of vp9_reconstruct.c:31-50 fused
+ * per row. The loops run over the union of the group's nonzero rows and
+ * columns so they stay warp-uniform; a term whose coefficient is zero in a
+ * lane's own TX adds +-0 to a sum that is never -0, leaving it unchanged.
+ * The next group's coefficients are loaded while the current one computes. */
+template <int N>
+__device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int lane)
+{
+    constexpr int G = 32 / N, NN = N * N;
+    constexpr int NH = N == 32 ? 2 : 1, NJ = N / NH;
+    constexpr unsigned kSeg = N == 32 ? 0xffffffffu : ((1u << N) - 1u);
+    const int g = lane / N, i = lane % N;
+    const int boff = N == 4 ? 0 : N == 8 ? 16 : N == 16 ? 80 : 336;
+    const double *Mg = g_dct + boff;     /* lane-varying reads */
+    const double *Mc = c_dct + boff;     /* warp-uniform reads */
+    int16_t *X = w.coef + g * NN;
+    uint32_t rv[N / 2];
+    int px0, py0;
+    bool have;
+    {
+        const int16_t *src = fast_tx_locate<N>(w, job, g, ntx, i, px0, py0, have);
+        if (have) fast_row_load<N>(rv, src);
+    }
+    for (int q0 = 0; q0 < ntx; q0 += G) {
+        if (have) {
+            uint32_t *dst = reinterpret_cast<uint32_t *>(X + i * N);
+#pragma unroll
+            for (int k = 0; k < N / 2; k++) dst[k] = rv[k];
+        }
+        __syncwarp();
+        int npx0, npy0;
+        bool nhave;
+        {
+            const int16_t *src = fast_tx_locate<N>(w, job, q0 + G + g, ntx, i, npx0, npy0, nhave);
+            if (nhave) fast_row_load<N>(rv, src);
+        }
+        uint32_t cm = 0;                     /* nonzero rows of column i of this lane's TX */
+        if (have) {
+#pragma unroll
+            for (int l = 0; l < N; l++) cm |= (X[l * N + i] != 0 ? 1u : 0u) << l;
+        }
+        const unsigned nzl = __ballot_sync(0xffffffffu, cm != 0);
+        unsigned U = 0;
+#pragma unroll
+        for (int s = 0; s < G; s++) U |= nzl >> (s * N);
+        U &= kSeg;
+        if (U) {
+#pragma unroll
+            for (int h = 0; h < NH; h++) {
+                double acc[NJ];
+#pragma unroll
+                for (int j = 0; j < NJ; j++) acc[j] = 0.0;
+                for (unsigned u = U; u; u &= u - 1) {
+                    const int k = __ffs(u) - 1;
+                    const uint32_t cmk = __shfl_sync(0xffffffffu, cm, g * N + k);
+                    const uint32_t cmu = __reduce_or_sync(0xffffffffu, cmk);
+                    double t = 0.0;
+                    for (uint32_t v = cmu; v; v &= v - 1) {
+                        const int l = __ffs(v) - 1;
+                        t = __dadd_rn(t, __dmul_rn(__ldg(Mg + l * N + i), (double)X[l * N + k]));
+                    }
+#pragma unroll
+                    for (int j = 0; j < NJ; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, Mc[k * N + h * NJ + j]));
+                }
+                if (have) {
+                    uint32_t *row = reinterpret_cast<uint32_t *>(w.ty + (py0 + i) * 64 + px0 + h * NJ);
+#pragma unroll
+                    for (int j4 = 0; j4 < NJ / 4; j4++) {
+                        uint32_t word = row[j4], outw = 0;
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            /* round half away from zero; the int16 saturation of
+                             * vp9_reconstruct.c:52-59 cannot change the result of
+                             * the 0..255 clamp that follows, so it is folded in */
+                            const int r = __double2int_rz(__dadd_rn(acc[j4 * 4 + e], copysign(0.5, acc[j4 * 4 + e])));
+                            const int px = (int)((word >> (8 * e)) & 0xffu);
+                            outw |= (uint32_t)clampi(px + r, 0, 255) << (8 * e);
+                        }
+                        row[j4] = outw;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        have = nhave;
+        px0 = npx0;
+        py0 = npy0;
+    }
+}
+
+} /* namespace */
+
+/* MINB: CTAs per SM the register allocation is sized for (5: up to 96
+ * registers, no spills; 6: 80 registers, a few spilled). */
+template <int A, int MINB>
+__global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_t *__restrict__ jobs,
+                                                            const uint32_t *__restrict__ tickets,
+                                                            uint32_t n_tickets, uint32_t *__restrict__ general)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FastSmem &w = reinterpret_cast<FastSmem *>(smem_raw)[warp];
+    const uint32_t t = blockIdx.x * kFastWarps + warp;
+    if (t >= n_tickets) return;
+    const uint32_t code = __ldg(tickets + t);
+    const cvp9_job_t &job = jobs[code >> 20];
+    const int sb = (int)(code & 0xFFFFFu);
+    const int sb_cols = job.sb_cols;
+    const int sbr = sb / sb_cols, sbc = sb - sbr * sb_cols;
+    const int sbx = sbc * 64, sby = sbr * 64;
+    const int W = job.W, H = job.H;
+    const uint32_t *rg = job.sb_range + 4 * sb;
+    const uint32_t start = rg[0], end = rg[1], groups = rg[2];
+    bool gen = groups != 1 || end < start || end > job.num_blocks || end - start > 64u ||
+               (*job.status & CVP9_JOB_BAD_BLOCK) != 0;
+    const int nb = gen ? 0 : (int)(end - start);
+
+    /* 1. blocks: load, check, pack; 4x4-cell occupancy */
+    if (lane < 8) w.cells[lane] = 0u;
+    __syncwarp();
+    bool bad = false, ovl = false;
+    int nch[2] = { 0, 0 };
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = lane + 32 * r;
+        if (i >= nb) continue;
+        const uint32_t *g = reinterpret_cast<const uint32_t *>(job.blocks + start + i);
+        const uint32_t g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2), g3 = __ldg(g + 3);
+        const uint32_t g5 = __ldg(g + 5), g6 = __ldg(g + 6);
+        const int gx = (int)(g0 & 0xffffu), gy = (int)(g0 >> 16);
+        const int bw = (int)(g1 & 0xffu), bh = (int)((g1 >> 8) & 0xffu);
+        const int txl = (int)((g1 >> 16) & 0xffu), intra = (int)(g1 >> 24);
+        const int ref0 = (int)((g2 >> 16) & 0xffu), skip = (int)(g5 & 0xffu);
+        const int lx = gx - sbx, ly = gy - sby;
+        const bool mb = lx < 0 || ly < 0 || (lx & 3) || (ly & 3) || (bw & 3) || (bh & 3) ||
+                        bw < 4 || bh < 4 || lx + bw > 64 || ly + bh > 64 || gx >= W || gy >= H || txl > 3 ||
+                        ((bw < 8 || bh < 8) && ((lx & 7) || (ly & 7)));
+        bad |= mb || intra;
+        if (mb) continue;
+        const int cw = min(bw, W - gx), ch = min(bh, H - gy);
+        FastBlk fb;
+        const uint32_t slot4 = (ref0 >= 1 && ref0 <= 8) ? (uint32_t)(ref0 - 1) : 15u;
+        fb.geo = (uint32_t)(lx >> 2) | (uint32_t)(ly >> 2) << 4 | (uint32_t)cw << 8 | (uint32_t)ch << 15 |
+                 slot4 << 22 | (uint32_t)txl << 26 | (skip ? 1u : 0u) << 28;
+        fb.mv = g3;
+        fb.coeff = g6;
+        w.blk[i] = fb;
+        nch[r] = ((cw + 7) >> 3) * ((ch + 7) >> 3);
+        const int c0x = lx >> 2, c1x = (lx + cw - 1) >> 2, c0y = ly >> 2, c1y = (ly + ch - 1) >> 2;
+        const uint32_t m = (2u << c1x) - (1u << c0x);
+        for (int cy = c0y; cy <= c1y; cy++) {
+            const uint32_t mm = m << (16 * (cy & 1));
+            ovl |= (atomicOr(&w.cells[cy >> 1], mm) & mm) != 0u;
+        }
+    }
+    __syncwarp();
+    const int vw = min(64, W - sbx), vh = min(64, H - sby);
+    bool gap = false;
+    if (lane < 8) {
+        const int ncx = (vw + 3) >> 2, ncy = (vh + 3) >> 2;
+        const uint32_t rowm = ncx >= 16 ? 0xffffu : ((1u << ncx) - 1u);
+        const uint32_t expect = (2 * lane < ncy ? rowm : 0u) | (2 * lane + 1 < ncy ? rowm << 16 : 0u);
+        gap = w.cells[lane] != expect;
+    }
+    gen = __any_sync(0xffffffffu, gen || bad || ovl || gap) != 0;
+    if (lane == 0) general[t] = gen ? 1u : 0u;
+    if (gen) return;
+
+    /* 2. chunk (8x8 luma + 4x4 chroma) offsets and map */
+    int nchunks;
+    {
+        const int x0 = warp_incl_scan(nch[0], lane), x1 = warp_incl_scan(nch[1], lane);
+        const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
+        nchunks = tot0 + tot1;
+        if (nchunks > 128) {             /* more chunks than the map holds (odd block sizes) */
+            if (lane == 0) general[t] = 1u;
+            return;
+        }
+        const int e0 = x0 - nch[0], e1 = tot0 + x1 - nch[1];
+        if (lane < nb) { w.choff[lane] = (uint16_t)e0; for (int c = 0; c < nch[0]; c++) w.chblk[e0 + c] = (uint8_t)lane; }
+        if (lane + 32 < nb) { w.choff[lane + 32] = (uint16_t)e1; for (int c = 0; c < nch[1]; c++) w.chblk[e1 + c] = (uint8_t)(lane + 32); }
+    }
+    __syncwarp();
+
+    /* 3. prediction (vp9_reconstruct.c:94-131). Luma passes: lane = (chunk
+     * c0 + lane/8, row lane%8); chroma passes: lane = (chunk c0 + lane/8,
+     * plane, row). Two passes are in flight: both issue their loads before
+     * either computes. */
+    for (int c0 = 0; c0 < nchunks; c0 += 8) {
+        const FastLuma a = fast_luma_issue(w, job, c0 + (lane >> 3), lane & 7, nchunks, sbx, sby);
+        const FastLuma b = fast_luma_issue(w, job, c0 + 4 + (lane >> 3), lane & 7, nchunks, sbx, sby);
+        fast_luma_finish(a);
+        fast_luma_finish(b);
+    }
+    for (int c0 = 0; c0 < nchunks; c0 += 8) {
+        const FastChroma a = fast_chroma_issue(w, job, c0 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
+        const FastChroma b = fast_chroma_issue(w, job, c0 + 4 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
+        fast_chroma_finish(a);
+        fast_chroma_finish(b);
+    }
+    __syncwarp();
+
+    /* 4. luma residual, one pass per TX size present */
+    unsigned sizes = 0;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = lane + 32 * r;
+        if (i < nb && !fb_skip(w.blk[i])) sizes |= 1u << fb_txl(w.blk[i]);
+    }
+    sizes = __reduce_or_sync(0xffffffffu, sizes);
+    for (unsigned sz = sizes; sz; sz &= sz - 1) {
+        const int txl = __ffs(sz) - 1, n = 4 << txl;
+        int cnt[2] = { 0, 0 };
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int i = lane + 32 * r;
+            if (i < nb) {
+                const FastBlk fb = w.blk[i];
+                if (!fb_skip(fb) && fb_txl(fb) == txl) cnt[r] = (fb_cw(fb) / n) * (fb_ch(fb) / n);
+            }
+        }
+        const int x0 = warp_incl_scan(cnt[0], lane), x1 = warp_incl_scan(cnt[1], lane);
+        const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
+        const int e0 = x0 - cnt[0], e1 = tot0 + x1 - cnt[1];
+        const int ntx = tot0 + tot1;        /* at most 256: the TXs tile the SB */
+        if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
+        if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
+        __syncwarp();
+        switch (txl) {
+        case 0: fast_residual<4>(w, job, ntx, lane); break;
+        case 1: fast_residual<8>(w, job, ntx, lane); break;
+        case 2: fast_residual<16>(w, job, ntx, lane); break;
+        default: fast_residual<32>(w, job, ntx, lane); break;
+        }
+        __syncwarp();
+    }
+
+    /* 5. write the tile (clipped to the frame) and release the SB */
+    {
+        uint8_t *Y = job.out;
+        if (!(W & 15) && !((uintptr_t)Y & 15)) {
+            for (int i = lane; i < vh * 4; i += 32) {
+                const int r = i >> 2, c16 = (i & 3) * 16;
+                if (c16 < vw)
+                    *reinterpret_cast<uint4 *>(Y + (size_t)(sby + r) * W + sbx + c16) =
+                        *reinterpret_cast<const uint4 *>(w.ty + r * 64 + c16);
+            }
+        } else if (!(W & 3) && !((uintptr_t)Y & 3)) {
+            for (int i = lane; i < vh * 16; i += 32) {
+                const int r = i >> 4, c4 = (i & 15) * 4;
+                if (c4 < vw)
+                    *reinterpret_cast<uint32_t *>(Y + (size_t)(sby + r) * W + sbx + c4) =
+                        *reinterpret_cast<const uint32_t *>(w.ty + r * 64 + c4);
+            }
+        } else {
+            for (int i = lane; i < vh * 64; i += 32) {
+                const int r = i >> 6, c = i & 63;
+                if (c < vw) Y[(size_t)(sby + r) * W + sbx + c] = w.ty[r * 64 + c];
+            }
+        }
+        const int CW = job.CW, CH = job.CH;
+        const int cvw = min(32, CW - (sbx >> 1)), cvh = min(32, CH - (sby >> 1));
+        uint8_t *U = Y + (size_t)W * H;
+        uint8_t *V = U + (size_t)CW * CH;
+        if (!(CW & 15) && !((uintptr_t)U & 15) && !((uintptr_t)V & 15)) {
+            for (int i = lane; i < 2 * cvh * 2; i += 32) {
+                const int p = i >= cvh * 2, k = p ? i - cvh * 2 : i;
+                const int r = k >> 1, c16 = (k & 1) * 16;
+                if (c16 < cvw)
+                    *reinterpret_cast<uint4 *>((p ? V : U) + (size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c16) =
+                        *reinterpret_cast<const uint4 *>((p ? w.tv : w.tu) + r * 32 + c16);
+            }
+        } else if (!(CW & 3) && !((uintptr_t)U & 3) && !((uintptr_t)V & 3)) {
+            for (int i = lane; i < 2 * cvh * 8; i += 32) {
+                const int p = i >= cvh * 8, k = p ? i - cvh * 8 : i;
+                const int r = k >> 3, c4 = (k & 7) * 4;
+                if (c4 < cvw)
+                    *reinterpret_cast<uint32_t *>((p ? V : U) + (size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c4) =
+                        *reinterpret_cast<const uint32_t *>((p ? w.tv : w.tu) + r * 32 + c4);
+            }
+        } else {
+            for (int i = lane; i < 2 * cvh * 32; i += 32) {
+                const int p = i >= cvh * 32, k = p ? i - cvh * 32 : i;
+                const int r = k >> 5, c = k & 31;
+                if (c < cvw) (p ? V : U)[(size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c] = (p ? w.tv : w.tu)[r * 32 + c];
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        st_release(job.sb_done + sb, job.epoch);
+    }
+}
+
+/* Order-preserving compaction of the tickets k_inter marked general, one
+ * CTA: each thread counts a contiguous segment, a CTA-wide scan places the
+ * segments, the thread copies its general tickets. */
+__global__ void __launch_bounds__(1024) k_compact(const uint32_t *__restrict__ tickets,
+                                                  const uint32_t *__restrict__ general, uint32_t n,
+                                                  uint32_t *__restrict__ out, uint32_t *__restrict__ count)
+{
+    __shared__ uint32_t wsum[32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint32_t per = (n + 1023u) / 1024u;
+    const uint32_t b = min(n, (uint32_t)tid * per), e = min(n, b + per);
+    uint32_t c = 0;
+    for (uint32_t i = b; i < e; i++) c += general[i] != 0u;
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t v = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        wsum[lane] = v;
+    }
+    __syncthreads();
+    uint32_t pos = x - c + (wid ? wsum[wid - 1] : 0u);
+    for (uint32_t i = b; i < e; i++)
+        if (general[i]) out[pos++] = tickets[i];
+    if (tid == 1023) *count = pos;
+}
+
 /* ── Loop filter ─────────────────────────────────────────────────────────── */
 
 __device__ __forceinline__ void filter4(uint8_t *p1, uint8_t *p0, uint8_t *q0, uint8_t *q1, int thr)
@@ -1759,7 +2447,8 @@ size_t cvp9k_recon_smem_bytes(void) { return sizeof(ReconSmem); }
 int cvp9k_upload_dct_basis(const double *basis, int count)
 {
     if (count != 16 + 64 + 256 + 1024) return -1;
-    return cudaMemcpyToSymbol(c_dct, basis, sizeof(double) * (size_t)count) == cudaSuccess ? 0 : -1;
+    if (cudaMemcpyToSymbol(c_dct, basis, sizeof(double) * (size_t)count) != cudaSuccess) return -1;
+    return cudaMemcpyToSymbol(g_dct, basis, sizeof(double) * (size_t)count) == cudaSuccess ? 0 : -1;
 }
 
 int cvp9k_configure(void)
@@ -1770,6 +2459,8 @@ int cvp9k_configure(void)
     /* all of the unified L1/shared storage as shared memory: three CTAs per SM */
     cudaFuncSetAttribute(k_recon<CVP9_ARITH_REFCPU>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_recon<CVP9_ARITH_SPEC>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_inter<CVP9_ARITH_REFCPU, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_inter<CVP9_ARITH_REFCPU, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return 0;
 }
 
@@ -1808,10 +2499,23 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
         int grid = L->recon_ctas > 0 ? L->recon_ctas : (int)L->n_tickets;
         if (grid > (int)L->n_tickets) grid = (int)L->n_tickets;
         size_t smem = sizeof(ReconSmem);
-        if (L->arith == CVP9_ARITH_SPEC)
-            k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter);
-        else
-            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter);
+        const bool fast = L->general && L->general_tickets && L->n_general && L->arith == CVP9_ARITH_REFCPU;
+        if (fast) {
+            const unsigned fg = (L->n_tickets + kFastWarps - 1) / kFastWarps;
+            if (L->inter_variant == 1)
+                k_inter<CVP9_ARITH_REFCPU, 5><<<fg, kFastWarps * 32, kFastWarps * sizeof(FastSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+            else
+                k_inter<CVP9_ARITH_REFCPU, 6><<<fg, kFastWarps * 32, kFastWarps * sizeof(FastSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+            k_compact<<<1, 1024, 0, st>>>(L->tickets, L->general, L->n_tickets, L->general_tickets, L->n_general);
+            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->general_tickets, L->n_tickets,
+                                                                      L->ticket_counter, L->n_general);
+        } else if (L->arith == CVP9_ARITH_SPEC) {
+            k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter, nullptr);
+        } else {
+            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter, nullptr);
+        }
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     if ((e = mark(L->ev[2], st, capturing)) != cudaSuccess) return (int)e;

@@ -28,6 +28,14 @@ typedef struct {
     int              lf_tiles_x, lf_tiles_y;   /* tiled filter grid (max over jobs) */
     int              flat_lf_max_w, flat_lf_max_h; /* >0: run the frame-wide filter */
     int              flat_nv12;
+    /* Inter fast path (REFCPU): when `general` is set, k_inter takes the
+     * superblocks that hold inter blocks only, one warp each, and k_recon
+     * runs on the rest. All three are device buffers: n_tickets words,
+     * n_tickets words, one word. */
+    uint32_t        *general;
+    uint32_t        *general_tickets;
+    uint32_t        *n_general;
+    int              inter_variant;  /* 0: default, 1: 96-register k_inter, 2: 80-register */
     cudaEvent_t      ev[4];        /* optional: before scan, recon, filter; after */
 } cvp9k_launch_t;
 

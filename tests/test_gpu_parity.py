@@ -1,7 +1,8 @@
 """Bit-exact parity of the CUDA backend (through the C ABI) with the oracle.
 
 REFCPU cases are the reference's CPU reconstruction (the restatement in
-oracle/, itself pinned to the compiled reference and to tests/golden); SPEC
+oracle/, itself pinned to the compiled reference and to tests/golden), run
+with the warp-per-superblock inter path on (the default) and off; SPEC
 cases are the shader-arithmetic restatement. Sizes keep the CPU oracle to
 seconds. Tolerance: none — every byte of every plane must match.
 """
@@ -53,6 +54,14 @@ def run_case(profile, preset, w, h, frames, overrides, seed=11):
 
 @pytest.mark.parametrize("name", list(CASES))
 def test_refcpu_parity(name):
+    run_case(REFCPU, *CASES[name])
+
+
+@pytest.mark.parametrize("name", ["c1_small", "c2_small", "edges_sub8", "big_tx", "flat_lf"])
+def test_refcpu_parity_without_inter_fast_path(name, monkeypatch):
+    """The general superblock kernel alone (CVP9_INTER_FAST=0) gives the same
+    bytes as with the warp-per-superblock inter path."""
+    monkeypatch.setenv("CVP9_INTER_FAST", "0")
     run_case(REFCPU, *CASES[name])
 
 
