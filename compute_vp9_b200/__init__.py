@@ -32,7 +32,8 @@ EXPORTED_SYMBOLS = [
     "cvp9_batch_open_stream", "cvp9_batch_close_stream", "cvp9_batch_submit",
     "cvp9_batch_wait", "cvp9_batch_poll", "cvp9_batch_get_frame", "cvp9_batch_stats",
     "cvp9_batch_last_error", "cvp9_batch_timer_start", "cvp9_batch_timer_stop",
-    "cvp9_batch_last_seq", "cvp9_batch_step_latency",
+    "cvp9_batch_last_seq", "cvp9_batch_step_latency", "cvp9_batch_tune_count",
+    "cvp9_batch_tune_entry",
 ]
 
 
@@ -143,17 +144,17 @@ def fnv1a64(buf):
 
 
 class BackendOptions(C.Structure):
-    _fields_ = [("device", C.c_int), ("arith", C.c_int)]
+    _fields_ = [("device", C.c_int), ("arith", C.c_int), ("autotune", C.c_int)]
 
 
 class CudaBackend:
     """One decoder stream on the CUDA backend (the drop-in ABI)."""
 
-    def __init__(self, device=-1, arith=-1):
+    def __init__(self, device=-1, arith=-1, autotune=0):
         lib = cuda_lib()
         self._lib = lib
         self._ctx = C.c_void_p()
-        opt = BackendOptions(device, arith)
+        opt = BackendOptions(device, arith, autotune)
         rc = lib.cuda_backend_init_ex(C.byref(self._ctx), C.byref(opt))
         if rc != CVP9_OK:
             raise Cvp9Error(rc, "cuda_backend_init")

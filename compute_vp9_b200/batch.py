@@ -11,7 +11,13 @@ NO_OUTPUT = 2
 
 class BatchConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("arith", C.c_int), ("hbm_budget", C.c_uint64),
-                ("max_streams", C.c_int), ("use_graphs", C.c_int)]
+                ("max_streams", C.c_int), ("use_graphs", C.c_int), ("autotune", C.c_int)]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("key", C.c_uint64), ("frames", C.c_int), ("settled", C.c_int),
+                ("inter_path", C.c_int), ("lf_tile_h", C.c_int), ("half_width", C.c_int),
+                ("trials", C.c_int), ("best_ms", C.c_float)]
 
 
 class BatchStats(C.Structure):
@@ -27,6 +33,8 @@ def _bind(lib):
     lib.cvp9_batch_create.argtypes = [C.POINTER(BatchConfig), C.POINTER(vp)]
     lib.cvp9_batch_destroy.argtypes = [vp]
     lib.cvp9_batch_destroy.restype = None
+    lib.cvp9_batch_tune_count.argtypes = [vp]
+    lib.cvp9_batch_tune_entry.argtypes = [vp, C.c_int, C.POINTER(TuneEntry)]
     lib.cvp9_batch_stream_bytes.argtypes = [C.c_uint32, C.c_uint32]
     lib.cvp9_batch_stream_bytes.restype = C.c_uint64
     lib.cvp9_batch_open_stream.argtypes = [vp, C.c_uint32, C.c_uint32]
@@ -58,11 +66,11 @@ class Batch:
     None when the budget is full); step() reconstructs one frame per listed
     stream in one launch chain."""
 
-    def __init__(self, device=-1, arith=-1, hbm_budget=0, max_streams=0, use_graphs=1):
+    def __init__(self, device=-1, arith=-1, hbm_budget=0, max_streams=0, use_graphs=1, autotune=1):
         from . import cuda_lib
         self._lib = cuda_lib()
         self._h = C.c_void_p()
-        cfg = BatchConfig(device, arith, hbm_budget, max_streams, use_graphs)
+        cfg = BatchConfig(device, arith, hbm_budget, max_streams, use_graphs, autotune)
         rc = self._lib.cvp9_batch_create(C.byref(cfg), C.byref(self._h))
         if rc != CVP9_OK:
             raise BatchError(rc, "cvp9_batch_create")
@@ -128,6 +136,16 @@ class Batch:
 
     def last_seq(self):
         return int(self._lib.cvp9_batch_last_seq(self._h))
+
+    def tuning(self):
+        """The tuner's buckets: list of dicts (key, frames, settled, inter_path,
+        lf_tile_h, half_width, trials, best_ms)."""
+        out = []
+        for i in range(self._lib.cvp9_batch_tune_count(self._h)):
+            e = TuneEntry()
+            if self._lib.cvp9_batch_tune_entry(self._h, i, C.byref(e)) == CVP9_OK:
+                out.append({k: getattr(e, k) for k, _ in TuneEntry._fields_})
+        return out
 
     def step_latency_ms(self, seq):
         ms = C.c_double()

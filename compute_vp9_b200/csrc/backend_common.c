@@ -86,6 +86,12 @@ int cvp9_env_device(void)
     return e && *e ? atoi(e) : 0;
 }
 
+int cvp9_env_autotune(void)
+{
+    const char *e = getenv("CVP9_AUTOTUNE");
+    return !(e && *e == '0');
+}
+
 int cvp9_env_inter_fast(void)
 {
     const char *e = getenv("CVP9_INTER_FAST");
@@ -126,4 +132,110 @@ double cvp9_now(void)
     struct timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
     return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* ── Autotuner ─────────────────────────────────────────────────────────── */
+
+static int ceil_log2_u64(uint64_t v)
+{
+    int l = 0;
+    while (l < 63 && (1ull << l) < v) l++;
+    return l;
+}
+
+uint64_t cvp9_tune_key(int arith, int frames, uint64_t superblocks)
+{
+    return ((uint64_t)(arith & 0xff) << 16) | ((uint64_t)ceil_log2_u64((uint64_t)(frames > 0 ? frames : 1)) << 8) |
+           (uint64_t)ceil_log2_u64(superblocks ? superblocks : 1);
+}
+
+void cvp9_tuner_init(cvp9_tuner_t *t, int arith, int enabled, cvp9_tcfg_t fixed)
+{
+    memset(t, 0, sizeof(*t));
+    t->arith = arith;
+    t->enabled = enabled;
+    t->fixed = fixed;
+}
+
+static int same_cfg(cvp9_tcfg_t a, cvp9_tcfg_t b)
+{
+    return a.inter == b.inter && a.lf32 == b.lf32 && a.half == b.half;
+}
+
+/* Move to the next candidate; settle when every knob is done. */
+static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
+{
+    for (;;) {
+        e->idx++;
+        if (e->stage == 0) {
+            /* inter path: the default was candidate 0; SPEC has no k_inter */
+            static const int8_t alts[2] = { 0, 2 };
+            if (t->arith == 0 && e->idx <= 2) {
+                e->cur = e->best;
+                e->cur.inter = alts[e->idx - 1];
+                break;
+            }
+            e->stage = 1;
+            e->idx = 0;
+        } else if (e->stage == 1) {
+            if (e->idx == 1) { e->cur = e->best; e->cur.lf32 = 1; break; }
+            e->stage = 2;
+            e->idx = 0;
+        } else if (e->stage == 2) {
+            if (e->idx == 1) { e->cur = e->best; e->cur.half = 1; break; }
+            e->state = 2;
+            return;
+        } else {
+            e->state = 2;
+            return;
+        }
+    }
+    e->cur_n = 0;
+    e->cur_ms = 0.f;
+}
+
+int cvp9_tuner_pick(cvp9_tuner_t *t, uint64_t key, int frames, cvp9_tcfg_t *cfg)
+{
+    *cfg = t->fixed;
+    if (!t->enabled) return -1;
+    t->clock++;
+    int free_i = -1, lru = 0;
+    for (int i = 0; i < CVP9_TUNE_BUCKETS; i++) {
+        cvp9_tbucket_t *e = &t->b[i];
+        if (e->state && e->key == key) {
+            e->last_use = t->clock;
+            if (e->state == 2) { *cfg = e->best; return -1; }
+            *cfg = e->cur;
+            return i;
+        }
+        if (!e->state && free_i < 0) free_i = i;
+        if (e->last_use < t->b[lru].last_use) lru = i;
+    }
+    int i = free_i >= 0 ? free_i : lru;
+    cvp9_tbucket_t *e = &t->b[i];
+    memset(e, 0, sizeof(*e));
+    e->key = key;
+    e->frames = frames;
+    e->state = 1;
+    e->cur = t->fixed;
+    e->best = t->fixed;
+    e->best_ms = 3.4e38f;
+    e->last_use = t->clock;
+    *cfg = e->cur;
+    return i;
+}
+
+void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms)
+{
+    if (idx < 0 || idx >= CVP9_TUNE_BUCKETS) return;
+    cvp9_tbucket_t *e = &t->b[idx];
+    if (e->state != 1 || !same_cfg(cfg, e->cur) || !(ms > 0.f)) return;   /* a stale sample */
+    e->cur_ms = e->cur_n ? (ms < e->cur_ms ? ms : e->cur_ms) : ms;
+    if (++e->cur_n < 2) return;
+    e->trials++;
+    if (e->cur_ms < e->best_ms) {
+        e->best_ms = e->cur_ms;
+        e->best = e->cur;
+    }
+    tune_advance(t, e);
 }

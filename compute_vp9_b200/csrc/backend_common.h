@@ -41,6 +41,7 @@ int cvp9_ac_q(int qindex);
 int cvp9_env_device(void);
 int cvp9_env_arith(void);
 int cvp9_env_inter_fast(void);
+int cvp9_env_autotune(void);        /* $CVP9_AUTOTUNE: 0 turns tuning off */
 
 /* Fill the frame-geometry and parameter fields of a job from a parsed
  * frame (inputs, output, refs and scratch pointers are set by the caller). */
@@ -54,3 +55,48 @@ double cvp9_now(void);
 #endif
 
 #endif /* CVP9_BACKEND_COMMON_H */
+
+/* ── Autotuner ──────────────────────────────────────────────────────────────
+ * Per shape bucket, the kernel configuration is chosen by timing: each
+ * candidate runs on two steps of that bucket (the faster counts), knobs are
+ * settled one at a time (coordinate descent): the inter path, then the
+ * loop-filter tile height, then the wavefront width. Every configuration
+ * produces the same bytes; only the speed differs. Pure host logic. */
+
+#define CVP9_TUNE_BUCKETS 64
+
+typedef struct {
+    int8_t inter;      /* 0 general kernel only, 1 k_inter (96 registers), 2 k_inter (80) */
+    int8_t lf32;       /* loop-filter tiles 32 rows high instead of 64 */
+    int8_t half;       /* wavefront kernel on half the resident CTAs */
+} cvp9_tcfg_t;
+
+typedef struct {
+    uint64_t    key;
+    int         frames;
+    int         state;         /* 0 free, 1 measuring, 2 settled */
+    int         stage, idx;    /* knob being settled, candidate within it */
+    int         trials;        /* candidates measured */
+    int         cur_n;         /* samples of the current candidate */
+    cvp9_tcfg_t best, cur;
+    float       best_ms, cur_ms;
+    uint64_t    last_use;
+} cvp9_tbucket_t;
+
+typedef struct {
+    cvp9_tbucket_t b[CVP9_TUNE_BUCKETS];
+    int         arith;
+    int         enabled;
+    cvp9_tcfg_t fixed;         /* configuration when tuning is off */
+    uint64_t    clock;
+} cvp9_tuner_t;
+
+void cvp9_tuner_init(cvp9_tuner_t *t, int arith, int enabled, cvp9_tcfg_t fixed);
+/* Configuration for a step of bucket `key`; returns the bucket index whose
+ * measurement this step feeds, or -1 (settled bucket or tuning off). */
+int  cvp9_tuner_pick(cvp9_tuner_t *t, uint64_t key, int frames, cvp9_tcfg_t *cfg);
+/* Kernel time of a completed step that ran `cfg` for bucket `idx`. */
+void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms);
+/* Coarse bucket of a step: arithmetic, frame count and superblock count,
+ * each rounded up to a power of two, so serving steps share buckets. */
+uint64_t cvp9_tune_key(int arith, int frames, uint64_t superblocks);

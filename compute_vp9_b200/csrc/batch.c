@@ -80,6 +80,8 @@ typedef struct {
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
     uint32_t       *h_tickets; size_t h_tickets_cap;
     uint32_t       *d_fast; size_t fast_cap;    /* inter fast path: flags, tickets, count */
+    int             tune_idx;                   /* tuner bucket this step measures, -1 none */
+    cvp9_tcfg_t     tune_cfg;
     size_t          h_jobs_bytes, d_jobs_bytes, h_misc_bytes, d_misc_bytes;
     cudaGraphExec_t graph; uint64_t graph_key;
     int             n;
@@ -89,7 +91,8 @@ typedef struct {
 } bslot_t;
 
 struct cvp9_batch {
-    int          device, arith, use_graphs, max_streams, inter_fast;
+    int          device, arith, use_graphs, max_streams;
+    cvp9_tuner_t tuner;      /* kernel configuration per shape bucket */
     uint64_t     budget, reserved;
     cudaStream_t cs, hs, ds;
     bstream_t   *st;
@@ -146,7 +149,10 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     b->budget = (cfg && cfg->hbm_budget) ? cfg->hbm_budget : 150ull * 1000 * 1000 * 1000;
     b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
     b->use_graphs = cfg ? cfg->use_graphs : 1;
-    b->inter_fast = cvp9_env_inter_fast();
+    {
+        cvp9_tcfg_t fixed = { (int8_t)(b->arith == CVP9_ARITH_REFCPU ? cvp9_env_inter_fast() : 0), 0, 0 };
+        cvp9_tuner_init(&b->tuner, b->arith, cfg && cfg->autotune && cvp9_env_autotune(), fixed);
+    }
     if (b->device >= ndev || cvp9_device_setup(b->device) != 0) { free(b); return CVP9_ERR_NO_BACKEND; }
     b->st = calloc((size_t)b->max_streams, sizeof(bstream_t));
     if (!b->st) { free(b); return CVP9_ERR_NOMEM; }
@@ -423,6 +429,7 @@ static void complete_slot(cvp9_batch_t *b, bslot_t *s)
     b->last.scan_ms = a;
     b->last.recon_ms = r;
     b->last.filter_ms = f;
+    cvp9_tuner_report(&b->tuner, s->tune_idx, s->tune_cfg, k);
     for (int i = 0; i < s->n; i++) {
         bstream_t *st = &b->st[s->sids[i]];
         if (st->open && st->last_seq == s->seq) st->last_status = s->h_misc[1 + i];
@@ -690,12 +697,19 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     L.tickets = s->d_tickets;
     L.n_tickets = s->n_tickets;
     L.ticket_counter = s->d_misc;
-    L.recon_ctas = (int)s->n_tickets < b->resident_ctas ? (int)s->n_tickets : b->resident_ctas;
-    if (b->inter_fast) {
+    cvp9_tcfg_t tc;
+    s->tune_idx = cvp9_tuner_pick(&b->tuner, cvp9_tune_key(b->arith, n, (uint64_t)n_sb), n, &tc);
+    s->tune_cfg = tc;
+    {
+        const int width = tc.half ? (b->resident_ctas + 1) / 2 : b->resident_ctas;
+        L.recon_ctas = (int)s->n_tickets < width ? (int)s->n_tickets : width;
+    }
+    L.lf_tile_h = tc.lf32 ? 32 : 64;
+    if (tc.inter) {
         L.general = s->d_fast;
         L.general_tickets = s->d_fast + s->n_tickets;
         L.n_general = s->d_fast + 2 * (size_t)s->n_tickets;
-        L.inter_variant = b->inter_fast;
+        L.inter_variant = tc.inter;
     }
     L.lf_tiles_x = lf_tx;
     L.lf_tiles_y = lf_ty;
@@ -707,6 +721,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
                           mix64((uint64_t)(uintptr_t)s->d_misc, (uint64_t)(uintptr_t)s->d_tickets));
     gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
+    gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
     s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + (lf_tx > 0) + (flat_w > 0 ? 2 : 0) +
                              (L.general && b->arith == CVP9_ARITH_REFCPU ? 2 : 0));
     if (b->use_graphs) {
@@ -918,4 +933,32 @@ cvp9_err_t cvp9_batch_step_latency(cvp9_batch_t *b, uint64_t seq, double *ms)
     if (d == 0.0) return CVP9_ERR_AGAIN;
     *ms = 1000.0 * (d - b->lat_submit[seq % LAT_RING]);
     return CVP9_OK;
+}
+
+int cvp9_batch_tune_count(cvp9_batch_t *b)
+{
+    if (!b) return 0;
+    int n = 0;
+    for (int i = 0; i < CVP9_TUNE_BUCKETS; i++) n += b->tuner.b[i].state != 0;
+    return n;
+}
+
+cvp9_err_t cvp9_batch_tune_entry(cvp9_batch_t *b, int i, cvp9_batch_tune_t *out)
+{
+    if (!b || !out || i < 0) return CVP9_ERR_INVALID_DATA;
+    for (int k = 0; k < CVP9_TUNE_BUCKETS; k++) {
+        const cvp9_tbucket_t *e = &b->tuner.b[k];
+        if (!e->state || i--) continue;
+        memset(out, 0, sizeof(*out));
+        out->key = e->key;
+        out->frames = e->frames;
+        out->settled = e->state == 2;
+        out->inter_path = e->best.inter;
+        out->lf_tile_h = e->best.lf32 ? 32 : 64;
+        out->half_width = e->best.half;
+        out->trials = e->trials;
+        out->best_ms = e->trials ? e->best_ms : 0.f;
+        return CVP9_OK;
+    }
+    return CVP9_ERR_INVALID_DATA;
 }

@@ -38,6 +38,8 @@ typedef struct {
     int64_t      pts;
     int32_t      w, h;
     cudaEvent_t  ev_start, ev_k0, ev_k1, ev_end;
+    int          tune_idx;             /* tuner bucket this frame measures, -1 none */
+    cvp9_tcfg_t  tune_cfg;
     /* pinned staging */
     void        *h_blocks;  size_t h_blocks_cap;
     void        *h_coeffs;  size_t h_coeffs_cap;
@@ -65,7 +67,8 @@ typedef struct {
     uint32_t    *d_misc;               /* [0] status, [1] ticket counter */
     uint32_t    *d_tickets;
     uint32_t    *d_fast;               /* inter fast path: general flags, tickets, count */
-    int          inter_fast;
+    cvp9_tuner_t tuner;                /* kernel configuration per frame size */
+    int          resident_ctas;
     uint32_t     n_tickets;
     int          recon_ctas;
     slot_t       slots[CVP9_CUDA_INFLIGHT];
@@ -122,7 +125,10 @@ cvp9_err_t cuda_backend_init_ex(void **out, const cuda_backend_options_t *opt)
     c->device = (opt && opt->device >= 0) ? opt->device : cvp9_env_device();
     c->arith = (opt && opt->arith >= 0) ? (opt->arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU)
                                         : cvp9_env_arith();
-    c->inter_fast = cvp9_env_inter_fast();
+    {
+        cvp9_tcfg_t fixed = { (int8_t)(c->arith == CVP9_ARITH_REFCPU ? cvp9_env_inter_fast() : 0), 0, 0 };
+        cvp9_tuner_init(&c->tuner, c->arith, !(opt && opt->autotune < 0) && cvp9_env_autotune(), fixed);
+    }
     if (c->device >= dev_count || cvp9_device_setup(c->device) != 0) { free(c); return CVP9_ERR_NO_BACKEND; }
     for (int i = 0; i < 8; i++) c->ref_slot[i] = -1;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -194,6 +200,7 @@ static cvp9_err_t set_geometry(cuctx_t *c, int32_t W, int32_t H)
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
     int resident = dev_sms * cvp9_recon_ctas_per_sm(c->device, c->arith);
+    c->resident_ctas = resident;
     c->recon_ctas = (int)n < resident ? (int)n : resident;
     c->epoch = 0;
     return CVP9_OK;
@@ -328,12 +335,16 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     L.tickets = c->d_tickets;
     L.n_tickets = c->n_tickets;
     L.ticket_counter = c->d_misc + 1;
-    L.recon_ctas = c->recon_ctas;
-    if (c->inter_fast) {
+    cvp9_tcfg_t tc;
+    s->tune_idx = cvp9_tuner_pick(&c->tuner, cvp9_tune_key(c->arith, 1, (uint64_t)c->n_sb), 1, &tc);
+    s->tune_cfg = tc;
+    L.recon_ctas = tc.half ? (c->recon_ctas + 1) / 2 : c->recon_ctas;
+    L.lf_tile_h = tc.lf32 ? 32 : 64;
+    if (tc.inter) {
         L.general = c->d_fast;
         L.general_tickets = c->d_fast + c->n_sb;
         L.n_general = c->d_fast + 2 * c->n_sb;
-        L.inter_variant = c->inter_fast;
+        L.inter_variant = tc.inter;
     }
     if (job->lf_tiled) {
         L.lf_tiles_x = (W + 4 + 63) / 64;
@@ -409,6 +420,7 @@ cvp9_err_t cuda_get_frame(void *ctx, cvp9_frame_info_t *info, int wait)
     cudaEventElapsedTime(&k, s->ev_k0, s->ev_k1);
     c->last_total_ms = t;
     c->last_kernel_ms = k;
+    cvp9_tuner_report(&c->tuner, s->tune_idx, s->tune_cfg, k);
 
     uint32_t status = *s->h_status;
     if (status & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) {

@@ -2312,78 +2312,101 @@ __device__ __forceinline__ int lf_threshold(int level, int sharp)
     return t < 1 ? 1 : t;
 }
 
-/* Tile (tx, ty) covers luma [64tx-4, 64tx+60) x [64ty-4, 64ty+60): every tap
- * of every 8-px edge (rows/cols e-2..e+1) lies in one tile, so the
- * horizontal pass then the vertical pass run tile-locally and in place with
- * the same result as the frame-wide passes (vp9_reconstruct.c:146-190).
- * Requires W and H not of the form 8k+1 (lf_tiled). */
-template <int A>
+/* Tile (tx, ty) covers luma [64tx-4, 64tx+60) x [TH ty-4, TH ty+TH-4): every
+ * tap of every 8-px edge (rows/cols e-2..e+1) lies in one tile and every
+ * row in one tile, so the horizontal pass then the vertical pass run
+ * tile-locally and in place with the same result as the frame-wide passes
+ * (vp9_reconstruct.c:146-190). TH is 64 or 32 (tile height, chosen per shape
+ * by the engine's tuner). Requires W and H not of the form 8k+1 (lf_tiled).
+ * Rows move as 32-bit words when the frame width allows. */
+template <int A, int TH>
 __global__ void __launch_bounds__(256) k_loopfilter(const cvp9_job_t *__restrict__ jobs)
 {
-    __shared__ __align__(16) uint8_t t[64 * 68];
+    __shared__ __align__(16) uint8_t t[TH * 68];
     const cvp9_job_t &job = jobs[blockIdx.z];
     const int tx = blockIdx.x, ty = blockIdx.y;
-    const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
+    const int x0 = tx * 64 - 4, y0 = ty * TH - 4;
     if (!job.lf_tiled || x0 >= job.W || y0 >= job.H) return;
     const bool filt = !(A == CVP9_ARITH_REFCPU && job.lf_level == 0);
     if (!filt && !job.nv12) return;
     const int tid = threadIdx.x;
     const int xa = max(x0, 0), xb = min(x0 + 64, job.W);
-    const int ya = max(y0, 0), yb = min(y0 + 64, job.H);
+    const int ya = max(y0, 0), yb = min(y0 + TH, job.H);
     uint8_t *Y = job.out;
     const int W = job.W;
+    const bool words = !(W & 3) && !((uintptr_t)Y & 3);
     /* tile byte (x - x0, y - y0) at t[(y - y0) * 68 + (x - x0)] */
-    for (int i = tid; i < (yb - ya) * 64; i += 256) {
-        int r = i >> 6, c = i & 63;
-        int gx = xa + c;
-        if (gx < xb) t[(ya - y0 + r) * 68 + (gx - x0)] = Y[(size_t)(ya + r) * W + gx];
+    if (words) {
+        const int w0 = (xa - x0) >> 2, nw = (xb - xa) >> 2;
+        for (int i = tid; i < (yb - ya) * 16; i += 256) {
+            const int r = i >> 4, c = i & 15;
+            if (c < nw)
+                *reinterpret_cast<uint32_t *>(&t[(ya - y0 + r) * 68 + 4 * (w0 + c)]) =
+                    *reinterpret_cast<const uint32_t *>(Y + (size_t)(ya + r) * W + xa + 4 * c);
+        }
+    } else {
+        for (int i = tid; i < (yb - ya) * 64; i += 256) {
+            const int r = i >> 6, c = i & 63;
+            const int gx = xa + c;
+            if (gx < xb) t[(ya - y0 + r) * 68 + (gx - x0)] = Y[(size_t)(ya + r) * W + gx];
+        }
     }
     __syncthreads();
     if (filt) {
         const int thr = lf_threshold(job.lf_level, job.lf_sharpness);
         /* horizontal edges e = y0 + 4 + 8k */
-        for (int i = tid; i < 8 * 64; i += 256) {
-            int k = i >> 6, c = i & 63;
-            int e = y0 + 4 + 8 * k, gx = x0 + c;
+        for (int i = tid; i < (TH / 8) * 64; i += 256) {
+            const int k = i >> 6, c = i & 63;
+            const int e = y0 + 4 + 8 * k, gx = x0 + c;
             if (e < 8 || e >= job.H || gx < xa || gx >= xb) continue;
-            int r = e - y0;
+            const int r = e - y0;
             filter4(&t[(r - 2) * 68 + c], &t[(r - 1) * 68 + c], &t[r * 68 + c], &t[(r + 1) * 68 + c], thr);
         }
         __syncthreads();
-        for (int i = tid; i < 8 * 64; i += 256) {
-            int k = i >> 6, r = i & 63;
-            int e = x0 + 4 + 8 * k, gy = y0 + r;
+        for (int i = tid; i < 8 * TH; i += 256) {
+            const int k = i / TH, r = i % TH;
+            const int e = x0 + 4 + 8 * k, gy = y0 + r;
             if (e < 8 || e >= job.W || gy < ya || gy >= yb) continue;
-            int c = e - x0;
+            const int c = e - x0;
             uint8_t *row = &t[r * 68];
             filter4(&row[c - 2], &row[c - 1], &row[c], &row[c + 1], thr);
         }
         __syncthreads();
-        for (int i = tid; i < (yb - ya) * 64; i += 256) {
-            int r = i >> 6, c = i & 63;
-            int gx = xa + c;
-            if (gx < xb) Y[(size_t)(ya + r) * W + gx] = t[(ya - y0 + r) * 68 + (gx - x0)];
+        if (words) {
+            const int w0 = (xa - x0) >> 2, nw = (xb - xa) >> 2;
+            for (int i = tid; i < (yb - ya) * 16; i += 256) {
+                const int r = i >> 4, c = i & 15;
+                if (c < nw)
+                    *reinterpret_cast<uint32_t *>(Y + (size_t)(ya + r) * W + xa + 4 * c) =
+                        *reinterpret_cast<const uint32_t *>(&t[(ya - y0 + r) * 68 + 4 * (w0 + c)]);
+            }
+        } else {
+            for (int i = tid; i < (yb - ya) * 64; i += 256) {
+                const int r = i >> 6, c = i & 63;
+                const int gx = xa + c;
+                if (gx < xb) Y[(size_t)(ya + r) * W + gx] = t[(ya - y0 + r) * 68 + (gx - x0)];
+            }
         }
     }
     if (job.nv12) {
         uint8_t *D = job.nv12;
         for (int i = tid; i < (yb - ya) * 64; i += 256) {
-            int r = i >> 6, c = i & 63;
-            int gx = xa + c;
+            const int r = i >> 6, c = i & 63;
+            const int gx = xa + c;
             if (gx < xb) D[(size_t)(ya + r) * W + gx] = t[(ya - y0 + r) * 68 + (gx - x0)];
         }
-        /* chroma [32tx-2, 32tx+30) x [32ty-2, 32ty+30) interleaved */
+        /* chroma [32tx-2, 32tx+30) x [TH/2 ty-2, TH/2 ty+TH/2-2) interleaved */
         const int cxa = max(tx * 32 - 2, 0), cxb = min(tx * 32 + 30, job.CW);
-        const int cya = max(ty * 32 - 2, 0), cyb = min(ty * 32 + 30, job.CH);
+        const int cya = max(ty * (TH / 2) - 2, 0), cyb = min(ty * (TH / 2) + TH / 2 - 2, job.CH);
         const uint8_t *U = job.out + (size_t)W * job.H;
         const uint8_t *V = U + (size_t)job.CW * job.CH;
         uint8_t *UV = D + (size_t)W * job.H;
         for (int i = tid; i < (cyb - cya) * 32; i += 256) {
-            int r = i >> 5, c = i & 31;
-            int gx = cxa + c, gy = cya + r;
+            const int r = i >> 5, c = i & 31;
+            const int gx = cxa + c, gy = cya + r;
             if (gx >= cxb) continue;
-            size_t so = (size_t)gy * job.CW + gx;
-            size_t d = (size_t)gy * 2 * job.CW + 2 * gx;
+            const size_t so = (size_t)gy * job.CW + gx;
+            const size_t d = (size_t)gy * 2 * job.CW + 2 * gx;
             UV[d] = U[so];
             UV[d + 1] = V[so];
         }
@@ -2520,9 +2543,17 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     if ((e = mark(L->ev[2], st, capturing)) != cudaSuccess) return (int)e;
     if (L->lf_tiles_x > 0 && L->lf_tiles_y > 0) {
-        dim3 g((unsigned)L->lf_tiles_x, (unsigned)L->lf_tiles_y, (unsigned)L->njobs);
-        if (L->arith == CVP9_ARITH_SPEC) k_loopfilter<CVP9_ARITH_SPEC><<<g, 256, 0, st>>>(L->jobs);
-        else k_loopfilter<CVP9_ARITH_REFCPU><<<g, 256, 0, st>>>(L->jobs);
+        /* lf_tiles_y counts 64-row tiles; 32-row tiles need twice as many
+         * (one more covers the 4-row shift) */
+        if (L->lf_tile_h == 32) {
+            dim3 g((unsigned)L->lf_tiles_x, (unsigned)(2 * L->lf_tiles_y), (unsigned)L->njobs);
+            if (L->arith == CVP9_ARITH_SPEC) k_loopfilter<CVP9_ARITH_SPEC, 32><<<g, 256, 0, st>>>(L->jobs);
+            else k_loopfilter<CVP9_ARITH_REFCPU, 32><<<g, 256, 0, st>>>(L->jobs);
+        } else {
+            dim3 g((unsigned)L->lf_tiles_x, (unsigned)L->lf_tiles_y, (unsigned)L->njobs);
+            if (L->arith == CVP9_ARITH_SPEC) k_loopfilter<CVP9_ARITH_SPEC, 64><<<g, 256, 0, st>>>(L->jobs);
+            else k_loopfilter<CVP9_ARITH_REFCPU, 64><<<g, 256, 0, st>>>(L->jobs);
+        }
     }
     if (L->flat_lf_max_w > 0) {
         long long nh = (long long)((L->flat_lf_max_h + 7) / 8) * L->flat_lf_max_w;

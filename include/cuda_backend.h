@@ -55,6 +55,9 @@ typedef enum {
 typedef struct {
     int device;     /* CUDA ordinal; -1: $CVP9_CUDA_DEVICE or 0        */
     int arith;      /* cvp9_cuda_arith_t; -1: $CVP9_ARITH or REFCPU     */
+    int autotune;   /* >= 0: time the kernel configurations on the first
+                     * frames of each size and keep the fastest (unless
+                     * $CVP9_AUTOTUNE=0); -1: fixed defaults              */
 } cuda_backend_options_t;
 
 /* ── Drop-in entry points (vulkan_backend.h:141-163) ────────────────────── */

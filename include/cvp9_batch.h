@@ -41,7 +41,24 @@ typedef struct {
     uint64_t hbm_budget;     /* bytes of stream state to admit; 0: 150 GB         */
     int      max_streams;    /* 0: 1024                                          */
     int      use_graphs;     /* replay the kernel chain from per-bucket graphs    */
+    int      autotune;       /* choose the kernel configuration per shape bucket
+                              * by timing its first steps ($CVP9_AUTOTUNE=0
+                              * overrides); 0: fixed defaults                    */
 } cvp9_batch_config_t;
+
+/* The tuner's record of one shape bucket (a step's arithmetic, frame count
+ * and superblock count, each rounded up to a power of two). */
+typedef struct {
+    uint64_t key;
+    int      frames;         /* frames per step when the bucket was opened       */
+    int      settled;        /* 1: every knob measured, the fields below hold     */
+    int      inter_path;     /* 0 general kernel only, 1 warp-per-SB inter kernel
+                              * (96 registers), 2 the same at 80 registers       */
+    int      lf_tile_h;      /* loop-filter tile height, 64 or 32                */
+    int      half_width;     /* 1: wavefront kernel on half the resident CTAs    */
+    int      trials;         /* configurations measured                          */
+    float    best_ms;        /* kernel time of the best configuration            */
+} cvp9_batch_tune_t;
 
 enum {
     CVP9_BATCH_DEVICE_INPUTS = 1u << 0,
@@ -108,6 +125,10 @@ uint64_t    cvp9_batch_last_seq(cvp9_batch_t *b);
  * landing in host memory (CVP9_ERR_AGAIN while it runs; the most recent
  * 4096 steps are kept). */
 cvp9_err_t  cvp9_batch_step_latency(cvp9_batch_t *b, uint64_t seq, double *ms);
+
+/* Tuner buckets in use, and a copy of bucket i (0 <= i < count). */
+int         cvp9_batch_tune_count(cvp9_batch_t *b);
+cvp9_err_t  cvp9_batch_tune_entry(cvp9_batch_t *b, int i, cvp9_batch_tune_t *out);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,7 @@ MIX = [
 ]
 
 
-def decode_mix(profile, streams, frames, graphs=1, order=None, seeds=None):
+def decode_mix(profile, streams, frames, graphs=1, order=None, seeds=None, tuning=None):
     eng = Batch(arith=profile, use_graphs=graphs)
     seeds = seeds or [10 + i for i in range(len(streams))]
     syns = [Synth(synth_config(p, w, h, seed=seeds[i], **ov)) for i, (p, w, h, ov) in enumerate(streams)]
@@ -36,6 +36,8 @@ def decode_mix(profile, streams, frames, graphs=1, order=None, seeds=None):
             rc, arr = eng.get_frame_array(sids[i])
             assert rc == CVP9_OK, (rc, eng.last_error())
             outs[i].append(arr)
+    if tuning is not None:
+        tuning.extend(eng.tuning())
     eng.close()
     return outs
 
@@ -104,3 +106,25 @@ def test_admission_budget():
     assert eng.open_stream(1920, 1080) is not None     # the freed reservation admits one more
     assert eng.open_stream(1920, 1080) is None
     eng.close()
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_autotune_settles_with_oracle_output(profile):
+    """The tuner runs every candidate configuration on real steps: each of
+    those steps still decodes to the oracle's bytes, and the bucket settles
+    after all knobs were measured (REFCPU: 3 inter paths + filter tile +
+    wavefront width = 5 configurations; SPEC: 3)."""
+    tuning = []
+    frames = 12
+    outs = decode_mix(profile, MIX, frames, tuning=tuning)
+    for i, (p, w, h, ov) in enumerate(MIX):
+        syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
+        orc = OracleStream(profile)
+        for f in range(frames):
+            want = orc.decode(syn.frame(f))
+            assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
+    assert len(tuning) == 1, tuning
+    e = tuning[0]
+    assert e["settled"] == 1 and e["trials"] == (5 if profile == REFCPU else 3), e
+    assert e["best_ms"] > 0 and e["lf_tile_h"] in (32, 64)
+    assert e["inter_path"] in ((0, 1, 2) if profile == REFCPU else (0,))
