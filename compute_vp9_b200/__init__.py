@@ -27,7 +27,7 @@ EXPORTED_SYMBOLS = [
     "cuda_backend_init", "cuda_backend_destroy", "cuda_decode_frame", "cuda_get_frame",
     "cuda_get_frame_dmabuf", "cuda_export_buffer_alloc", "cuda_export_buffer_free",
     "cuda_set_render_target", "cuda_backend_init_ex", "cuda_backend_last_timing",
-    "cuda_backend_last_error",
+    "cuda_backend_last_error", "cuda_backend_selftest_wait_limit",
     "cvp9_batch_create", "cvp9_batch_destroy", "cvp9_batch_stream_bytes",
     "cvp9_batch_open_stream", "cvp9_batch_close_stream", "cvp9_batch_submit",
     "cvp9_batch_wait", "cvp9_batch_poll", "cvp9_batch_get_frame", "cvp9_batch_stats",

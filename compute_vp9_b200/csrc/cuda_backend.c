@@ -511,3 +511,76 @@ const char *cuda_backend_last_error(void *ctx)
     cuctx_t *c = (cuctx_t *)ctx;
     return c ? c->last_error : "";
 }
+
+cvp9_err_t cuda_backend_selftest_wait_limit(int device, uint32_t *status, float *ms)
+{
+    if (!status || !ms) return CVP9_ERR_INVALID_DATA;
+    *status = 0;
+    *ms = 0.f;
+    if (device < 0) device = cvp9_env_device();
+    if (cudaSetDevice(device) != cudaSuccess || cvp9_device_setup(device) != 0) return CVP9_ERR_NO_BACKEND;
+    const int W = 128, H = 64;
+    vp9_macroblock_info_t blk[2];
+    memset(blk, 0, sizeof(blk));
+    blk[0].x = 0;  blk[0].width = 64; blk[0].height = 64; blk[0].tx_size = 3;
+    blk[0].ref_frame[0] = 1; blk[0].skip = 1;            /* inter, left SB   */
+    blk[1].x = 64; blk[1].width = 64; blk[1].height = 64; blk[1].tx_size = 3;
+    blk[1].is_intra = 1; blk[1].skip = 1;                /* intra, right SB  */
+    const size_t fb = (size_t)W * H + 2 * (size_t)(W / 2) * (H / 2);
+    const uint32_t ticket = 1u;                          /* job 0, SB 1 only */
+    vp9_macroblock_info_t *d_blk = NULL;
+    uint8_t *d_out = NULL;
+    uint32_t *d_u32 = NULL;                              /* sb_range 8, sb_done 2, status 1, counter 1, ticket 1 */
+    cvp9_job_t *d_job = NULL;
+    cudaEvent_t e0 = NULL, e1 = NULL;
+    cvp9_err_t rc = CVP9_ERR_GPU;
+    if (cudaMalloc((void **)&d_blk, sizeof(blk)) != cudaSuccess ||
+        cudaMalloc((void **)&d_out, fb) != cudaSuccess ||
+        cudaMalloc((void **)&d_u32, 13 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc((void **)&d_job, sizeof(cvp9_job_t)) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        goto done;
+    {
+        cvp9_job_t job;
+        memset(&job, 0, sizeof(job));
+        job.W = W; job.H = H; job.CW = W / 2; job.CH = H / 2;
+        job.sb_cols = 2; job.sb_rows = 1; job.mi_cols = W / 8; job.mi_rows = H / 8;
+        job.blocks = d_blk; job.num_blocks = 2;
+        job.coeffs = NULL; job.num_coeffs = 0;
+        job.out = d_out;
+        job.lf_level = 0; job.lf_tiled = 1;
+        job.epoch = 1;
+        job.sb_range = d_u32;
+        job.sb_done = d_u32 + 8;
+        job.status = d_u32 + 10;
+        if (cudaMemcpy(d_blk, blk, sizeof(blk), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(d_u32, 0, 13 * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMemcpy(d_u32 + 12, &ticket, 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_job, &job, sizeof(job), cudaMemcpyHostToDevice) != cudaSuccess)
+            goto done;
+        cvp9k_launch_t L;
+        memset(&L, 0, sizeof(L));
+        L.jobs = d_job;
+        L.njobs = 1;
+        L.arith = CVP9_ARITH_REFCPU;
+        L.max_blocks = 2;
+        L.tickets = d_u32 + 12;
+        L.n_tickets = 1;
+        L.ticket_counter = d_u32 + 11;
+        L.recon_ctas = 1;
+        if (cudaEventRecord(e0, 0) != cudaSuccess || cvp9k_launch_frame(&L, 0) != 0 ||
+            cudaEventRecord(e1, 0) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+            goto done;
+        cudaEventElapsedTime(ms, e0, e1);
+        if (cudaMemcpy(status, d_u32 + 10, 4, cudaMemcpyDeviceToHost) != cudaSuccess) goto done;
+        rc = CVP9_OK;
+    }
+done:
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_blk);
+    cudaFree(d_out);
+    cudaFree(d_u32);
+    cudaFree(d_job);
+    return rc;
+}

@@ -84,6 +84,17 @@ cvp9_err_t cuda_backend_last_timing(void *ctx, float *total_ms, float *kernels_m
 /* Text of the last CUDA error seen by this context ("" if none). */
 const char *cuda_backend_last_error(void *ctx);
 
+/* Diagnostic, no counterpart in the reference: exercises the bounded
+ * neighbour wait of the wavefront kernel. A 128x64 frame whose right
+ * superblock holds an intra block is reconstructed with only that superblock
+ * scheduled, so its wait for the left neighbour can never be satisfied; the
+ * wait gives up after its iteration limit and the kernel returns. *status
+ * receives the frame's CVP9_JOB_* word (CVP9_JOB_TIMEOUT set when the limit
+ * worked), *ms the kernel's device time. Returns CVP9_OK when the launch
+ * completed and the device stayed usable. Allocates and frees its own small
+ * buffers on `device` (-1: $CVP9_CUDA_DEVICE or 0). */
+cvp9_err_t cuda_backend_selftest_wait_limit(int device, uint32_t *status, float *ms);
+
 /* ── Allocation-free reconstruction of one frame ────────────────────────── *
  * No counterpart in the reference. For callers that must not allocate GPU
  * memory while decoding — a media framework or inference server that owns
