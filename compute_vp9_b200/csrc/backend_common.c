@@ -86,6 +86,12 @@ int cvp9_env_device(void)
     return e && *e ? atoi(e) : 0;
 }
 
+int cvp9_env_gather(void)
+{
+    const char *e = getenv("CVP9_GATHER");
+    return !(e && *e == '0');
+}
+
 int cvp9_env_autotune(void)
 {
     const char *e = getenv("CVP9_AUTOTUNE");

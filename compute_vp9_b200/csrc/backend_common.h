@@ -42,6 +42,7 @@ int cvp9_env_device(void);
 int cvp9_env_arith(void);
 int cvp9_env_inter_fast(void);
 int cvp9_env_autotune(void);        /* $CVP9_AUTOTUNE: 0 turns tuning off */
+int cvp9_env_gather(void);          /* $CVP9_GATHER: 0 uploads whole coefficient arrays */
 
 /* Fill the frame-geometry and parameter fields of a job from a parsed
  * frame (inputs, output, refs and scratch pointers are set by the caller). */

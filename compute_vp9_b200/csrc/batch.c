@@ -76,7 +76,7 @@ typedef struct {
     uint8_t        *d_in;   size_t d_in_cap;
     cvp9_job_t     *h_jobs; cvp9_job_t *d_jobs; int jobs_cap;
     uint32_t       *d_sb_range; size_t sb_cap;      /* uint32 entries */
-    uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status */
+    uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status, [n+1] gathered bytes */
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
     uint32_t       *h_tickets; size_t h_tickets_cap;
     uint32_t       *d_fast; size_t fast_cap;    /* inter fast path: flags, tickets, count */
@@ -88,10 +88,12 @@ typedef struct {
     int            *sids;  int sids_cap;
     uint64_t        h2d_bytes, d2h_bytes;
     uint32_t        launches;
+    uint32_t        launches_extra;  /* upload-stream kernels of the step */
 } bslot_t;
 
 struct cvp9_batch {
     int          device, arith, use_graphs, max_streams;
+    int          gather;     /* REFCPU: luma-only coefficient upload by kernel */
     cvp9_tuner_t tuner;      /* kernel configuration per shape bucket */
     uint64_t     budget, reserved;
     cudaStream_t cs, hs, ds;
@@ -149,6 +151,7 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     b->budget = (cfg && cfg->hbm_budget) ? cfg->hbm_budget : 150ull * 1000 * 1000 * 1000;
     b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
     b->use_graphs = cfg ? cfg->use_graphs : 1;
+    b->gather = b->arith == CVP9_ARITH_REFCPU && cvp9_env_gather();
     {
         cvp9_tcfg_t fixed = { (int8_t)(b->arith == CVP9_ARITH_REFCPU ? cvp9_env_inter_fast() : 0), 0, 0 };
         cvp9_tuner_init(&b->tuner, b->arith, cfg && cfg->autotune && cvp9_env_autotune(), fixed);
@@ -419,9 +422,9 @@ static void complete_slot(cvp9_batch_t *b, bslot_t *s)
     b->last.step_ms = t;
     b->last.kernels_ms = k;
     b->last.h2d_ms = u;
-    b->last.h2d_bytes = s->h2d_bytes;
+    b->last.h2d_bytes = s->h2d_bytes + s->h_misc[s->n + 1];
     b->last.d2h_bytes = s->d2h_bytes;
-    b->last.kernel_launches = s->launches;
+    b->last.kernel_launches = s->launches + s->launches_extra;
     float a = 0.f, r = 0.f, f = 0.f;
     cudaEventElapsedTime(&a, s->ev_kern[0], s->ev_kern[1]);
     cudaEventElapsedTime(&r, s->ev_kern[1], s->ev_kern[2]);
@@ -462,6 +465,14 @@ static int is_pinned(const void *p)
     struct cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return 0; }
     return a.type == cudaMemoryTypeHost;
+}
+
+/* Device address of page-locked host memory (NULL if it is not mapped). */
+static const void *mapped_ptr(const void *p)
+{
+    struct cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return NULL; }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : NULL;
 }
 
 static void CUDART_CB step_done_cb(void *p)
@@ -545,8 +556,8 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
             return err;
         s->jobs_cap = cap;
     }
-    if (s->misc_cap < n + 1) {
-        int cap = (n > b->nst ? n : b->nst) + 1;
+    if (s->misc_cap < n + 2) {
+        int cap = (n > b->nst ? n : b->nst) + 2;
         s->misc_cap = 0;
         if ((err = grow_host(b, (void **)&s->h_misc, &s->h_misc_bytes, (size_t)cap * 4)) ||
             (err = grow_dev(b, (void **)&s->d_misc, &s->d_misc_bytes, (size_t)cap * 4)))
@@ -585,9 +596,12 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     BCK(cudaEventRecord(s->ev_start, b->hs), "event");
     size_t off = 0;
     const uint8_t *dev_blocks[256], *dev_coeffs[256];
+    const void *gather_local[256];
     const uint8_t **dbp = n <= 256 ? dev_blocks : malloc((size_t)n * sizeof(void *));
     const uint8_t **dcp = n <= 256 ? dev_coeffs : malloc((size_t)n * sizeof(void *));
-    if (!dbp || !dcp) return CVP9_ERR_NOMEM;
+    const void **gsrc = n <= 256 ? gather_local : malloc((size_t)n * sizeof(void *));
+    if (!dbp || !dcp || !gsrc) return CVP9_ERR_NOMEM;
+    int any_gather = 0;
     typedef struct { const void *src; size_t off, n; } direct_t;
     direct_t direct_local[512];
     direct_t *direct = n <= 256 ? direct_local : malloc((size_t)2 * n * sizeof(direct_t));
@@ -595,17 +609,23 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     int ndirect = 0, any_staged = 0;
     for (int i = 0; i < n; i++) {
         const vp9_parsed_frame_t *pf = pfs[i];
+        gsrc[i] = NULL;
         if (dev_in) {
             dbp[i] = (const uint8_t *)pf->blocks;
             dcp[i] = (const uint8_t *)pf->coeffs;
             continue;
         }
+        /* REFCPU reads only each block's luma coefficients: from page-locked
+         * memory a kernel moves just those (k_gather_luma), not the array */
+        if (b->gather && pf->num_coeffs && pf->num_blocks)
+            gsrc[i] = mapped_ptr(pf->coeffs);
+        any_gather |= gsrc[i] != NULL;
         size_t nbb = (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t);
         size_t ncb = (size_t)pf->num_coeffs * sizeof(int16_t);
         const void *srcs[2] = { pf->blocks, pf->coeffs };
         size_t lens[2] = { nbb, ncb };
         for (int k = 0; k < 2; k++) {
-            if (lens[k]) {
+            if (lens[k] && !(k == 1 && gsrc[i])) {
                 if (is_pinned(srcs[k])) {
                     direct[ndirect].src = srcs[k];
                     direct[ndirect].off = off;
@@ -638,6 +658,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     if (ue != cudaSuccess) {
         if (dbp != dev_blocks) free(dbp);
         if (dcp != dev_coeffs) free(dcp);
+        if (gsrc != gather_local) free(gsrc);
         return bfail(b, ue, "upload inputs");
     }
 
@@ -670,6 +691,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
                 job->ref[r].h = st->f[f].h;
             }
         }
+        job->coeffs_src = (const int16_t *)gsrc[i];
         job->epoch = ++st->epoch;
         job->sb_range = s->d_sb_range + 4 * (size_t)sb_base;
         job->sb_done = st->d_sb_done;
@@ -679,9 +701,20 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     }
     if (dbp != dev_blocks) free(dbp);
     if (dcp != dev_coeffs) free(dcp);
+    if (gsrc != gather_local) free(gsrc);
     BCK(cudaMemcpyAsync(s->d_jobs, s->h_jobs, (size_t)n * sizeof(cvp9_job_t), cudaMemcpyHostToDevice, b->hs),
         "upload jobs");
     s->h2d_bytes += (size_t)n * sizeof(cvp9_job_t);
+    /* the counter of gathered bytes is cleared here, on the upload stream;
+     * the compute stream's clear of the status words stops before it */
+    BCK(cudaMemsetAsync(s->d_misc + n + 1, 0, 4, b->hs), "clear gather counter");
+    if (any_gather) {
+        int grc = cvp9k_launch_gather(s->d_jobs, n, max_blocks, s->d_misc + n + 1, b->hs);
+        if (grc != 0) return bfail(b, (cudaError_t)grc, "coefficient gather");
+        s->launches_extra = 1;
+    } else {
+        s->launches_extra = 0;
+    }
     BCK(cudaEventRecord(s->ev_h2d, b->hs), "event");
 
     /* kernels */
@@ -788,7 +821,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         }
     }
     if (ofr != out_frame) free(ofr);
-    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
+    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 2) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
     s->d2h_bytes += (size_t)(n + 1) * 4;
     /* ev_end, then the completion callback (so a stamped step is complete
      * for every other query), then ev_cb, which slot reuse waits on so the

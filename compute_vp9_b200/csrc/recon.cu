@@ -2461,11 +2461,70 @@ __global__ void k_nv12_pack(const cvp9_job_t *__restrict__ jobs)
     }
 }
 
+/* ── Coefficient upload over PCIe, REFCPU ────────────────────────────────
+ * The dense coefficient array interleaves each block's luma TXs with its
+ * chroma TXs; REFCPU reads only the luma ones (vp9_reconstruct.c:336-360).
+ * A warp per block copies that span, [coeff_offset, + (cw/n)(ch/n) n^2),
+ * from the page-locked host array to the same offset of the device array
+ * with 16-byte reads when both sides share their alignment; the chroma
+ * coefficients never cross the bus. */
+__global__ void __launch_bounds__(256) k_gather_luma(const cvp9_job_t *__restrict__ jobs, uint32_t *bytes)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    const int16_t *src = job.coeffs_src;
+    if (!src) return;
+    int16_t *dst = const_cast<int16_t *>(job.coeffs);
+    const int lane = threadIdx.x & 31;
+    uint32_t moved = 0;
+    for (uint32_t bi = blockIdx.x * 8u + (threadIdx.x >> 5); bi < job.num_blocks; bi += gridDim.x * 8u) {
+        const uint32_t *g = reinterpret_cast<const uint32_t *>(job.blocks + bi);
+        const uint32_t g0 = g[0], g1 = g[1], g5 = g[5], g6 = g[6];
+        const int x = (int)(g0 & 0xffffu), y = (int)(g0 >> 16);
+        const int w = (int)(g1 & 0xffu), h = (int)((g1 >> 8) & 0xffu), tx = (int)((g1 >> 16) & 0xffu);
+        if ((g5 & 0xffu) || tx > 3 || x >= job.W || y >= job.H) continue;
+        const int n = 4 << tx;
+        const int cw = min(w, job.W - x), ch = min(h, job.H - y);
+        const uint64_t a = g6;
+        uint64_t e = a + (uint64_t)((cw / n) * (ch / n)) * (uint64_t)(n * n);
+        if (e > job.num_coeffs) e = job.num_coeffs;
+        if (a >= e) continue;
+        const char *s = reinterpret_cast<const char *>(src + a);
+        char *d = reinterpret_cast<char *>(dst + a);
+        const uint64_t len = (e - a) * 2;
+        if ((((uintptr_t)s ^ (uintptr_t)d) & 15) == 0) {
+            const uint64_t head = (16 - ((uintptr_t)s & 15)) & 15;
+            const uint64_t h2 = head < len ? head : len;
+            for (uint64_t o = 2 * lane; o < h2; o += 64)
+                *reinterpret_cast<int16_t *>(d + o) = *reinterpret_cast<const int16_t *>(s + o);
+            const uint64_t nv = (len - h2) / 16;
+            const uint4 *sv = reinterpret_cast<const uint4 *>(s + h2);
+            uint4 *dv = reinterpret_cast<uint4 *>(d + h2);
+            for (uint64_t v = lane; v < nv; v += 32) dv[v] = sv[v];
+            for (uint64_t o = h2 + nv * 16 + 2 * lane; o < len; o += 64)
+                *reinterpret_cast<int16_t *>(d + o) = *reinterpret_cast<const int16_t *>(s + o);
+        } else {
+            for (uint64_t o = 2 * lane; o < len; o += 64)
+                *reinterpret_cast<int16_t *>(d + o) = *reinterpret_cast<const int16_t *>(s + o);
+        }
+        moved += (uint32_t)len;
+    }
+    if (lane == 0 && moved) atomicAdd(bytes, moved);
+}
+
 /* ── C-ABI launch shims ─────────────────────────────────────────────────── */
 
 extern "C" {
 
 size_t cvp9k_recon_smem_bytes(void) { return sizeof(ReconSmem); }
+
+int cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, uint32_t *bytes, cudaStream_t st)
+{
+    if (njobs <= 0 || max_blocks <= 0) return 0;
+    int gx = (max_blocks + 7) / 8;
+    if (gx > 2048) gx = 2048;
+    k_gather_luma<<<dim3((unsigned)gx, (unsigned)njobs), 256, 0, st>>>(jobs, bytes);
+    return (int)cudaGetLastError();
+}
 
 int cvp9k_upload_dct_basis(const double *basis, int count)
 {

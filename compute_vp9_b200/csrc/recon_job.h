@@ -51,6 +51,9 @@ typedef struct {
     uint32_t *sb_range;             /* per SB {start, end, groups, spare}         */
     uint32_t *sb_done;              /* per SB: epoch of the last finished frame   */
     uint32_t *status;               /* CVP9_JOB_* bits                            */
+    const int16_t *coeffs_src;      /* REFCPU upload: the parser's coefficient array
+                                     * in page-locked host memory, read by
+                                     * k_gather_luma (NULL: coeffs already on device) */
 } cvp9_job_t;
 
 #ifdef __cplusplus

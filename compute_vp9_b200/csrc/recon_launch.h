@@ -44,6 +44,13 @@ size_t cvp9k_recon_smem_bytes(void);
 int    cvp9k_upload_dct_basis(const double *basis, int count);
 int    cvp9k_configure(void);
 int    cvp9k_recon_ctas_per_sm(int arith);
+/* REFCPU upload of the coefficients the reconstruction reads — each block's
+ * luma TXs — straight from page-locked host memory into jobs[j].coeffs, for
+ * every job with coeffs_src set; adds the bytes moved to *bytes (device).
+ * Blocks must already be on the device. */
+int    cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, uint32_t *bytes,
+                           cudaStream_t stream);
+
 /* Enqueue the chain on `stream`; returns the cudaError_t of the first
  * failing call (0 on success). */
 int    cvp9k_launch_frame(const cvp9k_launch_t *launch, cudaStream_t stream);

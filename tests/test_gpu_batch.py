@@ -128,3 +128,45 @@ def test_autotune_settles_with_oracle_output(profile):
     assert e["settled"] == 1 and e["trials"] == (5 if profile == REFCPU else 3), e
     assert e["best_ms"] > 0 and e["lf_tile_h"] in (32, 64)
     assert e["inter_path"] in ((0, 1, 2) if profile == REFCPU else (0,))
+
+
+def _pinned_copy(pf, keep):
+    """The parsed frame with its block and coefficient arrays copied into
+    page-locked host memory (the engine then DMAs them directly and, under
+    REFCPU, moves only the luma coefficients with its gather kernel)."""
+    import torch
+    from compute_vp9_b200 import BlockInfo, ParsedFrame
+    p = pf.contents
+    nb, nc = p.num_blocks, p.num_coeffs
+    bt = torch.empty(max(1, nb * 32), dtype=torch.uint8, pin_memory=True)
+    ct = torch.empty(max(1, nc), dtype=torch.int16, pin_memory=True)
+    C.memmove(bt.data_ptr(), C.cast(p.blocks, C.c_void_p), nb * 32)
+    C.memmove(ct.data_ptr(), C.cast(p.coeffs, C.c_void_p), nc * 2)
+    out = ParsedFrame()
+    C.memmove(C.byref(out), C.byref(p), C.sizeof(ParsedFrame))
+    out.blocks = C.cast(C.c_void_p(bt.data_ptr()), C.POINTER(BlockInfo))
+    out.coeffs = C.cast(C.c_void_p(ct.data_ptr()), C.POINTER(C.c_int16))
+    keep += [bt, ct, out]
+    return C.pointer(out)
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_pinned_inputs_match_oracle(profile):
+    """Page-locked inputs take the direct upload path (REFCPU: the luma-only
+    coefficient gather from host memory); every frame equals the oracle."""
+    eng = Batch(arith=profile)
+    syns = [Synth(synth_config(p, w, h, seed=30 + i, **ov)) for i, (p, w, h, ov) in enumerate(MIX)]
+    orcs = [OracleStream(profile) for _ in MIX]
+    sids = [eng.open_stream(w, h) for (_, w, h, _) in MIX]
+    for f in range(4):
+        keep = []
+        pfs = [syn.frame(f) for syn in syns]
+        eng.submit(sids, [_pinned_copy(pf, keep) for pf in pfs], [f] * len(MIX))
+        assert eng.wait() == CVP9_OK, eng.last_error()
+        for i in range(len(MIX)):
+            rc, arr = eng.get_frame_array(sids[i])
+            assert rc == CVP9_OK
+            assert np.array_equal(arr, orcs[i].decode(pfs[i])), "stream %d frame %d" % (i, f)
+    st = eng.stats()
+    assert st.h2d_bytes > 0
+    eng.close()
