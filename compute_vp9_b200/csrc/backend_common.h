@@ -61,14 +61,15 @@ double cvp9_now(void);
  * Per shape bucket, the kernel configuration is chosen by timing: each
  * candidate runs on two steps of that bucket (the faster counts), knobs are
  * settled one at a time (coordinate descent): the inter path, then the
- * loop-filter tile height, then the wavefront width. Every configuration
+ * loop-filter layout, then the wavefront width. Every configuration
  * produces the same bytes; only the speed differs. Pure host logic. */
 
 #define CVP9_TUNE_BUCKETS 64
 
 typedef struct {
     int8_t inter;      /* 0 general kernel only, 1 k_inter (96 registers), 2 k_inter (80) */
-    int8_t lf32;       /* loop-filter tiles 32 rows high instead of 64 */
+    int8_t lf32;       /* loop filter in 64x32 shared-memory tiles instead of
+                        * 8x16 register strips */
     int8_t half;       /* wavefront kernel on half the resident CTAs */
 } cvp9_tcfg_t;
 

@@ -508,7 +508,8 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
 
     /* sizes */
     size_t in_bytes = 0, n_sb = 0;
-    int max_blocks = 0, max_mi = 0, lf_tx = 0, lf_ty = 0, flat_w = 0, flat_h = 0, flat_nv = 0;
+    int max_blocks = 0, max_mi = 0, lf_tx = 0, lf_ty = 0, lf_sx = 0, lf_sy = 0;
+    int flat_w = 0, flat_h = 0, flat_nv = 0;
     int maxd = 0;
     uint64_t key = mix64(0, (uint64_t)n);
     for (int i = 0; i < n; i++) {
@@ -524,9 +525,15 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         if (mi > max_mi) max_mi = mi;
         int tiled = (st->W % 8) != 1 && (st->H % 8) != 1;
         if (tiled) {
+            /* both grids; the tuned configuration picks one per step below */
             int tx = (st->W + 4 + 63) / 64, ty = (st->H + 4 + 63) / 64;
             if (tx > lf_tx) lf_tx = tx;
             if (ty > lf_ty) lf_ty = ty;
+            if (!(st->W & 3)) {
+                int sx = ((st->W + 4 + 7) / 8 + 127) / 128, sy = (st->H + 4 + 15) / 16;
+                if (sx > lf_sx) lf_sx = sx;
+                if (sy > lf_sy) lf_sy = sy;
+            }
         } else {
             if (st->W > flat_w) flat_w = st->W;
             if (st->H > flat_h) flat_h = st->H;
@@ -535,6 +542,12 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         if (d > maxd) maxd = d;
         key = mix64(key, ((uint64_t)st->W << 32) | (uint64_t)st->H);
     }
+
+    /* kernel configuration of this step (tuner) */
+    cvp9_tcfg_t tc;
+    s->tune_idx = cvp9_tuner_pick(&b->tuner, cvp9_tune_key(b->arith, n, (uint64_t)n_sb), n, &tc);
+    s->tune_cfg = tc;
+    int any_tile = 0, any_strip = 0;
 
     /* per-slot buffers; pinned staging only when some array is pageable */
     if (!dev_in && in_bytes) {
@@ -679,6 +692,9 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         cvp9_job_t *job = &s->h_jobs[i];
         memset(job, 0, sizeof(*job));
         cvp9_job_geometry(job, pf);
+        if (job->lf_tiled && !tc.lf32 && !(st->W & 3)) job->lf_tiled = 2;   /* register strips */
+        any_tile |= job->lf_tiled == 1;
+        any_strip |= job->lf_tiled == 2;
         job->blocks = (const vp9_macroblock_info_t *)dbp[i];
         job->coeffs = (const int16_t *)dcp[i];
         job->out = st->f[of].dev;
@@ -730,9 +746,6 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     L.tickets = s->d_tickets;
     L.n_tickets = s->n_tickets;
     L.ticket_counter = s->d_misc;
-    cvp9_tcfg_t tc;
-    s->tune_idx = cvp9_tuner_pick(&b->tuner, cvp9_tune_key(b->arith, n, (uint64_t)n_sb), n, &tc);
-    s->tune_cfg = tc;
     {
         const int width = tc.half ? (b->resident_ctas + 1) / 2 : b->resident_ctas;
         L.recon_ctas = (int)s->n_tickets < width ? (int)s->n_tickets : width;
@@ -744,8 +757,10 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         L.n_general = s->d_fast + 2 * (size_t)s->n_tickets;
         L.inter_variant = tc.inter;
     }
-    L.lf_tiles_x = lf_tx;
-    L.lf_tiles_y = lf_ty;
+    L.lf_tiles_x = any_tile ? lf_tx : 0;
+    L.lf_tiles_y = any_tile ? lf_ty : 0;
+    L.lf_strips_x = any_strip ? lf_sx : 0;
+    L.lf_strips_y = any_strip ? lf_sy : 0;
     L.flat_lf_max_w = flat_w;
     L.flat_lf_max_h = flat_h;
     L.flat_nv12 = flat_nv;
@@ -755,7 +770,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
     gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
-    s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + (lf_tx > 0) + (flat_w > 0 ? 2 : 0) +
+    s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
                              (L.general && b->arith == CVP9_ARITH_REFCPU ? 2 : 0));
     if (b->use_graphs) {
         if (!s->graph || s->graph_key != gkey) {
@@ -987,7 +1002,7 @@ cvp9_err_t cvp9_batch_tune_entry(cvp9_batch_t *b, int i, cvp9_batch_tune_t *out)
         out->frames = e->frames;
         out->settled = e->state == 2;
         out->inter_path = e->best.inter;
-        out->lf_tile_h = e->best.lf32 ? 32 : 64;
+        out->lf_tile_h = e->best.lf32 ? 32 : 16;
         out->half_width = e->best.half;
         out->trials = e->trials;
         out->best_ms = e->trials ? e->best_ms : 0.f;

@@ -300,10 +300,14 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     cvp9_job_t *job = s->h_job;
     memset(job, 0, sizeof(*job));
     cvp9_job_geometry(job, pf);
+    cvp9_tcfg_t tc;
+    s->tune_idx = cvp9_tuner_pick(&c->tuner, cvp9_tune_key(c->arith, 1, (uint64_t)c->n_sb), 1, &tc);
+    s->tune_cfg = tc;
     job->blocks = (const vp9_macroblock_info_t *)s->d_blocks;
     job->coeffs = (const int16_t *)s->d_coeffs;
     job->out = c->frames[of].dev;
     job->nv12 = (uint8_t *)c->pending_target;
+    if (job->lf_tiled && !tc.lf32 && !(W & 3) && !job->nv12) job->lf_tiled = 2;   /* register strips */
     for (int i = 0; i < 8; i++) {
         int f = c->ref_slot[i];
         if (f >= 0) {
@@ -335,9 +339,6 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     L.tickets = c->d_tickets;
     L.n_tickets = c->n_tickets;
     L.ticket_counter = c->d_misc + 1;
-    cvp9_tcfg_t tc;
-    s->tune_idx = cvp9_tuner_pick(&c->tuner, cvp9_tune_key(c->arith, 1, (uint64_t)c->n_sb), 1, &tc);
-    s->tune_cfg = tc;
     L.recon_ctas = tc.half ? (c->recon_ctas + 1) / 2 : c->recon_ctas;
     L.lf_tile_h = tc.lf32 ? 32 : 64;
     if (tc.inter) {
@@ -346,7 +347,10 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
         L.n_general = c->d_fast + 2 * c->n_sb;
         L.inter_variant = tc.inter;
     }
-    if (job->lf_tiled) {
+    if (job->lf_tiled == 2) {
+        L.lf_strips_x = ((W + 4 + 7) / 8 + 127) / 128;
+        L.lf_strips_y = (H + 4 + 15) / 16;
+    } else if (job->lf_tiled) {
         L.lf_tiles_x = (W + 4 + 63) / 64;
         L.lf_tiles_y = (H + 4 + 63) / 64;
     } else {

@@ -2326,7 +2326,7 @@ __global__ void __launch_bounds__(256) k_loopfilter(const cvp9_job_t *__restrict
     const cvp9_job_t &job = jobs[blockIdx.z];
     const int tx = blockIdx.x, ty = blockIdx.y;
     const int x0 = tx * 64 - 4, y0 = ty * TH - 4;
-    if (!job.lf_tiled || x0 >= job.W || y0 >= job.H) return;
+    if (job.lf_tiled != 1 || x0 >= job.W || y0 >= job.H) return;
     const bool filt = !(A == CVP9_ARITH_REFCPU && job.lf_level == 0);
     if (!filt && !job.nv12) return;
     const int tid = threadIdx.x;
@@ -2410,6 +2410,98 @@ __global__ void __launch_bounds__(256) k_loopfilter(const cvp9_job_t *__restrict
             UV[d] = U[so];
             UV[d + 1] = V[so];
         }
+    }
+}
+
+/* Register strips: thread (k, j) owns luma columns [8k-4, 8k+4) and rows
+ * [16j-4, 16j+12) as two 32-bit words per row. Its two horizontal edges
+ * (rows 16j, 16j+8) have every tap inside the strip's rows, and its one
+ * vertical edge (column 8k) every tap inside its columns; every pixel lies in
+ * one strip. So the horizontal pass then the vertical pass run in registers,
+ * with the frame-wide result (vp9_reconstruct.c:146-190) and no shared
+ * memory or barriers. Jobs with lf_tiled == 2: W a multiple of 4 (whole
+ * words), W and H not of the form 8k+1, no NV12 target. */
+__device__ __forceinline__ uint32_t lf_byte(uint32_t w, int i) { return (w >> (8 * i)) & 0xffu; }
+__device__ __forceinline__ uint32_t lf_put(uint32_t w, int i, int v)
+{
+    return (w & ~(0xffu << (8 * i))) | ((uint32_t)v << (8 * i));
+}
+
+__device__ __forceinline__ void lf_filter_vals(int &P1, int &P0, int &Q0, int &Q1, int thr)
+{
+    const int d0 = P0 - Q0, d1 = P1 - Q1;
+    if (abs(d0) * 2 + abs(d1) / 2 > thr) return;
+    const int delta = clampi((3 * (Q0 - P0) + 4) >> 3, -thr, thr);
+    P0 = clampi(P0 + delta, 0, 255);
+    Q0 = clampi(Q0 - delta, 0, 255);
+    P1 = clampi(P1 + delta / 2, 0, 255);
+    Q1 = clampi(Q1 - delta / 2, 0, 255);
+}
+
+template <int A>
+__global__ void __launch_bounds__(128) k_lf_strip(const cvp9_job_t *__restrict__ jobs)
+{
+    const cvp9_job_t &job = jobs[blockIdx.z];
+    const int k = blockIdx.x * 128 + threadIdx.x;
+    const int xs = 8 * k - 4, y0 = 16 * (int)blockIdx.y - 4;
+    if (job.lf_tiled != 2 || xs >= job.W || y0 >= job.H) return;
+    if (A == CVP9_ARITH_REFCPU && job.lf_level == 0) return;
+    const int W = job.W, H = job.H;
+    uint8_t *Y = job.out;
+    const bool hasA = xs >= 0, hasB = xs + 4 < W;     /* word A: xs..xs+3, word B: xs+4..xs+7 */
+    uint32_t a[16], b[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const int gy = y0 + r;
+        a[r] = 0u;
+        b[r] = 0u;
+        if (gy >= 0 && gy < H) {
+            const uint8_t *row = Y + (size_t)gy * W;
+            if (hasA) a[r] = *reinterpret_cast<const uint32_t *>(row + xs);
+            if (hasB) b[r] = *reinterpret_cast<const uint32_t *>(row + xs + 4);
+        }
+    }
+    const int thr = lf_threshold(job.lf_level, job.lf_sharpness);
+    /* horizontal edges at strip rows 4 and 12 */
+#pragma unroll
+    for (int m = 4; m <= 12; m += 8) {
+        const int e = y0 + m;
+        if (e < 8 || e >= H) continue;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            if (c < 4 ? !hasA : !hasB) continue;
+            uint32_t *wv = c < 4 ? a : b;
+            const int bi = c & 3;
+            int P1 = (int)lf_byte(wv[m - 2], bi), P0 = (int)lf_byte(wv[m - 1], bi);
+            int Q0 = (int)lf_byte(wv[m], bi), Q1 = (int)lf_byte(wv[m + 1], bi);
+            lf_filter_vals(P1, P0, Q0, Q1, thr);
+            wv[m - 2] = lf_put(wv[m - 2], bi, P1);
+            wv[m - 1] = lf_put(wv[m - 1], bi, P0);
+            wv[m] = lf_put(wv[m], bi, Q0);
+            wv[m + 1] = lf_put(wv[m + 1], bi, Q1);
+        }
+    }
+    /* vertical edge at column xs + 4 = 8k: bytes 2, 3 of A and 0, 1 of B */
+    const int ev = xs + 4;
+    if (ev >= 8 && ev < W) {
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const int gy = y0 + r;
+            if (gy < 0 || gy >= H) continue;
+            int P1 = (int)lf_byte(a[r], 2), P0 = (int)lf_byte(a[r], 3);
+            int Q0 = (int)lf_byte(b[r], 0), Q1 = (int)lf_byte(b[r], 1);
+            lf_filter_vals(P1, P0, Q0, Q1, thr);
+            a[r] = (a[r] & 0x0000ffffu) | (uint32_t)P1 << 16 | (uint32_t)P0 << 24;
+            b[r] = (b[r] & 0xffff0000u) | (uint32_t)Q0 | (uint32_t)Q1 << 8;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const int gy = y0 + r;
+        if (gy < 0 || gy >= H) continue;
+        uint8_t *row = Y + (size_t)gy * W;
+        if (hasA) *reinterpret_cast<uint32_t *>(row + xs) = a[r];
+        if (hasB) *reinterpret_cast<uint32_t *>(row + xs + 4) = b[r];
     }
 }
 
@@ -2613,6 +2705,11 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
             if (L->arith == CVP9_ARITH_SPEC) k_loopfilter<CVP9_ARITH_SPEC, 64><<<g, 256, 0, st>>>(L->jobs);
             else k_loopfilter<CVP9_ARITH_REFCPU, 64><<<g, 256, 0, st>>>(L->jobs);
         }
+    }
+    if (L->lf_strips_x > 0 && L->lf_strips_y > 0) {
+        dim3 g((unsigned)L->lf_strips_x, (unsigned)L->lf_strips_y, (unsigned)L->njobs);
+        if (L->arith == CVP9_ARITH_SPEC) k_lf_strip<CVP9_ARITH_SPEC><<<g, 128, 0, st>>>(L->jobs);
+        else k_lf_strip<CVP9_ARITH_REFCPU><<<g, 128, 0, st>>>(L->jobs);
     }
     if (L->flat_lf_max_w > 0) {
         long long nh = (long long)((L->flat_lf_max_h + 7) / 8) * L->flat_lf_max_w;

@@ -46,7 +46,8 @@ typedef struct {
     int32_t  q_dc, q_ac;            /* frame quantiser steps (SPEC residual)      */
     int32_t  lf_level, lf_sharpness;
     uint8_t  ref_slot_of[3];        /* SPEC: LAST/GOLDEN/ALTREF -> pool slot      */
-    uint8_t  lf_tiled;              /* 1: tile-local loop filter is exact         */
+    uint8_t  lf_tiled;              /* 0: frame-wide filter (W or H = 8k+1);
+                                     * 1: shared-memory tiles; 2: register strips */
     uint32_t epoch;                 /* frame sequence number for sb_done flags    */
     uint32_t *sb_range;             /* per SB {start, end, groups, spare}         */
     uint32_t *sb_done;              /* per SB: epoch of the last finished frame   */

@@ -27,6 +27,7 @@ typedef struct {
     int              recon_ctas;   /* grid of the persistent recon kernel        */
     int              lf_tiles_x, lf_tiles_y;   /* tiled filter grid in 64x64 tiles (max over jobs) */
     int              lf_tile_h;    /* 64 (default) or 32: filter tile height */
+    int              lf_strips_x, lf_strips_y;  /* register-strip filter grid (jobs with lf_tiled == 2) */
     int              flat_lf_max_w, flat_lf_max_h; /* >0: run the frame-wide filter */
     int              flat_nv12;
     /* Inter fast path (REFCPU): when `general` is set, k_inter takes the

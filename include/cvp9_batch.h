@@ -54,7 +54,8 @@ typedef struct {
     int      settled;        /* 1: every knob measured, the fields below hold     */
     int      inter_path;     /* 0 general kernel only, 1 warp-per-SB inter kernel
                               * (96 registers), 2 the same at 80 registers       */
-    int      lf_tile_h;      /* loop-filter tile height, 64 or 32                */
+    int      lf_tile_h;      /* loop filter: 16 register strips (8x16 per thread),
+                              * 32 shared-memory tiles (64x32 per CTA)           */
     int      half_width;     /* 1: wavefront kernel on half the resident CTAs    */
     int      trials;         /* configurations measured                          */
     float    best_ms;        /* kernel time of the best configuration            */

@@ -126,7 +126,7 @@ def test_autotune_settles_with_oracle_output(profile):
     assert len(tuning) == 1, tuning
     e = tuning[0]
     assert e["settled"] == 1 and e["trials"] == (5 if profile == REFCPU else 3), e
-    assert e["best_ms"] > 0 and e["lf_tile_h"] in (32, 64)
+    assert e["best_ms"] > 0 and e["lf_tile_h"] in (16, 32)
     assert e["inter_path"] in ((0, 1, 2) if profile == REFCPU else (0,))
 
 
