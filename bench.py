@@ -400,8 +400,9 @@ def read_peaks():
 
 
 def read_traffic():
-    """Per-launch DRAM bytes of the recon kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_recon_refcpu_1080p_x32.md")
+    """Per-launch DRAM bytes of the dominant recon kernel (k_inter) at the
+    bench workload, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_inter_refcpu_1080p_x16.md")
     try:
         with open(p) as f:
             for line in f:
