@@ -1637,12 +1637,16 @@ __device__ __forceinline__ int fb_slot(const FastBlk &b) { return (int)((b.geo >
 __device__ __forceinline__ int fb_txl(const FastBlk &b) { return (int)((b.geo >> 26) & 3u); }
 __device__ __forceinline__ bool fb_skip(const FastBlk &b) { return (b.geo >> 28) & 1u; }
 
+/* Tile pitches: 72 and 40 bytes put eight consecutive rows in eight
+ * different bank groups (a 64-byte pitch maps rows r and r+2 together). */
+constexpr int kFY = 72, kFC = 40;
+
 struct __align__(16) FastSmem {                   /* one per warp; 16-byte vector access */
-    uint8_t  ty[64 * 64];                         /* luma tile, pitch 64 */
-    uint8_t  tu[32 * 32];
-    uint8_t  tv[32 * 32];
+    uint8_t  ty[64 * kFY];                        /* luma tile */
+    uint8_t  tu[32 * kFC];
+    uint8_t  tv[32 * kFC];
     union {
-        int16_t  coef[1024];                      /* residual: coefficients of the TXs in flight */
+        int16_t  coef[1056];                      /* residual: the TXs in flight, (N*N + 2) apart */
         uint32_t cells[8];                        /* set-up: 4x4-cell occupancy, 2 cell rows per word */
     };
     FastBlk  blk[64];
@@ -1660,12 +1664,19 @@ struct __align__(16) FastSmem {                   /* one per warp; 16-byte vecto
 
 /* The basis again in global memory: lane-varying reads are served by L1
  * instead of being serialised by the constant cache. */
-__device__ double g_dct[16 + 64 + 256 + 1024];
+__device__ __align__(16) double g_dct[16 + 64 + 256 + 1024];
 
 static_assert(sizeof(FastSmem) % 16 == 0, "per-warp tiles must stay 16-byte aligned");
-static_assert(sizeof(FastSmem) * kFastWarps + 1024 <= 233472 / 6, "six CTAs of k_inter per SM");
+static_assert(sizeof(FastSmem) * kFastWarps + 1024 <= 233472 / 5, "five CTAs of k_inter per SM");
 static_assert(offsetof(FastSmem, coef) % 16 == 0 && offsetof(FastSmem, tu) % 16 == 0 &&
               offsetof(FastSmem, tv) % 16 == 0, "vector-accessed members must be 16-byte aligned");
+
+/* 16 bytes from an 8-byte-aligned shared-memory address */
+__device__ __forceinline__ uint4 ld_smem16(const uint8_t *p)
+{
+    const uint2 a = reinterpret_cast<const uint2 *>(p)[0], b = reinterpret_cast<const uint2 *>(p)[1];
+    return make_uint4(a.x, a.y, b.x, b.y);
+}
 
 __device__ __forceinline__ int warp_incl_scan(int x, int lane)
 {
@@ -1815,7 +1826,7 @@ __device__ __forceinline__ FastLuma fast_luma_issue(FastSmem &w, const cvp9_job_
     fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
     if (kk >= lh) return J;
     J.act = true;
-    J.d = w.ty + (ly0 + kk) * 64 + lx0;
+    J.d = w.ty + (ly0 + kk) * kFY + lx0;
     J.lw = lw;
     const int slot = fb_slot(fb);
     if (slot >= 8) return J;
@@ -1868,7 +1879,7 @@ __device__ __forceinline__ FastChroma fast_chroma_issue(FastSmem &w, const cvp9_
     fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
     if (r >= clh || clw <= 0) return J;
     J.act = true;
-    J.d = (p ? w.tv : w.tu) + (cy0 + r) * 32 + cx0;
+    J.d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
     J.clw = clw;
     const int slot = fb_slot(fb);
     if (slot >= 8) return J;
@@ -1971,7 +1982,7 @@ __device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int l
     const int boff = N == 4 ? 0 : N == 8 ? 16 : N == 16 ? 80 : 336;
     const double *Mg = g_dct + boff;     /* lane-varying reads */
     const double *Mc = c_dct + boff;     /* warp-uniform reads */
-    int16_t *X = w.coef + g * NN;
+    int16_t *X = w.coef + g * (NN + 2);      /* padded: the groups' rows fall in different banks */
     uint32_t rv[N / 2];
     int px0, py0;
     bool have;
@@ -2021,7 +2032,7 @@ __device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int l
                     for (int j = 0; j < NJ; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, Mc[k * N + h * NJ + j]));
                 }
                 if (have) {
-                    uint32_t *row = reinterpret_cast<uint32_t *>(w.ty + (py0 + i) * 64 + px0 + h * NJ);
+                    uint32_t *row = reinterpret_cast<uint32_t *>(w.ty + (py0 + i) * kFY + px0 + h * NJ);
 #pragma unroll
                     for (int j4 = 0; j4 < NJ / 4; j4++) {
                         uint32_t word = row[j4], outw = 0;
@@ -2142,19 +2153,17 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
 
     /* 3. prediction (vp9_reconstruct.c:94-131). Luma passes: lane = (chunk
      * c0 + lane/8, row lane%8); chroma passes: lane = (chunk c0 + lane/8,
-     * plane, row). Two passes are in flight: both issue their loads before
-     * either computes. */
+     * plane, row). Two luma and two chroma passes are in flight: all four
+     * issue their loads before any computes. */
     for (int c0 = 0; c0 < nchunks; c0 += 8) {
         const FastLuma a = fast_luma_issue(w, job, c0 + (lane >> 3), lane & 7, nchunks, sbx, sby);
         const FastLuma b = fast_luma_issue(w, job, c0 + 4 + (lane >> 3), lane & 7, nchunks, sbx, sby);
+        const FastChroma ca = fast_chroma_issue(w, job, c0 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
+        const FastChroma cb = fast_chroma_issue(w, job, c0 + 4 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
         fast_luma_finish(a);
         fast_luma_finish(b);
-    }
-    for (int c0 = 0; c0 < nchunks; c0 += 8) {
-        const FastChroma a = fast_chroma_issue(w, job, c0 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
-        const FastChroma b = fast_chroma_issue(w, job, c0 + 4 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
-        fast_chroma_finish(a);
-        fast_chroma_finish(b);
+        fast_chroma_finish(ca);
+        fast_chroma_finish(cb);
     }
     __syncwarp();
 
@@ -2201,19 +2210,19 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
                 const int r = i >> 2, c16 = (i & 3) * 16;
                 if (c16 < vw)
                     *reinterpret_cast<uint4 *>(Y + (size_t)(sby + r) * W + sbx + c16) =
-                        *reinterpret_cast<const uint4 *>(w.ty + r * 64 + c16);
+                        ld_smem16(w.ty + r * kFY + c16);
             }
         } else if (!(W & 3) && !((uintptr_t)Y & 3)) {
             for (int i = lane; i < vh * 16; i += 32) {
                 const int r = i >> 4, c4 = (i & 15) * 4;
                 if (c4 < vw)
                     *reinterpret_cast<uint32_t *>(Y + (size_t)(sby + r) * W + sbx + c4) =
-                        *reinterpret_cast<const uint32_t *>(w.ty + r * 64 + c4);
+                        *reinterpret_cast<const uint32_t *>(w.ty + r * kFY + c4);
             }
         } else {
             for (int i = lane; i < vh * 64; i += 32) {
                 const int r = i >> 6, c = i & 63;
-                if (c < vw) Y[(size_t)(sby + r) * W + sbx + c] = w.ty[r * 64 + c];
+                if (c < vw) Y[(size_t)(sby + r) * W + sbx + c] = w.ty[r * kFY + c];
             }
         }
         const int CW = job.CW, CH = job.CH;
@@ -2226,7 +2235,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
                 const int r = k >> 1, c16 = (k & 1) * 16;
                 if (c16 < cvw)
                     *reinterpret_cast<uint4 *>((p ? V : U) + (size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c16) =
-                        *reinterpret_cast<const uint4 *>((p ? w.tv : w.tu) + r * 32 + c16);
+                        ld_smem16((p ? w.tv : w.tu) + r * kFC + c16);
             }
         } else if (!(CW & 3) && !((uintptr_t)U & 3) && !((uintptr_t)V & 3)) {
             for (int i = lane; i < 2 * cvh * 8; i += 32) {
@@ -2234,13 +2243,13 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
                 const int r = k >> 3, c4 = (k & 7) * 4;
                 if (c4 < cvw)
                     *reinterpret_cast<uint32_t *>((p ? V : U) + (size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c4) =
-                        *reinterpret_cast<const uint32_t *>((p ? w.tv : w.tu) + r * 32 + c4);
+                        *reinterpret_cast<const uint32_t *>((p ? w.tv : w.tu) + r * kFC + c4);
             }
         } else {
             for (int i = lane; i < 2 * cvh * 32; i += 32) {
                 const int p = i >= cvh * 32, k = p ? i - cvh * 32 : i;
                 const int r = k >> 5, c = k & 31;
-                if (c < cvw) (p ? V : U)[(size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c] = (p ? w.tv : w.tu)[r * 32 + c];
+                if (c < cvw) (p ? V : U)[(size_t)((sby >> 1) + r) * CW + (sbx >> 1) + c] = (p ? w.tv : w.tu)[r * kFC + c];
             }
         }
     }
