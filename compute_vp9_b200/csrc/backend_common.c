@@ -174,9 +174,9 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
     for (;;) {
         e->idx++;
         if (e->stage == 0) {
-            /* inter path: the default was candidate 0; SPEC has no k_inter */
+            /* inter path: the default was candidate 0 */
             static const int8_t alts[2] = { 0, 2 };
-            if (t->arith == 0 && e->idx <= 2) {
+            if (e->idx <= 2) {
                 e->cur = e->best;
                 e->cur.inter = alts[e->idx - 1];
                 break;

@@ -153,7 +153,7 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     b->use_graphs = cfg ? cfg->use_graphs : 1;
     b->gather = b->arith == CVP9_ARITH_REFCPU && cvp9_env_gather();
     {
-        cvp9_tcfg_t fixed = { (int8_t)(b->arith == CVP9_ARITH_REFCPU ? cvp9_env_inter_fast() : 0), 0, 0 };
+        cvp9_tcfg_t fixed = { (int8_t)cvp9_env_inter_fast(), 0, 0 };
         cvp9_tuner_init(&b->tuner, b->arith, cfg && cfg->autotune && cvp9_env_autotune(), fixed);
     }
     if (b->device >= ndev || cvp9_device_setup(b->device) != 0) { free(b); return CVP9_ERR_NO_BACKEND; }
@@ -771,7 +771,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
     gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
     s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
-                             (L.general && b->arith == CVP9_ARITH_REFCPU ? 2 : 0));
+                             (L.general ? 2 : 0));
     if (b->use_graphs) {
         if (!s->graph || s->graph_key != gkey) {
             if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = NULL; }

@@ -126,7 +126,7 @@ cvp9_err_t cuda_backend_init_ex(void **out, const cuda_backend_options_t *opt)
     c->arith = (opt && opt->arith >= 0) ? (opt->arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU)
                                         : cvp9_env_arith();
     {
-        cvp9_tcfg_t fixed = { (int8_t)(c->arith == CVP9_ARITH_REFCPU ? cvp9_env_inter_fast() : 0), 0, 0 };
+        cvp9_tcfg_t fixed = { (int8_t)cvp9_env_inter_fast(), 0, 0 };
         cvp9_tuner_init(&c->tuner, c->arith, !(opt && opt->autotune < 0) && cvp9_env_autotune(), fixed);
     }
     if (c->device >= dev_count || cvp9_device_setup(c->device) != 0) { free(c); return CVP9_ERR_NO_BACKEND; }

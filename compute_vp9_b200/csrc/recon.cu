@@ -1621,12 +1621,16 @@ namespace {
 
 constexpr int kFastWarps = 4;                     /* SBs per CTA */
 
-/* One block, 12 bytes. geo: x/4 | y/4 << 4 | clamped cw << 8 | ch << 15 |
- * reference slot << 22 (15: none) | tx_size << 26 | skip << 28. */
+/* One block, 16 bytes. geo: x/4 | y/4 << 4 | clamped cw << 8 | ch << 15 |
+ * reference slot << 22 (REFCPU: pool slot, 15 none; SPEC: LAST/GOLDEN/ALTREF
+ * 0..2) | tx_size << 26 | skip << 28. ext (SPEC): luma TXs per row | per
+ * column << 5 | chroma TXs per row << 10 | per column << 14 | chroma
+ * tx_size << 18. */
 struct FastBlk {
     uint32_t geo;
     uint32_t mv;      /* mv[0]: col in the low half, row in the high half (1/8 pel) */
     uint32_t coeff;   /* first coefficient of the block */
+    uint32_t ext;
 };
 
 __device__ __forceinline__ int fb_x(const FastBlk &b) { return (int)(b.geo & 0xfu) << 2; }
@@ -2057,6 +2061,282 @@ __device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int l
     }
 }
 
+/* ── SPEC arithmetic in k_inter ─────────────────────────────────────────── */
+
+/* 16 consecutive bytes of a row at p as four words (aligned word reads;
+ * callers keep the aligned span inside the buffer) */
+__device__ __forceinline__ void ld16w(const uint8_t *p, uint32_t o[4])
+{
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    const unsigned sh = 8u * (unsigned)(a & 3);
+    const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3), w4 = __ldg(w + 4);
+    o[0] = __funnelshift_r(w0, w1, sh);
+    o[1] = __funnelshift_r(w1, w2, sh);
+    o[2] = __funnelshift_r(w2, w3, sh);
+    o[3] = __funnelshift_r(w3, w4, sh);
+}
+
+/* the same 16 bytes, every sample clamped into [0, pw-1] x [0, ph-1] */
+__device__ __forceinline__ void ld16c(const uint8_t *plane, int stride, int pw, int ph, int x0, int y, uint32_t o[4])
+{
+    const int xm = pw > 0 ? pw - 1 : 0, ym = ph > 0 ? ph - 1 : 0;
+    const uint8_t *row = plane + (size_t)clampi(y, 0, ym) * stride;
+    o[0] = o[1] = o[2] = o[3] = 0u;
+#pragma unroll
+    for (int x = 0; x < 16; x++) o[x >> 2] |= (uint32_t)__ldg(row + clampi(x0 + x, 0, xm)) << (8 * (x & 3));
+}
+
+__device__ __forceinline__ int bytek(const uint32_t o[4], int k) { return (int)((o[k >> 2] >> (8 * (k & 3))) & 0xffu); }
+
+/* shader rounding of one 8-tap sum: (acc + 64) >> 7 clipped to 8 bits */
+__device__ __forceinline__ uint32_t tap_round(int acc) { return (uint32_t)clampi((acc + 64) >> 7, 0, 255); }
+
+/* Luma prediction of four chunks (vp9_mc.comp.glsl:61-110): lane = (chunk
+ * c0 + lane/8, k = lane%8). Horizontal 8-tap rows k and k+8 of each chunk's
+ * 15-row window go to shared rows (rounded, clipped to 8 bits), then lane k
+ * filters output row k vertically. Fetches clamp into the reference. */
+__device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int nchunks, int sbx, int sby, int lane)
+{
+    uint8_t *hb = reinterpret_cast<uint8_t *>(w.coef);        /* 4 chunks x 15 rows x 8 */
+    const int q = lane >> 3, k = lane & 7, c = c0 + q;
+    FastBlk fb;
+    int lx0 = 0, ly0 = 0, lw = 0, lh = 0, cx0, cy0, clw, clh;
+    const uint8_t *rp = nullptr;
+    int rw = 0, rh = 0, fx = 0, fy = 0, bx = 0, by = 0;
+    if (c < nchunks) {
+        fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
+        const cvp9_ref_t &R = job.ref[job.ref_slot_of[fb_slot(fb) & 3] & 7];
+        rp = R.plane; rw = R.w; rh = R.h;
+        const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+        bx = sbx + lx0 + (mvx >> 3);
+        by = sby + ly0 + (mvy >> 3);
+        fx = (mvx & 7) << 1;
+        fy = (mvy & 7) << 1;
+        if (rp) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int hr = k + 8 * h;
+                if (hr >= lh + 7) continue;
+                const int y = by - 3 + hr, x0 = bx - 3;
+                uint32_t o[4];
+                if (x0 >= 0 && x0 + lw + 6 < rw && y >= 0 && y < rh) ld16w(rp + (size_t)y * rw + x0, o);
+                else ld16c(rp, rw, rw, rh, x0, y, o);
+                uint32_t out0 = 0, out1 = 0;
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) {
+                    int acc = 0;
+#pragma unroll
+                    for (int tt = 0; tt < 8; tt++) acc += c_subpel[fx][tt] * bytek(o, cc + tt);
+                    const uint32_t v = tap_round(acc);
+                    if (cc < 4) out0 |= v << (8 * cc); else out1 |= v << (8 * (cc - 4));
+                }
+                uint32_t *hrow = reinterpret_cast<uint32_t *>(hb + (q * 15 + hr) * 8);
+                hrow[0] = out0;
+                hrow[1] = out1;
+            }
+        }
+    }
+    __syncwarp();
+    if (c < nchunks && k < lh) {
+        uint32_t o0 = 0x80808080u, o1 = 0x80808080u;           /* missing reference: 128 */
+        if (rp) {
+            o0 = o1 = 0;
+            const uint8_t *hcol = hb + (q * 15 + k) * 8;
+#pragma unroll
+            for (int cc = 0; cc < 8; cc++) {
+                int acc = 0;
+#pragma unroll
+                for (int tt = 0; tt < 8; tt++) acc += c_subpel[fy][tt] * (int)hcol[tt * 8 + cc];
+                const uint32_t v = tap_round(acc);
+                if (cc < 4) o0 |= v << (8 * cc); else o1 |= v << (8 * (cc - 4));
+            }
+        }
+        uint8_t *d = w.ty + (ly0 + k) * kFY + lx0;
+        if (lw == 8) {
+            reinterpret_cast<uint32_t *>(d)[0] = o0;
+            reinterpret_cast<uint32_t *>(d)[1] = o1;
+        } else {
+#pragma unroll
+            for (int x = 0; x < 8; x++) if (x < lw) d[x] = (uint8_t)((x < 4 ? o0 : o1) >> (8 * (x & 3)));
+        }
+    }
+    __syncwarp();
+}
+
+/* Chroma prediction of four chunks, both planes: lane = (chunk c0 + lane/8,
+ * plane, r = lane%4); the chroma MV is read as 1/16 chroma pel (16 phases),
+ * fetches clamp into the ceil-half planes. */
+__device__ void spec_chroma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int nchunks, int sbx, int sby, int lane)
+{
+    uint8_t *hb = reinterpret_cast<uint8_t *>(w.coef) + 480;  /* 4 chunks x 2 planes x 11 rows x 4 */
+    const int q = lane >> 3, p = (lane >> 2) & 1, r = lane & 3, c = c0 + q;
+    FastBlk fb;
+    int lx0, ly0, lw, lh, cx0 = 0, cy0 = 0, clw = 0, clh = 0;
+    const uint8_t *pl = nullptr;
+    int cw2 = 0, ch2 = 0, rcs = 0, fx = 0, fy = 0, bx = 0, by = 0;
+    if (c < nchunks) {
+        fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
+        const cvp9_ref_t &R = job.ref[job.ref_slot_of[fb_slot(fb) & 3] & 7];
+        if (R.plane && clw > 0) {
+            const int rw = R.w, rh = R.h;
+            rcs = (rw + 1) >> 1;
+            cw2 = rcs;
+            ch2 = (rh + 1) >> 1;
+            pl = R.plane + (size_t)rw * rh + (p ? (size_t)rcs * ch2 : 0);
+            const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+            bx = (sbx >> 1) + cx0 + (mvx >> 4);
+            by = (sby >> 1) + cy0 + (mvy >> 4);
+            fx = mvx & 15;
+            fy = mvy & 15;
+#pragma unroll
+            for (int h = 0; h < 3; h++) {
+                const int hr = r + 4 * h;
+                if (hr >= clh + 7) continue;
+                const int y = by - 3 + hr, x0 = bx - 3;
+                uint32_t o[4];
+                /* a further chroma row exists below: word reads stay inside */
+                if (x0 >= 0 && x0 + clw + 6 < cw2 && y >= 0 && y + 1 < ch2) ld16w(pl + (size_t)y * rcs + x0, o);
+                else ld16c(pl, rcs, cw2, ch2, x0, y, o);
+                uint32_t out = 0;
+#pragma unroll
+                for (int cc = 0; cc < 4; cc++) {
+                    int acc = 0;
+#pragma unroll
+                    for (int tt = 0; tt < 8; tt++) acc += c_subpel[fx][tt] * bytek(o, cc + tt);
+                    out |= tap_round(acc) << (8 * cc);
+                }
+                *reinterpret_cast<uint32_t *>(hb + ((q * 2 + p) * 11 + hr) * 4) = out;
+            }
+        }
+    }
+    __syncwarp();
+    if (c < nchunks && clw > 0 && r < clh) {
+        uint32_t o = 0x80808080u;                             /* missing reference: 128 */
+        if (pl) {
+            o = 0;
+            const uint8_t *hcol = hb + ((q * 2 + p) * 11 + r) * 4;
+#pragma unroll
+            for (int cc = 0; cc < 4; cc++) {
+                int acc = 0;
+#pragma unroll
+                for (int tt = 0; tt < 8; tt++) acc += c_subpel[fy][tt] * (int)hcol[tt * 4 + cc];
+                o |= tap_round(acc) << (8 * cc);
+            }
+        }
+        uint8_t *d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
+        if (clw == 4 && !((uintptr_t)d & 3)) {
+            *reinterpret_cast<uint32_t *>(d) = o;
+        } else {
+#pragma unroll
+            for (int x = 0; x < 4; x++) if (x < clw) d[x] = (uint8_t)(o >> (8 * x));
+        }
+    }
+    __syncwarp();
+}
+
+/* SPEC TX layout of a block in plane p (vp9_kf_tile.c:320-396 for blocks of
+ * 8x8 and up): TX log2 size, TXs per row and column (MI-clipped), plane
+ * origin in the SB tile, coefficients before this plane. */
+struct SpecTx {
+    int txl, nx, ny, ox, oy;
+    uint64_t base;
+};
+
+__device__ __forceinline__ SpecTx spec_tx_layout(const FastBlk &b, int p)
+{
+    SpecTx s;
+    const int l_nx = (int)(b.ext & 0x1fu), l_ny = (int)((b.ext >> 5) & 0x1fu);
+    const int c_nx = (int)((b.ext >> 10) & 0xfu), c_ny = (int)((b.ext >> 14) & 0xfu);
+    const int ltx = fb_txl(b), ctx = (int)((b.ext >> 18) & 3u);
+    const int lc = l_nx * l_ny * (16 << (2 * ltx)), cc = c_nx * c_ny * (16 << (2 * ctx));
+    if (p == 0) { s.txl = ltx; s.nx = l_nx; s.ny = l_ny; s.ox = fb_x(b); s.oy = fb_y(b); s.base = 0; }
+    else { s.txl = ctx; s.nx = c_nx; s.ny = c_ny; s.ox = fb_x(b) >> 1; s.oy = fb_y(b) >> 1;
+           s.base = (uint64_t)lc + (p == 2 ? (uint64_t)cc : 0); }
+    return s;
+}
+
+/* SPEC residual of every TX of size N in plane P: 32/N TXs at a time.
+ * Column pass, lane = (TX, column j): dequantise (DC step at [0][0] only),
+ * 1-D butterfly down the column (vp9_idct.comp.glsl:666-679); the group's
+ * int32 column results replace its staged coefficients in shared memory;
+ * row pass, lane = (TX, row i): butterfly along the row, final shift 4/5/6,
+ * add and clamp into the tile (:680-789). A group with no nonzero
+ * coefficient adds nothing and is skipped. */
+template <int N>
+__device__ void spec_fast_residual(FastSmem &w, const cvp9_job_t &job, int P, int ntx, int lane)
+{
+    constexpr int G = 32 / N, NN = N * N;
+    const int g = lane / N, i = lane % N;
+    int16_t *X = w.coef + g * NN;
+    int32_t *T = reinterpret_cast<int32_t *>(w.coef) + g * NN;
+    uint8_t *tile = P == 0 ? w.ty : (P == 1 ? w.tu : w.tv);
+    const int pitch = P == 0 ? kFY : kFC;
+    const int sh = N == 4 ? 4 : (N == 8 ? 5 : 6);
+    for (int q0 = 0; q0 < ntx; q0 += G) {
+        const int q = q0 + g;
+        bool have = q < ntx;
+        int px0 = 0, py0 = 0;
+        if (have) {
+            const int b = w.txblk[q];
+            const FastBlk fb = w.blk[b];
+            const SpecTx L = spec_tx_layout(fb, P);
+            const int tq = q - w.txoff[b];
+            const int tyy = L.nx == 1 ? tq : tq / L.nx, txx = tq - tyy * L.nx;
+            px0 = L.ox + txx * N;
+            py0 = L.oy + tyy * N;
+            const uint64_t c0 = (uint64_t)fb.coeff + L.base + (uint64_t)tq * NN;
+            if (c0 + NN > (uint64_t)job.num_coeffs) have = false;
+            else {
+                uint32_t rv[N / 2];
+                fast_row_load<N>(rv, job.coeffs + c0 + (uint64_t)i * N);
+                uint32_t *dst = reinterpret_cast<uint32_t *>(X + i * N);
+#pragma unroll
+                for (int k = 0; k < N / 2; k++) dst[k] = rv[k];
+            }
+        }
+        __syncwarp();
+        wi v[N];
+        bool any = false;
+        if (have) {
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                const int cf = X[k * N + i];
+                any |= cf != 0;
+                v[k] = wi(cf) * ((k == 0 && i == 0) ? job.q_dc : job.q_ac);
+            }
+            if (any) idct_n(v, N);
+        }
+        const bool grp_any = __any_sync(0xffffffffu, any);
+        __syncwarp();                          /* every lane has read its column */
+        if (grp_any) {
+            if (have) {
+#pragma unroll
+                for (int k = 0; k < N; k++) T[k * N + i] = any ? v[k].v : 0;
+            }
+            __syncwarp();
+            if (have) {
+#pragma unroll
+                for (int k = 0; k < N; k++) v[k] = wi(T[i * N + k]);
+                idct_n(v, N);
+                uint32_t *row = reinterpret_cast<uint32_t *>(tile + (py0 + i) * pitch + px0);
+#pragma unroll
+                for (int j4 = 0; j4 < N / 4; j4++) {
+                    const uint32_t word = row[j4];
+                    uint32_t outw = 0;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int r = ((int)((unsigned)v[j4 * 4 + e].v + (1u << (sh - 1)))) >> sh;
+                        outw |= (uint32_t)clampi((int)((word >> (8 * e)) & 0xffu) + r, 0, 255) << (8 * e);
+                    }
+                    row[j4] = outw;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 } /* namespace */
 
 /* MINB: CTAs per SM the register allocation is sized for (5: up to 96
@@ -2108,7 +2388,33 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
         if (mb) continue;
         const int cw = min(bw, W - gx), ch = min(bh, H - gy);
         FastBlk fb;
-        const uint32_t slot4 = (ref0 >= 1 && ref0 <= 8) ? (uint32_t)(ref0 - 1) : 15u;
+        uint32_t slot4 = (ref0 >= 1 && ref0 <= 8) ? (uint32_t)(ref0 - 1) : 15u;
+        fb.ext = 0u;
+        if (A == CVP9_ARITH_SPEC) {
+            /* sub-8x8 residuals span their whole 8x8 MI (they overlap), and
+             * 32x32 TXs need more staging than a warp has: general path */
+            slot4 = (uint32_t)clampi(ref0 - 1, 0, 2);
+            int uvtx = min(txl, max_tx_for(max(bw / 2, 4), max(bh / 2, 4)));
+            /* the fast path keeps every TX inside its block and its rows
+             * word-aligned: MI-aligned power-of-two blocks, TX <= block */
+            bad |= bw < 8 || bh < 8 || txl == 3 || uvtx == 3 || (lx & 7) || (ly & 7) ||
+                   (bw & (bw - 1)) || (bh & (bh - 1)) || (4 << txl) > min(bw, bh);
+            if (!skip) {
+                int nxy[2][2];
+#pragma unroll
+                for (int pp = 0; pp < 2; pp++) {
+                    const int t4 = 1 << (pp ? uvtx : txl);
+                    const int pw = max(pp ? bw / 2 : bw, 4), ph = max(pp ? bh / 2 : bh, 4);
+                    const int o4x = ((gx >> 3) * 2) >> pp, o4y = ((gy >> 3) * 2) >> pp;
+                    const int mw = min(pw / 4, ((job.mi_cols * 2) >> pp) - o4x);
+                    const int mh = min(ph / 4, ((job.mi_rows * 2) >> pp) - o4y);
+                    nxy[pp][0] = mw > 0 ? (mw + t4 - 1) / t4 : 0;
+                    nxy[pp][1] = mh > 0 ? (mh + t4 - 1) / t4 : 0;
+                }
+                fb.ext = (uint32_t)nxy[0][0] | (uint32_t)nxy[0][1] << 5 | (uint32_t)nxy[1][0] << 10 |
+                         (uint32_t)nxy[1][1] << 14 | (uint32_t)uvtx << 18;
+            }
+        }
         fb.geo = (uint32_t)(lx >> 2) | (uint32_t)(ly >> 2) << 4 | (uint32_t)cw << 8 | (uint32_t)ch << 15 |
                  slot4 << 22 | (uint32_t)txl << 26 | (skip ? 1u : 0u) << 28;
         fb.mv = g3;
@@ -2155,6 +2461,11 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
      * c0 + lane/8, row lane%8); chroma passes: lane = (chunk c0 + lane/8,
      * plane, row). Two luma and two chroma passes are in flight: all four
      * issue their loads before any computes. */
+    if (A == CVP9_ARITH_SPEC) {
+        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_luma_pass(w, job, c0, nchunks, sbx, sby, lane);
+        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_chroma_pass(w, job, c0, nchunks, sbx, sby, lane);
+        nchunks = 0;                      /* the REFCPU passes below do nothing */
+    }
     for (int c0 = 0; c0 < nchunks; c0 += 8) {
         const FastLuma a = fast_luma_issue(w, job, c0 + (lane >> 3), lane & 7, nchunks, sbx, sby);
         const FastLuma b = fast_luma_issue(w, job, c0 + 4 + (lane >> 3), lane & 7, nchunks, sbx, sby);
@@ -2167,39 +2478,58 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
     }
     __syncwarp();
 
-    /* 4. luma residual, one pass per TX size present */
-    unsigned sizes = 0;
-#pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const int i = lane + 32 * r;
-        if (i < nb && !fb_skip(w.blk[i])) sizes |= 1u << fb_txl(w.blk[i]);
-    }
-    sizes = __reduce_or_sync(0xffffffffu, sizes);
-    for (unsigned sz = sizes; sz; sz &= sz - 1) {
-        const int txl = __ffs(sz) - 1, n = 4 << txl;
-        int cnt[2] = { 0, 0 };
+    /* 4. residual, one pass per (plane, TX size) present: REFCPU luma only
+     * with TXs counted on the frame-clamped block; SPEC every plane in the
+     * tile parser's MI-clipped layout */
+    for (int P = 0; P < (A == CVP9_ARITH_SPEC ? 3 : 1); P++) {
+        unsigned sizes = 0;
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int i = lane + 32 * r;
-            if (i < nb) {
-                const FastBlk fb = w.blk[i];
-                if (!fb_skip(fb) && fb_txl(fb) == txl) cnt[r] = (fb_cw(fb) / n) * (fb_ch(fb) / n);
+            if (i < nb && !fb_skip(w.blk[i]))
+                sizes |= 1u << (A == CVP9_ARITH_SPEC ? spec_tx_layout(w.blk[i], P).txl : fb_txl(w.blk[i]));
+        }
+        sizes = __reduce_or_sync(0xffffffffu, sizes);
+        for (unsigned sz = sizes; sz; sz &= sz - 1) {
+            const int txl = __ffs(sz) - 1, n = 4 << txl;
+            int cnt[2] = { 0, 0 };
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const int i = lane + 32 * r;
+                if (i < nb) {
+                    const FastBlk fb = w.blk[i];
+                    if (fb_skip(fb)) continue;
+                    if (A == CVP9_ARITH_SPEC) {
+                        const SpecTx L = spec_tx_layout(fb, P);
+                        if (L.txl == txl) cnt[r] = L.nx * L.ny;
+                    } else if (fb_txl(fb) == txl) {
+                        cnt[r] = (fb_cw(fb) / n) * (fb_ch(fb) / n);
+                    }
+                }
             }
+            const int x0 = warp_incl_scan(cnt[0], lane), x1 = warp_incl_scan(cnt[1], lane);
+            const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
+            const int e0 = x0 - cnt[0], e1 = tot0 + x1 - cnt[1];
+            const int ntx = tot0 + tot1;    /* at most 256: the TXs tile the SB's plane */
+            if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
+            if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
+            __syncwarp();
+            if (A == CVP9_ARITH_SPEC) {
+                switch (txl) {
+                case 0: spec_fast_residual<4>(w, job, P, ntx, lane); break;
+                case 1: spec_fast_residual<8>(w, job, P, ntx, lane); break;
+                default: spec_fast_residual<16>(w, job, P, ntx, lane); break;   /* 32 went general */
+                }
+            } else {
+                switch (txl) {
+                case 0: fast_residual<4>(w, job, ntx, lane); break;
+                case 1: fast_residual<8>(w, job, ntx, lane); break;
+                case 2: fast_residual<16>(w, job, ntx, lane); break;
+                default: fast_residual<32>(w, job, ntx, lane); break;
+                }
+            }
+            __syncwarp();
         }
-        const int x0 = warp_incl_scan(cnt[0], lane), x1 = warp_incl_scan(cnt[1], lane);
-        const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
-        const int e0 = x0 - cnt[0], e1 = tot0 + x1 - cnt[1];
-        const int ntx = tot0 + tot1;        /* at most 256: the TXs tile the SB */
-        if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
-        if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
-        __syncwarp();
-        switch (txl) {
-        case 0: fast_residual<4>(w, job, ntx, lane); break;
-        case 1: fast_residual<8>(w, job, ntx, lane); break;
-        case 2: fast_residual<16>(w, job, ntx, lane); break;
-        default: fast_residual<32>(w, job, ntx, lane); break;
-        }
-        __syncwarp();
     }
 
     /* 5. write the tile (clipped to the frame) and release the SB */
@@ -2644,6 +2974,8 @@ int cvp9k_configure(void)
     cudaFuncSetAttribute(k_recon<CVP9_ARITH_SPEC>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_REFCPU, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_REFCPU, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_inter<CVP9_ARITH_SPEC, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_inter<CVP9_ARITH_SPEC, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return 0;
 }
 
@@ -2682,18 +3014,25 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
         int grid = L->recon_ctas > 0 ? L->recon_ctas : (int)L->n_tickets;
         if (grid > (int)L->n_tickets) grid = (int)L->n_tickets;
         size_t smem = sizeof(ReconSmem);
-        const bool fast = L->general && L->general_tickets && L->n_general && L->arith == CVP9_ARITH_REFCPU;
+        const bool fast = L->general && L->general_tickets && L->n_general;
         if (fast) {
             const unsigned fg = (L->n_tickets + kFastWarps - 1) / kFastWarps;
-            if (L->inter_variant == 1)
-                k_inter<CVP9_ARITH_REFCPU, 5><<<fg, kFastWarps * 32, kFastWarps * sizeof(FastSmem), st>>>(
-                    L->jobs, L->tickets, L->n_tickets, L->general);
-            else
-                k_inter<CVP9_ARITH_REFCPU, 6><<<fg, kFastWarps * 32, kFastWarps * sizeof(FastSmem), st>>>(
-                    L->jobs, L->tickets, L->n_tickets, L->general);
+            const size_t fs = kFastWarps * sizeof(FastSmem);
+            const bool spec = L->arith == CVP9_ARITH_SPEC;
+            if (L->inter_variant == 2) {
+                if (spec) k_inter<CVP9_ARITH_SPEC, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
+                else k_inter<CVP9_ARITH_REFCPU, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
+            } else {
+                if (spec) k_inter<CVP9_ARITH_SPEC, 5><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
+                else k_inter<CVP9_ARITH_REFCPU, 5><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
+            }
             k_compact<<<1, 1024, 0, st>>>(L->tickets, L->general, L->n_tickets, L->general_tickets, L->n_general);
-            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->general_tickets, L->n_tickets,
-                                                                      L->ticket_counter, L->n_general);
+            if (spec)
+                k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->general_tickets, L->n_tickets,
+                                                                        L->ticket_counter, L->n_general);
+            else
+                k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->general_tickets, L->n_tickets,
+                                                                          L->ticket_counter, L->n_general);
         } else if (L->arith == CVP9_ARITH_SPEC) {
             k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter, nullptr);
         } else {

@@ -30,7 +30,7 @@ typedef struct {
     int              lf_strips_x, lf_strips_y;  /* register-strip filter grid (jobs with lf_tiled == 2) */
     int              flat_lf_max_w, flat_lf_max_h; /* >0: run the frame-wide filter */
     int              flat_nv12;
-    /* Inter fast path (REFCPU): when `general` is set, k_inter takes the
+    /* Inter fast path: when `general` is set, k_inter takes the
      * superblocks that hold inter blocks only, one warp each, and k_recon
      * runs on the rest. All three are device buffers: n_tickets words,
      * n_tickets words, one word. */

@@ -112,8 +112,8 @@ def test_admission_budget():
 def test_autotune_settles_with_oracle_output(profile):
     """The tuner runs every candidate configuration on real steps: each of
     those steps still decodes to the oracle's bytes, and the bucket settles
-    after all knobs were measured (REFCPU: 3 inter paths + filter tile +
-    wavefront width = 5 configurations; SPEC: 3)."""
+    after all knobs were measured (3 inter paths + filter layout +
+    wavefront width = 5 configurations)."""
     tuning = []
     frames = 12
     outs = decode_mix(profile, MIX, frames, tuning=tuning)
@@ -125,9 +125,9 @@ def test_autotune_settles_with_oracle_output(profile):
             assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
     assert len(tuning) == 1, tuning
     e = tuning[0]
-    assert e["settled"] == 1 and e["trials"] == (5 if profile == REFCPU else 3), e
+    assert e["settled"] == 1 and e["trials"] == 5, e
     assert e["best_ms"] > 0 and e["lf_tile_h"] in (16, 32)
-    assert e["inter_path"] in ((0, 1, 2) if profile == REFCPU else (0,))
+    assert e["inter_path"] in (0, 1, 2)
 
 
 def _pinned_copy(pf, keep):

@@ -3,7 +3,7 @@
 REFCPU cases are the reference's CPU reconstruction (the restatement in
 oracle/, itself pinned to the compiled reference and to tests/golden), run
 with the warp-per-superblock inter path on (the default) and off; SPEC
-cases are the shader-arithmetic restatement. Sizes keep the CPU oracle to
+cases are the shader-arithmetic restatement, also with the path on and off. Sizes keep the CPU oracle to
 seconds. Tolerance: none — every byte of every plane must match.
 """
 import numpy as np
@@ -57,12 +57,13 @@ def test_refcpu_parity(name):
     run_case(REFCPU, *CASES[name])
 
 
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
 @pytest.mark.parametrize("name", ["c1_small", "c2_small", "edges_sub8", "big_tx", "flat_lf"])
-def test_refcpu_parity_without_inter_fast_path(name, monkeypatch):
+def test_parity_without_inter_fast_path(name, profile, monkeypatch):
     """The general superblock kernel alone (CVP9_INTER_FAST=0) gives the same
     bytes as with the warp-per-superblock inter path."""
     monkeypatch.setenv("CVP9_INTER_FAST", "0")
-    run_case(REFCPU, *CASES[name])
+    run_case(profile, *CASES[name])
 
 
 @pytest.mark.parametrize("name", list(CASES))

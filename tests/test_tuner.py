@@ -75,17 +75,17 @@ def test_stale_samples_are_ignored(lib):
     assert nxt.t() == (0, 0, 0)
 
 
-def test_spec_skips_the_inter_knob(lib):
-    t = make(lib, arith=1, fixed=(0, 0, 0))
+def test_spec_tunes_the_same_knobs(lib):
+    t = make(lib, arith=1, fixed=(1, 0, 0))
     seen = []
     for _ in range(20):
-        idx, cfg = step(lib, t, 5, lambda c: 1.0 + 0.1 * c[1] - 0.2 * c[2])
+        idx, cfg = step(lib, t, 5, lambda c: 1.0 + 0.1 * c[1] - 0.2 * c[2] + (0.5 if c[0] != 1 else 0))
         if idx < 0:
             break
         if not seen or seen[-1] != cfg:
             seen.append(cfg)
-    assert seen == [(0, 0, 0), (0, 1, 0), (0, 0, 1)]
-    assert step(lib, t, 5, lambda c: 1.0) == (-1, (0, 0, 1))
+    assert seen == [(1, 0, 0), (0, 0, 0), (2, 0, 0), (1, 1, 0), (1, 0, 1)]
+    assert step(lib, t, 5, lambda c: 1.0) == (-1, (1, 0, 1))
 
 
 def test_disabled_returns_the_fixed_configuration(lib):
