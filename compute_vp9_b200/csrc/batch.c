@@ -578,7 +578,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         s->misc_cap = cap;
     }
     if ((err = grow_dev(b, (void **)&s->d_sb_range, &s->sb_cap, n_sb * 16))) return err;
-    if ((err = grow_dev(b, (void **)&s->d_fast, &s->fast_cap, (2 * n_sb + 1) * 4))) return err;
+    if ((err = grow_dev(b, (void **)&s->d_fast, &s->fast_cap, (2 * n_sb + 2) * 4))) return err;
     if (s->sids_cap < n) {
         free(s->sids);
         s->sids = malloc((size_t)n * sizeof(int));

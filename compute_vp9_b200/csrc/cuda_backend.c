@@ -187,7 +187,7 @@ static cvp9_err_t set_geometry(cuctx_t *c, int32_t W, int32_t H)
     CK(cudaMalloc((void **)&c->d_sb_done, (size_t)c->n_sb * 4), "alloc sb_done");
     CK(cudaMemset(c->d_sb_done, 0, (size_t)c->n_sb * 4), "clear sb_done");
     CK(cudaMalloc((void **)&c->d_tickets, (size_t)c->n_sb * 4), "alloc tickets");
-    CK(cudaMalloc((void **)&c->d_fast, (size_t)(2 * c->n_sb + 1) * 4), "alloc fast-path scratch");
+    CK(cudaMalloc((void **)&c->d_fast, (size_t)(2 * c->n_sb + 2) * 4), "alloc fast-path scratch");
     uint32_t *t = malloc((size_t)c->n_sb * 4);
     if (!t) return CVP9_ERR_NOMEM;
     uint32_t n = 0;

@@ -2439,7 +2439,10 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
     }
     gen = __any_sync(0xffffffffu, gen || bad || ovl || gap) != 0;
     if (lane == 0) general[t] = gen ? 1u : 0u;
-    if (gen) return;
+    if (gen) {
+        if (lane == 0) atomicAdd(general + 2 * n_tickets + 1, 1u);   /* k_compact skips when 0 */
+        return;
+    }
 
     /* 2. chunk (8x8 luma + 4x4 chroma) offsets and map */
     int nchunks;
@@ -2448,7 +2451,10 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
         const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
         nchunks = tot0 + tot1;
         if (nchunks > 128) {             /* more chunks than the map holds (odd block sizes) */
-            if (lane == 0) general[t] = 1u;
+            if (lane == 0) {
+                general[t] = 1u;
+                atomicAdd(general + 2 * n_tickets + 1, 1u);
+            }
             return;
         }
         const int e0 = x0 - nch[0], e1 = tot0 + x1 - nch[1];
@@ -2599,6 +2605,10 @@ __global__ void __launch_bounds__(1024) k_compact(const uint32_t *__restrict__ t
 {
     __shared__ uint32_t wsum[32];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (count[1] == 0u) {                /* k_inter took every superblock */
+        if (tid == 0) *count = 0u;
+        return;
+    }
     const uint32_t per = (n + 1023u) / 1024u;
     const uint32_t b = min(n, (uint32_t)tid * per), e = min(n, b + per);
     uint32_t c = 0;
@@ -3017,6 +3027,8 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
         const bool fast = L->general && L->general_tickets && L->n_general;
         if (fast) {
             const unsigned fg = (L->n_tickets + kFastWarps - 1) / kFastWarps;
+            /* the count of general superblocks that k_inter raises */
+            if ((e = cudaMemsetAsync(L->n_general + 1, 0, 4, st)) != cudaSuccess) return (int)e;
             const size_t fs = kFastWarps * sizeof(FastSmem);
             const bool spec = L->arith == CVP9_ARITH_SPEC;
             if (L->inter_variant == 2) {

@@ -32,8 +32,9 @@ typedef struct {
     int              flat_nv12;
     /* Inter fast path: when `general` is set, k_inter takes the
      * superblocks that hold inter blocks only, one warp each, and k_recon
-     * runs on the rest. All three are device buffers: n_tickets words,
-     * n_tickets words, one word. */
+     * runs on the rest. One device buffer of 2 n_tickets + 2 words:
+     * general = its start (flags), general_tickets = + n_tickets,
+     * n_general = + 2 n_tickets (count, then a scratch counter). */
     uint32_t        *general;
     uint32_t        *general_tickets;
     uint32_t        *n_general;
