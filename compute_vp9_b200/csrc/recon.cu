@@ -530,22 +530,6 @@ __device__ __forceinline__ bool refcpu_geo(const ReconSmem &s, const BlkS &b, in
  * and V rows. Rows needing bytes past the first 16 take a second copy. */
 constexpr int kChunkStage = 608;
 
-__device__ __forceinline__ void refcpu_issue(uint8_t *st, const McGeo &g, int lw, int lh,
-                                             int clw, int clh, int lane)
-{
-    if (g.lfast) {
-        const int row = lane >> 1, half = lane & 1;
-        if (row <= lh && (half == 0 || (g.ix - g.la) + lw >= 16))
-            cp_async16(st + row * 32 + half * 16, g.rp + (size_t)(g.iy + row) * g.rw + g.la + half * 16);
-    }
-    if (g.cfast) {
-        const int pl = lane >> 4, row = (lane & 15) >> 1, half = lane & 1;
-        if (row <= clh && (half == 0 || (g.cix - g.ca) + clw >= 16))
-            cp_async16(st + 288 + pl * 160 + row * 32 + half * 16,
-                       (pl ? g.rv : g.ru) + (size_t)(g.ciy + row) * g.rcs + g.ca + half * 16);
-    }
-}
-
 /* Lane-group variants: 8 lanes per chunk (k = lane & 7). Issue: the group's
  * lanes share the chunk's window copies. Compute: lane k produces luma row k
  * (up to 8 samples) and, for k < 4 / k >= 4, row k&3 of U / V. */
@@ -651,60 +635,6 @@ __device__ __forceinline__ void refcpu_compute8(ReconSmem &s, const uint8_t *st,
                 const unsigned u = (b[c] * (8 - g.cfx) + b[c + 1] * g.cfx + 4) >> 3;
                 d[c] = (uint8_t)((t * (8 - g.cfy) + u * g.cfy + 4) >> 3);
             }
-        }
-    }
-}
-
-/* Bilinear with a per-sample clamp into the reference (vp9_reconstruct.c:
- * 105-128): from the staged window on the fast path, else from clamped
- * byte reads. */
-__device__ __forceinline__ void refcpu_compute(ReconSmem &s, const uint8_t *st, const McGeo &g,
-                                               int lx0, int ly0, int lw, int lh,
-                                               int cx0, int cy0, int clw, int clh, int lane)
-{
-    {
-        const int r = lane >> 2, c = (lane & 3) * 2;
-        if (r < lh && c < lw) {
-            unsigned a0, a1, a2, b0, b1, b2;
-            if (g.lfast) {
-                const uint8_t *s0 = st + r * 32 + (g.ix - g.la) + c, *s1 = s0 + 32;
-                a0 = s0[0]; a1 = s0[1]; a2 = s0[2];
-                b0 = s1[0]; b1 = s1[1]; b2 = s1[2];
-            } else {
-                int y0 = clampi(g.iy + r, 0, g.rh - 1), y1 = clampi(g.iy + r + 1, 0, g.rh - 1);
-                int xa = clampi(g.ix + c, 0, g.rw - 1), xb = clampi(g.ix + c + 1, 0, g.rw - 1);
-                int xc = clampi(g.ix + c + 2, 0, g.rw - 1);
-                const uint8_t *r0 = g.rp + (size_t)y0 * g.rw, *r1 = g.rp + (size_t)y1 * g.rw;
-                a0 = __ldg(r0 + xa); a1 = __ldg(r0 + xb); a2 = __ldg(r0 + xc);
-                b0 = __ldg(r1 + xa); b1 = __ldg(r1 + xb); b2 = __ldg(r1 + xc);
-            }
-            const unsigned wx = 8 - g.fx, wy = 8 - g.fy;
-            unsigned t0 = (a0 * wx + a1 * g.fx + 4) >> 3, u0 = (b0 * wx + b1 * g.fx + 4) >> 3;
-            TY(s, lx0 + c, ly0 + r) = (uint8_t)((t0 * wy + u0 * g.fy + 4) >> 3);
-            if (c + 1 < lw) {
-                unsigned t1 = (a1 * wx + a2 * g.fx + 4) >> 3, u1 = (b1 * wx + b2 * g.fx + 4) >> 3;
-                TY(s, lx0 + c + 1, ly0 + r) = (uint8_t)((t1 * wy + u1 * g.fy + 4) >> 3);
-            }
-        }
-    }
-    {
-        const int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
-        if (r < clh && c < clw) {
-            unsigned a0, a1, b0, b1;
-            if (g.cfast) {
-                const uint8_t *s0 = st + 288 + (p - 1) * 160 + r * 32 + (g.cix - g.ca) + c, *s1 = s0 + 32;
-                a0 = s0[0]; a1 = s0[1]; b0 = s1[0]; b1 = s1[1];
-            } else {
-                const int crw = g.rw >> 1, crh = g.rh >> 1;
-                int xm = crw > 0 ? crw - 1 : 0, ym = crh > 0 ? crh - 1 : 0;
-                const uint8_t *pl = p == 1 ? g.ru : g.rv;
-                int y0 = clampi(g.ciy + r, 0, ym), y1 = clampi(g.ciy + r + 1, 0, ym);
-                int xa = clampi(g.cix + c, 0, xm), xb = clampi(g.cix + c + 1, 0, xm);
-                a0 = __ldg(pl + (size_t)y0 * g.rcs + xa); a1 = __ldg(pl + (size_t)y0 * g.rcs + xb);
-                b0 = __ldg(pl + (size_t)y1 * g.rcs + xa); b1 = __ldg(pl + (size_t)y1 * g.rcs + xb);
-            }
-            unsigned t0 = (a0 * (8 - g.cfx) + a1 * g.cfx + 4) >> 3, u0 = (b0 * (8 - g.cfx) + b1 * g.cfx + 4) >> 3;
-            TC(s, p, cx0 + c, cy0 + r) = (uint8_t)((t0 * (8 - g.cfy) + u0 * g.cfy + 4) >> 3);
         }
     }
 }
