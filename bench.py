@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-single", action="store_true", help="skip the single-stream leg")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
+    ap.add_argument("--serve-speed", type=float, default=4.0,
+                    help="pacing compression of the serving run (1 = the config's real time)")
     return ap.parse_args()
 
 
@@ -515,6 +518,18 @@ def main():
                       "kernel_ms_per_frame": plain_kern,
                       "workload": "stream 0 alone, %dx%d; value device-resident, e2e through "
                                   "cuda_decode_frame/cuda_get_frame with host inputs" % (one.w, one.h)}
+        serving = None
+        if not args.no_serve:
+            from compute_vp9_b200 import serve
+            sv = serve.run(streams=256, rate=2.0, frames=120, fps=30.0, speed=args.serve_speed,
+                           hbm_budget=150e9, arith=arith, seed=1)
+            serving = {"workload": "256 streams, Poisson arrivals 2/s, 640x360/1280x720/1920x1080/"
+                                   "3840x2160 in 4:3:2:1, 120 frames at 30 fps, GOP 60, 150 GB budget; "
+                                   "arrivals and pacing compressed %gx" % args.serve_speed,
+                       "speed": args.serve_speed, "frames": sv["frames"], "steps": sv["steps"],
+                       "mean_batch": sv["mean_batch"], "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
+                       "value": sv["mpx_per_s"], "unit": UNIT, "admission_waits": sv["admission_waits"],
+                       "latency": "frame due -> its planes in host memory"}
         cpu = None
         if not args.no_cpu:
             v, kind, cores, sample = cpu_leg(wl, host_cores())
@@ -546,6 +561,7 @@ def main():
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "single_stream": single,
+            "serving": serving,
             "batched_vs_single": (value / single["value"]) if single else None,
         }
     barrier(ws)
