@@ -239,7 +239,9 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms)
     e->cur_ms = e->cur_n ? (ms < e->cur_ms ? ms : e->cur_ms) : ms;
     if (++e->cur_n < 2) return;
     e->trials++;
-    if (e->cur_ms < e->best_ms) {
+    /* a challenger must win by more than 2% (timing noise keeps the
+     * incumbent) */
+    if (e->cur_ms < (e->trials == 1 ? 3.4e38f : 0.98f * e->best_ms)) {
         e->best_ms = e->cur_ms;
         e->best = e->cur;
     }

@@ -59,7 +59,8 @@ double cvp9_now(void);
 
 /* ── Autotuner ──────────────────────────────────────────────────────────────
  * Per shape bucket, the kernel configuration is chosen by timing: each
- * candidate runs on two steps of that bucket (the faster counts), knobs are
+ * candidate runs on two steps of that bucket (the faster counts) and
+ * replaces the best so far only if it is more than 2% faster; knobs are
  * settled one at a time (coordinate descent): the inter path, then the
  * loop-filter layout, then the wavefront width. Every configuration
  * produces the same bytes; only the speed differs. Pure host logic. */

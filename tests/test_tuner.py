@@ -110,3 +110,13 @@ def test_bucket_key_rounding(lib):
     assert k(0, 64, 32768) != k(0, 65, 32768)
     assert k(0, 64, 32768) != k(0, 64, 32769)
     assert k(0, 64, 32768) != k(1, 64, 32768)
+
+
+def test_a_challenger_needs_a_clear_win(lib):
+    # every alternative is 1% faster than the default: noise, the default stays
+    t = make(lib)
+    for _ in range(20):
+        idx, cfg = step(lib, t, 9, lambda c: 1.0 if c == (1, 0, 0) else 0.99)
+        if idx < 0:
+            break
+    assert step(lib, t, 9, lambda c: 1.0) == (-1, (1, 0, 0))
