@@ -1748,43 +1748,72 @@ __device__ __forceinline__ void fast_chunk(const FastSmem &w, int c, FastBlk &fb
     clh = min(4, ((ch + 1) >> 1) - ccy * 4);
 }
 
-__device__ __forceinline__ FastLuma fast_luma_issue(FastSmem &w, const cvp9_job_t &job, int c, int kk,
-                                                   int nchunks, int sbx, int sby)
+/* One lane's luma row (chunk c, row lane%8) and chroma row (plane
+ * (lane/4)%2, row lane%4) of chunk c: geometry, reference and MV decoded
+ * once for both, reads issued, nothing computed yet. */
+__device__ __forceinline__ void fast_pred_issue(FastSmem &w, const cvp9_job_t &job, int c, int lane, int nchunks,
+                                                int sbx, int sby, FastLuma &J, FastChroma &K)
 {
-    FastLuma J;
-    J.act = false;
-    J.ref = false;
-    if (c >= nchunks) return J;
+    J.act = J.ref = false;
+    K.act = K.ref = false;
+    if (c >= nchunks) return;
     FastBlk fb;
     int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
     fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
-    if (kk >= lh) return J;
-    J.act = true;
-    J.d = w.ty + (ly0 + kk) * kFY + lx0;
-    J.lw = lw;
+    const int kk = lane & 7, p = (lane >> 2) & 1, r = lane & 3;
     const int slot = fb_slot(fb);
-    if (slot >= 8) return J;
-    const cvp9_ref_t &R = job.ref[slot];
-    const uint8_t *rp = R.plane;
-    if (!rp) return J;
-    J.ref = true;
-    const int rw = R.w, rh = R.h;
-    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
-    const int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
-    const int ix = px8 >> 3, iy = py8 >> 3;
-    J.fx = px8 & 7;
-    J.fy = py8 & 7;
-    const int y0 = iy + kk;
-    if (ix >= 0 && ix + lw < rw && y0 >= 0 && y0 + 1 < rh) {
-        /* luma rows are followed by the chroma planes: the word reads past
-         * a row end stay inside the frame */
-        ld9w(rp + (size_t)y0 * rw + ix, J.lo0, J.mid0, J.hi0);
-        ld9w(rp + (size_t)(y0 + 1) * rw + ix, J.lo1, J.mid1, J.hi1);
-    } else {
-        ld9c(rp, rw, rh, ix, y0, J.lo0, J.mid0, J.hi0);
-        ld9c(rp, rw, rh, ix, y0 + 1, J.lo1, J.mid1, J.hi1);
+    const uint8_t *rp = nullptr;
+    int rw = 0, rh = 0;
+    if (slot < 8) {
+        const cvp9_ref_t &R = job.ref[slot];
+        rp = R.plane;
+        rw = R.w;
+        rh = R.h;
     }
-    return J;
+    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+    if (kk < lh) {
+        J.act = true;
+        J.d = w.ty + (ly0 + kk) * kFY + lx0;
+        J.lw = lw;
+        if (rp) {
+            J.ref = true;
+            const int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
+            const int ix = px8 >> 3, y0 = (py8 >> 3) + kk;
+            J.fx = px8 & 7;
+            J.fy = py8 & 7;
+            if (ix >= 0 && ix + lw < rw && y0 >= 0 && y0 + 1 < rh) {
+                /* luma rows are followed by the chroma planes: the word
+                 * reads past a row end stay inside the frame */
+                ld9w(rp + (size_t)y0 * rw + ix, J.lo0, J.mid0, J.hi0);
+                ld9w(rp + (size_t)(y0 + 1) * rw + ix, J.lo1, J.mid1, J.hi1);
+            } else {
+                ld9c(rp, rw, rh, ix, y0, J.lo0, J.mid0, J.hi0);
+                ld9c(rp, rw, rh, ix, y0 + 1, J.lo1, J.mid1, J.hi1);
+            }
+        }
+    }
+    if (r < clh && clw > 0) {
+        K.act = true;
+        K.d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
+        K.clw = clw;
+        if (rp) {
+            K.ref = true;
+            const int rcs = (rw + 1) >> 1, crw = rw >> 1, crh = rh >> 1;
+            const uint8_t *pl = rp + (size_t)rw * rh + (p ? (size_t)rcs * ((rh + 1) >> 1) : 0);
+            const int cpx8 = ((sbx >> 1) + cx0) * 8 + mvx / 2, cpy8 = ((sby >> 1) + cy0) * 8 + mvy / 2;
+            const int cix = cpx8 >> 3, y0 = (cpy8 >> 3) + r;
+            K.fx = cpx8 & 7;
+            K.fy = cpy8 & 7;
+            if (cix >= 0 && cix + clw < crw && y0 >= 0 && y0 + 2 < crh) {
+                /* a further chroma row exists below: word reads stay inside */
+                ld5w(pl + (size_t)y0 * rcs + cix, K.lo0, K.hi0);
+                ld5w(pl + (size_t)(y0 + 1) * rcs + cix, K.lo1, K.hi1);
+            } else {
+                ld5c(pl, rcs, crw, crh, cix, y0, K.lo0, K.hi0);
+                ld5c(pl, rcs, crw, crh, cix, y0 + 1, K.lo1, K.hi1);
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ void fast_luma_finish(const FastLuma &J)
@@ -1799,47 +1828,6 @@ __device__ __forceinline__ void fast_luma_finish(const FastLuma &J)
 #pragma unroll
         for (int x = 0; x < 8; x++) if (x < J.lw) J.d[x] = (uint8_t)((x < 4 ? o0 : o1) >> (8 * (x & 3)));
     }
-}
-
-__device__ __forceinline__ FastChroma fast_chroma_issue(FastSmem &w, const cvp9_job_t &job, int c, int p, int r,
-                                                       int nchunks, int sbx, int sby)
-{
-    FastChroma J;
-    J.act = false;
-    J.ref = false;
-    if (c >= nchunks) return J;
-    FastBlk fb;
-    int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
-    fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
-    if (r >= clh || clw <= 0) return J;
-    J.act = true;
-    J.d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
-    J.clw = clw;
-    const int slot = fb_slot(fb);
-    if (slot >= 8) return J;
-    const cvp9_ref_t &R = job.ref[slot];
-    const uint8_t *rp = R.plane;
-    if (!rp) return J;
-    J.ref = true;
-    const int rw = R.w, rh = R.h;
-    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
-    const int rcs = (rw + 1) >> 1, crw = rw >> 1, crh = rh >> 1;
-    const uint8_t *pl = rp + (size_t)rw * rh + (p ? (size_t)rcs * ((rh + 1) >> 1) : 0);
-    const int cmx = mvx / 2, cmy = mvy / 2;          /* halves toward zero */
-    const int cpx8 = ((sbx >> 1) + cx0) * 8 + cmx, cpy8 = ((sby >> 1) + cy0) * 8 + cmy;
-    const int cix = cpx8 >> 3, ciy = cpy8 >> 3;
-    J.fx = cpx8 & 7;
-    J.fy = cpy8 & 7;
-    const int y0 = ciy + r;
-    if (cix >= 0 && cix + clw < crw && y0 >= 0 && y0 + 2 < crh) {
-        /* a further chroma row exists below: word reads stay inside */
-        ld5w(pl + (size_t)y0 * rcs + cix, J.lo0, J.hi0);
-        ld5w(pl + (size_t)(y0 + 1) * rcs + cix, J.lo1, J.hi1);
-    } else {
-        ld5c(pl, rcs, crw, crh, cix, y0, J.lo0, J.hi0);
-        ld5c(pl, rcs, crw, crh, cix, y0 + 1, J.lo1, J.hi1);
-    }
-    return J;
 }
 
 __device__ __forceinline__ void fast_chroma_finish(const FastChroma &J)
@@ -2403,10 +2391,10 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
         nchunks = 0;                      /* the REFCPU passes below do nothing */
     }
     for (int c0 = 0; c0 < nchunks; c0 += 8) {
-        const FastLuma a = fast_luma_issue(w, job, c0 + (lane >> 3), lane & 7, nchunks, sbx, sby);
-        const FastLuma b = fast_luma_issue(w, job, c0 + 4 + (lane >> 3), lane & 7, nchunks, sbx, sby);
-        const FastChroma ca = fast_chroma_issue(w, job, c0 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
-        const FastChroma cb = fast_chroma_issue(w, job, c0 + 4 + (lane >> 3), (lane >> 2) & 1, lane & 3, nchunks, sbx, sby);
+        FastLuma a, b;
+        FastChroma ca, cb;
+        fast_pred_issue(w, job, c0 + (lane >> 3), lane, nchunks, sbx, sby, a, ca);
+        fast_pred_issue(w, job, c0 + 4 + (lane >> 3), lane, nchunks, sbx, sby, b, cb);
         fast_luma_finish(a);
         fast_luma_finish(b);
         fast_chroma_finish(ca);
