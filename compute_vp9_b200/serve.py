@@ -1,6 +1,6 @@
 """Continuous-batching serving loop over the multi-stream engine.
 
-    python -m compute_vp9_b200.serve [--streams 256] [--rate 2] [--speed 20]
+    python -m compute_vp9_b200.serve [--streams 256] [--rate 2] [--speed 1]
 
 Streams arrive as a Poisson process; each carries `frames` frames paced at
 `fps`. A stream is admitted when the engine's HBM budget has room
@@ -111,7 +111,7 @@ class Stream:
         return base + i / self.fps
 
 
-def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=20.0, hbm_budget=150e9,
+def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9,
         arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None,
         trace=None):
     """Serve a Poisson arrival of `streams` streams; returns a summary dict.
@@ -241,7 +241,7 @@ def main():
     ap.add_argument("--rate", type=float, default=2.0, help="stream arrivals per second (real time)")
     ap.add_argument("--frames", type=int, default=120)
     ap.add_argument("--fps", type=float, default=30.0)
-    ap.add_argument("--speed", type=float, default=20.0)
+    ap.add_argument("--speed", type=float, default=1.0, help="pacing compression (1 = real time)")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec"])
     a = ap.parse_args()
