@@ -201,6 +201,48 @@ class Workload:
         nzc = np.concatenate([[0], np.cumsum(coeffs != 0)])
         return int((nzc[off + ln] - nzc[off]).sum())
 
+    def build_sparse(self):
+        """(index, value) lists of every frame's nonzero coefficients in one
+        page-locked arena — what a parser emitting coefficients as it decodes
+        tokens would hand over; built once, outside any timed region."""
+        import numpy as np
+        import torch
+        from compute_vp9_b200.batch import CoeffList
+        hv = self.host.numpy()
+        hbase = self.host.data_ptr()
+        per_frame = []
+        total = 0
+        for s in range(self.S):
+            row = []
+            for f in range(DISTINCT):
+                pf = self.pfs_host[s][f]
+                oc = C.cast(pf.coeffs, C.c_void_p).value - hbase
+                dense = hv[oc:oc + 2 * pf.num_coeffs].view(np.int16)
+                pos = np.nonzero(dense)[0].astype(np.uint32)
+                row.append((pos, dense[pos]))
+                total += (pos.nbytes + 255) // 256 * 256 + (pos.size * 2 + 255) // 256 * 256
+            per_frame.append(row)
+        self.sparse_arena = torch.empty(max(1, total), dtype=torch.uint8, pin_memory=torch.cuda.is_available())
+        av = self.sparse_arena.numpy()
+        base = self.sparse_arena.data_ptr()
+        off = 0
+        self.lists = []
+        for row in per_frame:
+            lr = []
+            for pos, val in row:
+                op = off
+                av[op:op + pos.nbytes] = pos.view(np.uint8)
+                off += (pos.nbytes + 255) // 256 * 256
+                ov = off
+                av[ov:ov + val.nbytes] = val.view(np.uint8)
+                off += (val.nbytes + 255) // 256 * 256
+                lr.append(CoeffList(pos.size, base + op, base + ov))
+            self.lists.append(lr)
+
+    def step_lists(self, t):
+        f = step_frame(t)
+        return [self.lists[s][f] for s in range(self.S)]
+
     def step_pfs(self, t, device):
         f = step_frame(t)
         src = self.pfs_dev if device else self.pfs_host
@@ -271,7 +313,7 @@ class ClockSampler:
 
 # ── legs ─────────────────────────────────────────────────────────────────────
 
-def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None):
+def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False):
     """K timed steps of all streams; returns (ms, per-step stats list, latencies).
     The engine's tuner first settles this shape's kernel configuration on
     untimed steps (a few per candidate); `tuned` receives its choice."""
@@ -281,15 +323,21 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None)
     sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
     assert all(s is not None for s in sids), "admission refused"
     flags = (DEVICE_INPUTS | NO_OUTPUT) if device_inputs else 0
+
+    def submit(t):
+        if sparse:
+            eng.submit_sparse(sids, wl.step_pfs(t, False), wl.step_lists(t), [t] * wl.S, flags)
+        else:
+            eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags)
     for t in range(40):
-        eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags)
+        submit(t)
         assert eng.wait() == 0, eng.last_error()
         if all(e["settled"] for e in eng.tuning()):
             break
     if tuned is not None:
         tuned.extend(eng.tuning())
     for t in range(warmup):
-        eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags)
+        submit(t)
     rc = eng.wait()
     assert rc == 0, eng.last_error()
     torch.cuda.synchronize()
@@ -298,7 +346,7 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None)
     seq0 = eng.last_seq()
     eng.timer_start()
     for t in range(warmup, warmup + steps):
-        eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags)
+        submit(t)
     ms = eng.timer_stop()
     rc = eng.wait()
     assert rc == 0, eng.last_error()
@@ -309,7 +357,7 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None)
     # per-kernel device times: a few more steps, each waited for
     prof = []
     for t in range(warmup + steps, warmup + steps + 3):
-        eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags)
+        submit(t)
         eng.wait()
         st = eng.stats()
         prof.append((st.scan_ms, st.recon_ms, st.filter_ms, st.kernels_ms, st.step_ms))
@@ -500,6 +548,13 @@ def main():
     ms_e2e = allreduce_max(ws, ms_e2e)
     e2e = ws * px_step * args.steps / (ms_e2e / 1000.0) / 1e6
 
+    # the same, coefficients as (index, value) lists (cvp9_batch_submit_sparse)
+    wl.build_sparse()
+    ms_sp, st_sp, _, _ = run_batched(wl, args.steps, args.warmup, arith, False,
+                                     not args.no_graphs, ws, sparse=True)
+    ms_sp = allreduce_max(ws, ms_sp)
+    e2e_sp = ws * px_step * args.steps / (ms_sp / 1000.0) / 1e6
+
     out = None
     if rank == 0:
         recon_ms = statistics.mean(p[1] for p in prof)
@@ -544,6 +599,13 @@ def main():
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(st_e2e.h2d_bytes),
                     "d2h_bytes_per_step": int(st_e2e.d2h_bytes),
                     "ms_per_step": ms_e2e / args.steps},
+            "e2e_sparse_input": {"value": e2e_sp, "unit": UNIT,
+                                 "h2d_bytes_per_step": int(st_sp.h2d_bytes),
+                                 "d2h_bytes_per_step": int(st_sp.d2h_bytes),
+                                 "ms_per_step": ms_sp / args.steps,
+                                 "what": "as e2e, with each frame's coefficients handed over as (index, "
+                                         "value) lists through cvp9_batch_submit_sparse (built before "
+                                         "timing, as a parser emitting them would); outputs identical"},
             "latency_ms": {"p50": statistics.median(lat) if lat else None,
                            "p99": (sorted(lat)[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None),
                            "what": "host clock, submit to frame in pinned host memory, e2e steps (2 in flight)"},

@@ -14,6 +14,11 @@ class BatchConfig(C.Structure):
                 ("max_streams", C.c_int), ("use_graphs", C.c_int), ("autotune", C.c_int)]
 
 
+class CoeffList(C.Structure):
+    """cvp9_coeff_list_t: a frame's nonzero coefficients (index, value)."""
+    _fields_ = [("n", C.c_uint32), ("pos", C.c_void_p), ("val", C.c_void_p)]
+
+
 class TuneEntry(C.Structure):
     _fields_ = [("key", C.c_uint64), ("frames", C.c_int), ("settled", C.c_int),
                 ("inter_path", C.c_int), ("lf_tile_h", C.c_int), ("half_width", C.c_int),
@@ -34,6 +39,9 @@ def _bind(lib):
     lib.cvp9_batch_destroy.argtypes = [vp]
     lib.cvp9_batch_destroy.restype = None
     lib.cvp9_batch_tune_count.argtypes = [vp]
+    lib.cvp9_batch_submit_sparse.argtypes = [vp, C.c_int, C.POINTER(C.c_int),
+                                             C.POINTER(C.POINTER(ParsedFrame)), C.POINTER(CoeffList),
+                                             C.POINTER(C.c_int64), C.c_uint32]
     lib.cvp9_batch_tune_entry.argtypes = [vp, C.c_int, C.POINTER(TuneEntry)]
     lib.cvp9_batch_stream_bytes.argtypes = [C.c_uint32, C.c_uint32]
     lib.cvp9_batch_stream_bytes.restype = C.c_uint64
@@ -95,6 +103,17 @@ class Batch:
         rc = self._lib.cvp9_batch_submit(self._h, n, arr_s, arr_p, arr_t, flags)
         if rc != CVP9_OK:
             raise BatchError(rc, "cvp9_batch_submit", self.last_error())
+
+    def submit_sparse(self, sids, pfs, lists, pts=None, flags=0):
+        """Like submit, with each frame's coefficients as a CoeffList."""
+        n = len(sids)
+        arr_s = (C.c_int * n)(*sids)
+        arr_p = (C.POINTER(ParsedFrame) * n)(*pfs)
+        arr_l = (CoeffList * n)(*lists)
+        arr_t = (C.c_int64 * n)(*(pts if pts is not None else [0] * n))
+        rc = self._lib.cvp9_batch_submit_sparse(self._h, n, arr_s, arr_p, arr_l, arr_t, flags)
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_submit_sparse", self.last_error())
 
     def wait(self):
         return self._lib.cvp9_batch_wait(self._h)

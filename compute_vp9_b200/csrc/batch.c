@@ -481,8 +481,25 @@ static void CUDART_CB step_done_cb(void *p)
     a->b->lat_done[a->seq % LAT_RING] = cvp9_now();
 }
 
+static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9_parsed_frame_t *const *pfs,
+                              const cvp9_coeff_list_t *lists, const int64_t *pts, uint32_t flags);
+
 cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
                              const vp9_parsed_frame_t *const *pfs, const int64_t *pts, uint32_t flags)
+{
+    return submit_impl(b, n, sids, pfs, NULL, pts, flags);
+}
+
+cvp9_err_t cvp9_batch_submit_sparse(cvp9_batch_t *b, int n, const int *sids,
+                                    const vp9_parsed_frame_t *const *pfs, const cvp9_coeff_list_t *lists,
+                                    const int64_t *pts, uint32_t flags)
+{
+    if (!lists || (flags & CVP9_BATCH_DEVICE_INPUTS)) return CVP9_ERR_INVALID_DATA;
+    return submit_impl(b, n, sids, pfs, lists, pts, flags);
+}
+
+static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9_parsed_frame_t *const *pfs,
+                              const cvp9_coeff_list_t *lists, const int64_t *pts, uint32_t flags)
 {
     if (!b || n <= 0 || !sids || !pfs) return CVP9_ERR_INVALID_DATA;
     if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
@@ -496,7 +513,9 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         const vp9_parsed_frame_t *pf = pfs[i];
         if ((int32_t)pf->hdr.width != b->st[sid].W || (int32_t)pf->hdr.height != b->st[sid].H)
             return CVP9_ERR_INVALID_DATA;
-        if ((pf->num_blocks && !pf->blocks) || (pf->num_coeffs && !pf->coeffs)) return CVP9_ERR_INVALID_DATA;
+        if (pf->num_blocks && !pf->blocks) return CVP9_ERR_INVALID_DATA;
+        if (lists ? (lists[i].n && (!lists[i].pos || !lists[i].val)) : (pf->num_coeffs && !pf->coeffs))
+            return CVP9_ERR_INVALID_DATA;
         for (int j = 0; j < i; j++) if (sids[j] == sid) return CVP9_ERR_INVALID_DATA;
     }
 
@@ -518,6 +537,8 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         if (!dev_in) {
             in_bytes += ALIGN_UP((size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t), 256);
             in_bytes += ALIGN_UP((size_t)pf->num_coeffs * sizeof(int16_t), 256);
+            if (lists)
+                in_bytes += ALIGN_UP((size_t)lists[i].n * 4, 256) + ALIGN_UP((size_t)lists[i].n * 2, 256);
         }
         n_sb += (size_t)st->n_sb;
         if ((int)pf->num_blocks > max_blocks) max_blocks = (int)pf->num_blocks;
@@ -554,7 +575,8 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         int staged = 0;
         for (int i = 0; i < n && !staged; i++)
             staged = (pfs[i]->num_blocks && !is_pinned(pfs[i]->blocks)) ||
-                     (pfs[i]->num_coeffs && !is_pinned(pfs[i]->coeffs));
+                     (lists ? (lists[i].n && (!is_pinned(lists[i].pos) || !is_pinned(lists[i].val)))
+                            : (pfs[i]->num_coeffs && !is_pinned(pfs[i]->coeffs)));
         if ((staged && (err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes))) ||
             (err = grow_dev(b, (void **)&s->d_in, &s->d_in_cap, in_bytes)))
             return err;
@@ -610,14 +632,16 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     size_t off = 0;
     const uint8_t *dev_blocks[256], *dev_coeffs[256];
     const void *gather_local[256];
+    size_t sp_local[256];
     const uint8_t **dbp = n <= 256 ? dev_blocks : malloc((size_t)n * sizeof(void *));
     const uint8_t **dcp = n <= 256 ? dev_coeffs : malloc((size_t)n * sizeof(void *));
     const void **gsrc = n <= 256 ? gather_local : malloc((size_t)n * sizeof(void *));
-    if (!dbp || !dcp || !gsrc) return CVP9_ERR_NOMEM;
+    size_t *spo = n <= 256 ? sp_local : malloc((size_t)n * sizeof(size_t));   /* pos list offset in d_in */
+    if (!dbp || !dcp || !gsrc || !spo) return CVP9_ERR_NOMEM;
     int any_gather = 0;
     typedef struct { const void *src; size_t off, n; } direct_t;
-    direct_t direct_local[512];
-    direct_t *direct = n <= 256 ? direct_local : malloc((size_t)2 * n * sizeof(direct_t));
+    direct_t direct_local[1024];
+    direct_t *direct = n <= 256 ? direct_local : malloc((size_t)4 * n * sizeof(direct_t));
     if (!direct) return CVP9_ERR_NOMEM;
     int ndirect = 0, any_staged = 0;
     for (int i = 0; i < n; i++) {
@@ -630,15 +654,19 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         }
         /* REFCPU reads only each block's luma coefficients: from page-locked
          * memory a kernel moves just those (k_gather_luma), not the array */
-        if (b->gather && pf->num_coeffs && pf->num_blocks)
+        if (b->gather && !lists && pf->num_coeffs && pf->num_blocks)
             gsrc[i] = mapped_ptr(pf->coeffs);
         any_gather |= gsrc[i] != NULL;
         size_t nbb = (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t);
         size_t ncb = (size_t)pf->num_coeffs * sizeof(int16_t);
-        const void *srcs[2] = { pf->blocks, pf->coeffs };
-        size_t lens[2] = { nbb, ncb };
-        for (int k = 0; k < 2; k++) {
-            if (lens[k] && !(k == 1 && gsrc[i])) {
+        /* blocks, dense coefficients, then (sparse input) positions, values;
+         * the dense region of a sparse frame is filled on the device */
+        const void *srcs[4] = { pf->blocks, pf->coeffs, lists ? lists[i].pos : NULL, lists ? lists[i].val : NULL };
+        size_t lens[4] = { nbb, ncb, lists ? (size_t)lists[i].n * 4 : 0, lists ? (size_t)lists[i].n * 2 : 0 };
+        const int narr = lists ? 4 : 2;
+        for (int k = 0; k < narr; k++) {
+            if (k == 2) spo[i] = off;
+            if (lens[k] && !(k == 1 && (gsrc[i] || lists))) {
                 if (is_pinned(srcs[k])) {
                     direct[ndirect].src = srcs[k];
                     direct[ndirect].off = off;
@@ -650,7 +678,7 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
                     any_staged = 1;
                 }
             }
-            (k == 0 ? dbp : dcp)[i] = s->d_in + off;
+            if (k < 2) (k == 0 ? dbp : dcp)[i] = s->d_in + off;
             off += ALIGN_UP(lens[k], 256);
         }
     }
@@ -668,10 +696,15 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
         }
     }
     if (direct != direct_local) free(direct);
+    /* sparse frames: their dense coefficient regions start at zero */
+    for (int i = 0; lists && i < n && ue == cudaSuccess; i++)
+        if (pfs[i]->num_coeffs)
+            ue = cudaMemsetAsync((void *)dcp[i], 0, (size_t)pfs[i]->num_coeffs * 2, b->hs);
     if (ue != cudaSuccess) {
         if (dbp != dev_blocks) free(dbp);
         if (dcp != dev_coeffs) free(dcp);
         if (gsrc != gather_local) free(gsrc);
+        if (spo != sp_local) free(spo);
         return bfail(b, ue, "upload inputs");
     }
 
@@ -708,6 +741,11 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
             }
         }
         job->coeffs_src = (const int16_t *)gsrc[i];
+        if (lists && lists[i].n) {
+            job->sp_pos = (const uint32_t *)(s->d_in + spo[i]);
+            job->sp_val = (const int16_t *)(s->d_in + spo[i] + ALIGN_UP((size_t)lists[i].n * 4, 256));
+            job->sp_n = lists[i].n;
+        }
         job->epoch = ++st->epoch;
         job->sb_range = s->d_sb_range + 4 * (size_t)sb_base;
         job->sb_done = st->d_sb_done;
@@ -718,18 +756,25 @@ cvp9_err_t cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
     if (dbp != dev_blocks) free(dbp);
     if (dcp != dev_coeffs) free(dcp);
     if (gsrc != gather_local) free(gsrc);
+    if (spo != sp_local) free(spo);
     BCK(cudaMemcpyAsync(s->d_jobs, s->h_jobs, (size_t)n * sizeof(cvp9_job_t), cudaMemcpyHostToDevice, b->hs),
         "upload jobs");
     s->h2d_bytes += (size_t)n * sizeof(cvp9_job_t);
     /* the counter of gathered bytes is cleared here, on the upload stream;
      * the compute stream's clear of the status words stops before it */
     BCK(cudaMemsetAsync(s->d_misc + n + 1, 0, 4, b->hs), "clear gather counter");
+    s->launches_extra = 0;
     if (any_gather) {
         int grc = cvp9k_launch_gather(s->d_jobs, n, max_blocks, s->d_misc + n + 1, b->hs);
         if (grc != 0) return bfail(b, (cudaError_t)grc, "coefficient gather");
-        s->launches_extra = 1;
-    } else {
-        s->launches_extra = 0;
+        s->launches_extra++;
+    }
+    if (lists) {
+        uint32_t max_n = 0;
+        for (int i = 0; i < n; i++) if (lists[i].n > max_n) max_n = lists[i].n;
+        int src = cvp9k_launch_scatter(s->d_jobs, n, max_n, b->hs);
+        if (src != 0) return bfail(b, (cudaError_t)src, "coefficient scatter");
+        s->launches_extra++;
     }
     BCK(cudaEventRecord(s->ev_h2d, b->hs), "event");
 

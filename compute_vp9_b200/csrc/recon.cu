@@ -2870,11 +2870,34 @@ __global__ void __launch_bounds__(256) k_gather_luma(const cvp9_job_t *__restric
     if (lane == 0 && moved) atomicAdd(bytes, moved);
 }
 
+/* Sparse coefficient upload: the caller's (index, value) list of a frame
+ * is scattered into its zeroed dense array, which the reconstruction then
+ * reads exactly as if the dense array had been uploaded. */
+__global__ void __launch_bounds__(256) k_scatter_coeffs(const cvp9_job_t *__restrict__ jobs)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    const uint32_t n = job.sp_n;
+    int16_t *dst = const_cast<int16_t *>(job.coeffs);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t p = job.sp_pos[k];
+        if (p < job.num_coeffs) dst[p] = job.sp_val[k];
+    }
+}
+
 /* ── C-ABI launch shims ─────────────────────────────────────────────────── */
 
 extern "C" {
 
 size_t cvp9k_recon_smem_bytes(void) { return sizeof(ReconSmem); }
+
+int cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, cudaStream_t st)
+{
+    if (njobs <= 0 || max_n == 0) return 0;
+    unsigned gx = (max_n + 255u) / 256u;
+    if (gx > 4096u) gx = 4096u;
+    k_scatter_coeffs<<<dim3(gx, (unsigned)njobs), 256, 0, st>>>(jobs);
+    return (int)cudaGetLastError();
+}
 
 int cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, uint32_t *bytes, cudaStream_t st)
 {

@@ -55,6 +55,9 @@ typedef struct {
     const int16_t *coeffs_src;      /* REFCPU upload: the parser's coefficient array
                                      * in page-locked host memory, read by
                                      * k_gather_luma (NULL: coeffs already on device) */
+    const uint32_t *sp_pos;         /* sparse upload: indices into coeffs (device)  */
+    const int16_t  *sp_val;         /* and their values; coeffs zeroed beforehand   */
+    uint32_t        sp_n;           /* k_scatter_coeffs writes them; 0: none        */
 } cvp9_job_t;
 
 #ifdef __cplusplus

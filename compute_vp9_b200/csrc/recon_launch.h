@@ -53,6 +53,10 @@ int    cvp9k_recon_ctas_per_sm(int arith);
 int    cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, uint32_t *bytes,
                            cudaStream_t stream);
 
+/* Sparse coefficient upload: jobs[j].coeffs[sp_pos[k]] = sp_val[k] for
+ * every job with sp_n > 0 (indices past num_coeffs are ignored). */
+int    cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, cudaStream_t stream);
+
 /* Enqueue the chain on `stream`; returns the cudaError_t of the first
  * failing call (0 on success). */
 int    cvp9k_launch_frame(const cvp9k_launch_t *launch, cudaStream_t stream);

@@ -98,6 +98,28 @@ cvp9_err_t  cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
                               const vp9_parsed_frame_t *const *pfs, const int64_t *pts,
                               uint32_t flags);
 
+/* Sparse coefficients of one frame: the nonzero entries of the dense int16
+ * coefficient array the parser would have written (same layout, same
+ * indices), as parallel arrays. A parser that emits coefficients as it
+ * decodes tokens can fill these instead of a mostly-zero dense array;
+ * indices must be distinct. */
+typedef struct {
+    uint32_t        n;       /* nonzero coefficients                            */
+    const uint32_t *pos;     /* index into the dense array (< num_coeffs)       */
+    const int16_t  *val;     /* their values                                    */
+} cvp9_coeff_list_t;
+
+/* As cvp9_batch_submit, with coefficients given as lists[i] instead of
+ * pfs[i]->coeffs (ignored; pfs[i]->num_coeffs still gives the dense size).
+ * Only the lists cross the bus: the engine zeroes each frame's dense array
+ * on the device and scatters the list into it, so every output byte is the
+ * one the dense submit gives. Host inputs only (no CVP9_BATCH_DEVICE_INPUTS).
+ * No counterpart in the reference, whose parser writes the dense array. */
+cvp9_err_t  cvp9_batch_submit_sparse(cvp9_batch_t *b, int n, const int *sids,
+                                     const vp9_parsed_frame_t *const *pfs,
+                                     const cvp9_coeff_list_t *lists, const int64_t *pts,
+                                     uint32_t flags);
+
 /* Block (bounded) until every submitted step is complete. Returns the first
  * per-stream error of those steps (CVP9_ERR_INVALID_DATA for a rejected
  * block layout, CVP9_ERR_GPU for an expired device wait), else CVP9_OK. */

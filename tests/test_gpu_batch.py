@@ -170,3 +170,41 @@ def test_pinned_inputs_match_oracle(profile):
     st = eng.stats()
     assert st.h2d_bytes > 0
     eng.close()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_sparse_coefficients_match_oracle(profile, pinned):
+    """Coefficients given as (index, value) lists (cvp9_batch_submit_sparse)
+    decode to the oracle's bytes, from page-locked and from pageable memory."""
+    import torch
+    from compute_vp9_b200.batch import CoeffList
+    eng = Batch(arith=profile)
+    syns = [Synth(synth_config(p, w, h, seed=50 + i, **ov)) for i, (p, w, h, ov) in enumerate(MIX)]
+    orcs = [OracleStream(profile) for _ in MIX]
+    sids = [eng.open_stream(w, h) for (_, w, h, _) in MIX]
+    for f in range(3):
+        keep, lists = [], []
+        pfs = [syn.frame(f) for syn in syns]
+        for pf in pfs:
+            p = pf.contents
+            dense = np.ctypeslib.as_array(p.coeffs, shape=(p.num_coeffs,)) if p.num_coeffs else np.zeros(0, np.int16)
+            pos = np.nonzero(dense)[0].astype(np.uint32)
+            val = dense[pos].astype(np.int16)
+            if pinned:
+                tp = torch.empty(max(1, pos.size), dtype=torch.int32, pin_memory=True)
+                tv = torch.empty(max(1, val.size), dtype=torch.int16, pin_memory=True)
+                tp.numpy()[:pos.size] = pos.view(np.int32)
+                tv.numpy()[:val.size] = val
+                keep += [tp, tv]
+                lists.append(CoeffList(pos.size, tp.data_ptr(), tv.data_ptr()))
+            else:
+                keep += [pos, val]
+                lists.append(CoeffList(pos.size, pos.ctypes.data, val.ctypes.data))
+        eng.submit_sparse(sids, pfs, lists, [f] * len(MIX))
+        assert eng.wait() == CVP9_OK, eng.last_error()
+        for i in range(len(MIX)):
+            rc, arr = eng.get_frame_array(sids[i])
+            assert rc == CVP9_OK
+            assert np.array_equal(arr, orcs[i].decode(pfs[i])), "stream %d frame %d" % (i, f)
+    eng.close()
