@@ -247,3 +247,81 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms)
     }
     tune_advance(t, e);
 }
+
+/* ── Host copy pool ───────────────────────────────────────────────────── */
+
+#define COPY_MAX_THREADS 8
+
+typedef struct { char *dst; const char *src; size_t n; } copy_part_t;
+
+static struct {
+    pthread_mutex_t mu;
+    pthread_cond_t  work, done;
+    pthread_mutex_t busy;            /* one parallel copy at a time */
+    copy_part_t     part[COPY_MAX_THREADS];
+    int             nparts, next, pending;
+    int             nthreads;        /* workers (the caller is one more) */
+} g_copy = { PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, PTHREAD_COND_INITIALIZER,
+             PTHREAD_MUTEX_INITIALIZER, { { 0, 0, 0 } }, 0, 0, 0, -1 };
+static pthread_once_t g_copy_once = PTHREAD_ONCE_INIT;
+
+static void *copy_worker(void *arg)
+{
+    (void)arg;
+    pthread_mutex_lock(&g_copy.mu);
+    for (;;) {
+        while (g_copy.next >= g_copy.nparts) pthread_cond_wait(&g_copy.work, &g_copy.mu);
+        copy_part_t p = g_copy.part[g_copy.next++];
+        pthread_mutex_unlock(&g_copy.mu);
+        memcpy(p.dst, p.src, p.n);
+        pthread_mutex_lock(&g_copy.mu);
+        if (--g_copy.pending == 0) pthread_cond_signal(&g_copy.done);
+    }
+    return NULL;
+}
+
+static void copy_pool_start(void)
+{
+    int want = 3;                                    /* 3 workers + the caller */
+    const char *e = getenv("CVP9_COPY_THREADS");
+    if (e && *e) want = atoi(e) - 1;
+    if (want > COPY_MAX_THREADS - 1) want = COPY_MAX_THREADS - 1;
+    int started = 0;
+    for (int i = 0; i < want; i++) {
+        pthread_t t;
+        pthread_attr_t at;
+        pthread_attr_init(&at);
+        pthread_attr_setdetachstate(&at, PTHREAD_CREATE_DETACHED);
+        if (pthread_create(&t, &at, copy_worker, NULL) == 0) started++;
+        pthread_attr_destroy(&at);
+    }
+    g_copy.nthreads = started;
+}
+
+void cvp9_parallel_memcpy(void *dst, const void *src, size_t n)
+{
+    if (n < (1u << 20)) { memcpy(dst, src, n); return; }
+    pthread_once(&g_copy_once, copy_pool_start);
+    if (g_copy.nthreads <= 0 || pthread_mutex_trylock(&g_copy.busy) != 0) { memcpy(dst, src, n); return; }
+    const int parts = g_copy.nthreads + 1;
+    size_t chunk = (n / parts + 4095) & ~(size_t)4095;
+    pthread_mutex_lock(&g_copy.mu);
+    int k = 0;
+    for (size_t off = chunk; off < n && k < parts - 1; off += chunk, k++) {
+        g_copy.part[k].dst = (char *)dst + off;
+        g_copy.part[k].src = (const char *)src + off;
+        g_copy.part[k].n = off + chunk <= n ? chunk : n - off;
+    }
+    g_copy.nparts = k;
+    g_copy.next = 0;
+    g_copy.pending = k;
+    pthread_cond_broadcast(&g_copy.work);
+    pthread_mutex_unlock(&g_copy.mu);
+    memcpy(dst, src, chunk < n ? chunk : n);          /* the caller's share */
+    pthread_mutex_lock(&g_copy.mu);
+    while (g_copy.pending > 0) pthread_cond_wait(&g_copy.done, &g_copy.mu);
+    g_copy.nparts = 0;
+    g_copy.next = 0;
+    pthread_mutex_unlock(&g_copy.mu);
+    pthread_mutex_unlock(&g_copy.busy);
+}

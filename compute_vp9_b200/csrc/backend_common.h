@@ -103,3 +103,9 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms);
 /* Coarse bucket of a step: arithmetic, frame count and superblock count,
  * each rounded up to a power of two, so serving steps share buckets. */
 uint64_t cvp9_tune_key(int arith, int frames, uint64_t superblocks);
+
+/* memcpy split across a small pool of host threads (the caller copies one
+ * share); plain memcpy below 1 MB, when another copy holds the pool, or
+ * with $CVP9_COPY_THREADS=1. The per-stream backend stages the parser's
+ * arrays with it: one thread moves ~12 GB/s, slower than the PCIe link. */
+void cvp9_parallel_memcpy(void *dst, const void *src, size_t n);

@@ -291,8 +291,9 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
         (err = grow_device(c, &s->d_blocks, &s->d_blocks_cap, nbb ? nbb : 64)) ||
         (err = grow_device(c, &s->d_coeffs, &s->d_coeffs_cap, ncb ? ncb : 64)))
         return err;
-    if (nbb) memcpy(s->h_blocks, pf->blocks, nbb);
-    if (ncb) memcpy(s->h_coeffs, pf->coeffs, ncb);
+    /* the parser's arrays are borrowed for this call only: stage them now */
+    if (nbb) cvp9_parallel_memcpy(s->h_blocks, pf->blocks, nbb);
+    if (ncb) cvp9_parallel_memcpy(s->h_coeffs, pf->coeffs, ncb);
 
     int of = acquire_dframe(c, W, H);
     if (of < 0) return fail(c, cudaErrorMemoryAllocation, "frame pool");

@@ -113,7 +113,9 @@ typedef struct {
  * pfs[i]->coeffs (ignored; pfs[i]->num_coeffs still gives the dense size).
  * Only the lists cross the bus: the engine zeroes each frame's dense array
  * on the device and scatters the list into it, so every output byte is the
- * one the dense submit gives. Host inputs only (no CVP9_BATCH_DEVICE_INPUTS).
+ * one the dense submit gives. Host inputs only (no CVP9_BATCH_DEVICE_INPUTS);
+ * lists in page-locked memory are read after the call returns and must stay
+ * unchanged until the step completes, like page-locked dense inputs.
  * No counterpart in the reference, whose parser writes the dense array. */
 cvp9_err_t  cvp9_batch_submit_sparse(cvp9_batch_t *b, int n, const int *sids,
                                      const vp9_parsed_frame_t *const *pfs,

@@ -96,3 +96,34 @@ def test_job_struct_is_word_copyable():
     # the recon kernel copies the job descriptor into shared memory as 32-bit words
     text = open(os.path.join(ROOT, "compute_vp9_b200", "csrc", "recon_job.h")).read()
     assert "cvp9_ref_t ref[8]" in text
+
+
+def test_parallel_memcpy_copies_every_byte():
+    """The host copy pool the per-stream backend stages frames with: sizes
+    around the 1 MB threshold and the chunk edges, and concurrent callers
+    (one takes the pool, the others fall back to memcpy)."""
+    import threading
+    import numpy as np
+    from compute_vp9_b200 import cuda_lib
+    lib = cuda_lib()
+    lib.cvp9_parallel_memcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.cvp9_parallel_memcpy.restype = None
+    rng = np.random.default_rng(5)
+    for n in (0, 17, (1 << 20) - 1, 1 << 20, (1 << 20) + 4097, 7_300_001, 16 << 20):
+        src = rng.integers(0, 256, size=n, dtype=np.uint8)
+        dst = np.zeros(n + 64, np.uint8)
+        lib.cvp9_parallel_memcpy(dst.ctypes.data, src.ctypes.data, n)
+        assert np.array_equal(dst[:n], src) and not dst[n:].any(), n
+    srcs = [rng.integers(0, 256, size=3_000_000 + k, dtype=np.uint8) for k in range(6)]
+    dsts = [np.zeros_like(s) for s in srcs]
+
+    def work(k):
+        for _ in range(20):
+            lib.cvp9_parallel_memcpy(dsts[k].ctypes.data, srcs[k].ctypes.data, srcs[k].size)
+
+    ts = [threading.Thread(target=work, args=(k,)) for k in range(6)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert all(np.array_equal(d, s) for d, s in zip(dsts, srcs))
