@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-single", action="store_true", help="skip the single-stream leg")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
+    ap.add_argument("--no-parity", action="store_true", help="skip the bit-exactness check of the e2e run")
     ap.add_argument("--serve-speed", type=float, default=4.0,
                     help="pacing compression of the serving run (1 = the config's real time)")
     return ap.parse_args()
@@ -313,7 +314,7 @@ class ClockSampler:
 
 # ── legs ─────────────────────────────────────────────────────────────────────
 
-def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False):
+def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False, record=None):
     """K timed steps of all streams; returns (ms, per-step stats list, latencies).
     The engine's tuner first settles this shape's kernel configuration on
     untimed steps (a few per candidate); `tuned` receives its choice."""
@@ -325,6 +326,8 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None,
     flags = (DEVICE_INPUTS | NO_OUTPUT) if device_inputs else 0
 
     def submit(t):
+        if record is not None:
+            record.append(t)
         if sparse:
             eng.submit_sparse(sids, wl.step_pfs(t, False), wl.step_lists(t), [t] * wl.S, flags)
         else:
@@ -361,7 +364,14 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None,
         eng.wait()
         st = eng.stats()
         prof.append((st.scan_ms, st.recon_ms, st.filter_ms, st.kernels_ms, st.step_ms))
+    if record is not None and not device_inputs:
+        rc, arr = eng.get_frame_array(sids[0])
+        record_out = arr if rc == 0 else None
+    else:
+        record_out = None
     eng.close()
+    if record is not None:
+        record.append(record_out)
     return ms, last, prof, [x for x in lat if x is not None]
 
 
@@ -543,8 +553,9 @@ def main():
     ms_dev = allreduce_max(ws, ms_dev)
     value = ws * px_step * args.steps / (ms_dev / 1000.0) / 1e6
 
+    seq0 = []
     ms_e2e, st_e2e, _, lat = run_batched(wl, args.steps, args.warmup, arith, False,
-                                         not args.no_graphs, ws)
+                                         not args.no_graphs, ws, record=seq0)
     ms_e2e = allreduce_max(ws, ms_e2e)
     e2e = ws * px_step * args.steps / (ms_e2e / 1000.0) / 1e6
 
@@ -573,6 +584,22 @@ def main():
                       "kernel_ms_per_frame": plain_kern,
                       "workload": "stream 0 alone, %dx%d; value device-resident, e2e through "
                                   "cuda_decode_frame/cuda_get_frame with host inputs" % (one.w, one.h)}
+        # bit-exactness of the timed run: stream 0's last frame against the
+        # CPU reference (REFCPU: the reference's own code when built here,
+        # else the restatement) replaying the same frame sequence
+        parity = None
+        if not args.no_parity and seq0 and seq0[-1] is not None:
+            from oracle.oracle_py import REFCPU, SPEC, OracleStream, RefStream, ref_available
+            use_ref = arith == ARITH_REFCPU and ref_available()
+            chk = RefStream() if use_ref else OracleStream(SPEC if arith == ARITH_SPEC else REFCPU)
+            want = None
+            for t in seq0[:-1]:
+                want = chk.decode(C.pointer(wl.pfs_host[0][step_frame(t)]))
+            chk.close()
+            parity = {"checked": "stream 0, final frame after %d frames of the e2e run" % (len(seq0) - 1),
+                      "against": "oracle/_ref (the reference's vp9_reconstruct_frame)" if use_ref
+                                 else "oracle restatement",
+                      "bit_exact": bool(want is not None and (want == seq0[-1]).all())}
         serving = None
         if not args.no_serve:
             from compute_vp9_b200 import serve
@@ -622,6 +649,7 @@ def main():
                                           "best_ms")} for e in tuned],
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "parity": parity,
             "single_stream": single,
             "serving": serving,
             "batched_vs_single": (value / single["value"]) if single else None,
