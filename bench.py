@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
     ap.add_argument("--no-parity", action="store_true", help="skip the bit-exactness check of the e2e run")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the second batched run on mixed block/TX-size content")
     ap.add_argument("--serve-speed", type=float, default=4.0,
                     help="pacing compression of the serving run (1 = the config's real time)")
     return ap.parse_args()
@@ -113,7 +115,7 @@ class Workload:
     optional device copy. pfs_host[s][f] / pfs_dev[s][f] are ParsedFrame
     structs whose arrays live in those arenas."""
 
-    def __init__(self, streams, w, h, device_copy=True, seeds=None):
+    def __init__(self, streams, w, h, device_copy=True, seeds=None, preset=1, overrides=None):
         import numpy as np
         import torch
         from compute_vp9_b200 import ParsedFrame, Synth, synth_config
@@ -123,7 +125,7 @@ class Workload:
         frames = []
         seeds = seeds if seeds is not None else list(range(streams))
         for s in range(streams):
-            syn = Synth(synth_config(1, w, h, seed=seeds[s]))
+            syn = Synth(synth_config(preset, w, h, seed=seeds[s], **(overrides or {})))
             per = []
             for f in range(DISTINCT):
                 pf = syn.frame(f).contents
@@ -617,6 +619,29 @@ def main():
             v, kind, cores, sample = cpu_leg(wl, host_cores())
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
         launches_per_step = int(st_dev.kernel_launches)
+        # the batched step again on the other single-stream config's
+        # statistics (blocks 8-64, TX 4x4-32x32, 2-20% coefficients, +-128 px
+        # MVs from LAST/GOLDEN/ALTREF, GOP 60 with intra on key frames only)
+        mixed = None
+        if not args.no_mixed:
+            n_steps = args.steps
+            del wl
+            wl = None
+            wl2 = Workload(args.streams, args.width, args.height, device_copy=True,
+                           seeds=rank_seeds(rank, args.streams), preset=2, overrides={"intra_in_inter": 0.0})
+            tuned2 = []
+            ms2, _, prof2, _ = run_batched(wl2, n_steps, args.warmup, arith, True, not args.no_graphs, 1, tuned2)
+            v2 = wl2.S * wl2.w * wl2.h * n_steps / (ms2 / 1000.0) / 1e6
+            r2 = statistics.mean(p[1] for p in prof2)
+            a2 = statistics.mean(wl2.alg_bytes(t) for t in range(args.warmup + n_steps, args.warmup + n_steps + 3))
+            mixed = {"workload": "%d x %dx%d streams, blocks 8-64 (rectangular partitions), TX 4x4..32x32 "
+                                 "weighted 30/30/25/15, 2-20%% coefficients, +-128 px MVs over LAST/GOLDEN/"
+                                 "ALTREF, GOP 60, intra on key frames only; device-resident inputs"
+                                 % (wl2.S, wl2.w, wl2.h),
+                     "value": v2, "unit": UNIT, "ms_per_step": ms2 / n_steps, "recon_ms": r2,
+                     "roofline_frac": (a2 / (r2 / 1000.0) / 1e9) / peak,
+                     "tuning": [{k: e[k] for k in ("inter_path", "lf_tile_h", "half_width")} for e in tuned2]}
+            del wl2
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
@@ -650,6 +675,7 @@ def main():
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "parity": parity,
+            "value_mixed_content": mixed,
             "single_stream": single,
             "serving": serving,
             "batched_vs_single": (value / single["value"]) if single else None,
