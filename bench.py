@@ -316,13 +316,14 @@ class ClockSampler:
 
 # ── legs ─────────────────────────────────────────────────────────────────────
 
-def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False, record=None):
+def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False, record=None,
+                pack=0):
     """K timed steps of all streams; returns (ms, per-step stats list, latencies).
     The engine's tuner first settles this shape's kernel configuration on
     untimed steps (a few per candidate); `tuned` receives its choice."""
     import torch
     from compute_vp9_b200.batch import DEVICE_INPUTS, NO_OUTPUT, Batch
-    eng = Batch(arith=arith, use_graphs=1 if graphs else 0, autotune=1)
+    eng = Batch(arith=arith, use_graphs=1 if graphs else 0, autotune=1, pack=pack)
     sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
     assert all(s is not None for s in sids), "admission refused"
     flags = (DEVICE_INPUTS | NO_OUTPUT) if device_inputs else 0
@@ -561,6 +562,12 @@ def main():
     ms_e2e = allreduce_max(ws, ms_e2e)
     e2e = ws * px_step * args.steps / (ms_e2e / 1000.0) / 1e6
 
+    # the same without host-side coefficient packing (dense arrays over PCIe)
+    ms_np, st_np, _, _ = run_batched(wl, args.steps, args.warmup, arith, False,
+                                     not args.no_graphs, ws, pack=-1)
+    ms_np = allreduce_max(ws, ms_np)
+    e2e_np = ws * px_step * args.steps / (ms_np / 1000.0) / 1e6
+
     # the same, coefficients as (index, value) lists (cvp9_batch_submit_sparse)
     wl.build_sparse()
     ms_sp, st_sp, _, _ = run_batched(wl, args.steps, args.warmup, arith, False,
@@ -650,7 +657,15 @@ def main():
             "config": workload_config(args),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(st_e2e.h2d_bytes),
                     "d2h_bytes_per_step": int(st_e2e.d2h_bytes),
-                    "ms_per_step": ms_e2e / args.steps},
+                    "ms_per_step": ms_e2e / args.steps,
+                    "packed_frames_per_step": int(st_e2e.packed_frames),
+                    "host_pack_ms_per_step": float(st_e2e.submit_pack_ms),
+                    "what": "cvp9_batch_submit from page-locked host arrays in the parser's dense layout; "
+                            "the engine packs coefficients on host threads inside the timed region"},
+            "e2e_without_packing": {"value": e2e_np, "unit": UNIT,
+                                    "h2d_bytes_per_step": int(st_np.h2d_bytes),
+                                    "d2h_bytes_per_step": int(st_np.d2h_bytes),
+                                    "ms_per_step": ms_np / args.steps},
             "e2e_sparse_input": {"value": e2e_sp, "unit": UNIT,
                                  "h2d_bytes_per_step": int(st_sp.h2d_bytes),
                                  "d2h_bytes_per_step": int(st_sp.d2h_bytes),
@@ -660,7 +675,7 @@ def main():
                                          "timing, as a parser emitting them would); outputs identical"},
             "latency_ms": {"p50": statistics.median(lat) if lat else None,
                            "p99": (sorted(lat)[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None),
-                           "what": "host clock, submit to frame in pinned host memory, e2e steps (2 in flight)"},
+                           "what": "host clock, submit to frame in pinned host memory, e2e steps (3 in flight)"},
             "roofline": {"bound": "hbm", "kernel": "recon phase (k_inter, k_compact, k_recon)",
                          "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

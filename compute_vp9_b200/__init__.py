@@ -33,7 +33,8 @@ EXPORTED_SYMBOLS = [
     "cvp9_batch_wait", "cvp9_batch_poll", "cvp9_batch_get_frame", "cvp9_batch_stats",
     "cvp9_batch_last_error", "cvp9_batch_timer_start", "cvp9_batch_timer_stop",
     "cvp9_batch_last_seq", "cvp9_batch_step_latency", "cvp9_batch_tune_count",
-    "cvp9_batch_tune_entry", "cvp9_batch_submit_sparse",
+    "cvp9_batch_tune_entry", "cvp9_batch_submit_sparse", "cvp9_pack_bound_words",
+    "cvp9_pack_coeffs",
 ]
 
 

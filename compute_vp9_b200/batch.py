@@ -11,7 +11,8 @@ NO_OUTPUT = 2
 
 class BatchConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("arith", C.c_int), ("hbm_budget", C.c_uint64),
-                ("max_streams", C.c_int), ("use_graphs", C.c_int), ("autotune", C.c_int)]
+                ("max_streams", C.c_int), ("use_graphs", C.c_int), ("autotune", C.c_int),
+                ("pack", C.c_int)]
 
 
 class CoeffList(C.Structure):
@@ -30,7 +31,9 @@ class BatchStats(C.Structure):
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
                 ("reserved_bytes", C.c_uint64), ("open_streams", C.c_int),
                 ("graph_replays", C.c_int), ("kernel_launches", C.c_uint32),
-                ("scan_ms", C.c_float), ("recon_ms", C.c_float), ("filter_ms", C.c_float)]
+                ("scan_ms", C.c_float), ("recon_ms", C.c_float), ("filter_ms", C.c_float),
+                ("packed_frames", C.c_uint32), ("submit_pack_ms", C.c_float),
+                ("submit_wait_ms", C.c_float)]
 
 
 def _bind(lib):
@@ -61,6 +64,23 @@ def _bind(lib):
     lib.cvp9_batch_last_seq.argtypes = [vp]
     lib.cvp9_batch_last_seq.restype = C.c_uint64
     lib.cvp9_batch_step_latency.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double)]
+    lib.cvp9_pack_bound_words.argtypes = [C.c_uint32]
+    lib.cvp9_pack_bound_words.restype = C.c_size_t
+    lib.cvp9_pack_coeffs.argtypes = [C.c_int, C.POINTER(ParsedFrame), vp, C.c_size_t]
+    lib.cvp9_pack_coeffs.restype = C.c_int64
+
+
+def pack_coeffs(pf, arith=0):
+    """The engine's host-side packing of one parsed frame's coefficients
+    (cvp9_pack_coeffs) as a numpy uint32 array, or None when the frame is
+    not packable. pf: a ParsedFrame pointer."""
+    import numpy as np
+    from . import cuda_lib
+    lib = cuda_lib()
+    cap = int(lib.cvp9_pack_bound_words(pf.contents.num_coeffs))
+    out = np.zeros(cap, dtype=np.uint32)
+    w = lib.cvp9_pack_coeffs(arith, pf, out.ctypes.data, cap)
+    return None if w < 0 else out[:w].copy()
 
 
 class BatchError(RuntimeError):
@@ -74,11 +94,11 @@ class Batch:
     None when the budget is full); step() reconstructs one frame per listed
     stream in one launch chain."""
 
-    def __init__(self, device=-1, arith=-1, hbm_budget=0, max_streams=0, use_graphs=1, autotune=1):
+    def __init__(self, device=-1, arith=-1, hbm_budget=0, max_streams=0, use_graphs=1, autotune=1, pack=0):
         from . import cuda_lib
         self._lib = cuda_lib()
         self._h = C.c_void_p()
-        cfg = BatchConfig(device, arith, hbm_budget, max_streams, use_graphs, autotune)
+        cfg = BatchConfig(device, arith, hbm_budget, max_streams, use_graphs, autotune, pack)
         rc = self._lib.cvp9_batch_create(C.byref(cfg), C.byref(self._h))
         if rc != CVP9_OK:
             raise BatchError(rc, "cvp9_batch_create")

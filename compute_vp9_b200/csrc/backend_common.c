@@ -9,6 +9,7 @@
 
 #include <math.h>
 #include <pthread.h>
+#include <unistd.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -90,6 +91,14 @@ int cvp9_env_gather(void)
 {
     const char *e = getenv("CVP9_GATHER");
     return !(e && *e == '0');
+}
+
+int cvp9_env_pack(int configured)
+{
+    const char *e = getenv("CVP9_PACK");
+    if (e && *e == '0') return -1;
+    if (e && *e == '1') return 1;
+    return configured < 0 ? -1 : configured > 0 ? 1 : 0;
 }
 
 int cvp9_env_autotune(void)
@@ -248,80 +257,110 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms)
     tune_advance(t, e);
 }
 
-/* ── Host copy pool ───────────────────────────────────────────────────── */
+/* ── Host worker pool ─────────────────────────────────────────────────── */
 
-#define COPY_MAX_THREADS 8
-
-typedef struct { char *dst; const char *src; size_t n; } copy_part_t;
+#define POOL_MAX_THREADS 16
 
 static struct {
     pthread_mutex_t mu;
     pthread_cond_t  work, done;
-    pthread_mutex_t busy;            /* one parallel copy at a time */
-    copy_part_t     part[COPY_MAX_THREADS];
-    int             nparts, next, pending;
+    pthread_mutex_t busy;            /* one parallel job at a time */
+    void          (*fn)(void *, int);
+    void           *ctx;
+    int             ntasks, next, pending;
     int             nthreads;        /* workers (the caller is one more) */
-} g_copy = { PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, PTHREAD_COND_INITIALIZER,
-             PTHREAD_MUTEX_INITIALIZER, { { 0, 0, 0 } }, 0, 0, 0, -1 };
-static pthread_once_t g_copy_once = PTHREAD_ONCE_INIT;
+} g_pool = { PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, PTHREAD_COND_INITIALIZER,
+             PTHREAD_MUTEX_INITIALIZER, NULL, NULL, 0, 0, 0, -1 };
+static pthread_once_t g_pool_once = PTHREAD_ONCE_INIT;
 
-static void *copy_worker(void *arg)
+/* takes tasks until none is left; called with g_pool.mu held */
+static void pool_drain(void)
+{
+    while (g_pool.next < g_pool.ntasks) {
+        int k = g_pool.next++;
+        void (*fn)(void *, int) = g_pool.fn;
+        void *ctx = g_pool.ctx;
+        pthread_mutex_unlock(&g_pool.mu);
+        fn(ctx, k);
+        pthread_mutex_lock(&g_pool.mu);
+        if (--g_pool.pending == 0) pthread_cond_broadcast(&g_pool.done);
+    }
+}
+
+static void *pool_worker(void *arg)
 {
     (void)arg;
-    pthread_mutex_lock(&g_copy.mu);
+    pthread_mutex_lock(&g_pool.mu);
     for (;;) {
-        while (g_copy.next >= g_copy.nparts) pthread_cond_wait(&g_copy.work, &g_copy.mu);
-        copy_part_t p = g_copy.part[g_copy.next++];
-        pthread_mutex_unlock(&g_copy.mu);
-        memcpy(p.dst, p.src, p.n);
-        pthread_mutex_lock(&g_copy.mu);
-        if (--g_copy.pending == 0) pthread_cond_signal(&g_copy.done);
+        while (g_pool.next >= g_pool.ntasks) pthread_cond_wait(&g_pool.work, &g_pool.mu);
+        pool_drain();
     }
     return NULL;
 }
 
-static void copy_pool_start(void)
+static void pool_start(void)
 {
-    int want = 3;                                    /* 3 workers + the caller */
+    long cpus = sysconf(_SC_NPROCESSORS_ONLN);
+    int want = cpus > 1 ? (int)(cpus < POOL_MAX_THREADS ? cpus : POOL_MAX_THREADS) - 1 : 0;  /* + the caller */
     const char *e = getenv("CVP9_COPY_THREADS");
     if (e && *e) want = atoi(e) - 1;
-    if (want > COPY_MAX_THREADS - 1) want = COPY_MAX_THREADS - 1;
+    if (want > POOL_MAX_THREADS - 1) want = POOL_MAX_THREADS - 1;
     int started = 0;
     for (int i = 0; i < want; i++) {
         pthread_t t;
         pthread_attr_t at;
         pthread_attr_init(&at);
         pthread_attr_setdetachstate(&at, PTHREAD_CREATE_DETACHED);
-        if (pthread_create(&t, &at, copy_worker, NULL) == 0) started++;
+        if (pthread_create(&t, &at, pool_worker, NULL) == 0) started++;
         pthread_attr_destroy(&at);
     }
-    g_copy.nthreads = started;
+    g_pool.nthreads = started;
+}
+
+int cvp9_pool_threads(void)
+{
+    pthread_once(&g_pool_once, pool_start);
+    return g_pool.nthreads + 1;
+}
+
+void cvp9_parallel_for(int ntasks, void (*fn)(void *ctx, int task), void *ctx)
+{
+    if (ntasks <= 0) return;
+    pthread_once(&g_pool_once, pool_start);
+    if (ntasks == 1 || g_pool.nthreads <= 0 || pthread_mutex_trylock(&g_pool.busy) != 0) {
+        for (int k = 0; k < ntasks; k++) fn(ctx, k);
+        return;
+    }
+    pthread_mutex_lock(&g_pool.mu);
+    g_pool.fn = fn;
+    g_pool.ctx = ctx;
+    g_pool.ntasks = ntasks;
+    g_pool.next = 0;
+    g_pool.pending = ntasks;
+    /* wake only as many workers as there are tasks besides the caller's */
+    for (int k = 1; k < ntasks && k <= g_pool.nthreads; k++) pthread_cond_signal(&g_pool.work);
+    pool_drain();                                    /* the caller works too */
+    while (g_pool.pending > 0) pthread_cond_wait(&g_pool.done, &g_pool.mu);
+    g_pool.ntasks = 0;
+    g_pool.next = 0;
+    pthread_mutex_unlock(&g_pool.mu);
+    pthread_mutex_unlock(&g_pool.busy);
+}
+
+typedef struct { char *dst; const char *src; size_t n, chunk; } copy_job_t;
+
+static void copy_task(void *ctx, int k)
+{
+    const copy_job_t *j = (const copy_job_t *)ctx;
+    size_t off = (size_t)k * j->chunk;
+    if (off < j->n) memcpy(j->dst + off, j->src + off, off + j->chunk <= j->n ? j->chunk : j->n - off);
 }
 
 void cvp9_parallel_memcpy(void *dst, const void *src, size_t n)
 {
     if (n < (1u << 20)) { memcpy(dst, src, n); return; }
-    pthread_once(&g_copy_once, copy_pool_start);
-    if (g_copy.nthreads <= 0 || pthread_mutex_trylock(&g_copy.busy) != 0) { memcpy(dst, src, n); return; }
-    const int parts = g_copy.nthreads + 1;
-    size_t chunk = (n / parts + 4095) & ~(size_t)4095;
-    pthread_mutex_lock(&g_copy.mu);
-    int k = 0;
-    for (size_t off = chunk; off < n && k < parts - 1; off += chunk, k++) {
-        g_copy.part[k].dst = (char *)dst + off;
-        g_copy.part[k].src = (const char *)src + off;
-        g_copy.part[k].n = off + chunk <= n ? chunk : n - off;
-    }
-    g_copy.nparts = k;
-    g_copy.next = 0;
-    g_copy.pending = k;
-    pthread_cond_broadcast(&g_copy.work);
-    pthread_mutex_unlock(&g_copy.mu);
-    memcpy(dst, src, chunk < n ? chunk : n);          /* the caller's share */
-    pthread_mutex_lock(&g_copy.mu);
-    while (g_copy.pending > 0) pthread_cond_wait(&g_copy.done, &g_copy.mu);
-    g_copy.nparts = 0;
-    g_copy.next = 0;
-    pthread_mutex_unlock(&g_copy.mu);
-    pthread_mutex_unlock(&g_copy.busy);
+    /* four threads already move more than the PCIe link takes */
+    const int parts = cvp9_pool_threads() < 4 ? cvp9_pool_threads() : 4;
+    copy_job_t j = { (char *)dst, (const char *)src, n, (n / parts + 4095) & ~(size_t)4095 };
+    cvp9_parallel_for((int)((n + j.chunk - 1) / j.chunk), copy_task, &j);
 }

@@ -43,6 +43,9 @@ int cvp9_env_arith(void);
 int cvp9_env_inter_fast(void);
 int cvp9_env_autotune(void);        /* $CVP9_AUTOTUNE: 0 turns tuning off */
 int cvp9_env_gather(void);          /* $CVP9_GATHER: 0 uploads whole coefficient arrays */
+/* coefficient packing: -1 never, 0 large steps, 1 always ($CVP9_PACK=0|1
+ * overrides the configured value) */
+int cvp9_env_pack(int configured);
 
 /* Fill the frame-geometry and parameter fields of a job from a parsed
  * frame (inputs, output, refs and scratch pointers are set by the caller). */
@@ -104,8 +107,14 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms);
  * each rounded up to a power of two, so serving steps share buckets. */
 uint64_t cvp9_tune_key(int arith, int frames, uint64_t superblocks);
 
-/* memcpy split across a small pool of host threads (the caller copies one
- * share); plain memcpy below 1 MB, when another copy holds the pool, or
- * with $CVP9_COPY_THREADS=1. The per-stream backend stages the parser's
- * arrays with it: one thread moves ~12 GB/s, slower than the PCIe link. */
+/* A pool of host worker threads (one per online CPU up to 16, the caller
+ * included; $CVP9_COPY_THREADS overrides). cvp9_parallel_for runs fn(ctx, k) for k in
+ * [0, ntasks), the caller taking tasks too, and returns when all are done;
+ * one job holds the pool at a time (a second caller runs its tasks alone). */
+int  cvp9_pool_threads(void);
+void cvp9_parallel_for(int ntasks, void (*fn)(void *ctx, int task), void *ctx);
+
+/* memcpy split across the pool; plain memcpy below 1 MB. The per-stream
+ * backend stages the parser's arrays with it: one thread moves ~12 GB/s,
+ * slower than the PCIe link. */
 void cvp9_parallel_memcpy(void *dst, const void *src, size_t n);

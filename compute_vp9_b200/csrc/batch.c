@@ -28,11 +28,13 @@
 #include <string.h>
 #include <time.h>
 
-#define BSLOTS 2
+#define BSLOTS 3
 #define MAXF 12
 #define WAIT_LIMIT_S 60.0
 #define ALIGN_UP(x, a) (((x) + (a) - 1) / (a) * (a))
 #define LAT_RING 4096
+#define PACK_AUTO_BYTES (64ull << 20)   /* dense coefficient bytes from which a step packs */
+#define PACK_WAIT_MS    0.05            /* a submit that waited this long for its slot */
 
 typedef struct {
     uint8_t *dev;
@@ -65,6 +67,16 @@ typedef struct {
 struct cvp9_batch;
 typedef struct { struct cvp9_batch *b; uint64_t seq; } lat_arg_t;
 
+/* A frame's host inputs in the step's device buffer: arrays k = blocks,
+ * dense coefficients, list positions, list values, packed coefficients. */
+enum { IN_BLOCKS, IN_COEFFS, IN_POS, IN_VAL, IN_PACKED, IN_N };
+typedef struct {
+    size_t      at[IN_N];  /* byte offsets in d_in */
+    const void *gsrc;      /* REFCPU gather source: device view of page-locked coefficients */
+    unsigned    staged;    /* bit k: array k goes through the pinned staging buffer */
+} bfin_t;
+typedef struct { const void *src; size_t off, n; } bdirect_t;
+
 typedef struct {
     uint64_t        seq;
     int             busy;
@@ -73,10 +85,16 @@ typedef struct {
     cudaEvent_t     ev_cb;       /* after the completion callback: slot reuse waits on it */
     cudaEvent_t     ev_kern[4];
     uint8_t        *h_in;   size_t h_in_cap;
+    uint32_t       *h_pack; size_t h_pack_cap;     /* packed coefficients (pinned) */
+    bfin_t         *fin; bdirect_t *direct;        /* per frame / per array of the step */
+    int64_t        *pk_words; size_t *pk_off;     /* packed words (-1: not packed), offset in h_pack */
+    int             fin_cap;
+    uint32_t        packed;                     /* frames uploaded packed */
     uint8_t        *d_in;   size_t d_in_cap;
     cvp9_job_t     *h_jobs; cvp9_job_t *d_jobs; int jobs_cap;
     uint32_t       *d_sb_range; size_t sb_cap;      /* uint32 entries */
-    uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status, [n+1] gathered bytes */
+    uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status, [n+1] gathered
+                                                     * bytes, [n+2] malformed packed frames */
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
     uint32_t       *h_tickets; size_t h_tickets_cap;
     uint32_t       *d_fast; size_t fast_cap;    /* inter fast path: flags, tickets, count */
@@ -94,6 +112,8 @@ typedef struct {
 struct cvp9_batch {
     int          device, arith, use_graphs, max_streams;
     int          gather;     /* REFCPU: luma-only coefficient upload by kernel */
+    int          pack;       /* host coefficient packing: -1 never, 0 large steps, 1 always */
+    int          pack_q;     /* large steps: frames packed, in 16ths of the step (0..16) */
     cvp9_tuner_t tuner;      /* kernel configuration per shape bucket */
     uint64_t     budget, reserved;
     cudaStream_t cs, hs, ds;
@@ -109,6 +129,7 @@ struct cvp9_batch {
     double       lat_submit[LAT_RING];
     volatile double lat_done[LAT_RING];
     uint64_t     lat_seq[LAT_RING];
+    float        submit_pack_ms, submit_wait_ms;   /* the last submit's host time */
     cvp9_batch_stats_t last;
     arena_t      dev;        /* device buffers: frames, flags, step inputs      */
     arena_t      pin;        /* pinned host buffers: downloads, job tables      */
@@ -131,11 +152,12 @@ static size_t frame_bytes(int32_t w, int32_t h)
 uint64_t cvp9_batch_stream_bytes(uint32_t w, uint32_t h)
 {
     /* reference frames (LAST, GOLDEN, ALTREF, a stale key frame), the frame
-     * being written, one whose download is in flight; SB flags; per-step
-     * inputs at the dense coefficient size (2 bytes per sample) x 2 slots */
+     * being written, two whose downloads are in flight; SB flags; per-step
+     * inputs x BSLOTS: the dense coefficient array (2 bytes per sample), its
+     * packed form (at most as large) and the blocks */
     uint64_t fb = frame_bytes((int32_t)w, (int32_t)h);
     uint64_t nsb = (uint64_t)((w + 63) / 64) * ((h + 63) / 64);
-    return 6 * fb + nsb * 20 + 2 * (2 * fb + (uint64_t)((w + 7) / 8) * ((h + 7) / 8) * 32);
+    return 7 * fb + nsb * 20 + BSLOTS * (4 * fb + (uint64_t)((w + 7) / 8) * ((h + 7) / 8) * 32);
 }
 
 cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
@@ -152,6 +174,8 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
     b->use_graphs = cfg ? cfg->use_graphs : 1;
     b->gather = b->arith == CVP9_ARITH_REFCPU && cvp9_env_gather();
+    b->pack = cvp9_env_pack(cfg ? cfg->pack : 0);
+    b->pack_q = 16;
     {
         cvp9_tcfg_t fixed = { (int8_t)cvp9_env_inter_fast(), 0, 0 };
         cvp9_tuner_init(&b->tuner, b->arith, cfg && cfg->autotune && cvp9_env_autotune(), fixed);
@@ -231,6 +255,10 @@ void cvp9_batch_destroy(cvp9_batch_t *b)
         if (s->ev_cb) cudaEventDestroy(s->ev_cb);
         for (int k = 0; k < 4; k++) if (s->ev_kern[k]) cudaEventDestroy(s->ev_kern[k]);
         free(s->sids);
+        free(s->fin);
+        free(s->direct);
+        free(s->pk_words);
+        free(s->pk_off);
     }
     /* every stream and slot buffer lives in the arenas; the streams were
      * synchronised above */
@@ -376,16 +404,23 @@ static cvp9_err_t grow_host(cvp9_batch_t *b, void **p, size_t *cap, size_t need)
 static int acquire_frame(cvp9_batch_t *b, bstream_t *s)
 {
     size_t need = frame_bytes(s->W, s->H);
-    int pick = -1;
+    /* an allocated frame whose download is done, else one still being
+     * downloaded (the kernels then wait for that download), else a new one */
+    int pick = -1, busy = -1, fresh = -1;
     for (int i = 0; i < MAXF; i++) {
         if (s->f[i].users) continue;
-        if (s->f[i].dev && s->f[i].cap >= need) { pick = i; break; }
-        if (pick < 0) pick = i;
+        if (s->f[i].dev && s->f[i].cap >= need) {
+            if (s->f[i].d2h_seq <= b->done_seq) { pick = i; break; }
+            if (busy < 0) busy = i;
+        } else if (!s->f[i].dev && fresh < 0) {
+            fresh = i;
+        }
     }
+    if (pick < 0) pick = fresh >= 0 ? fresh : busy;
     if (pick < 0) return -1;
     bframe_t *f = &s->f[pick];
     if (f->d2h_seq > b->done_seq) {
-        /* only the previous step can still be downloading it */
+        /* a step still in flight downloads it */
         bslot_t *o = &b->slot[f->d2h_seq % BSLOTS];
         if (o->seq == f->d2h_seq) cudaStreamWaitEvent(b->cs, o->ev_end, 0);
     }
@@ -413,6 +448,15 @@ static uint64_t mix64(uint64_t h, uint64_t v)
     return h * 0xBF58476D1CE4E5B9ull;
 }
 
+/* Status word of job i of a completed slot; a malformed packed upload
+ * (bit i % 32 of the unpack error word) reads as a bad block. */
+static uint32_t slot_status(const bslot_t *s, int i)
+{
+    uint32_t st = s->h_misc[1 + i];
+    if (s->h_misc[s->n + 2] & (1u << (i & 31))) st |= CVP9_JOB_BAD_BLOCK;
+    return st;
+}
+
 static void complete_slot(cvp9_batch_t *b, bslot_t *s)
 {
     float t = 0.f, k = 0.f, u = 0.f;
@@ -425,6 +469,7 @@ static void complete_slot(cvp9_batch_t *b, bslot_t *s)
     b->last.h2d_bytes = s->h2d_bytes + s->h_misc[s->n + 1];
     b->last.d2h_bytes = s->d2h_bytes;
     b->last.kernel_launches = s->launches + s->launches_extra;
+    b->last.packed_frames = s->packed;
     float a = 0.f, r = 0.f, f = 0.f;
     cudaEventElapsedTime(&a, s->ev_kern[0], s->ev_kern[1]);
     cudaEventElapsedTime(&r, s->ev_kern[1], s->ev_kern[2]);
@@ -435,7 +480,7 @@ static void complete_slot(cvp9_batch_t *b, bslot_t *s)
     cvp9_tuner_report(&b->tuner, s->tune_idx, s->tune_cfg, k);
     for (int i = 0; i < s->n; i++) {
         bstream_t *st = &b->st[s->sids[i]];
-        if (st->open && st->last_seq == s->seq) st->last_status = s->h_misc[1 + i];
+        if (st->open && st->last_seq == s->seq) st->last_status = slot_status(s, i);
     }
     if (s->seq > b->done_seq) b->done_seq = s->seq;
     s->busy = 0;
@@ -473,6 +518,40 @@ static const void *mapped_ptr(const void *p)
     struct cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return NULL; }
     return a.type == cudaMemoryTypeHost ? a.devicePointer : NULL;
+}
+
+/* Per-frame bookkeeping of a slot for steps of up to n frames. */
+static cvp9_err_t slot_frames(bslot_t *s, int n)
+{
+    if (s->fin_cap >= n) return CVP9_OK;
+    free(s->fin);
+    free(s->direct);
+    free(s->pk_words);
+    free(s->pk_off);
+    s->fin = malloc((size_t)n * sizeof(bfin_t));
+    s->direct = malloc((size_t)n * IN_N * sizeof(bdirect_t));
+    s->pk_words = malloc((size_t)n * sizeof(int64_t));
+    s->pk_off = malloc((size_t)n * sizeof(size_t));
+    s->fin_cap = (s->fin && s->direct && s->pk_words && s->pk_off) ? n : 0;
+    return s->fin_cap ? CVP9_OK : CVP9_ERR_NOMEM;
+}
+
+/* Packing runs on the host pool, a task per frame. */
+typedef struct {
+    int                              arith;
+    const vp9_parsed_frame_t *const *pfs;
+    uint32_t                        *base;
+    const size_t                    *off;
+    int64_t                         *words;
+} pack_job_t;
+
+static void pack_task(void *ctx, int i)
+{
+    pack_job_t *j = (pack_job_t *)ctx;
+    const vp9_parsed_frame_t *pf = j->pfs[i];
+    j->words[i] = pf->num_coeffs ? cvp9_pack_coeffs(j->arith, pf, j->base + j->off[i],
+                                                    cvp9_pack_bound_words(pf->num_coeffs))
+                                 : -1;
 }
 
 static void CUDART_CB step_done_cb(void *p)
@@ -521,9 +600,14 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
 
     const uint64_t seq = b->seq + 1;
     bslot_t *s = &b->slot[seq % BSLOTS];
+    const double tw0 = cvp9_now();
+    const int pipelined = b->seq > b->done_seq;    /* an earlier step still in flight */
     cvp9_err_t err = wait_slot(b, s);
     if (err != CVP9_OK) return err;
     b->lat_submit[seq % LAT_RING] = cvp9_now();
+    const double waited_ms = (b->lat_submit[seq % LAT_RING] - tw0) * 1e3;
+    b->submit_wait_ms = (float)waited_ms;
+    b->submit_pack_ms = 0.f;
 
     /* sizes */
     size_t in_bytes = 0, n_sb = 0;
@@ -570,14 +654,73 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     s->tune_cfg = tc;
     int any_tile = 0, any_strip = 0;
 
-    /* per-slot buffers; pinned staging only when some array is pageable */
+    if ((err = slot_frames(s, n))) return err;
+
+    /* Large steps of dense host arrays: pack the coefficients on the host
+     * pool (the PCIe link, not the host, bounds such a step) */
+    int any_packed = 0;
+    uint32_t max_pages = 0;
+    s->packed = 0;
+    for (int i = 0; i < n; i++) s->pk_words[i] = -1;
+    if (!dev_in && !lists && b->pack >= 0) {
+        size_t cb = 0, tot = 0;
+        for (int i = 0; i < n; i++) cb += (size_t)pfs[i]->num_coeffs * 2;
+        int npack = 0;
+        if (b->pack == 1) {
+            npack = n;
+        } else if (cb >= PACK_AUTO_BYTES) {
+            /* Packing trades host time (reading every dense array) for link
+             * time. Balance the two while steps are pipelined: a submit that
+             * had to wait for its slot found the link (or the GPU) behind, so
+             * the host can pack more; one that did not wait found the host
+             * behind, so it packs less. A caller that waits for each step
+             * first gives no signal and leaves the share as it is. */
+            if (pipelined && waited_ms > PACK_WAIT_MS) { if (b->pack_q < 16) b->pack_q++; }
+            else if (pipelined && b->pack_q > 0) b->pack_q--;
+            npack = (b->pack_q * n + 8) / 16;
+        }
+        if (npack) {
+            for (int i = 0; i < npack; i++) {
+                s->pk_off[i] = tot;
+                if (pfs[i]->num_coeffs) tot += ALIGN_UP(cvp9_pack_bound_words(pfs[i]->num_coeffs), 64);
+            }
+            if (tot) {
+                if ((err = grow_host(b, (void **)&s->h_pack, &s->h_pack_cap, tot * 4))) return err;
+                pack_job_t pj = { b->arith, pfs, s->h_pack, s->pk_off, s->pk_words };
+                const double tp0 = cvp9_now();
+                cvp9_parallel_for(npack, pack_task, &pj);
+                b->submit_pack_ms = (float)((cvp9_now() - tp0) * 1e3);
+            }
+            for (int i = 0; i < n; i++) {
+                if (s->pk_words[i] < 0) continue;
+                any_packed = 1;
+                s->packed++;
+                in_bytes += ALIGN_UP((size_t)s->pk_words[i] * 4, 256);
+                uint32_t np = (uint32_t)(((uint64_t)pfs[i]->num_coeffs + 65535) >> 16);
+                if (np > max_pages) max_pages = np;
+            }
+        }
+    }
+
+    /* how each host array travels: the gather kernel (REFCPU coefficients in
+     * page-locked memory), direct DMA (page-locked), or the pinned staging
+     * buffer (pageable); coefficient regions the device fills get no copy */
+    int any_staged = 0;
+    for (int i = 0; i < n && !dev_in; i++) {
+        const vp9_parsed_frame_t *pf = pfs[i];
+        bfin_t *f = &s->fin[i];
+        const int packed = s->pk_words[i] >= 0;
+        f->gsrc = NULL;
+        f->staged = 0;
+        if (b->gather && !lists && !packed && pf->num_coeffs && pf->num_blocks) f->gsrc = mapped_ptr(pf->coeffs);
+        if (pf->num_blocks && !is_pinned(pf->blocks)) f->staged |= 1u << IN_BLOCKS;
+        if (!lists && !packed && !f->gsrc && pf->num_coeffs && !is_pinned(pf->coeffs)) f->staged |= 1u << IN_COEFFS;
+        if (lists && lists[i].n && !is_pinned(lists[i].pos)) f->staged |= 1u << IN_POS;
+        if (lists && lists[i].n && !is_pinned(lists[i].val)) f->staged |= 1u << IN_VAL;
+        any_staged |= f->staged != 0;
+    }
     if (!dev_in && in_bytes) {
-        int staged = 0;
-        for (int i = 0; i < n && !staged; i++)
-            staged = (pfs[i]->num_blocks && !is_pinned(pfs[i]->blocks)) ||
-                     (lists ? (lists[i].n && (!is_pinned(lists[i].pos) || !is_pinned(lists[i].val)))
-                            : (pfs[i]->num_coeffs && !is_pinned(pfs[i]->coeffs)));
-        if ((staged && (err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes))) ||
+        if ((any_staged && (err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes))) ||
             (err = grow_dev(b, (void **)&s->d_in, &s->d_in_cap, in_bytes)))
             return err;
     }
@@ -591,8 +734,8 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             return err;
         s->jobs_cap = cap;
     }
-    if (s->misc_cap < n + 2) {
-        int cap = (n > b->nst ? n : b->nst) + 2;
+    if (s->misc_cap < n + 3) {
+        int cap = (n > b->nst ? n : b->nst) + 3;
         s->misc_cap = 0;
         if ((err = grow_host(b, (void **)&s->h_misc, &s->h_misc_bytes, (size_t)cap * 4)) ||
             (err = grow_dev(b, (void **)&s->d_misc, &s->d_misc_bytes, (size_t)cap * 4)))
@@ -626,87 +769,61 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         s->tickets_key = key;
     }
 
-    /* inputs: bulk copy of everything staged, then direct DMA of pinned arrays */
+    /* inputs: the staged arrays first, side by side in h_in and up in one
+     * copy; then direct DMA of page-locked arrays (the caller's, and the
+     * packed frames); regions the device fills (gathered, scattered or
+     * unpacked coefficients) get space only */
     s->h2d_bytes = 0;
     BCK(cudaEventRecord(s->ev_start, b->hs), "event");
-    size_t off = 0;
-    const uint8_t *dev_blocks[256], *dev_coeffs[256];
-    const void *gather_local[256];
-    size_t sp_local[256];
-    const uint8_t **dbp = n <= 256 ? dev_blocks : malloc((size_t)n * sizeof(void *));
-    const uint8_t **dcp = n <= 256 ? dev_coeffs : malloc((size_t)n * sizeof(void *));
-    const void **gsrc = n <= 256 ? gather_local : malloc((size_t)n * sizeof(void *));
-    size_t *spo = n <= 256 ? sp_local : malloc((size_t)n * sizeof(size_t));   /* pos list offset in d_in */
-    if (!dbp || !dcp || !gsrc || !spo) return CVP9_ERR_NOMEM;
-    int any_gather = 0;
-    typedef struct { const void *src; size_t off, n; } direct_t;
-    direct_t direct_local[1024];
-    direct_t *direct = n <= 256 ? direct_local : malloc((size_t)4 * n * sizeof(direct_t));
-    if (!direct) return CVP9_ERR_NOMEM;
-    int ndirect = 0, any_staged = 0;
-    for (int i = 0; i < n; i++) {
-        const vp9_parsed_frame_t *pf = pfs[i];
-        gsrc[i] = NULL;
-        if (dev_in) {
-            dbp[i] = (const uint8_t *)pf->blocks;
-            dcp[i] = (const uint8_t *)pf->coeffs;
-            continue;
-        }
-        /* REFCPU reads only each block's luma coefficients: from page-locked
-         * memory a kernel moves just those (k_gather_luma), not the array */
-        if (b->gather && !lists && pf->num_coeffs && pf->num_blocks)
-            gsrc[i] = mapped_ptr(pf->coeffs);
-        any_gather |= gsrc[i] != NULL;
-        size_t nbb = (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t);
-        size_t ncb = (size_t)pf->num_coeffs * sizeof(int16_t);
-        /* blocks, dense coefficients, then (sparse input) positions, values;
-         * the dense region of a sparse frame is filled on the device */
-        const void *srcs[4] = { pf->blocks, pf->coeffs, lists ? lists[i].pos : NULL, lists ? lists[i].val : NULL };
-        size_t lens[4] = { nbb, ncb, lists ? (size_t)lists[i].n * 4 : 0, lists ? (size_t)lists[i].n * 2 : 0 };
-        const int narr = lists ? 4 : 2;
-        for (int k = 0; k < narr; k++) {
-            if (k == 2) spo[i] = off;
-            if (lens[k] && !(k == 1 && (gsrc[i] || lists))) {
-                if (is_pinned(srcs[k])) {
-                    direct[ndirect].src = srcs[k];
-                    direct[ndirect].off = off;
-                    direct[ndirect].n = lens[k];
-                    ndirect++;
-                } else {
-                    /* h_in was sized above because a pageable array exists */
-                    memcpy(s->h_in + off, srcs[k], lens[k]);
-                    any_staged = 1;
+    int any_gather = 0, ndirect = 0;
+    size_t off = 0, staged_end = 0;
+    for (int phase = 0; phase < 2 && !dev_in; phase++) {
+        for (int i = 0; i < n; i++) {
+            const vp9_parsed_frame_t *pf = pfs[i];
+            bfin_t *f = &s->fin[i];
+            const int packed = s->pk_words[i] >= 0;
+            const void *src[IN_N] = { pf->blocks, pf->coeffs, lists ? lists[i].pos : NULL,
+                                      lists ? lists[i].val : NULL, packed ? s->h_pack + s->pk_off[i] : NULL };
+            const size_t len[IN_N] = { (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t),
+                                       (size_t)pf->num_coeffs * sizeof(int16_t),
+                                       lists ? (size_t)lists[i].n * 4 : 0, lists ? (size_t)lists[i].n * 2 : 0,
+                                       packed ? (size_t)s->pk_words[i] * 4 : 0 };
+            const int copied[IN_N] = { 1, !(f->gsrc || lists || packed), 1, 1, 1 };
+            for (int k = 0; k < IN_N; k++) {
+                const int stg = (f->staged >> k) & 1;
+                if (stg != (phase == 0)) continue;
+                f->at[k] = off;
+                if (len[k] && copied[k]) {
+                    if (stg) {
+                        cvp9_parallel_memcpy(s->h_in + off, src[k], len[k]);
+                    } else {
+                        s->direct[ndirect].src = src[k];
+                        s->direct[ndirect].off = off;
+                        s->direct[ndirect].n = len[k];
+                        ndirect++;
+                    }
                 }
+                off += ALIGN_UP(len[k], 256);
             }
-            if (k < 2) (k == 0 ? dbp : dcp)[i] = s->d_in + off;
-            off += ALIGN_UP(lens[k], 256);
+            any_gather |= phase == 1 && f->gsrc != NULL;
         }
+        if (phase == 0) staged_end = off;
     }
     cudaError_t ue = cudaSuccess;
-    if (!dev_in && off) {
-        /* staged ranges go up in one copy; direct copies land afterwards */
-        if (any_staged) {
-            ue = cudaMemcpyAsync(s->d_in, s->h_in, off, cudaMemcpyHostToDevice, b->hs);
-            s->h2d_bytes += off;
-        }
-        for (int k = 0; k < ndirect && ue == cudaSuccess; k++) {
-            ue = cudaMemcpyAsync(s->d_in + direct[k].off, direct[k].src, direct[k].n,
-                                 cudaMemcpyHostToDevice, b->hs);
-            if (!any_staged) s->h2d_bytes += direct[k].n;
-        }
+    if (staged_end) {
+        ue = cudaMemcpyAsync(s->d_in, s->h_in, staged_end, cudaMemcpyHostToDevice, b->hs);
+        s->h2d_bytes += staged_end;
     }
-    if (direct != direct_local) free(direct);
+    for (int k = 0; k < ndirect && ue == cudaSuccess; k++) {
+        ue = cudaMemcpyAsync(s->d_in + s->direct[k].off, s->direct[k].src, s->direct[k].n,
+                             cudaMemcpyHostToDevice, b->hs);
+        s->h2d_bytes += s->direct[k].n;
+    }
     /* sparse frames: their dense coefficient regions start at zero */
     for (int i = 0; lists && i < n && ue == cudaSuccess; i++)
         if (pfs[i]->num_coeffs)
-            ue = cudaMemsetAsync((void *)dcp[i], 0, (size_t)pfs[i]->num_coeffs * 2, b->hs);
-    if (ue != cudaSuccess) {
-        if (dbp != dev_blocks) free(dbp);
-        if (dcp != dev_coeffs) free(dcp);
-        if (gsrc != gather_local) free(gsrc);
-        if (spo != sp_local) free(spo);
-        return bfail(b, ue, "upload inputs");
-    }
+            ue = cudaMemsetAsync(s->d_in + s->fin[i].at[IN_COEFFS], 0, (size_t)pfs[i]->num_coeffs * 2, b->hs);
+    if (ue != cudaSuccess) return bfail(b, ue, "upload inputs");
 
     /* jobs, outputs, reference pools */
     uint32_t sb_base = 0;
@@ -728,8 +845,9 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         if (job->lf_tiled && !tc.lf32 && !(st->W & 3)) job->lf_tiled = 2;   /* register strips */
         any_tile |= job->lf_tiled == 1;
         any_strip |= job->lf_tiled == 2;
-        job->blocks = (const vp9_macroblock_info_t *)dbp[i];
-        job->coeffs = (const int16_t *)dcp[i];
+        const bfin_t *f = &s->fin[i];
+        job->blocks = dev_in ? pf->blocks : (const vp9_macroblock_info_t *)(s->d_in + f->at[IN_BLOCKS]);
+        job->coeffs = dev_in ? pf->coeffs : (const int16_t *)(s->d_in + f->at[IN_COEFFS]);
         job->out = st->f[of].dev;
         job->nv12 = NULL;
         for (int r = 0; r < 8; r++) {
@@ -740,11 +858,15 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
                 job->ref[r].h = st->f[f].h;
             }
         }
-        job->coeffs_src = (const int16_t *)gsrc[i];
+        job->coeffs_src = dev_in ? NULL : (const int16_t *)f->gsrc;
         if (lists && lists[i].n) {
-            job->sp_pos = (const uint32_t *)(s->d_in + spo[i]);
-            job->sp_val = (const int16_t *)(s->d_in + spo[i] + ALIGN_UP((size_t)lists[i].n * 4, 256));
+            job->sp_pos = (const uint32_t *)(s->d_in + f->at[IN_POS]);
+            job->sp_val = (const int16_t *)(s->d_in + f->at[IN_VAL]);
             job->sp_n = lists[i].n;
+        }
+        if (!dev_in && s->pk_words[i] >= 0) {
+            job->packed = (const uint32_t *)(s->d_in + f->at[IN_PACKED]);
+            job->packed_words = (uint32_t)s->pk_words[i];
         }
         job->epoch = ++st->epoch;
         job->sb_range = s->d_sb_range + 4 * (size_t)sb_base;
@@ -753,16 +875,13 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         sb_base += (uint32_t)st->n_sb;
         s->sids[i] = sids[i];
     }
-    if (dbp != dev_blocks) free(dbp);
-    if (dcp != dev_coeffs) free(dcp);
-    if (gsrc != gather_local) free(gsrc);
-    if (spo != sp_local) free(spo);
     BCK(cudaMemcpyAsync(s->d_jobs, s->h_jobs, (size_t)n * sizeof(cvp9_job_t), cudaMemcpyHostToDevice, b->hs),
         "upload jobs");
     s->h2d_bytes += (size_t)n * sizeof(cvp9_job_t);
-    /* the counter of gathered bytes is cleared here, on the upload stream;
-     * the compute stream's clear of the status words stops before it */
-    BCK(cudaMemsetAsync(s->d_misc + n + 1, 0, 4, b->hs), "clear gather counter");
+    /* the counter of gathered bytes and the unpack error word are cleared
+     * here, on the upload stream; the compute stream's clear of the status
+     * words stops before them */
+    BCK(cudaMemsetAsync(s->d_misc + n + 1, 0, 8, b->hs), "clear upload words");
     s->launches_extra = 0;
     if (any_gather) {
         int grc = cvp9k_launch_gather(s->d_jobs, n, max_blocks, s->d_misc + n + 1, b->hs);
@@ -774,6 +893,11 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         for (int i = 0; i < n; i++) if (lists[i].n > max_n) max_n = lists[i].n;
         int src = cvp9k_launch_scatter(s->d_jobs, n, max_n, b->hs);
         if (src != 0) return bfail(b, (cudaError_t)src, "coefficient scatter");
+        s->launches_extra++;
+    }
+    if (any_packed) {
+        int urc = cvp9k_launch_unpack(s->d_jobs, n, max_pages, s->d_misc + n + 2, b->hs);
+        if (urc != 0) return bfail(b, (cudaError_t)urc, "coefficient unpack");
         s->launches_extra++;
     }
     BCK(cudaEventRecord(s->ev_h2d, b->hs), "event");
@@ -881,8 +1005,8 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         }
     }
     if (ofr != out_frame) free(ofr);
-    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 2) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
-    s->d2h_bytes += (size_t)(n + 1) * 4;
+    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 3) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
+    s->d2h_bytes += (size_t)(n + 3) * 4;
     /* ev_end, then the completion callback (so a stamped step is complete
      * for every other query), then ev_cb, which slot reuse waits on so the
      * callback's argument is never overwritten while pending */
@@ -911,7 +1035,7 @@ cvp9_err_t cvp9_batch_wait(cvp9_batch_t *b)
         cvp9_err_t e = wait_slot(b, s);
         if (e != CVP9_OK) return e;
         for (int i = 0; i < s->n && first == CVP9_OK; i++) {
-            uint32_t stt = s->h_misc[1 + i];
+            uint32_t stt = slot_status(s, i);
             if (stt & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) first = CVP9_ERR_INVALID_DATA;
             else if (stt & CVP9_JOB_TIMEOUT) first = CVP9_ERR_GPU;
         }
@@ -949,7 +1073,7 @@ cvp9_err_t cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *inf
             if (e == cudaErrorNotReady) return CVP9_ERR_AGAIN;
             if (e != cudaSuccess) return bfail(b, e, "step completion");
             for (int i = 0; i < s->n; i++)
-                if (s->sids[i] == sid) st->last_status = s->h_misc[1 + i];
+                if (s->sids[i] == sid) st->last_status = slot_status(s, i);
             if (cudaEventQuery(s->ev_cb) == cudaSuccess) complete_slot(b, s);
         }
     }
@@ -977,6 +1101,8 @@ cvp9_err_t cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *out)
     for (int i = 0; i < b->nst; i++) open += b->st[i].open;
     out->open_streams = open;
     out->graph_replays = b->graph_replays;
+    out->submit_pack_ms = b->submit_pack_ms;
+    out->submit_wait_ms = b->submit_wait_ms;
     return CVP9_OK;
 }
 

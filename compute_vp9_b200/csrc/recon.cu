@@ -2884,6 +2884,55 @@ __global__ void __launch_bounds__(256) k_scatter_coeffs(const cvp9_job_t *__rest
     }
 }
 
+/* Packed coefficient upload (format of cvp9_pack_coeffs): a CTA per (page,
+ * frame) rebuilds 65536 coefficients of the dense array — a dense page is
+ * copied, an entry page is zero-filled and then scattered. A malformed
+ * page (data past the buffer, counts out of range) is left alone and sets
+ * bit (job index) % 32 of *err, which the host reads with the step. */
+__global__ void __launch_bounds__(256) k_unpack_coeffs(const cvp9_job_t *__restrict__ jobs, uint32_t *err)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    const uint32_t *pk = job.packed;
+    if (!pk) return;
+    const uint32_t nw = job.packed_words, np = nw ? pk[0] : 0u;
+    if (1u + 2u * (uint64_t)np > nw) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(err, 1u << (blockIdx.y & 31));
+        return;
+    }
+    for (uint32_t p = blockIdx.x; p < np; p += gridDim.x) {
+        const uint32_t base = p << 16;
+        if (p >= 65536u || base >= job.num_coeffs) break;
+        const uint32_t st = pk[1 + 2 * p], cnt = pk[2 + 2 * p];
+        const uint32_t s0 = st & 0x7fffffffu;
+        const uint32_t len = min(65536u, job.num_coeffs - base);
+        const bool dense = st >> 31;
+        const uint64_t words = dense ? ((uint64_t)len + 1) / 2 : cnt;
+        if ((s0 & 3u) || (dense && cnt != len) || (!dense && cnt > (len + 1) / 2) || s0 + words > nw) {
+            if (threadIdx.x == 0) atomicOr(err, 1u << (blockIdx.y & 31));
+            continue;
+        }
+        int16_t *dst = const_cast<int16_t *>(job.coeffs) + base;     /* 16-byte aligned */
+        const uint32_t *src = pk + s0;                               /* 16-byte aligned */
+        uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+        const uint32_t nv = len >> 3;
+        if (dense) {
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+            for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) d4[v] = __ldg(s4 + v);
+            const int16_t *s16 = reinterpret_cast<const int16_t *>(src);
+            for (uint32_t k = nv * 8 + threadIdx.x; k < len; k += blockDim.x) dst[k] = s16[k];
+        } else {
+            for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) d4[v] = make_uint4(0u, 0u, 0u, 0u);
+            for (uint32_t k = nv * 8 + threadIdx.x; k < len; k += blockDim.x) dst[k] = 0;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
+                const uint32_t e = __ldg(src + k), o = e & 0xffffu;
+                if (o < len) dst[o] = (int16_t)(e >> 16);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 /* ── C-ABI launch shims ─────────────────────────────────────────────────── */
 
 extern "C" {
@@ -2896,6 +2945,14 @@ int cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, cuda
     unsigned gx = (max_n + 255u) / 256u;
     if (gx > 4096u) gx = 4096u;
     k_scatter_coeffs<<<dim3(gx, (unsigned)njobs), 256, 0, st>>>(jobs);
+    return (int)cudaGetLastError();
+}
+
+int cvp9k_launch_unpack(const cvp9_job_t *jobs, int njobs, uint32_t max_pages, uint32_t *err, cudaStream_t st)
+{
+    if (njobs <= 0 || max_pages == 0) return 0;
+    const unsigned gx = max_pages < 65535u ? max_pages : 65535u;
+    k_unpack_coeffs<<<dim3(gx, (unsigned)njobs), 256, 0, st>>>(jobs, err);
     return (int)cudaGetLastError();
 }
 

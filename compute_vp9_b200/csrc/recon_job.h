@@ -58,6 +58,9 @@ typedef struct {
     const uint32_t *sp_pos;         /* sparse upload: indices into coeffs (device)  */
     const int16_t  *sp_val;         /* and their values; coeffs zeroed beforehand   */
     uint32_t        sp_n;           /* k_scatter_coeffs writes them; 0: none        */
+    uint32_t        packed_words;   /* packed upload (cvp9_pack_coeffs): its words  */
+    const uint32_t *packed;         /* (device), expanded into coeffs by
+                                     * k_unpack_coeffs; NULL: none                  */
 } cvp9_job_t;
 
 #ifdef __cplusplus

@@ -57,6 +57,13 @@ int    cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, ui
  * every job with sp_n > 0 (indices past num_coeffs are ignored). */
 int    cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, cudaStream_t stream);
 
+/* Packed coefficient upload: every job with `packed` set gets its dense
+ * coeffs array rebuilt from the pages (entry pages zero-filled, then
+ * scattered; dense pages copied). max_pages: most pages of any job; a
+ * malformed page of job j sets bit j % 32 of *err (device word). */
+int    cvp9k_launch_unpack(const cvp9_job_t *jobs, int njobs, uint32_t max_pages, uint32_t *err,
+                           cudaStream_t stream);
+
 /* Enqueue the chain on `stream`; returns the cudaError_t of the first
  * failing call (0 on success). */
 int    cvp9k_launch_frame(const cvp9k_launch_t *launch, cudaStream_t stream);

@@ -8,7 +8,7 @@ Streams arrive as a Poisson process; each carries `frames` frames paced at
 admitted as soon as a finished stream frees its reservation. Every loop
 iteration gathers the frames that are due from all admitted streams — new
 arrivals join the very next step — and reconstructs them in one engine step;
-up to two steps are in flight, so frames that become due while the GPU works
+up to three steps are in flight, so frames that become due while the GPU works
 go into the next step. Latency of a frame = time its reconstructed planes
 reach host memory minus the time it became due. `speed` compresses the
 arrival and pacing schedule (20 = twenty times faster than real time) so a

@@ -44,6 +44,12 @@ typedef struct {
     int      autotune;       /* choose the kernel configuration per shape bucket
                               * by timing its first steps ($CVP9_AUTOTUNE=0
                               * overrides); 0: fixed defaults                    */
+    int      pack;           /* pack dense host coefficient arrays before the
+                              * upload (cvp9_pack_coeffs). 0: steps that move at
+                              * least 64 MB of them pack a share of their frames,
+                              * raised while submits wait for the link and
+                              * lowered while they do not; 1 always; -1 never
+                              * ($CVP9_PACK=0|1 overrides)                       */
 } cvp9_batch_config_t;
 
 /* The tuner's record of one shape bucket (a step's arithmetic, frame count
@@ -79,6 +85,9 @@ typedef struct {
     float    scan_ms;        /* per-kernel device times of that step             */
     float    recon_ms;
     float    filter_ms;
+    uint32_t packed_frames;  /* frames of that step uploaded packed              */
+    float    submit_pack_ms; /* host time the last submit spent packing          */
+    float    submit_wait_ms; /* and waiting for a free step slot                 */
 } cvp9_batch_stats_t;
 
 cvp9_err_t  cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out);
@@ -93,7 +102,7 @@ int         cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t width, uint32_t hei
 cvp9_err_t  cvp9_batch_close_stream(cvp9_batch_t *b, int sid);
 
 /* Enqueue one step: frame pfs[i] for stream sids[i] (each stream at most
- * once). Returns once inputs are staged; up to two steps are in flight. */
+ * once). Returns once inputs are staged; up to three steps are in flight. */
 cvp9_err_t  cvp9_batch_submit(cvp9_batch_t *b, int n, const int *sids,
                               const vp9_parsed_frame_t *const *pfs, const int64_t *pts,
                               uint32_t flags);
@@ -121,6 +130,31 @@ cvp9_err_t  cvp9_batch_submit_sparse(cvp9_batch_t *b, int n, const int *sids,
                                      const vp9_parsed_frame_t *const *pfs,
                                      const cvp9_coeff_list_t *lists, const int64_t *pts,
                                      uint32_t flags);
+
+/* Coefficient packing. Dense coefficient arrays are mostly zeros, and a
+ * large step's upload is bound by the PCIe link, so the engine packs the
+ * coefficients the reconstruction reads on its host worker threads, uploads
+ * the packed frames and rebuilds the dense arrays on the device. Exposed so
+ * that the format can be checked on its own.
+ *
+ * A packed frame is 32-bit words: [0] P, the number of 65536-coefficient
+ * pages (ceil(num_coeffs / 65536)); for page p, [1 + 2p] the first word of
+ * its data (a multiple of 4; bit 31 set: dense page) and [2 + 2p] its count.
+ * An entry page holds `count` words (offset in the page) | (value << 16) and
+ * is zero everywhere else; a dense page holds its `count` coefficients as
+ * int16, two per word. A page becomes dense when its entries would outgrow
+ * the dense form. Coefficients read: SPEC every one; REFCPU each non-skip
+ * block's luma TXs, [coeff_offset, + (cw/n)(ch/n) n^2) with the block
+ * clipped to the frame (cw x ch) and n the TX size; the others come out as
+ * zeros.
+ *
+ * cvp9_pack_bound_words: words that packing a frame may need.
+ * cvp9_pack_coeffs: packs pf's coefficients into out, returns the words
+ * used; -1 when cap_words is short, the arrays are missing, or (REFCPU) the
+ * blocks' spans are not in ascending order (the engine then uploads that
+ * frame's coefficients as it would without packing). */
+size_t      cvp9_pack_bound_words(uint32_t num_coeffs);
+int64_t     cvp9_pack_coeffs(int arith, const vp9_parsed_frame_t *pf, uint32_t *out, size_t cap_words);
 
 /* Block (bounded) until every submitted step is complete. Returns the first
  * per-stream error of those steps (CVP9_ERR_INVALID_DATA for a rejected

@@ -208,3 +208,30 @@ def test_sparse_coefficients_match_oracle(profile, pinned):
             assert rc == CVP9_OK
             assert np.array_equal(arr, orcs[i].decode(pfs[i])), "stream %d frame %d" % (i, f)
     eng.close()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_packed_coefficients_match_oracle(profile, pinned):
+    """Dense coefficient arrays packed on the host (cvp9_pack_coeffs) and
+    rebuilt on the device (k_unpack_coeffs) decode to the oracle's bytes,
+    from page-locked and from pageable memory, and move fewer bytes."""
+    eng = Batch(arith=profile, pack=1)
+    syns = [Synth(synth_config(p, w, h, seed=70 + i, **ov)) for i, (p, w, h, ov) in enumerate(MIX)]
+    orcs = [OracleStream(profile) for _ in MIX]
+    sids = [eng.open_stream(w, h) for (_, w, h, _) in MIX]
+    for f in range(4):
+        keep = []
+        pfs = [syn.frame(f) for syn in syns]
+        sub = [_pinned_copy(pf, keep) for pf in pfs] if pinned else pfs
+        eng.submit(sids, sub, [f] * len(MIX))
+        assert eng.wait() == CVP9_OK, eng.last_error()
+        for i in range(len(MIX)):
+            rc, arr = eng.get_frame_array(sids[i])
+            assert rc == CVP9_OK
+            assert np.array_equal(arr, orcs[i].decode(pfs[i])), "stream %d frame %d" % (i, f)
+        dense = sum(pf.contents.num_coeffs * 2 + pf.contents.num_blocks * 32 for pf in pfs)
+        st = eng.stats()
+        assert 0 < st.h2d_bytes < dense
+        assert st.kernel_launches >= 1
+    eng.close()
