@@ -257,94 +257,114 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms)
     tune_advance(t, e);
 }
 
-/* ── Host worker pool ─────────────────────────────────────────────────── */
+/* ── Host worker pools ────────────────────────────────────────────────── */
 
+/* Two pools: a small one for staging copies (the per-stream backend, on
+ * every frame) and a large one for packing (large batch steps). Copies
+ * measured slower on the GPU hosts whenever their tasks could land on any
+ * of 16 workers, so they keep a pool of their own. */
 #define POOL_MAX_THREADS 16
 
-static struct {
+typedef struct {
     pthread_mutex_t mu;
     pthread_cond_t  work, done;
     pthread_mutex_t busy;            /* one parallel job at a time */
+    pthread_once_t  once;
     void          (*fn)(void *, int);
     void           *ctx;
     int             ntasks, next, pending;
     int             nthreads;        /* workers (the caller is one more) */
-} g_pool = { PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, PTHREAD_COND_INITIALIZER,
-             PTHREAD_MUTEX_INITIALIZER, NULL, NULL, 0, 0, 0, -1 };
-static pthread_once_t g_pool_once = PTHREAD_ONCE_INIT;
+    const char     *env;             /* total threads override */
+    int             deflt;           /* total threads by default; 0: one per CPU up to 16 */
+} pool_t;
 
-/* takes tasks until none is left; called with g_pool.mu held */
-static void pool_drain(void)
+#define POOL_INIT(env, deflt) { PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, PTHREAD_COND_INITIALIZER, \
+                                PTHREAD_MUTEX_INITIALIZER, PTHREAD_ONCE_INIT, NULL, NULL, 0, 0, 0, -1, env, deflt }
+static pool_t g_copy_pool = POOL_INIT("CVP9_COPY_THREADS", 4);
+static pool_t g_work_pool = POOL_INIT("CVP9_HOST_THREADS", 0);
+
+/* takes tasks until none is left; called with p->mu held */
+static void pool_drain(pool_t *p)
 {
-    while (g_pool.next < g_pool.ntasks) {
-        int k = g_pool.next++;
-        void (*fn)(void *, int) = g_pool.fn;
-        void *ctx = g_pool.ctx;
-        pthread_mutex_unlock(&g_pool.mu);
+    while (p->next < p->ntasks) {
+        int k = p->next++;
+        void (*fn)(void *, int) = p->fn;
+        void *ctx = p->ctx;
+        pthread_mutex_unlock(&p->mu);
         fn(ctx, k);
-        pthread_mutex_lock(&g_pool.mu);
-        if (--g_pool.pending == 0) pthread_cond_broadcast(&g_pool.done);
+        pthread_mutex_lock(&p->mu);
+        if (--p->pending == 0) pthread_cond_broadcast(&p->done);
     }
 }
 
 static void *pool_worker(void *arg)
 {
-    (void)arg;
-    pthread_mutex_lock(&g_pool.mu);
+    pool_t *p = (pool_t *)arg;
+    pthread_mutex_lock(&p->mu);
     for (;;) {
-        while (g_pool.next >= g_pool.ntasks) pthread_cond_wait(&g_pool.work, &g_pool.mu);
-        pool_drain();
+        while (p->next >= p->ntasks) pthread_cond_wait(&p->work, &p->mu);
+        pool_drain(p);
     }
     return NULL;
 }
 
-static void pool_start(void)
+static void pool_start(pool_t *p)
 {
     long cpus = sysconf(_SC_NPROCESSORS_ONLN);
-    int want = cpus > 1 ? (int)(cpus < POOL_MAX_THREADS ? cpus : POOL_MAX_THREADS) - 1 : 0;  /* + the caller */
-    const char *e = getenv("CVP9_COPY_THREADS");
-    if (e && *e) want = atoi(e) - 1;
-    if (want > POOL_MAX_THREADS - 1) want = POOL_MAX_THREADS - 1;
+    int total = p->deflt ? p->deflt : (int)(cpus < POOL_MAX_THREADS ? cpus : POOL_MAX_THREADS);
+    const char *e = getenv(p->env);
+    if (e && *e) total = atoi(e);
+    if (total > POOL_MAX_THREADS) total = POOL_MAX_THREADS;
     int started = 0;
-    for (int i = 0; i < want; i++) {
+    for (int i = 0; i < total - 1; i++) {
         pthread_t t;
         pthread_attr_t at;
         pthread_attr_init(&at);
         pthread_attr_setdetachstate(&at, PTHREAD_CREATE_DETACHED);
-        if (pthread_create(&t, &at, pool_worker, NULL) == 0) started++;
+        if (pthread_create(&t, &at, pool_worker, p) == 0) started++;
         pthread_attr_destroy(&at);
     }
-    g_pool.nthreads = started;
+    p->nthreads = started;
 }
 
-int cvp9_pool_threads(void)
+static void copy_pool_start(void) { pool_start(&g_copy_pool); }
+static void work_pool_start(void) { pool_start(&g_work_pool); }
+
+static int pool_threads(pool_t *p)
 {
-    pthread_once(&g_pool_once, pool_start);
-    return g_pool.nthreads + 1;
+    pthread_once(&p->once, p == &g_copy_pool ? copy_pool_start : work_pool_start);
+    return p->nthreads + 1;
 }
 
-void cvp9_parallel_for(int ntasks, void (*fn)(void *ctx, int task), void *ctx)
+static void pool_run(pool_t *p, int ntasks, void (*fn)(void *ctx, int task), void *ctx)
 {
     if (ntasks <= 0) return;
-    pthread_once(&g_pool_once, pool_start);
-    if (ntasks == 1 || g_pool.nthreads <= 0 || pthread_mutex_trylock(&g_pool.busy) != 0) {
+    pool_threads(p);
+    if (ntasks == 1 || p->nthreads <= 0 || pthread_mutex_trylock(&p->busy) != 0) {
         for (int k = 0; k < ntasks; k++) fn(ctx, k);
         return;
     }
-    pthread_mutex_lock(&g_pool.mu);
-    g_pool.fn = fn;
-    g_pool.ctx = ctx;
-    g_pool.ntasks = ntasks;
-    g_pool.next = 0;
-    g_pool.pending = ntasks;
+    pthread_mutex_lock(&p->mu);
+    p->fn = fn;
+    p->ctx = ctx;
+    p->ntasks = ntasks;
+    p->next = 0;
+    p->pending = ntasks;
     /* wake only as many workers as there are tasks besides the caller's */
-    for (int k = 1; k < ntasks && k <= g_pool.nthreads; k++) pthread_cond_signal(&g_pool.work);
-    pool_drain();                                    /* the caller works too */
-    while (g_pool.pending > 0) pthread_cond_wait(&g_pool.done, &g_pool.mu);
-    g_pool.ntasks = 0;
-    g_pool.next = 0;
-    pthread_mutex_unlock(&g_pool.mu);
-    pthread_mutex_unlock(&g_pool.busy);
+    for (int k = 1; k < ntasks && k <= p->nthreads; k++) pthread_cond_signal(&p->work);
+    pool_drain(p);                                   /* the caller works too */
+    while (p->pending > 0) pthread_cond_wait(&p->done, &p->mu);
+    p->ntasks = 0;
+    p->next = 0;
+    pthread_mutex_unlock(&p->mu);
+    pthread_mutex_unlock(&p->busy);
+}
+
+int cvp9_pool_threads(void) { return pool_threads(&g_work_pool); }
+
+void cvp9_parallel_for(int ntasks, void (*fn)(void *ctx, int task), void *ctx)
+{
+    pool_run(&g_work_pool, ntasks, fn, ctx);
 }
 
 typedef struct { char *dst; const char *src; size_t n, chunk; } copy_job_t;
@@ -359,8 +379,7 @@ static void copy_task(void *ctx, int k)
 void cvp9_parallel_memcpy(void *dst, const void *src, size_t n)
 {
     if (n < (1u << 20)) { memcpy(dst, src, n); return; }
-    /* four threads already move more than the PCIe link takes */
-    const int parts = cvp9_pool_threads() < 4 ? cvp9_pool_threads() : 4;
+    const int parts = pool_threads(&g_copy_pool);
     copy_job_t j = { (char *)dst, (const char *)src, n, (n / parts + 4095) & ~(size_t)4095 };
-    cvp9_parallel_for((int)((n + j.chunk - 1) / j.chunk), copy_task, &j);
+    pool_run(&g_copy_pool, (int)((n + j.chunk - 1) / j.chunk), copy_task, &j);
 }

@@ -107,14 +107,16 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms);
  * each rounded up to a power of two, so serving steps share buckets. */
 uint64_t cvp9_tune_key(int arith, int frames, uint64_t superblocks);
 
-/* A pool of host worker threads (one per online CPU up to 16, the caller
- * included; $CVP9_COPY_THREADS overrides). cvp9_parallel_for runs fn(ctx, k) for k in
- * [0, ntasks), the caller taking tasks too, and returns when all are done;
- * one job holds the pool at a time (a second caller runs its tasks alone). */
+/* Host worker threads. cvp9_parallel_for runs fn(ctx, k) for k in
+ * [0, ntasks) on a pool of one thread per online CPU up to 16, the caller
+ * included ($CVP9_HOST_THREADS overrides), taking tasks itself, and returns
+ * when all are done; one job holds the pool at a time (a second caller runs
+ * its tasks alone). */
 int  cvp9_pool_threads(void);
 void cvp9_parallel_for(int ntasks, void (*fn)(void *ctx, int task), void *ctx);
 
-/* memcpy split across the pool; plain memcpy below 1 MB. The per-stream
+/* memcpy split across a pool of its own, 4 threads with the caller
+ * ($CVP9_COPY_THREADS overrides); plain memcpy below 1 MB. The per-stream
  * backend stages the parser's arrays with it: one thread moves ~12 GB/s,
  * slower than the PCIe link. */
 void cvp9_parallel_memcpy(void *dst, const void *src, size_t n);
