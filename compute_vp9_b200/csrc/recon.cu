@@ -1729,7 +1729,8 @@ struct FastChroma {
 };
 
 /* Chunk k of block b: its 8x8 luma and 4x4 chroma regions (clipped). */
-__device__ __forceinline__ void fast_chunk(const FastSmem &w, int c, FastBlk &fb, int &lx0, int &ly0, int &lw,
+template <class S>
+__device__ __forceinline__ void fast_chunk(const S &w, int c, FastBlk &fb, int &lx0, int &ly0, int &lw,
                                            int &lh, int &cx0, int &cy0, int &clw, int &clh)
 {
     const int b = w.chblk[c];
@@ -1748,11 +1749,19 @@ __device__ __forceinline__ void fast_chunk(const FastSmem &w, int c, FastBlk &fb
     clh = min(4, ((ch + 1) >> 1) - ccy * 4);
 }
 
+/* Where a superblock's prediction lands: its luma and chroma origins and
+ * pitches (the warp's shared tiles, or the frame itself). */
+struct PredDst {
+    uint8_t *y, *u, *v;
+    int      py, pc;
+};
+
 /* One lane's luma row (chunk c, row lane%8) and chroma row (plane
  * (lane/4)%2, row lane%4) of chunk c: geometry, reference and MV decoded
  * once for both, reads issued, nothing computed yet. */
-__device__ __forceinline__ void fast_pred_issue(FastSmem &w, const cvp9_job_t &job, int c, int lane, int nchunks,
-                                                int sbx, int sby, FastLuma &J, FastChroma &K)
+template <class S>
+__device__ __forceinline__ void fast_pred_issue(const S &w, const PredDst &D, const cvp9_job_t &job, int c, int lane,
+                                                int nchunks, int sbx, int sby, FastLuma &J, FastChroma &K)
 {
     J.act = J.ref = false;
     K.act = K.ref = false;
@@ -1773,7 +1782,7 @@ __device__ __forceinline__ void fast_pred_issue(FastSmem &w, const cvp9_job_t &j
     const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
     if (kk < lh) {
         J.act = true;
-        J.d = w.ty + (ly0 + kk) * kFY + lx0;
+        J.d = D.y + (ly0 + kk) * D.py + lx0;
         J.lw = lw;
         if (rp) {
             J.ref = true;
@@ -1794,7 +1803,7 @@ __device__ __forceinline__ void fast_pred_issue(FastSmem &w, const cvp9_job_t &j
     }
     if (r < clh && clw > 0) {
         K.act = true;
-        K.d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
+        K.d = (p ? D.v : D.u) + (cy0 + r) * D.pc + cx0;
         K.clw = clw;
         if (rp) {
             K.ref = true;
@@ -1821,7 +1830,7 @@ __device__ __forceinline__ void fast_luma_finish(const FastLuma &J)
     if (!J.act) return;
     uint32_t o0 = 0x7f7f7f7fu, o1 = 0x7f7f7f7fu;     /* missing reference: 127 */
     if (J.ref) bilinear8(J.lo0, J.mid0, J.hi0, J.lo1, J.mid1, J.hi1, J.fx, J.fy, o0, o1);
-    if (J.lw == 8) {
+    if (J.lw == 8 && !((uintptr_t)J.d & 3)) {
         reinterpret_cast<uint32_t *>(J.d)[0] = o0;
         reinterpret_cast<uint32_t *>(J.d)[1] = o1;
     } else {
@@ -1844,8 +1853,8 @@ __device__ __forceinline__ void fast_chroma_finish(const FastChroma &J)
 
 /* Where the q-th TX of size N in the SB sits; `ok` is false past the last
  * TX or when the TX's coefficients run past the array. */
-template <int N>
-__device__ __forceinline__ const int16_t *fast_tx_locate(const FastSmem &w, const cvp9_job_t &job, int q, int ntx,
+template <int N, class S>
+__device__ __forceinline__ const int16_t *fast_tx_locate(const S &w, const cvp9_job_t &job, int q, int ntx,
                                                         int i, int &px0, int &py0, bool &ok)
 {
     ok = false;
@@ -1893,9 +1902,13 @@ __device__ __forceinline__ void fast_row_load(uint32_t (&v)[N / 2], const int16_
  * per row. The loops run over the union of the group's nonzero rows and
  * columns so they stay warp-uniform; a term whose coefficient is zero in a
  * lane's own TX adds +-0 to a sum that is never -0, leaving it unchanged.
- * The next group's coefficients are loaded while the current one computes. */
-template <int N>
-__device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int lane)
+ * The next group's coefficients are loaded while the current one computes.
+ * The predicted rows are read from, and the results written to, dst (the
+ * warp's luma tile or the frame: row r of the superblock at dst + r *
+ * pitch); frame rows (GLOBAL) are read before the transform, so that they
+ * arrive while it computes. */
+template <int N, bool GLOBAL, class S>
+__device__ void fast_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int ntx, int lane)
 {
     constexpr int G = 32 / N, NN = N * N;
     constexpr int NH = N == 32 ? 2 : 1, NJ = N / NH;
@@ -1938,6 +1951,20 @@ __device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int l
         if (U) {
 #pragma unroll
             for (int h = 0; h < NH; h++) {
+                uint8_t *rowp = dst + (py0 + i) * pitch + px0 + h * NJ;
+                const bool words = !GLOBAL || !((uintptr_t)rowp & 3);
+                uint32_t pix[NJ / 4];
+#pragma unroll
+                for (int j4 = 0; j4 < NJ / 4; j4++) pix[j4] = 0u;
+                if (GLOBAL && have) {
+                    if (words) {
+#pragma unroll
+                        for (int j4 = 0; j4 < NJ / 4; j4++) pix[j4] = reinterpret_cast<const uint32_t *>(rowp)[j4];
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < NJ; j++) pix[j >> 2] |= (uint32_t)rowp[j] << (8 * (j & 3));
+                    }
+                }
                 double acc[NJ];
 #pragma unroll
                 for (int j = 0; j < NJ; j++) acc[j] = 0.0;
@@ -1954,10 +1981,9 @@ __device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int l
                     for (int j = 0; j < NJ; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, Mc[k * N + h * NJ + j]));
                 }
                 if (have) {
-                    uint32_t *row = reinterpret_cast<uint32_t *>(w.ty + (py0 + i) * kFY + px0 + h * NJ);
 #pragma unroll
                     for (int j4 = 0; j4 < NJ / 4; j4++) {
-                        uint32_t word = row[j4], outw = 0;
+                        uint32_t word = GLOBAL ? pix[j4] : reinterpret_cast<const uint32_t *>(rowp)[j4], outw = 0;
 #pragma unroll
                         for (int e = 0; e < 4; e++) {
                             /* round half away from zero; the int16 saturation of
@@ -1967,7 +1993,12 @@ __device__ void fast_residual(FastSmem &w, const cvp9_job_t &job, int ntx, int l
                             const int px = (int)((word >> (8 * e)) & 0xffu);
                             outw |= (uint32_t)clampi(px + r, 0, 255) << (8 * e);
                         }
-                        row[j4] = outw;
+                        if (words) {
+                            reinterpret_cast<uint32_t *>(rowp)[j4] = outw;
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 4; e++) rowp[4 * j4 + e] = (uint8_t)(outw >> (8 * e));
+                        }
                     }
                 }
             }
@@ -2257,30 +2288,22 @@ __device__ void spec_fast_residual(FastSmem &w, const cvp9_job_t &job, int P, in
 
 } /* namespace */
 
-/* MINB: CTAs per SM the register allocation is sized for (5: up to 96
- * registers, no spills; 6: 80 registers, a few spilled). */
-template <int A, int MINB>
-__global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_t *__restrict__ jobs,
-                                                            const uint32_t *__restrict__ tickets,
-                                                            uint32_t n_tickets, uint32_t *__restrict__ general)
+/* Steps 1-2 of a superblock on the warp-per-SB paths: load, check and pack
+ * its block descriptors (w.blk), check that they tile the visible SB exactly
+ * (4x4-cell occupancy in w.cells), and map its 8x8 prediction chunks
+ * (w.choff, w.chblk). Returns the number of chunks, or -1 when the SB
+ * belongs to the general kernel (intra, malformed, odd layouts). nb_out: the
+ * SB's block count. */
+template <int A, class S>
+__device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int sby, int lane, int &nb_out)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    FastSmem &w = reinterpret_cast<FastSmem *>(smem_raw)[warp];
-    const uint32_t t = blockIdx.x * kFastWarps + warp;
-    if (t >= n_tickets) return;
-    const uint32_t code = __ldg(tickets + t);
-    const cvp9_job_t &job = jobs[code >> 20];
-    const int sb = (int)(code & 0xFFFFFu);
-    const int sb_cols = job.sb_cols;
-    const int sbr = sb / sb_cols, sbc = sb - sbr * sb_cols;
-    const int sbx = sbc * 64, sby = sbr * 64;
     const int W = job.W, H = job.H;
     const uint32_t *rg = job.sb_range + 4 * sb;
     const uint32_t start = rg[0], end = rg[1], groups = rg[2];
     bool gen = groups != 1 || end < start || end > job.num_blocks || end - start > 64u ||
                (*job.status & CVP9_JOB_BAD_BLOCK) != 0;
     const int nb = gen ? 0 : (int)(end - start);
+    nb_out = nb;
 
     /* 1. blocks: load, check, pack; 4x4-cell occupancy */
     if (lane < 8) w.cells[lane] = 0u;
@@ -2356,11 +2379,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
         gap = w.cells[lane] != expect;
     }
     gen = __any_sync(0xffffffffu, gen || bad || ovl || gap) != 0;
-    if (lane == 0) general[t] = gen ? 1u : 0u;
-    if (gen) {
-        if (lane == 0) atomicAdd(general + 2 * n_tickets + 1, 1u);   /* k_compact skips when 0 */
-        return;
-    }
+    if (gen) return -1;
 
     /* 2. chunk (8x8 luma + 4x4 chroma) offsets and map */
     int nchunks;
@@ -2368,18 +2387,82 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
         const int x0 = warp_incl_scan(nch[0], lane), x1 = warp_incl_scan(nch[1], lane);
         const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
         nchunks = tot0 + tot1;
-        if (nchunks > 128) {             /* more chunks than the map holds (odd block sizes) */
-            if (lane == 0) {
-                general[t] = 1u;
-                atomicAdd(general + 2 * n_tickets + 1, 1u);
-            }
-            return;
-        }
+        if (nchunks > 128) return -1;   /* more chunks than the map holds (odd block sizes) */
         const int e0 = x0 - nch[0], e1 = tot0 + x1 - nch[1];
         if (lane < nb) { w.choff[lane] = (uint16_t)e0; for (int c = 0; c < nch[0]; c++) w.chblk[e0 + c] = (uint8_t)lane; }
         if (lane + 32 < nb) { w.choff[lane + 32] = (uint16_t)e1; for (int c = 0; c < nch[1]; c++) w.chblk[e1 + c] = (uint8_t)(lane + 32); }
     }
     __syncwarp();
+    return nchunks;
+}
+
+/* REFCPU luma residual of a set-up superblock (fast_sb_setup): one pass
+ * per TX size present, TXs counted on the frame-clamped block
+ * (vp9_reconstruct.c:338-340), added to the predicted rows at dst. */
+template <bool GLOBAL, class S>
+__device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int nb, int lane)
+{
+    unsigned sizes = 0;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = lane + 32 * r;
+        if (i < nb && !fb_skip(w.blk[i])) sizes |= 1u << fb_txl(w.blk[i]);
+    }
+    sizes = __reduce_or_sync(0xffffffffu, sizes);
+    for (unsigned sz = sizes; sz; sz &= sz - 1) {
+        const int txl = __ffs(sz) - 1, n = 4 << txl;
+        int cnt[2] = { 0, 0 };
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int i = lane + 32 * r;
+            if (i < nb) {
+                const FastBlk fb = w.blk[i];
+                if (!fb_skip(fb) && fb_txl(fb) == txl) cnt[r] = (fb_cw(fb) / n) * (fb_ch(fb) / n);
+            }
+        }
+        const int x0 = warp_incl_scan(cnt[0], lane), x1 = warp_incl_scan(cnt[1], lane);
+        const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
+        const int e0 = x0 - cnt[0], e1 = tot0 + x1 - cnt[1];
+        const int ntx = tot0 + tot1;        /* at most 256: the TXs tile the SB's luma */
+        if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
+        if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
+        __syncwarp();
+        switch (txl) {
+        case 0: fast_residual<4, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+        case 1: fast_residual<8, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+        case 2: fast_residual<16, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+        default: fast_residual<32, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+        }
+        __syncwarp();
+    }
+}
+
+/* MINB: CTAs per SM the register allocation is sized for (5: up to 96
+ * registers, no spills; 6: 80 registers, a few spilled). */
+template <int A, int MINB>
+__global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_t *__restrict__ jobs,
+                                                            const uint32_t *__restrict__ tickets,
+                                                            uint32_t n_tickets, uint32_t *__restrict__ general)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FastSmem &w = reinterpret_cast<FastSmem *>(smem_raw)[warp];
+    const uint32_t t = blockIdx.x * kFastWarps + warp;
+    if (t >= n_tickets) return;
+    const uint32_t code = __ldg(tickets + t);
+    const cvp9_job_t &job = jobs[code >> 20];
+    const int sb = (int)(code & 0xFFFFFu);
+    const int sb_cols = job.sb_cols;
+    const int sbr = sb / sb_cols, sbc = sb - sbr * sb_cols;
+    const int sbx = sbc * 64, sby = sbr * 64;
+    const int W = job.W, H = job.H;
+    int nb;
+    int nchunks = fast_sb_setup<A>(w, job, sb, sbx, sby, lane, nb);
+    if (lane == 0) general[t] = nchunks < 0 ? 1u : 0u;
+    if (nchunks < 0) {
+        if (lane == 0) atomicAdd(general + 2 * n_tickets + 1, 1u);   /* k_compact skips when 0 */
+        return;
+    }
 
     /* 3. prediction (vp9_reconstruct.c:94-131). Luma passes: lane = (chunk
      * c0 + lane/8, row lane%8); chroma passes: lane = (chunk c0 + lane/8,
@@ -2393,8 +2476,9 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
     for (int c0 = 0; c0 < nchunks; c0 += 8) {
         FastLuma a, b;
         FastChroma ca, cb;
-        fast_pred_issue(w, job, c0 + (lane >> 3), lane, nchunks, sbx, sby, a, ca);
-        fast_pred_issue(w, job, c0 + 4 + (lane >> 3), lane, nchunks, sbx, sby, b, cb);
+        const PredDst D = { w.ty, w.tu, w.tv, kFY, kFC };
+        fast_pred_issue(w, D, job, c0 + (lane >> 3), lane, nchunks, sbx, sby, a, ca);
+        fast_pred_issue(w, D, job, c0 + 4 + (lane >> 3), lane, nchunks, sbx, sby, b, cb);
         fast_luma_finish(a);
         fast_luma_finish(b);
         fast_chroma_finish(ca);
@@ -2405,7 +2489,8 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
     /* 4. residual, one pass per (plane, TX size) present: REFCPU luma only
      * with TXs counted on the frame-clamped block; SPEC every plane in the
      * tile parser's MI-clipped layout */
-    for (int P = 0; P < (A == CVP9_ARITH_SPEC ? 3 : 1); P++) {
+    if (A == CVP9_ARITH_REFCPU) fast_refcpu_residual<false>(w, w.ty, kFY, job, nb, lane);
+    for (int P = 0; P < (A == CVP9_ARITH_SPEC ? 3 : 0); P++) {
         unsigned sizes = 0;
 #pragma unroll
         for (int r = 0; r < 2; r++) {
@@ -2446,10 +2531,10 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
                 }
             } else {
                 switch (txl) {
-                case 0: fast_residual<4>(w, job, ntx, lane); break;
-                case 1: fast_residual<8>(w, job, ntx, lane); break;
-                case 2: fast_residual<16>(w, job, ntx, lane); break;
-                default: fast_residual<32>(w, job, ntx, lane); break;
+                case 0: fast_residual<4, false>(w, w.ty, kFY, job, ntx, lane); break;
+                case 1: fast_residual<8, false>(w, w.ty, kFY, job, ntx, lane); break;
+                case 2: fast_residual<16, false>(w, w.ty, kFY, job, ntx, lane); break;
+                default: fast_residual<32, false>(w, w.ty, kFY, job, ntx, lane); break;
                 }
             }
             __syncwarp();
@@ -2458,6 +2543,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
 
     /* 5. write the tile (clipped to the frame) and release the SB */
     {
+        const int vw = min(64, W - sbx), vh = min(64, H - sby);
         uint8_t *Y = job.out;
         if (!(W & 15) && !((uintptr_t)Y & 15)) {
             for (int i = lane; i < vh * 4; i += 32) {
@@ -2507,6 +2593,115 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
             }
         }
     }
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        st_release(job.sb_done + sb, job.epoch);
+    }
+}
+
+/* ── REFCPU superblocks in two kernels ──────────────────────────────────
+ * k_inter's REFCPU work split in two leaner kernels. k_inter holds a
+ * superblock's tiles, its coefficient staging and the transform's registers
+ * at once, which caps it at 20 warps per SM; its time follows the warps it
+ * keeps resident. k_pred predicts straight into the output frame and marks
+ * the general superblocks; k_resid adds the luma residual to the frame in
+ * place and releases the superblock. Same operations in the same order as
+ * k_inter, so the same bytes; the frame's luma makes one more round trip
+ * through L2/HBM. */
+struct __align__(16) PredSmem {                   /* k_pred, one per warp */
+    FastBlk  blk[64];
+    uint32_t cells[8];
+    uint16_t choff[65];
+    uint8_t  chblk[128];
+};
+
+struct __align__(16) ResidSmem {                  /* k_resid, one per warp */
+    union {
+        int16_t  coef[1056];
+        uint32_t cells[8];
+    };
+    FastBlk  blk[64];
+    union {
+        struct {
+            uint16_t choff[65];
+            uint8_t  chblk[128];
+        };
+        struct {
+            uint16_t txoff[65];
+            uint8_t  txblk[256];
+        };
+    };
+};
+
+static_assert(sizeof(PredSmem) % 16 == 0 && sizeof(ResidSmem) % 16 == 0, "per-warp areas stay 16-byte aligned");
+static_assert(offsetof(ResidSmem, coef) % 16 == 0, "coefficient rows are written as words");
+
+/* CTAs of 4 warps per SM the registers are sized for: prediction at 80
+ * registers (24 warps), residual at 64 (32 warps); measured best of 6/7/8
+ * each on 64 x 1080p steps. */
+constexpr int kPredMinB = 6, kResidMinB = 8;
+
+template <int MINB>
+__global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t *__restrict__ jobs,
+                                                           const uint32_t *__restrict__ tickets,
+                                                           uint32_t n_tickets, uint32_t *__restrict__ general)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    PredSmem &w = reinterpret_cast<PredSmem *>(smem_raw)[warp];
+    const uint32_t t = blockIdx.x * kFastWarps + warp;
+    if (t >= n_tickets) return;
+    const uint32_t code = __ldg(tickets + t);
+    const cvp9_job_t &job = jobs[code >> 20];
+    const int sb = (int)(code & 0xFFFFFu);
+    const int sbr = sb / job.sb_cols, sbc = sb - sbr * job.sb_cols;
+    const int sbx = sbc * 64, sby = sbr * 64;
+    int nb;
+    const int nchunks = fast_sb_setup<CVP9_ARITH_REFCPU>(w, job, sb, sbx, sby, lane, nb);
+    if (lane == 0) general[t] = nchunks < 0 ? 1u : 0u;
+    if (nchunks < 0) {
+        if (lane == 0) atomicAdd(general + 2 * n_tickets + 1, 1u);   /* k_compact skips when 0 */
+        return;
+    }
+    const int W = job.W, H = job.H, CW = job.CW, CH = job.CH;
+    uint8_t *Y = job.out;
+    uint8_t *U = Y + (size_t)W * H;
+    uint8_t *V = U + (size_t)CW * CH;
+    const size_t coff = (size_t)(sby >> 1) * CW + (sbx >> 1);
+    const PredDst D = { Y + (size_t)sby * W + sbx, U + coff, V + coff, W, CW };
+    for (int c0 = 0; c0 < nchunks; c0 += 8) {
+        FastLuma a, b;
+        FastChroma ca, cb;
+        fast_pred_issue(w, D, job, c0 + (lane >> 3), lane, nchunks, sbx, sby, a, ca);
+        fast_pred_issue(w, D, job, c0 + 4 + (lane >> 3), lane, nchunks, sbx, sby, b, cb);
+        fast_luma_finish(a);
+        fast_luma_finish(b);
+        fast_chroma_finish(ca);
+        fast_chroma_finish(cb);
+    }
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_t *__restrict__ jobs,
+                                                            const uint32_t *__restrict__ tickets,
+                                                            uint32_t n_tickets, const uint32_t *__restrict__ general)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    ResidSmem &w = reinterpret_cast<ResidSmem *>(smem_raw)[warp];
+    const uint32_t t = blockIdx.x * kFastWarps + warp;
+    if (t >= n_tickets || general[t]) return;    /* general superblocks: k_recon */
+    const uint32_t code = __ldg(tickets + t);
+    const cvp9_job_t &job = jobs[code >> 20];
+    const int sb = (int)(code & 0xFFFFFu);
+    const int sbr = sb / job.sb_cols, sbc = sb - sbr * job.sb_cols;
+    const int sbx = sbc * 64, sby = sbr * 64;
+    int nb;
+    /* the same inputs as k_pred saw: the same descriptors, never general */
+    if (fast_sb_setup<CVP9_ARITH_REFCPU>(w, job, sb, sbx, sby, lane, nb) < 0) return;
+    __syncwarp();
+    fast_refcpu_residual<true>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
     __syncwarp();
     if (lane == 0) {
         __threadfence();
@@ -3029,7 +3224,12 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
             if ((e = cudaMemsetAsync(L->n_general + 1, 0, 4, st)) != cudaSuccess) return (int)e;
             const size_t fs = kFastWarps * sizeof(FastSmem);
             const bool spec = L->arith == CVP9_ARITH_SPEC;
-            if (L->inter_variant == 2) {
+            if (L->inter_variant == 3 && !spec) {
+                k_pred<kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+                k_resid<kResidMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+            } else if (L->inter_variant == 2) {
                 if (spec) k_inter<CVP9_ARITH_SPEC, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
                 else k_inter<CVP9_ARITH_REFCPU, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
             } else {

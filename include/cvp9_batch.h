@@ -59,7 +59,9 @@ typedef struct {
     int      frames;         /* frames per step when the bucket was opened       */
     int      settled;        /* 1: every knob measured, the fields below hold     */
     int      inter_path;     /* 0 general kernel only, 1 warp-per-SB inter kernel
-                              * (96 registers), 2 the same at 80 registers       */
+                              * (96 registers), 2 the same at 80 registers,
+                              * 3 (REFCPU) prediction and residual as two
+                              * kernels at 80 and 64 registers                   */
     int      lf_tile_h;      /* loop filter: 16 register strips (8x16 per thread),
                               * 32 shared-memory tiles (64x32 per CTA)           */
     int      half_width;     /* 1: wavefront kernel on half the resident CTAs    */

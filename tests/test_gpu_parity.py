@@ -67,5 +67,13 @@ def test_parity_without_inter_fast_path(name, profile, monkeypatch):
 
 
 @pytest.mark.parametrize("name", list(CASES))
+def test_refcpu_parity_prediction_residual_split(name, monkeypatch):
+    """REFCPU's two-kernel inter path (k_pred into the frame, then k_resid in
+    place; CVP9_INTER_FAST=3) gives the oracle's bytes on every case."""
+    monkeypatch.setenv("CVP9_INTER_FAST", "3")
+    run_case(REFCPU, *CASES[name])
+
+
+@pytest.mark.parametrize("name", list(CASES))
 def test_spec_parity(name):
     run_case(SPEC, *CASES[name])
