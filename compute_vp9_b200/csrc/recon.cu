@@ -1622,14 +1622,18 @@ __device__ __forceinline__ int warp_incl_scan(int x, int lane)
     return x;
 }
 
-/* Bytes r[0..8] of a row at p, as r0..r3 / r4..r7 / r8 in three words,
- * from aligned word reads (callers keep the aligned span inside the buffer). */
-__device__ __forceinline__ void ld9w(const uint8_t *p, uint32_t &lo, uint32_t &mid, uint32_t &hi)
+/* The same nine bytes from two 8-byte reads of the aligned 16 bytes around
+ * them (p & 7 <= 7, so r[0..8] always lie inside; callers keep the span
+ * inside the buffer): fewer L1 requests than three word reads. */
+__device__ __forceinline__ void ld9d(const uint8_t *p, uint32_t &lo, uint32_t &mid, uint32_t &hi)
 {
     const uintptr_t a = (uintptr_t)p;
-    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
-    const unsigned sh = 8u * (unsigned)(a & 3);
-    const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+    const uint2 *q = reinterpret_cast<const uint2 *>(a & ~(uintptr_t)7);
+    const uint2 v0 = __ldg(q), v1 = __ldg(q + 1);
+    const unsigned o = (unsigned)(a & 7), sh = 8u * (o & 3u);
+    /* words w[o/4 .. o/4 + 2] of the four, by whether o >= 4 */
+    const bool up = o >= 4;
+    const uint32_t w0 = up ? v0.y : v0.x, w1 = up ? v1.x : v0.y, w2 = up ? v1.y : v1.x;
     lo = __funnelshift_r(w0, w1, sh);
     mid = __funnelshift_r(w1, w2, sh);
     hi = w2 >> sh;
@@ -1763,65 +1767,88 @@ template <class S>
 __device__ __forceinline__ void fast_pred_issue(const S &w, const PredDst &D, const cvp9_job_t &job, int c, int lane,
                                                 int nchunks, int sbx, int sby, FastLuma &J, FastChroma &K)
 {
+    /* Each lane reads one reference row of its chunk (luma row kk, chroma
+     * row r of its plane) and takes the row below from the next lane; the
+     * last lane of a chunk (plane) reads its second row itself. Lanes below
+     * the chunk's clipped height still read, for their upper neighbours.
+     * A row is read as aligned words when its needed bytes are inside the
+     * reference and the words past its end stay inside the frame, else byte
+     * by byte with every sample clamped — the same bytes wherever used. */
     J.act = J.ref = false;
     K.act = K.ref = false;
-    if (c >= nchunks) return;
-    FastBlk fb;
-    int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
-    fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
     const int kk = lane & 7, p = (lane >> 2) & 1, r = lane & 3;
-    const int slot = fb_slot(fb);
-    const uint8_t *rp = nullptr;
-    int rw = 0, rh = 0;
-    if (slot < 8) {
-        const cvp9_ref_t &R = job.ref[slot];
-        rp = R.plane;
-        rw = R.w;
-        rh = R.h;
-    }
-    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
-    if (kk < lh) {
-        J.act = true;
+    uint32_t l0 = 0, m0 = 0, h0 = 0, cl0 = 0, ch0 = 0;
+    if (c < nchunks) {
+        FastBlk fb;
+        int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
+        fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
+        const int slot = fb_slot(fb);
+        const uint8_t *rp = nullptr;
+        int rw = 0, rh = 0;
+        if (slot < 8) {
+            const cvp9_ref_t &R = job.ref[slot];
+            rp = R.plane;
+            rw = R.w;
+            rh = R.h;
+        }
+        const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+        J.act = kk < lh;
         J.d = D.y + (ly0 + kk) * D.py + lx0;
         J.lw = lw;
+        K.act = r < clh && clw > 0;
+        K.d = (p ? D.v : D.u) + (cy0 + r) * D.pc + cx0;
+        K.clw = clw;
         if (rp) {
             J.ref = true;
             const int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
             const int ix = px8 >> 3, y0 = (py8 >> 3) + kk;
             J.fx = px8 & 7;
             J.fy = py8 & 7;
-            if (ix >= 0 && ix + lw < rw && y0 >= 0 && y0 + 1 < rh) {
-                /* luma rows are followed by the chroma planes: the word
-                 * reads past a row end stay inside the frame */
-                ld9w(rp + (size_t)y0 * rw + ix, J.lo0, J.mid0, J.hi0);
-                ld9w(rp + (size_t)(y0 + 1) * rw + ix, J.lo1, J.mid1, J.hi1);
-            } else {
-                ld9c(rp, rw, rh, ix, y0, J.lo0, J.mid0, J.hi0);
-                ld9c(rp, rw, rh, ix, y0 + 1, J.lo1, J.mid1, J.hi1);
+            /* luma rows are followed by the chroma planes: reads past a row
+             * end stay inside the frame; the plane starts 8-byte aligned, so
+             * with ix >= 0 they never start before it */
+            const bool hin = ix >= 0 && ix + lw < rw;
+            if (hin && y0 >= 0 && y0 < rh) ld9d(rp + (size_t)y0 * rw + ix, l0, m0, h0);
+            else ld9c(rp, rw, rh, ix, y0, l0, m0, h0);
+            if (kk == 7) {
+                if (hin && y0 + 1 >= 0 && y0 + 1 < rh) ld9d(rp + (size_t)(y0 + 1) * rw + ix, J.lo1, J.mid1, J.hi1);
+                else ld9c(rp, rw, rh, ix, y0 + 1, J.lo1, J.mid1, J.hi1);
+            }
+            if (clw > 0) {
+                K.ref = true;
+                const int rcs = (rw + 1) >> 1, crw = rw >> 1, crh = rh >> 1;
+                const uint8_t *pl = rp + (size_t)rw * rh + (p ? (size_t)rcs * ((rh + 1) >> 1) : 0);
+                const int cpx8 = ((sbx >> 1) + cx0) * 8 + mvx / 2, cpy8 = ((sby >> 1) + cy0) * 8 + mvy / 2;
+                const int cix = cpx8 >> 3, y1 = (cpy8 >> 3) + r;
+                K.fx = cpx8 & 7;
+                K.fy = cpy8 & 7;
+                /* a further chroma row below the one read: word reads stay inside */
+                const bool chin = cix >= 0 && cix + clw < crw;
+                if (chin && y1 >= 0 && y1 + 1 < crh) ld5w(pl + (size_t)y1 * rcs + cix, cl0, ch0);
+                else ld5c(pl, rcs, crw, crh, cix, y1, cl0, ch0);
+                if (r == 3) {
+                    if (chin && y1 + 1 >= 0 && y1 + 2 < crh) ld5w(pl + (size_t)(y1 + 1) * rcs + cix, K.lo1, K.hi1);
+                    else ld5c(pl, rcs, crw, crh, cix, y1 + 1, K.lo1, K.hi1);
+                }
             }
         }
     }
-    if (r < clh && clw > 0) {
-        K.act = true;
-        K.d = (p ? D.v : D.u) + (cy0 + r) * D.pc + cx0;
-        K.clw = clw;
-        if (rp) {
-            K.ref = true;
-            const int rcs = (rw + 1) >> 1, crw = rw >> 1, crh = rh >> 1;
-            const uint8_t *pl = rp + (size_t)rw * rh + (p ? (size_t)rcs * ((rh + 1) >> 1) : 0);
-            const int cpx8 = ((sbx >> 1) + cx0) * 8 + mvx / 2, cpy8 = ((sby >> 1) + cy0) * 8 + mvy / 2;
-            const int cix = cpx8 >> 3, y0 = (cpy8 >> 3) + r;
-            K.fx = cpx8 & 7;
-            K.fy = cpy8 & 7;
-            if (cix >= 0 && cix + clw < crw && y0 >= 0 && y0 + 2 < crh) {
-                /* a further chroma row exists below: word reads stay inside */
-                ld5w(pl + (size_t)y0 * rcs + cix, K.lo0, K.hi0);
-                ld5w(pl + (size_t)(y0 + 1) * rcs + cix, K.lo1, K.hi1);
-            } else {
-                ld5c(pl, rcs, crw, crh, cix, y0, K.lo0, K.hi0);
-                ld5c(pl, rcs, crw, crh, cix, y0 + 1, K.lo1, K.hi1);
-            }
-        }
+    const uint32_t nl = __shfl_down_sync(0xffffffffu, l0, 1), nm = __shfl_down_sync(0xffffffffu, m0, 1);
+    const uint32_t nh = __shfl_down_sync(0xffffffffu, h0, 1);
+    const uint32_t ncl = __shfl_down_sync(0xffffffffu, cl0, 1), nch = __shfl_down_sync(0xffffffffu, ch0, 1);
+    J.lo0 = l0;
+    J.mid0 = m0;
+    J.hi0 = h0;
+    if (kk != 7) {
+        J.lo1 = nl;
+        J.mid1 = nm;
+        J.hi1 = nh;
+    }
+    K.lo0 = cl0;
+    K.hi0 = ch0;
+    if (r != 3) {
+        K.lo1 = ncl;
+        K.hi1 = nch;
     }
 }
 
