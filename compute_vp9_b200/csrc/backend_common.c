@@ -110,7 +110,7 @@ int cvp9_env_autotune(void)
 int cvp9_env_inter_fast(void)
 {
     const char *e = getenv("CVP9_INTER_FAST");
-    if (e && *e >= '0' && *e <= '3' && !e[1]) return *e - '0';
+    if (e && *e >= '0' && *e <= '4' && !e[1]) return *e - '0';
     return 1;
 }
 
@@ -184,9 +184,9 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
         e->idx++;
         if (e->stage == 0) {
             /* inter path: the default was candidate 0; REFCPU also has the
-             * two-kernel split (3) */
-            static const int8_t alts[3] = { 0, 2, 3 };
-            if (e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 3 : 2)) {
+             * two-kernel split (3) and the split with unrolled 8x8 TXs (4) */
+            static const int8_t alts[4] = { 0, 2, 3, 4 };
+            if (e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 2)) {
                 e->cur = e->best;
                 e->cur.inter = alts[e->idx - 1];
                 break;

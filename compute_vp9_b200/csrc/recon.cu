@@ -2037,6 +2037,113 @@ __device__ void fast_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &j
     }
 }
 
+/* fast_residual for N <= 8 with the column loop unrolled: column k is a
+ * compile-time index, so the basis row M[k][.] comes as constant operands,
+ * and the masks come from ballots of the lanes' own rows (bit (TX, l) of
+ * column k's ballot: X[l][k] != 0) instead of scans of the staged tile and
+ * per-column shuffles. Same operations in the same order: the columns of
+ * the union of the group's nonzero columns, ascending; per column, the rows
+ * of the union of its nonzero rows, ascending. */
+template <int N, bool GLOBAL, class S>
+__device__ void fast_residual_u(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int ntx, int lane)
+{
+    static_assert(N <= 8, "unrolled for the small transforms");
+    constexpr int G = 32 / N, NN = N * N;
+    constexpr unsigned kSeg = (1u << N) - 1u;
+    constexpr int boff = N == 4 ? 0 : 16;
+    const int g = lane / N, i = lane % N;
+    const double *Mg = g_dct + boff;     /* lane-varying reads */
+    int16_t *X = w.coef + g * (NN + 2);
+    uint32_t rv[N / 2];
+    int px0, py0;
+    bool have;
+    {
+        const int16_t *src = fast_tx_locate<N>(w, job, g, ntx, i, px0, py0, have);
+        if (have) fast_row_load<N>(rv, src);
+    }
+    for (int q0 = 0; q0 < ntx; q0 += G) {
+        uint32_t rm = 0;                     /* nonzero columns of this lane's row */
+        if (have) {
+            uint32_t *xs = reinterpret_cast<uint32_t *>(X + i * N);
+#pragma unroll
+            for (int k = 0; k < N / 2; k++) {
+                xs[k] = rv[k];
+                const uint32_t m = __vcmpne2(rv[k], 0u);
+                rm |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * k);
+            }
+        }
+        __syncwarp();
+        uint8_t *rowp = dst + (py0 + i) * pitch + px0;
+        const bool words = !GLOBAL || !((uintptr_t)rowp & 3);
+        uint32_t pix[N / 4];
+#pragma unroll
+        for (int j4 = 0; j4 < N / 4; j4++) pix[j4] = 0u;
+        const bool anynz = __any_sync(0xffffffffu, rm != 0);   /* every lane: a warp vote */
+        if (GLOBAL && have && anynz) {
+            if (words) {
+#pragma unroll
+                for (int j4 = 0; j4 < N / 4; j4++) pix[j4] = reinterpret_cast<const uint32_t *>(rowp)[j4];
+            } else {
+#pragma unroll
+                for (int j = 0; j < N; j++) pix[j >> 2] |= (uint32_t)rowp[j] << (8 * (j & 3));
+            }
+        }
+        int npx0, npy0;
+        bool nhave;
+        {
+            const int16_t *src = fast_tx_locate<N>(w, job, q0 + G + g, ntx, i, npx0, npy0, nhave);
+            if (nhave) fast_row_load<N>(rv, src);
+        }
+        double acc[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) acc[j] = 0.0;
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            const unsigned B = __ballot_sync(0xffffffffu, (rm >> k) & 1u);
+            if (!B) continue;
+            any = true;
+            unsigned rows = B;
+#pragma unroll
+            for (int s2 = 16; s2 >= N; s2 >>= 1) rows |= rows >> s2;
+            rows &= kSeg;
+            double t = 0.0;
+            for (unsigned v = rows; v; v &= v - 1) {
+                const int l = __ffs(v) - 1;
+                t = __dadd_rn(t, __dmul_rn(__ldg(Mg + l * N + i), (double)X[l * N + k]));
+            }
+#pragma unroll
+            for (int j = 0; j < N; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, c_dct[boff + k * N + j]));
+        }
+        if (any && have) {
+#pragma unroll
+            for (int j4 = 0; j4 < N / 4; j4++) {
+                const uint32_t word = GLOBAL ? pix[j4] : reinterpret_cast<const uint32_t *>(rowp)[j4];
+                uint32_t outw = 0;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    /* round half away from zero; the int16 saturation of
+                     * vp9_reconstruct.c:52-59 cannot change the result of
+                     * the 0..255 clamp that follows, so it is folded in */
+                    const int r = __double2int_rz(__dadd_rn(acc[j4 * 4 + e], copysign(0.5, acc[j4 * 4 + e])));
+                    const int px = (int)((word >> (8 * e)) & 0xffu);
+                    outw |= (uint32_t)clampi(px + r, 0, 255) << (8 * e);
+                }
+                if (words) {
+                    reinterpret_cast<uint32_t *>(rowp)[j4] = outw;
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) rowp[4 * j4 + e] = (uint8_t)(outw >> (8 * e));
+                }
+            }
+        }
+        __syncwarp();
+        have = nhave;
+        px0 = npx0;
+        py0 = npy0;
+    }
+}
+
 /* ── SPEC arithmetic in k_inter ─────────────────────────────────────────── */
 
 /* 16 consecutive bytes of a row at p as four words (aligned word reads;
@@ -2425,8 +2532,11 @@ __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int s
 
 /* REFCPU luma residual of a set-up superblock (fast_sb_setup): one pass
  * per TX size present, TXs counted on the frame-clamped block
- * (vp9_reconstruct.c:338-340), added to the predicted rows at dst. */
-template <bool GLOBAL, class S>
+ * (vp9_reconstruct.c:338-340), added to the predicted rows at dst. U8: 8x8
+ * TXs through the unrolled fast_residual_u (fewer instructions, much more
+ * code: it pays on content of 8x8 TXs alone and costs on mixed sizes, where
+ * the warps of an SM run every size's code at once). */
+template <bool GLOBAL, bool U8, class S>
 __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int nb, int lane)
 {
     unsigned sizes = 0;
@@ -2456,7 +2566,10 @@ __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_j
         __syncwarp();
         switch (txl) {
         case 0: fast_residual<4, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
-        case 1: fast_residual<8, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+        case 1:
+            if (U8) fast_residual_u<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
+            else fast_residual<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
+            break;
         case 2: fast_residual<16, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
         default: fast_residual<32, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
         }
@@ -2516,7 +2629,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
     /* 4. residual, one pass per (plane, TX size) present: REFCPU luma only
      * with TXs counted on the frame-clamped block; SPEC every plane in the
      * tile parser's MI-clipped layout */
-    if (A == CVP9_ARITH_REFCPU) fast_refcpu_residual<false>(w, w.ty, kFY, job, nb, lane);
+    if (A == CVP9_ARITH_REFCPU) fast_refcpu_residual<false, false>(w, w.ty, kFY, job, nb, lane);
     for (int P = 0; P < (A == CVP9_ARITH_SPEC ? 3 : 0); P++) {
         unsigned sizes = 0;
 #pragma unroll
@@ -2709,7 +2822,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     }
 }
 
-template <int MINB>
+template <int MINB, bool U8>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_t *__restrict__ jobs,
                                                             const uint32_t *__restrict__ tickets,
                                                             uint32_t n_tickets, const uint32_t *__restrict__ general)
@@ -2728,7 +2841,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_
     /* the same inputs as k_pred saw: the same descriptors, never general */
     if (fast_sb_setup<CVP9_ARITH_REFCPU>(w, job, sb, sbx, sby, lane, nb) < 0) return;
     __syncwarp();
-    fast_refcpu_residual<true>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
+    fast_refcpu_residual<true, U8>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
     __syncwarp();
     if (lane == 0) {
         __threadfence();
@@ -3251,11 +3364,15 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
             if ((e = cudaMemsetAsync(L->n_general + 1, 0, 4, st)) != cudaSuccess) return (int)e;
             const size_t fs = kFastWarps * sizeof(FastSmem);
             const bool spec = L->arith == CVP9_ARITH_SPEC;
-            if (L->inter_variant == 3 && !spec) {
+            if ((L->inter_variant == 3 || L->inter_variant == 4) && !spec) {
                 k_pred<kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
                     L->jobs, L->tickets, L->n_tickets, L->general);
-                k_resid<kResidMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
-                    L->jobs, L->tickets, L->n_tickets, L->general);
+                if (L->inter_variant == 4)
+                    k_resid<kResidMinB, true><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
+                        L->jobs, L->tickets, L->n_tickets, L->general);
+                else
+                    k_resid<kResidMinB, false><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
+                        L->jobs, L->tickets, L->n_tickets, L->general);
             } else if (L->inter_variant == 2) {
                 if (spec) k_inter<CVP9_ARITH_SPEC, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);
                 else k_inter<CVP9_ARITH_REFCPU, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);

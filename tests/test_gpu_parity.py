@@ -66,11 +66,13 @@ def test_parity_without_inter_fast_path(name, profile, monkeypatch):
     run_case(profile, *CASES[name])
 
 
+@pytest.mark.parametrize("variant", ["3", "4"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_refcpu_parity_prediction_residual_split(name, monkeypatch):
+def test_refcpu_parity_prediction_residual_split(name, variant, monkeypatch):
     """REFCPU's two-kernel inter path (k_pred into the frame, then k_resid in
-    place; CVP9_INTER_FAST=3) gives the oracle's bytes on every case."""
-    monkeypatch.setenv("CVP9_INTER_FAST", "3")
+    place; CVP9_INTER_FAST=3, and 4 with the 8x8 transform unrolled) gives
+    the oracle's bytes on every case."""
+    monkeypatch.setenv("CVP9_INTER_FAST", variant)
     run_case(REFCPU, *CASES[name])
 
 
