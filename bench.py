@@ -463,10 +463,12 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
-def read_traffic():
-    """Per-launch DRAM bytes of the dominant recon kernel (k_inter) at the
-    bench workload, from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_inter_refcpu_1080p_x16.md")
+def read_traffic(split=False):
+    """Per-step DRAM bytes of the warp-per-superblock recon kernels (k_inter,
+    or k_pred + k_resid) at the bench workload, from the committed ncu
+    summary."""
+    name = "k_pred_k_resid_refcpu_1080p_x16.md" if split else "k_inter_refcpu_1080p_x16.md"
+    p = os.path.join(ROOT, "profiles", name)
     try:
         with open(p) as f:
             for line in f:
@@ -582,7 +584,8 @@ def main():
                                                                args.warmup + args.steps + 3))
         peak, peak_kind = read_peaks()
         achieved = alg / (recon_ms / 1000.0) / 1e9
-        traffic = read_traffic()
+        split = bool(tuned) and tuned[0].get("inter_path") in (3, 4)
+        traffic = read_traffic(split)
         single = None
         if not args.no_single:
             one = Workload(1, args.width, args.height, device_copy=True)
@@ -676,7 +679,9 @@ def main():
             "latency_ms": {"p50": statistics.median(lat) if lat else None,
                            "p99": (sorted(lat)[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None),
                            "what": "host clock, submit to frame in pinned host memory, e2e steps (3 in flight)"},
-            "roofline": {"bound": "hbm", "kernel": "recon phase (k_inter, k_compact, k_recon)",
+            "roofline": {"bound": "hbm",
+                         "kernel": ("recon phase (k_pred, k_resid, k_compact, k_recon)" if split
+                                    else "recon phase (k_inter, k_compact, k_recon)"),
                          "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"

@@ -939,8 +939,10 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
     gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
+    /* k_inter + k_compact, or k_pred + k_resid + k_compact (REFCPU split) */
+    const int split = L.inter_variant >= 3 && b->arith == CVP9_ARITH_REFCPU;
     s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
-                             (L.general ? 2 : 0));
+                             (L.general ? (split ? 3 : 2) : 0));
     if (b->use_graphs) {
         if (!s->graph || s->graph_key != gkey) {
             if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = NULL; }

@@ -2777,10 +2777,11 @@ struct __align__(16) ResidSmem {                  /* k_resid, one per warp */
 static_assert(sizeof(PredSmem) % 16 == 0 && sizeof(ResidSmem) % 16 == 0, "per-warp areas stay 16-byte aligned");
 static_assert(offsetof(ResidSmem, coef) % 16 == 0, "coefficient rows are written as words");
 
-/* CTAs of 4 warps per SM the registers are sized for: prediction at 80
- * registers (24 warps), residual at 64 (32 warps); measured best of 6/7/8
- * each on 64 x 1080p steps. */
-constexpr int kPredMinB = 6, kResidMinB = 8;
+/* CTAs of 4 warps per SM the registers are sized for: prediction at 96
+ * registers (20 warps), residual at 64 (32 warps, some spilled); measured
+ * best of 5..8 each on 64 x 1080p steps (1.016 ms against 1.028 for 80/64
+ * and 1.10 for 80/80). */
+constexpr int kPredMinB = 5, kResidMinB = 8;
 
 template <int MINB>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t *__restrict__ jobs,

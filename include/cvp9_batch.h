@@ -61,7 +61,7 @@ typedef struct {
     int      inter_path;     /* 0 general kernel only, 1 warp-per-SB inter kernel
                               * (96 registers), 2 the same at 80 registers,
                               * 3 (REFCPU) prediction and residual as two
-                              * kernels at 80 and 64 registers, 4 the same with
+                              * kernels at 96 and 64 registers, 4 the same with
                               * the 8x8 transform unrolled                       */
     int      lf_tile_h;      /* loop filter: 16 register strips (8x16 per thread),
                               * 32 shared-memory tiles (64x32 per CTA)           */
