@@ -2427,8 +2427,9 @@ __device__ void spec_fast_residual(FastSmem &w, const cvp9_job_t &job, int P, in
  * (4x4-cell occupancy in w.cells), and map its 8x8 prediction chunks
  * (w.choff, w.chblk). Returns the number of chunks, or -1 when the SB
  * belongs to the general kernel (intra, malformed, odd layouts). nb_out: the
- * SB's block count. */
-template <int A, class S>
+ * SB's block count. CHECK = false: only load and pack the descriptors (a
+ * second kernel on an SB the first one already took; returns 0). */
+template <int A, bool CHECK = true, class S>
 __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int sby, int lane, int &nb_out)
 {
     const int W = job.W, H = job.H;
@@ -2440,8 +2441,10 @@ __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int s
     nb_out = nb;
 
     /* 1. blocks: load, check, pack; 4x4-cell occupancy */
-    if (lane < 8) w.cells[lane] = 0u;
-    __syncwarp();
+    if (CHECK) {
+        if (lane < 8) w.cells[lane] = 0u;
+        __syncwarp();
+    }
     bool bad = false, ovl = false;
     int nch[2] = { 0, 0 };
 #pragma unroll
@@ -2495,6 +2498,7 @@ __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int s
         fb.mv = g3;
         fb.coeff = g6;
         w.blk[i] = fb;
+        if (!CHECK) continue;
         nch[r] = ((cw + 7) >> 3) * ((ch + 7) >> 3);
         const int c0x = lx >> 2, c1x = (lx + cw - 1) >> 2, c0y = ly >> 2, c1y = (ly + ch - 1) >> 2;
         const uint32_t m = (2u << c1x) - (1u << c0x);
@@ -2504,6 +2508,7 @@ __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int s
         }
     }
     __syncwarp();
+    if (!CHECK) return 0;
     const int vw = min(64, W - sbx), vh = min(64, H - sby);
     bool gap = false;
     if (lane < 8) {
@@ -2839,8 +2844,8 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_
     const int sbr = sb / job.sb_cols, sbc = sb - sbr * job.sb_cols;
     const int sbx = sbc * 64, sby = sbr * 64;
     int nb;
-    /* the same inputs as k_pred saw: the same descriptors, never general */
-    if (fast_sb_setup<CVP9_ARITH_REFCPU>(w, job, sb, sbx, sby, lane, nb) < 0) return;
+    /* the same descriptors k_pred checked and packed: packing alone */
+    fast_sb_setup<CVP9_ARITH_REFCPU, false>(w, job, sb, sbx, sby, lane, nb);
     __syncwarp();
     fast_refcpu_residual<true, U8>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
     __syncwarp();
