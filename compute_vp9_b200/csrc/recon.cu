@@ -58,6 +58,10 @@ constexpr long long kSpinLimit = 1ll << 20;   /* ~0.25 s of polling */
 
 __constant__ double c_dct[16 + 64 + 256 + 1024];      /* N = 4, 8, 16, 32 */
 __constant__ int c_subpel[16][8] = CVP9_SUBPEL_REGULAR_INIT;
+/* the same taps as signed bytes, taps 0-3 and 4-7 in two words, for dp4a
+ * (phase 0's 128 does not fit a byte: callers take the centre sample for
+ * it, which is what its filter computes); uploaded by cvp9k_configure */
+__constant__ uint32_t c_subpel_pk[16][2];
 
 __device__ __forceinline__ const double *dct_basis(int txl)
 {
@@ -2170,10 +2174,42 @@ __device__ __forceinline__ void ld16c(const uint8_t *plane, int stride, int pw, 
     for (int x = 0; x < 16; x++) o[x >> 2] |= (uint32_t)__ldg(row + clampi(x0 + x, 0, xm)) << (8 * (x & 3));
 }
 
-__device__ __forceinline__ int bytek(const uint32_t o[4], int k) { return (int)((o[k >> 2] >> (8 * (k & 3))) & 0xffu); }
 
 /* shader rounding of one 8-tap sum: (acc + 64) >> 7 clipped to 8 bits */
 __device__ __forceinline__ uint32_t tap_round(int acc) { return (uint32_t)clampi((acc + 64) >> 7, 0, 255); }
+
+/* bytes k..k+3 of o[] as one word (k a compile-time index) */
+__device__ __forceinline__ uint32_t win4(const uint32_t o[4], int k)
+{
+    return (k & 3) ? __funnelshift_r(o[k >> 2], o[(k >> 2) + 1], 8 * (k & 3)) : o[k >> 2];
+}
+
+/* c + the dot product of four signed taps with four unsigned samples */
+__device__ __forceinline__ int dp4a_su(uint32_t taps, uint32_t px, int c)
+{
+    int d;
+    asm("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(taps), "r"(px), "r"(c));
+    return d;
+}
+
+/* One 8-tap output from samples s0 (samples 0-3 of the window) and s1
+ * (4-7): phase 0 is the centre sample itself. */
+__device__ __forceinline__ uint32_t tap8(uint32_t ta, uint32_t tb, int phase, uint32_t s0, uint32_t s1)
+{
+    return phase ? tap_round(dp4a_su(tb, s1, dp4a_su(ta, s0, 0))) : (s0 >> 24);
+}
+
+/* 4x4 byte transpose: rows a..d (one word of four columns each) to four
+ * words, one column each (its bytes in row order) */
+__device__ __forceinline__ void tr4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t col[4])
+{
+    const uint32_t x0 = __byte_perm(a, b, 0x5140), x1 = __byte_perm(a, b, 0x7362);
+    const uint32_t y0 = __byte_perm(c, d, 0x5140), y1 = __byte_perm(c, d, 0x7362);
+    col[0] = __byte_perm(x0, y0, 0x5410);
+    col[1] = __byte_perm(x0, y0, 0x7632);
+    col[2] = __byte_perm(x1, y1, 0x5410);
+    col[3] = __byte_perm(x1, y1, 0x7632);
+}
 
 /* Luma prediction of four chunks (vp9_mc.comp.glsl:61-110): lane = (chunk
  * c0 + lane/8, k = lane%8). Horizontal 8-tap rows k and k+8 of each chunk's
@@ -2197,6 +2233,7 @@ __device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int n
         fx = (mvx & 7) << 1;
         fy = (mvy & 7) << 1;
         if (rp) {
+            const uint32_t ta = c_subpel_pk[fx][0], tb = c_subpel_pk[fx][1];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int hr = k + 8 * h;
@@ -2208,10 +2245,7 @@ __device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int n
                 uint32_t out0 = 0, out1 = 0;
 #pragma unroll
                 for (int cc = 0; cc < 8; cc++) {
-                    int acc = 0;
-#pragma unroll
-                    for (int tt = 0; tt < 8; tt++) acc += c_subpel[fx][tt] * bytek(o, cc + tt);
-                    const uint32_t v = tap_round(acc);
+                    const uint32_t v = tap8(ta, tb, fx, win4(o, cc), win4(o, cc + 4));
                     if (cc < 4) out0 |= v << (8 * cc); else out1 |= v << (8 * (cc - 4));
                 }
                 uint32_t *hrow = reinterpret_cast<uint32_t *>(hb + (q * 15 + hr) * 8);
@@ -2225,14 +2259,27 @@ __device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int n
         uint32_t o0 = 0x80808080u, o1 = 0x80808080u;           /* missing reference: 128 */
         if (rp) {
             o0 = o1 = 0;
-            const uint8_t *hcol = hb + (q * 15 + k) * 8;
+            /* rows k..k+7 of the filtered window, transposed four by four
+             * so that a column's taps meet as one word */
+            const uint2 *hrows = reinterpret_cast<const uint2 *>(hb + (q * 15 + k) * 8);
+            uint32_t lo[8], hi[8];
 #pragma unroll
-            for (int cc = 0; cc < 8; cc++) {
-                int acc = 0;
+            for (int tt = 0; tt < 8; tt++) {
+                const uint2 v = hrows[tt];
+                lo[tt] = v.x;
+                hi[tt] = v.y;
+            }
+            const uint32_t va = c_subpel_pk[fy][0], vb = c_subpel_pk[fy][1];
 #pragma unroll
-                for (int tt = 0; tt < 8; tt++) acc += c_subpel[fy][tt] * (int)hcol[tt * 8 + cc];
-                const uint32_t v = tap_round(acc);
-                if (cc < 4) o0 |= v << (8 * cc); else o1 |= v << (8 * (cc - 4));
+            for (int half = 0; half < 2; half++) {
+                const uint32_t *rw8 = half ? hi : lo;
+                uint32_t ca[4], cb[4];
+                tr4(rw8[0], rw8[1], rw8[2], rw8[3], ca);
+                tr4(rw8[4], rw8[5], rw8[6], rw8[7], cb);
+                uint32_t word = 0;
+#pragma unroll
+                for (int j = 0; j < 4; j++) word |= tap8(va, vb, fy, ca[j], cb[j]) << (8 * j);
+                if (half) o1 = word; else o0 = word;
             }
         }
         uint8_t *d = w.ty + (ly0 + k) * kFY + lx0;
@@ -2272,6 +2319,7 @@ __device__ void spec_chroma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int
             by = (sby >> 1) + cy0 + (mvy >> 4);
             fx = mvx & 15;
             fy = mvy & 15;
+            const uint32_t ta = c_subpel_pk[fx][0], tb = c_subpel_pk[fx][1];
 #pragma unroll
             for (int h = 0; h < 3; h++) {
                 const int hr = r + 4 * h;
@@ -2283,12 +2331,7 @@ __device__ void spec_chroma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int
                 else ld16c(pl, rcs, cw2, ch2, x0, y, o);
                 uint32_t out = 0;
 #pragma unroll
-                for (int cc = 0; cc < 4; cc++) {
-                    int acc = 0;
-#pragma unroll
-                    for (int tt = 0; tt < 8; tt++) acc += c_subpel[fx][tt] * bytek(o, cc + tt);
-                    out |= tap_round(acc) << (8 * cc);
-                }
+                for (int cc = 0; cc < 4; cc++) out |= tap8(ta, tb, fx, win4(o, cc), win4(o, cc + 4)) << (8 * cc);
                 *reinterpret_cast<uint32_t *>(hb + ((q * 2 + p) * 11 + hr) * 4) = out;
             }
         }
@@ -2298,14 +2341,13 @@ __device__ void spec_chroma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int
         uint32_t o = 0x80808080u;                             /* missing reference: 128 */
         if (pl) {
             o = 0;
-            const uint8_t *hcol = hb + ((q * 2 + p) * 11 + r) * 4;
+            const uint32_t *hrows = reinterpret_cast<const uint32_t *>(hb + ((q * 2 + p) * 11 + r) * 4);
+            uint32_t ca[4], cb[4];
+            tr4(hrows[0], hrows[1], hrows[2], hrows[3], ca);
+            tr4(hrows[4], hrows[5], hrows[6], hrows[7], cb);
+            const uint32_t va = c_subpel_pk[fy][0], vb = c_subpel_pk[fy][1];
 #pragma unroll
-            for (int cc = 0; cc < 4; cc++) {
-                int acc = 0;
-#pragma unroll
-                for (int tt = 0; tt < 8; tt++) acc += c_subpel[fy][tt] * (int)hcol[tt * 4 + cc];
-                o |= tap_round(acc) << (8 * cc);
-            }
+            for (int j = 0; j < 4; j++) o |= tap8(va, vb, fy, ca[j], cb[j]) << (8 * j);
         }
         uint8_t *d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
         if (clw == 4 && !((uintptr_t)d & 3)) {
@@ -3315,6 +3357,17 @@ int cvp9k_upload_dct_basis(const double *basis, int count)
 
 int cvp9k_configure(void)
 {
+    {
+        static const int taps[16][8] = CVP9_SUBPEL_REGULAR_INIT;
+        uint32_t pk[16][2];
+        for (int f = 0; f < 16; f++)
+            for (int h = 0; h < 2; h++) {
+                uint32_t w = 0;
+                for (int t = 0; t < 4; t++) w |= (uint32_t)(uint8_t)(int8_t)taps[f][4 * h + t] << (8 * t);
+                pk[f][h] = w;
+            }
+        if (cudaMemcpyToSymbol(c_subpel_pk, pk, sizeof(pk)) != cudaSuccess) return -1;
+    }
     size_t smem = sizeof(ReconSmem);
     if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_REFCPU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
     if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
