@@ -258,6 +258,19 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms)
     tune_advance(t, e);
 }
 
+/* ── Share of a large step's frames that are packed ─────────────────────── */
+
+int cvp9_pack_share_update(int q, int pipelined, double waited_ms)
+{
+    /* Packing trades host time (reading every dense array) for link time.
+     * Balance the two while steps are pipelined: a submit that had to wait
+     * for its slot found the link (or the GPU) behind, so the host can pack
+     * more; one that did not wait found the host behind, so it packs less.
+     * A caller that waits for each step first gives no signal. */
+    if (pipelined) q += waited_ms > 0.05 ? 1 : -1;
+    return q < 0 ? 0 : q > 16 ? 16 : q;
+}
+
 /* ── Host worker pools ────────────────────────────────────────────────── */
 
 /* Two pools: a small one for staging copies (the per-stream backend, on

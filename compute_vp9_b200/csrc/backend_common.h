@@ -109,6 +109,12 @@ void cvp9_tuner_report(cvp9_tuner_t *t, int idx, cvp9_tcfg_t cfg, float ms);
  * each rounded up to a power of two, so serving steps share buckets. */
 uint64_t cvp9_tune_key(int arith, int frames, uint64_t superblocks);
 
+/* Share of a large step's frames the batch engine packs, in 16ths: one
+ * more after a pipelined submit that waited over 0.05 ms for its step slot
+ * (the link is behind), one fewer after one that did not (the host is);
+ * unchanged when no step was in flight. Clamped to 0..16. */
+int cvp9_pack_share_update(int q, int pipelined, double waited_ms);
+
 /* Host worker threads. cvp9_parallel_for runs fn(ctx, k) for k in
  * [0, ntasks) on a pool of one thread per online CPU up to 16, the caller
  * included ($CVP9_HOST_THREADS overrides), taking tasks itself, and returns

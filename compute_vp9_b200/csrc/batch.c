@@ -34,7 +34,6 @@
 #define ALIGN_UP(x, a) (((x) + (a) - 1) / (a) * (a))
 #define LAT_RING 4096
 #define PACK_AUTO_BYTES (64ull << 20)   /* dense coefficient bytes from which a step packs */
-#define PACK_WAIT_MS    0.05            /* a submit that waited this long for its slot */
 
 typedef struct {
     uint8_t *dev;
@@ -669,14 +668,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         if (b->pack == 1) {
             npack = n;
         } else if (cb >= PACK_AUTO_BYTES) {
-            /* Packing trades host time (reading every dense array) for link
-             * time. Balance the two while steps are pipelined: a submit that
-             * had to wait for its slot found the link (or the GPU) behind, so
-             * the host can pack more; one that did not wait found the host
-             * behind, so it packs less. A caller that waits for each step
-             * first gives no signal and leaves the share as it is. */
-            if (pipelined && waited_ms > PACK_WAIT_MS) { if (b->pack_q < 16) b->pack_q++; }
-            else if (pipelined && b->pack_q > 0) b->pack_q--;
+            b->pack_q = cvp9_pack_share_update(b->pack_q, pipelined, waited_ms);
             npack = (b->pack_q * n + 8) / 16;
         }
         if (npack) {

@@ -127,3 +127,79 @@ def test_parallel_memcpy_copies_every_byte():
     for t in ts:
         t.join()
     assert all(np.array_equal(d, s) for d, s in zip(dsts, srcs))
+
+
+def test_parallel_for_runs_every_task_once():
+    """The host worker pool the batch engine packs frames on: every task
+    index runs exactly once, on more than one thread when the pool has
+    workers, for task counts around the pool size; a second job started
+    while one holds the pool runs its tasks on its own caller."""
+    import threading
+    from compute_vp9_b200 import cuda_lib
+    lib = cuda_lib()
+    CB = C.CFUNCTYPE(None, C.c_void_p, C.c_int)
+    lib.cvp9_parallel_for.argtypes = [C.c_int, CB, C.c_void_p]
+    lib.cvp9_parallel_for.restype = None
+    lib.cvp9_pool_threads.restype = C.c_int
+    threads = lib.cvp9_pool_threads()
+    assert threads >= 1
+    for ntasks in (0, 1, 2, threads - 1, threads, threads + 1, 3 * threads + 5, 200):
+        if ntasks < 0:
+            continue
+        seen, tids = [], set()
+        lock = threading.Lock()
+
+        def task(ctx, k, seen=seen, tids=tids, lock=lock):
+            with lock:
+                seen.append(k)
+                tids.add(threading.get_ident())
+
+        cb = CB(task)
+        lib.cvp9_parallel_for(ntasks, cb, None)
+        assert sorted(seen) == list(range(ntasks)), ntasks
+    # nested use from inside a task: the pool is held, so the inner job runs
+    # serially on the calling worker and still covers every index
+    inner_seen = []
+    inner_lock = threading.Lock()
+
+    def inner(ctx, k):
+        with inner_lock:
+            inner_seen.append(k)
+
+    inner_cb = CB(inner)
+
+    def outer(ctx, k):
+        lib.cvp9_parallel_for(5, inner_cb, None)
+
+    outer_cb = CB(outer)
+    lib.cvp9_parallel_for(4, outer_cb, None)
+    assert sorted(inner_seen) == sorted(list(range(5)) * 4)
+
+
+def test_pack_share_balances_host_and_link():
+    """The share of a large step's frames packed on the host, in 16ths:
+    raised after a pipelined submit that waited for its slot, lowered after
+    one that did not, untouched by callers that wait for every step."""
+    from compute_vp9_b200 import cuda_lib
+    lib = cuda_lib()
+    f = lib.cvp9_pack_share_update
+    f.argtypes = [C.c_int, C.c_int, C.c_double]
+    f.restype = C.c_int
+    assert f(16, 1, 1.0) == 16          # saturates
+    assert f(0, 1, 0.0) == 0
+    assert f(8, 1, 0.2) == 9
+    assert f(8, 1, 0.01) == 7
+    assert f(8, 0, 5.0) == 8            # nothing in flight: no signal
+    # a host that is always behind drains the share, a link that is always
+    # behind fills it, an alternation holds it near where it started
+    q = 16
+    for _ in range(40):
+        q = f(q, 1, 0.0)
+    assert q == 0
+    for _ in range(40):
+        q = f(q, 1, 3.0)
+    assert q == 16
+    q = 10
+    for i in range(41):
+        q = f(q, 1, 3.0 if i % 2 else 0.0)
+    assert 9 <= q <= 10
