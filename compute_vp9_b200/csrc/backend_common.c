@@ -184,7 +184,7 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
         e->idx++;
         if (e->stage == 0) {
             /* inter path: the default was candidate 0; REFCPU also has the
-             * two-kernel split (3) and the split with unrolled 8x8 TXs (4) */
+             * two-kernel split (3) and the split walking 8x8 TXs per TX (4) */
             static const int8_t alts[4] = { 0, 2, 3, 4 };
             if (e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 2)) {
                 e->cur = e->best;

@@ -2041,22 +2041,20 @@ __device__ void fast_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &j
     }
 }
 
-/* fast_residual for N <= 8 with the column loop unrolled: column k is a
- * compile-time index, so the basis row M[k][.] comes as constant operands,
- * and the masks come from ballots of the lanes' own rows (bit (TX, l) of
- * column k's ballot: X[l][k] != 0) instead of scans of the staged tile and
- * per-column shuffles. Same operations in the same order: the columns of
- * the union of the group's nonzero columns, ascending; per column, the rows
- * of the union of its nonzero rows, ascending. */
+/* fast_residual with each group walking its own TX's nonzero columns
+ * (ascending) instead of the union over the warp's groups: the warp loops
+ * as long as its busiest group. Column k differs between groups, so the
+ * basis row M[k][.] is read from the global copy (four 16-byte loads, L1
+ * hits). Same operations and order per TX as fast_residual — the terms the
+ * union adds are exact zeros. */
 template <int N, bool GLOBAL, class S>
-__device__ void fast_residual_u(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int ntx, int lane)
+__device__ void fast_residual_d(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int ntx, int lane)
 {
-    static_assert(N <= 8, "unrolled for the small transforms");
+    static_assert(N == 8, "the 8x8 transform");
     constexpr int G = 32 / N, NN = N * N;
-    constexpr unsigned kSeg = (1u << N) - 1u;
-    constexpr int boff = N == 4 ? 0 : 16;
+    constexpr int boff = 16;
     const int g = lane / N, i = lane % N;
-    const double *Mg = g_dct + boff;     /* lane-varying reads */
+    const double *Mg = g_dct + boff;
     int16_t *X = w.coef + g * (NN + 2);
     uint32_t rv[N / 2];
     int px0, py0;
@@ -2076,14 +2074,17 @@ __device__ void fast_residual_u(S &w, uint8_t *dst, int pitch, const cvp9_job_t 
                 rm |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * k);
             }
         }
+        /* nonzero columns of this lane's TX: OR over its group's lanes */
+        uint32_t cols = rm;
+#pragma unroll
+        for (int o = 1; o < N; o <<= 1) cols |= __shfl_xor_sync(0xffffffffu, cols, o);
         __syncwarp();
         uint8_t *rowp = dst + (py0 + i) * pitch + px0;
         const bool words = !GLOBAL || !((uintptr_t)rowp & 3);
         uint32_t pix[N / 4];
 #pragma unroll
         for (int j4 = 0; j4 < N / 4; j4++) pix[j4] = 0u;
-        const bool anynz = __any_sync(0xffffffffu, rm != 0);   /* every lane: a warp vote */
-        if (GLOBAL && have && anynz) {
+        if (GLOBAL && have && cols) {
             if (words) {
 #pragma unroll
                 for (int j4 = 0; j4 < N / 4; j4++) pix[j4] = reinterpret_cast<const uint32_t *>(rowp)[j4];
@@ -2101,23 +2102,29 @@ __device__ void fast_residual_u(S &w, uint8_t *dst, int pitch, const cvp9_job_t 
         double acc[N];
 #pragma unroll
         for (int j = 0; j < N; j++) acc[j] = 0.0;
-        bool any = false;
+        const bool any = cols != 0;
+        uint32_t left = cols;
+        while (__any_sync(0xffffffffu, left != 0)) {
+            const bool act = left != 0;
+            const int k = act ? __ffs(left) - 1 : 0;
+            left &= left - 1;
+            /* rows of column k of this lane's TX: bit (group, row) of the ballot */
+            const unsigned B = __ballot_sync(0xffffffffu, act && ((rm >> k) & 1u));
+            if (act) {
+                const unsigned rows = (B >> (g * N)) & ((1u << N) - 1u);
+                double t = 0.0;
+                for (unsigned v = rows; v; v &= v - 1) {
+                    const int l = __ffs(v) - 1;
+                    t = __dadd_rn(t, __dmul_rn(__ldg(Mg + l * N + i), (double)X[l * N + k]));
+                }
+                const double2 *Mr = reinterpret_cast<const double2 *>(Mg + k * N);
 #pragma unroll
-        for (int k = 0; k < N; k++) {
-            const unsigned B = __ballot_sync(0xffffffffu, (rm >> k) & 1u);
-            if (!B) continue;
-            any = true;
-            unsigned rows = B;
-#pragma unroll
-            for (int s2 = 16; s2 >= N; s2 >>= 1) rows |= rows >> s2;
-            rows &= kSeg;
-            double t = 0.0;
-            for (unsigned v = rows; v; v &= v - 1) {
-                const int l = __ffs(v) - 1;
-                t = __dadd_rn(t, __dmul_rn(__ldg(Mg + l * N + i), (double)X[l * N + k]));
+                for (int j2 = 0; j2 < N / 2; j2++) {
+                    const double2 m = __ldg(Mr + j2);
+                    acc[2 * j2] = __dadd_rn(acc[2 * j2], __dmul_rn(t, m.x));
+                    acc[2 * j2 + 1] = __dadd_rn(acc[2 * j2 + 1], __dmul_rn(t, m.y));
+                }
             }
-#pragma unroll
-            for (int j = 0; j < N; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, c_dct[boff + k * N + j]));
         }
         if (any && have) {
 #pragma unroll
@@ -2580,9 +2587,10 @@ __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int s
 /* REFCPU luma residual of a set-up superblock (fast_sb_setup): one pass
  * per TX size present, TXs counted on the frame-clamped block
  * (vp9_reconstruct.c:338-340), added to the predicted rows at dst. U8: 8x8
- * TXs through the unrolled fast_residual_u (fewer instructions, much more
- * code: it pays on content of 8x8 TXs alone and costs on mixed sizes, where
- * the warps of an SM run every size's code at once). */
+ * TXs through fast_residual_d, each TX walking its own nonzero columns
+ * (measured faster on both 8x8-only and mixed content; an unrolled
+ * union-of-columns form, tried before it, cut instructions on 8x8 content
+ * but its code size cost more on mixed TX sizes). */
 template <bool GLOBAL, bool U8, class S>
 __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int nb, int lane)
 {
@@ -2614,7 +2622,7 @@ __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_j
         switch (txl) {
         case 0: fast_residual<4, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
         case 1:
-            if (U8) fast_residual_u<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
+            if (U8) fast_residual_d<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
             else fast_residual<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
             break;
         case 2: fast_residual<16, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
@@ -2870,6 +2878,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     }
 }
 
+/* U8: the 8x8 transform through fast_residual_d (inter path 4) */
 template <int MINB, bool U8>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_t *__restrict__ jobs,
                                                             const uint32_t *__restrict__ tickets,

@@ -62,7 +62,7 @@ typedef struct {
                               * (96 registers), 2 the same at 80 registers,
                               * 3 (REFCPU) prediction and residual as two
                               * kernels at 96 and 64 registers, 4 the same with
-                              * the 8x8 transform unrolled                       */
+                              * 8x8 TXs walked TX by TX                          */
     int      lf_tile_h;      /* loop filter: 16 register strips (8x16 per thread),
                               * 32 shared-memory tiles (64x32 per CTA)           */
     int      half_width;     /* 1: wavefront kernel on half the resident CTAs    */

@@ -70,7 +70,7 @@ def test_parity_without_inter_fast_path(name, profile, monkeypatch):
 @pytest.mark.parametrize("name", list(CASES))
 def test_refcpu_parity_prediction_residual_split(name, variant, monkeypatch):
     """REFCPU's two-kernel inter path (k_pred into the frame, then k_resid in
-    place; CVP9_INTER_FAST=3, and 4 with the 8x8 transform unrolled) gives
+    place; CVP9_INTER_FAST=3, and 4 walking 8x8 TXs per TX) gives
     the oracle's bytes on every case."""
     monkeypatch.setenv("CVP9_INTER_FAST", variant)
     run_case(REFCPU, *CASES[name])

@@ -56,7 +56,7 @@ def test_coordinate_descent_order_and_choice(lib):
         if not seen or seen[-1] != cfg:
             seen.append(cfg)
     # default, the other four inter paths (REFCPU has the two-kernel split,
-    # with and without unrolled 8x8 TXs), then lf tiles, then wavefront
+    # in two forms), then lf tiles, then wavefront
     # width, each varied from the best
     assert seen == [(1, 0, 0), (0, 0, 0), (2, 0, 0), (3, 0, 0), (4, 0, 0), (2, 1, 0), (2, 0, 1)]
     idx, cfg = step(lib, t, 7, lambda c: 9.0)
