@@ -87,6 +87,20 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+/* 8 and 4 bytes (both sides aligned to the size) */
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(sa), "l"(gmem) : "memory");
+}
+/* all but the newest group have landed */
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 
 /* ── 32-bit wrap-around integer for the shader butterflies ───────────────── */
 struct wi {
@@ -1811,7 +1825,7 @@ __device__ __forceinline__ void fast_pred_issue(const S &w, const PredDst &D, co
             /* luma rows are followed by the chroma planes: reads past a row
              * end stay inside the frame; the plane starts 8-byte aligned, so
              * with ix >= 0 they never start before it */
-            const bool hin = ix >= 0 && ix + lw < rw;
+            const bool hin = ix >= 0 && ix + lw < rw && rw >= 16;   /* 16-byte reads stay in the frame */
             if (hin && y0 >= 0 && y0 < rh) ld9d(rp + (size_t)y0 * rw + ix, l0, m0, h0);
             else ld9c(rp, rw, rh, ix, y0, l0, m0, h0);
             if (kk == 7) {
@@ -1827,7 +1841,7 @@ __device__ __forceinline__ void fast_pred_issue(const S &w, const PredDst &D, co
                 K.fx = cpx8 & 7;
                 K.fy = cpy8 & 7;
                 /* a further chroma row below the one read: word reads stay inside */
-                const bool chin = cix >= 0 && cix + clw < crw;
+                const bool chin = cix >= 0 && cix + clw < crw && rcs >= 8;   /* 8-byte reads stay in the plane */
                 if (chin && y1 >= 0 && y1 + 1 < crh) ld5w(pl + (size_t)y1 * rcs + cix, cl0, ch0);
                 else ld5c(pl, rcs, crw, crh, cix, y1, cl0, ch0);
                 if (r == 3) {
@@ -2795,6 +2809,174 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
     }
 }
 
+/* ── Prediction with its reads one pass ahead (k_pred) ──────────────────
+ * The passes of fast_pred_issue / fast_*_finish, but each lane's reference
+ * rows go to a shared-memory slot by cp.async, and the next iteration's
+ * rows are requested before the current one is filtered, so a warp has two
+ * iterations' reads in flight instead of waiting on each. A lane's slot:
+ * its luma row (16 bytes around the 9 it needs), the row below (the chunk's
+ * last lane only), its chroma row (8 bytes around 5) and the row below
+ * (the plane's last lane only). The rows below of the other lanes are their
+ * neighbours' rows, read from the neighbour's slot. Rows that need clamped
+ * samples are read at once, byte by byte, and stored already extracted. */
+constexpr int kSlot = 48, kSlotLB = 16, kSlotCA = 32, kSlotCB = 40;
+
+struct PredGeo {                 /* one lane's pass: what the filter step needs */
+    uint8_t *dl, *dc;            /* luma / chroma destination (frame) */
+    uint32_t fl;                 /* lw | fx << 4 | fy << 7 | act << 10 | ref << 11 | o0 << 12 | o1 << 15 */
+    uint32_t fc;                 /* clw | fx << 3 | fy << 6 | act << 9 | ref << 10 | o0 << 11 | o1 << 13 */
+};
+
+/* 9 bytes at offset o (0..7) of the 16 at q (shared memory, 16-byte aligned) */
+__device__ __forceinline__ void slot9(const uint8_t *q, unsigned o, uint32_t &lo, uint32_t &mid, uint32_t &hi)
+{
+    const uint4 v = *reinterpret_cast<const uint4 *>(q);
+    const bool up = o >= 4;
+    const unsigned sh = 8u * (o & 3u);
+    const uint32_t w0 = up ? v.y : v.x, w1 = up ? v.z : v.y, w2 = up ? v.w : v.z;
+    lo = __funnelshift_r(w0, w1, sh);
+    mid = __funnelshift_r(w1, w2, sh);
+    hi = w2 >> sh;
+}
+
+/* 5 bytes at offset o (0..3) of the 8 at q (shared memory, 8-byte aligned) */
+__device__ __forceinline__ void slot5(const uint8_t *q, unsigned o, uint32_t &lo, uint32_t &hi)
+{
+    const uint2 v = *reinterpret_cast<const uint2 *>(q);
+    const unsigned sh = 8u * o;
+    lo = __funnelshift_r(v.x, v.y, sh);
+    hi = v.y >> sh;
+}
+
+/* Geometry of chunk c for this lane (as fast_pred_issue) and its row reads,
+ * into slot (this lane's, this pass's). */
+template <class S>
+__device__ __forceinline__ void pred_request(const S &w, const PredDst &D, const cvp9_job_t &job, int c, int lane,
+                                             int nchunks, int sbx, int sby, uint8_t *slot, PredGeo &G)
+{
+    G.fl = 0u;
+    G.fc = 0u;
+    if (c >= nchunks) return;
+    const int kk = lane & 7, p = (lane >> 2) & 1, r = lane & 3;
+    FastBlk fb;
+    int lx0, ly0, lw, lh, cx0, cy0, clw, clh;
+    fast_chunk(w, c, fb, lx0, ly0, lw, lh, cx0, cy0, clw, clh);
+    const int slotr = fb_slot(fb);
+    const uint8_t *rp = nullptr;
+    int rw = 0, rh = 0;
+    if (slotr < 8) {
+        const cvp9_ref_t &R = job.ref[slotr];
+        rp = R.plane;
+        rw = R.w;
+        rh = R.h;
+    }
+    const int mvx = (int16_t)(fb.mv & 0xffffu), mvy = (int16_t)(fb.mv >> 16);
+    G.dl = D.y + (ly0 + kk) * D.py + lx0;
+    G.dc = (p ? D.v : D.u) + (cy0 + r) * D.pc + cx0;
+    uint32_t fl = (uint32_t)lw | (kk < lh ? 1u << 10 : 0u);
+    uint32_t fc = (uint32_t)max(clw, 0) | (r < clh && clw > 0 ? 1u << 9 : 0u);
+    if (rp) {
+        const int px8 = (sbx + lx0) * 8 + mvx, py8 = (sby + ly0) * 8 + mvy;
+        const int ix = px8 >> 3, y0 = (py8 >> 3) + kk;
+        fl |= (uint32_t)(px8 & 7) << 4 | (uint32_t)(py8 & 7) << 7 | 1u << 11;
+        /* luma rows are followed by the chroma planes: 16-byte reads past a
+         * row end stay inside the frame; the plane starts 8-byte aligned */
+        const bool hin = ix >= 0 && ix + lw < rw && rw >= 16;   /* 16-byte reads stay in the frame */
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            if (e == 1 && kk != 7) break;            /* the row below: the chunk's last lane */
+            const int y = y0 + e;
+            uint8_t *dst = slot + (e ? kSlotLB : 0);
+            if (hin && y >= 0 && y < rh) {
+                const uint8_t *a = rp + (size_t)y * rw + ix;
+                const uint8_t *a8 = reinterpret_cast<const uint8_t *>((uintptr_t)a & ~(uintptr_t)7);
+                cp_async8(dst, a8);
+                cp_async8(dst + 8, a8 + 8);
+                fl |= (uint32_t)((uintptr_t)a & 7) << (12 + 3 * e);
+            } else {
+                uint32_t lo, mid, hi;
+                ld9c(rp, rw, rh, ix, y, lo, mid, hi);
+                *reinterpret_cast<uint4 *>(dst) = make_uint4(lo, mid, hi, 0u);
+            }
+        }
+        /* the row below of the other lanes is their neighbour's row: the
+         * filter step needs its offset, from the same column and y0 + 1 */
+        if (kk != 7 && hin && y0 + 1 >= 0 && y0 + 1 < rh)
+            fl |= (uint32_t)(((uintptr_t)rp + (size_t)(y0 + 1) * rw + ix) & 7) << 15;
+        if (clw > 0) {
+            const int rcs = (rw + 1) >> 1, crw = rw >> 1, crh = rh >> 1;
+            const uint8_t *pl = rp + (size_t)rw * rh + (p ? (size_t)rcs * ((rh + 1) >> 1) : 0);
+            const int cpx8 = ((sbx >> 1) + cx0) * 8 + mvx / 2, cpy8 = ((sby >> 1) + cy0) * 8 + mvy / 2;
+            const int cix = cpx8 >> 3, y1 = (cpy8 >> 3) + r;
+            fc |= (uint32_t)(cpx8 & 7) << 3 | (uint32_t)(cpy8 & 7) << 6 | 1u << 10;
+            /* a further chroma row below the one read: reads stay inside */
+            const bool chin = cix >= 0 && cix + clw < crw && rcs >= 8;   /* 8-byte reads stay in the plane */
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                if (e == 1 && r != 3) break;         /* the row below: the plane's last lane */
+                const int y = y1 + e;
+                uint8_t *dst = slot + (e ? kSlotCB : kSlotCA);
+                if (chin && y >= 0 && y + 1 < crh) {
+                    const uint8_t *a = pl + (size_t)y * rcs + cix;
+                    const uint8_t *a4 = reinterpret_cast<const uint8_t *>((uintptr_t)a & ~(uintptr_t)3);
+                    cp_async4(dst, a4);
+                    cp_async4(dst + 4, a4 + 4);
+                    fc |= (uint32_t)((uintptr_t)a & 3) << (11 + 2 * e);
+                } else {
+                    uint32_t lo, hi;
+                    ld5c(pl, rcs, crw, crh, cix, y, lo, hi);
+                    *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+                }
+            }
+            if (r != 3 && chin && y1 + 1 >= 0 && y1 + 2 < crh)
+                fc |= (uint32_t)(((uintptr_t)pl + (size_t)(y1 + 1) * rcs + cix) & 3) << 13;
+        }
+    }
+    G.fl = fl;
+    G.fc = fc;
+}
+
+/* The filter step of a pass whose rows have landed: base is the warp's
+ * slots for this pass (lane i at base + i * kSlot). */
+__device__ __forceinline__ void pred_filter(const PredGeo &G, const uint8_t *base, int lane)
+{
+    const int kk = lane & 7, r = lane & 3;
+    const uint8_t *own = base + lane * kSlot;
+    if (G.fl & (1u << 10)) {
+        uint32_t o0 = 0x7f7f7f7fu, o1 = 0x7f7f7f7fu;     /* missing reference: 127 */
+        if (G.fl & (1u << 11)) {
+            uint32_t lo0, mid0, hi0, lo1, mid1, hi1;
+            slot9(own, (G.fl >> 12) & 7u, lo0, mid0, hi0);
+            slot9(kk == 7 ? own + kSlotLB : own + kSlot, (G.fl >> 15) & 7u, lo1, mid1, hi1);
+            bilinear8(lo0, mid0, hi0, lo1, mid1, hi1, (G.fl >> 4) & 7, (G.fl >> 7) & 7, o0, o1);
+        }
+        const int lw = G.fl & 15u;
+        if (lw == 8 && !((uintptr_t)G.dl & 3)) {
+            reinterpret_cast<uint32_t *>(G.dl)[0] = o0;
+            reinterpret_cast<uint32_t *>(G.dl)[1] = o1;
+        } else {
+#pragma unroll
+            for (int x = 0; x < 8; x++) if (x < lw) G.dl[x] = (uint8_t)((x < 4 ? o0 : o1) >> (8 * (x & 3)));
+        }
+    }
+    if (G.fc & (1u << 9)) {
+        uint32_t o = 0x7f7f7f7fu;
+        if (G.fc & (1u << 10)) {
+            uint32_t lo0, hi0, lo1, hi1;
+            slot5(own + kSlotCA, (G.fc >> 11) & 3u, lo0, hi0);
+            slot5(r == 3 ? own + kSlotCB : own + kSlot + kSlotCA, (G.fc >> 13) & 3u, lo1, hi1);
+            o = bilinear4(lo0, hi0, lo1, hi1, (G.fc >> 3) & 7, (G.fc >> 6) & 7);
+        }
+        const int clw = G.fc & 7u;
+        if (clw == 4 && !((uintptr_t)G.dc & 3)) {
+            *reinterpret_cast<uint32_t *>(G.dc) = o;
+        } else {
+#pragma unroll
+            for (int x = 0; x < 4; x++) if (x < clw) G.dc[x] = (uint8_t)(o >> (8 * x));
+        }
+    }
+}
+
 /* ── REFCPU superblocks in two kernels ──────────────────────────────────
  * k_inter's REFCPU work split in two leaner kernels. k_inter holds a
  * superblock's tiles, its coefficient staging and the transform's registers
@@ -2805,6 +2987,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
  * k_inter, so the same bytes; the frame's luma makes one more round trip
  * through L2/HBM. */
 struct __align__(16) PredSmem {                   /* k_pred, one per warp */
+    uint8_t  stage[2 * 2 * 32 * kSlot];           /* 2 iterations x 2 passes x 32 lane slots */
     FastBlk  blk[64];
     uint32_t cells[8];
     uint16_t choff[65];
@@ -2866,15 +3049,33 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     uint8_t *V = U + (size_t)CW * CH;
     const size_t coff = (size_t)(sby >> 1) * CW + (sbx >> 1);
     const PredDst D = { Y + (size_t)sby * W + sbx, U + coff, V + coff, W, CW };
-    for (int c0 = 0; c0 < nchunks; c0 += 8) {
-        FastLuma a, b;
-        FastChroma ca, cb;
-        fast_pred_issue(w, D, job, c0 + (lane >> 3), lane, nchunks, sbx, sby, a, ca);
-        fast_pred_issue(w, D, job, c0 + 4 + (lane >> 3), lane, nchunks, sbx, sby, b, cb);
-        fast_luma_finish(a);
-        fast_luma_finish(b);
-        fast_chroma_finish(ca);
-        fast_chroma_finish(cb);
+    /* two passes of four chunks per iteration; the next iteration's rows
+     * are requested before this one's are filtered */
+    const int nit = (nchunks + 7) >> 3;
+    auto slots = [&](int st, int pass) { return w.stage + (st * 2 + pass) * 32 * kSlot; };
+    PredGeo a, b, na, nx;
+    na.fl = na.fc = nx.fl = nx.fc = 0u;
+    na.dl = na.dc = nx.dl = nx.dc = nullptr;
+    pred_request(w, D, job, lane >> 3, lane, nchunks, sbx, sby, slots(0, 0) + lane * kSlot, a);
+    pred_request(w, D, job, 4 + (lane >> 3), lane, nchunks, sbx, sby, slots(0, 1) + lane * kSlot, b);
+    cp_async_commit();
+    for (int it = 0; it < nit; it++) {
+        const int cur = it & 1;
+        if (it + 1 < nit) {
+            const int c1 = (it + 1) * 8;
+            pred_request(w, D, job, c1 + (lane >> 3), lane, nchunks, sbx, sby, slots(cur ^ 1, 0) + lane * kSlot, na);
+            pred_request(w, D, job, c1 + 4 + (lane >> 3), lane, nchunks, sbx, sby, slots(cur ^ 1, 1) + lane * kSlot, nx);
+            cp_async_commit();
+            cp_async_wait_prev();
+        } else {
+            cp_async_wait_all();
+        }
+        __syncwarp();
+        pred_filter(a, slots(cur, 0), lane);
+        pred_filter(b, slots(cur, 1), lane);
+        __syncwarp();                    /* the stage is refilled next iteration */
+        a = na;
+        b = nx;
     }
 }
 
