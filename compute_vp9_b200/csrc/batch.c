@@ -676,8 +676,8 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
                 s->pk_off[i] = tot;
                 if (pfs[i]->num_coeffs) tot += ALIGN_UP(cvp9_pack_bound_words(pfs[i]->num_coeffs), 64);
             }
-            if (tot) {
-                if ((err = grow_host(b, (void **)&s->h_pack, &s->h_pack_cap, tot * 4))) return err;
+            /* no page-locked room for the packed frames: they go up dense */
+            if (tot && grow_host(b, (void **)&s->h_pack, &s->h_pack_cap, tot * 4) == CVP9_OK) {
                 pack_job_t pj = { b->arith, pfs, s->h_pack, s->pk_off, s->pk_words };
                 const double tp0 = cvp9_now();
                 cvp9_parallel_for(npack, pack_task, &pj);
