@@ -290,8 +290,14 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def __enter__(self):
+        # the first nvidia-smi of a fresh box is slow and was seen to stall
+        # the GPU work beside it: take one sample before anything is timed
+        self._stop.clear()
+        t0 = time.perf_counter()
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        while not self.samples and self._t.is_alive() and time.perf_counter() - t0 < 10.0:
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
