@@ -183,10 +183,11 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
     for (;;) {
         e->idx++;
         if (e->stage == 0) {
-            /* inter path: the default was candidate 0; REFCPU also has the
-             * two-kernel split (3) and the split walking 8x8 TXs per TX (4) */
+            /* inter path: the default was candidate 0; then the general
+             * kernel alone, k_inter at 80 registers, the two-kernel split
+             * and (REFCPU) the split walking 8x8 TXs per TX */
             static const int8_t alts[4] = { 0, 2, 3, 4 };
-            if (e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 2)) {
+            if (e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 3)) {
                 e->cur = e->best;
                 e->cur.inter = alts[e->idx - 1];
                 break;

@@ -1772,10 +1772,14 @@ __device__ __forceinline__ void fast_chunk(const S &w, int c, FastBlk &fb, int &
 }
 
 /* Where a superblock's prediction lands: its luma and chroma origins and
- * pitches (the warp's shared tiles, or the frame itself). */
+ * pitches (the warp's shared tiles, or the frame itself), and the extent
+ * inside the frame from those origins (luma vw x vh, chroma cvw x cvh):
+ * SPEC TXs follow the MI grid and can reach past the frame edge, where
+ * nothing is written. */
 struct PredDst {
     uint8_t *y, *u, *v;
     int      py, pc;
+    int      vw, vh, cvw, cvh;
 };
 
 /* One lane's luma row (chunk c, row lane%8) and chroma row (plane
@@ -2236,7 +2240,9 @@ __device__ __forceinline__ void tr4(uint32_t a, uint32_t b, uint32_t c, uint32_t
  * c0 + lane/8, k = lane%8). Horizontal 8-tap rows k and k+8 of each chunk's
  * 15-row window go to shared rows (rounded, clipped to 8 bits), then lane k
  * filters output row k vertically. Fetches clamp into the reference. */
-__device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int nchunks, int sbx, int sby, int lane)
+template <class S>
+__device__ void spec_luma_pass(S &w, const PredDst &D, const cvp9_job_t &job, int c0, int nchunks, int sbx, int sby,
+                               int lane)
 {
     uint8_t *hb = reinterpret_cast<uint8_t *>(w.coef);        /* 4 chunks x 15 rows x 8 */
     const int q = lane >> 3, k = lane & 7, c = c0 + q;
@@ -2303,8 +2309,8 @@ __device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int n
                 if (half) o1 = word; else o0 = word;
             }
         }
-        uint8_t *d = w.ty + (ly0 + k) * kFY + lx0;
-        if (lw == 8) {
+        uint8_t *d = D.y + (ly0 + k) * D.py + lx0;
+        if (lw == 8 && !((uintptr_t)d & 3)) {
             reinterpret_cast<uint32_t *>(d)[0] = o0;
             reinterpret_cast<uint32_t *>(d)[1] = o1;
         } else {
@@ -2318,7 +2324,9 @@ __device__ void spec_luma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int n
 /* Chroma prediction of four chunks, both planes: lane = (chunk c0 + lane/8,
  * plane, r = lane%4); the chroma MV is read as 1/16 chroma pel (16 phases),
  * fetches clamp into the ceil-half planes. */
-__device__ void spec_chroma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int nchunks, int sbx, int sby, int lane)
+template <class S>
+__device__ void spec_chroma_pass(S &w, const PredDst &D, const cvp9_job_t &job, int c0, int nchunks, int sbx, int sby,
+                                 int lane)
 {
     uint8_t *hb = reinterpret_cast<uint8_t *>(w.coef) + 480;  /* 4 chunks x 2 planes x 11 rows x 4 */
     const int q = lane >> 3, p = (lane >> 2) & 1, r = lane & 3, c = c0 + q;
@@ -2370,7 +2378,7 @@ __device__ void spec_chroma_pass(FastSmem &w, const cvp9_job_t &job, int c0, int
 #pragma unroll
             for (int j = 0; j < 4; j++) o |= tap8(va, vb, fy, ca[j], cb[j]) << (8 * j);
         }
-        uint8_t *d = (p ? w.tv : w.tu) + (cy0 + r) * kFC + cx0;
+        uint8_t *d = (p ? D.v : D.u) + (cy0 + r) * D.pc + cx0;
         if (clw == 4 && !((uintptr_t)d & 3)) {
             *reinterpret_cast<uint32_t *>(d) = o;
         } else {
@@ -2409,15 +2417,15 @@ __device__ __forceinline__ SpecTx spec_tx_layout(const FastBlk &b, int p)
  * row pass, lane = (TX, row i): butterfly along the row, final shift 4/5/6,
  * add and clamp into the tile (:680-789). A group with no nonzero
  * coefficient adds nothing and is skipped. */
-template <int N>
-__device__ void spec_fast_residual(FastSmem &w, const cvp9_job_t &job, int P, int ntx, int lane)
+template <int N, bool GLOBAL, class S>
+__device__ void spec_fast_residual(S &w, const PredDst &D, const cvp9_job_t &job, int P, int ntx, int lane)
 {
     constexpr int G = 32 / N, NN = N * N;
     const int g = lane / N, i = lane % N;
     int16_t *X = w.coef + g * NN;
     int32_t *T = reinterpret_cast<int32_t *>(w.coef) + g * NN;
-    uint8_t *tile = P == 0 ? w.ty : (P == 1 ? w.tu : w.tv);
-    const int pitch = P == 0 ? kFY : kFC;
+    uint8_t *tile = P == 0 ? D.y : (P == 1 ? D.u : D.v);
+    const int pitch = P == 0 ? D.py : D.pc;
     const int sh = N == 4 ? 4 : (N == 8 ? 5 : 6);
     for (int q0 = 0; q0 < ntx; q0 += G) {
         const int q = q0 + g;
@@ -2465,17 +2473,36 @@ __device__ void spec_fast_residual(FastSmem &w, const cvp9_job_t &job, int P, in
 #pragma unroll
                 for (int k = 0; k < N; k++) v[k] = wi(T[i * N + k]);
                 idct_n(v, N);
-                uint32_t *row = reinterpret_cast<uint32_t *>(tile + (py0 + i) * pitch + px0);
+                uint8_t *rowp = tile + (py0 + i) * pitch + px0;
+                const int vw = P == 0 ? D.vw : D.cvw, vh = P == 0 ? D.vh : D.cvh;
+                const int xin = vw - px0;            /* samples of the row inside the frame */
+                const bool rowin = py0 + i < vh;
+                const bool words = (!GLOBAL || !((uintptr_t)rowp & 3)) && xin >= N;
 #pragma unroll
                 for (int j4 = 0; j4 < N / 4; j4++) {
-                    const uint32_t word = row[j4];
+                    if (!rowin || 4 * j4 >= xin) continue;
+                    uint32_t word;
+                    if (words) {
+                        word = reinterpret_cast<const uint32_t *>(rowp)[j4];
+                    } else {
+                        word = 0;
+#pragma unroll
+                        for (int e = 0; e < 4; e++)
+                            if (4 * j4 + e < xin) word |= (uint32_t)rowp[4 * j4 + e] << (8 * e);
+                    }
                     uint32_t outw = 0;
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const int r = ((int)((unsigned)v[j4 * 4 + e].v + (1u << (sh - 1)))) >> sh;
                         outw |= (uint32_t)clampi((int)((word >> (8 * e)) & 0xffu) + r, 0, 255) << (8 * e);
                     }
-                    row[j4] = outw;
+                    if (words) {
+                        reinterpret_cast<uint32_t *>(rowp)[j4] = outw;
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 4; e++)
+                            if (4 * j4 + e < xin) rowp[4 * j4 + e] = (uint8_t)(outw >> (8 * e));
+                    }
                 }
             }
         }
@@ -2646,6 +2673,50 @@ __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_j
     }
 }
 
+/* SPEC residual of a set-up superblock: one pass per (plane, TX size)
+ * present, every plane in the tile parser's MI-clipped layout, added to the
+ * predicted planes at D. */
+template <bool GLOBAL, class S>
+__device__ void fast_spec_residual(S &w, const PredDst &D, const cvp9_job_t &job, int nb, int lane)
+{
+    for (int P = 0; P < 3; P++) {
+        unsigned sizes = 0;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int i = lane + 32 * r;
+            if (i < nb && !fb_skip(w.blk[i])) sizes |= 1u << spec_tx_layout(w.blk[i], P).txl;
+        }
+        sizes = __reduce_or_sync(0xffffffffu, sizes);
+        for (unsigned sz = sizes; sz; sz &= sz - 1) {
+            const int txl = __ffs(sz) - 1;
+            int cnt[2] = { 0, 0 };
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const int i = lane + 32 * r;
+                if (i < nb) {
+                    const FastBlk fb = w.blk[i];
+                    if (fb_skip(fb)) continue;
+                    const SpecTx L = spec_tx_layout(fb, P);
+                    if (L.txl == txl) cnt[r] = L.nx * L.ny;
+                }
+            }
+            const int x0 = warp_incl_scan(cnt[0], lane), x1 = warp_incl_scan(cnt[1], lane);
+            const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
+            const int e0 = x0 - cnt[0], e1 = tot0 + x1 - cnt[1];
+            const int ntx = tot0 + tot1;    /* at most 256: the TXs tile the SB's plane */
+            if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
+            if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
+            __syncwarp();
+            switch (txl) {
+            case 0: spec_fast_residual<4, GLOBAL>(w, D, job, P, ntx, lane); break;
+            case 1: spec_fast_residual<8, GLOBAL>(w, D, job, P, ntx, lane); break;
+            default: spec_fast_residual<16, GLOBAL>(w, D, job, P, ntx, lane); break;   /* 32 went general */
+            }
+            __syncwarp();
+        }
+    }
+}
+
 /* MINB: CTAs per SM the register allocation is sized for (5: up to 96
  * registers, no spills; 6: 80 registers, a few spilled). */
 template <int A, int MINB>
@@ -2678,14 +2749,15 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
      * plane, row). Two luma and two chroma passes are in flight: all four
      * issue their loads before any computes. */
     if (A == CVP9_ARITH_SPEC) {
-        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_luma_pass(w, job, c0, nchunks, sbx, sby, lane);
-        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_chroma_pass(w, job, c0, nchunks, sbx, sby, lane);
+        const PredDst DS = { w.ty, w.tu, w.tv, kFY, kFC, 64, 64, 32, 32 };
+        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_luma_pass(w, DS, job, c0, nchunks, sbx, sby, lane);
+        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_chroma_pass(w, DS, job, c0, nchunks, sbx, sby, lane);
         nchunks = 0;                      /* the REFCPU passes below do nothing */
     }
     for (int c0 = 0; c0 < nchunks; c0 += 8) {
         FastLuma a, b;
         FastChroma ca, cb;
-        const PredDst D = { w.ty, w.tu, w.tv, kFY, kFC };
+        const PredDst D = { w.ty, w.tu, w.tv, kFY, kFC, 64, 64, 32, 32 };
         fast_pred_issue(w, D, job, c0 + (lane >> 3), lane, nchunks, sbx, sby, a, ca);
         fast_pred_issue(w, D, job, c0 + 4 + (lane >> 3), lane, nchunks, sbx, sby, b, cb);
         fast_luma_finish(a);
@@ -2699,55 +2771,9 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_inter(const cvp9_job_
      * with TXs counted on the frame-clamped block; SPEC every plane in the
      * tile parser's MI-clipped layout */
     if (A == CVP9_ARITH_REFCPU) fast_refcpu_residual<false, false>(w, w.ty, kFY, job, nb, lane);
-    for (int P = 0; P < (A == CVP9_ARITH_SPEC ? 3 : 0); P++) {
-        unsigned sizes = 0;
-#pragma unroll
-        for (int r = 0; r < 2; r++) {
-            const int i = lane + 32 * r;
-            if (i < nb && !fb_skip(w.blk[i]))
-                sizes |= 1u << (A == CVP9_ARITH_SPEC ? spec_tx_layout(w.blk[i], P).txl : fb_txl(w.blk[i]));
-        }
-        sizes = __reduce_or_sync(0xffffffffu, sizes);
-        for (unsigned sz = sizes; sz; sz &= sz - 1) {
-            const int txl = __ffs(sz) - 1, n = 4 << txl;
-            int cnt[2] = { 0, 0 };
-#pragma unroll
-            for (int r = 0; r < 2; r++) {
-                const int i = lane + 32 * r;
-                if (i < nb) {
-                    const FastBlk fb = w.blk[i];
-                    if (fb_skip(fb)) continue;
-                    if (A == CVP9_ARITH_SPEC) {
-                        const SpecTx L = spec_tx_layout(fb, P);
-                        if (L.txl == txl) cnt[r] = L.nx * L.ny;
-                    } else if (fb_txl(fb) == txl) {
-                        cnt[r] = (fb_cw(fb) / n) * (fb_ch(fb) / n);
-                    }
-                }
-            }
-            const int x0 = warp_incl_scan(cnt[0], lane), x1 = warp_incl_scan(cnt[1], lane);
-            const int tot0 = __shfl_sync(0xffffffffu, x0, 31), tot1 = __shfl_sync(0xffffffffu, x1, 31);
-            const int e0 = x0 - cnt[0], e1 = tot0 + x1 - cnt[1];
-            const int ntx = tot0 + tot1;    /* at most 256: the TXs tile the SB's plane */
-            if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
-            if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
-            __syncwarp();
-            if (A == CVP9_ARITH_SPEC) {
-                switch (txl) {
-                case 0: spec_fast_residual<4>(w, job, P, ntx, lane); break;
-                case 1: spec_fast_residual<8>(w, job, P, ntx, lane); break;
-                default: spec_fast_residual<16>(w, job, P, ntx, lane); break;   /* 32 went general */
-                }
-            } else {
-                switch (txl) {
-                case 0: fast_residual<4, false>(w, w.ty, kFY, job, ntx, lane); break;
-                case 1: fast_residual<8, false>(w, w.ty, kFY, job, ntx, lane); break;
-                case 2: fast_residual<16, false>(w, w.ty, kFY, job, ntx, lane); break;
-                default: fast_residual<32, false>(w, w.ty, kFY, job, ntx, lane); break;
-                }
-            }
-            __syncwarp();
-        }
+    if (A == CVP9_ARITH_SPEC) {
+        const PredDst D = { w.ty, w.tu, w.tv, kFY, kFC, 64, 64, 32, 32 };
+        fast_spec_residual<false>(w, D, job, nb, lane);
     }
 
     /* 5. write the tile (clipped to the frame) and release the SB */
@@ -2987,7 +3013,10 @@ __device__ __forceinline__ void pred_filter(const PredGeo &G, const uint8_t *bas
  * k_inter, so the same bytes; the frame's luma makes one more round trip
  * through L2/HBM. */
 struct __align__(16) PredSmem {                   /* k_pred, one per warp */
-    uint8_t  stage[2 * 2 * 32 * kSlot];           /* 2 iterations x 2 passes x 32 lane slots */
+    union {
+        uint8_t stage[2 * 2 * 32 * kSlot];        /* REFCPU: 2 iterations x 2 passes x 32 lane slots */
+        int16_t coef[2 * 32 * kSlot];             /* SPEC: the filtered rows of the 8-tap passes */
+    };
     FastBlk  blk[64];
     uint32_t cells[8];
     uint16_t choff[65];
@@ -3021,7 +3050,7 @@ static_assert(offsetof(ResidSmem, coef) % 16 == 0, "coefficient rows are written
  * and 1.10 for 80/80). */
 constexpr int kPredMinB = 5, kResidMinB = 8;
 
-template <int MINB>
+template <int A, int MINB>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t *__restrict__ jobs,
                                                            const uint32_t *__restrict__ tickets,
                                                            uint32_t n_tickets, uint32_t *__restrict__ general)
@@ -3037,7 +3066,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     const int sbr = sb / job.sb_cols, sbc = sb - sbr * job.sb_cols;
     const int sbx = sbc * 64, sby = sbr * 64;
     int nb;
-    const int nchunks = fast_sb_setup<CVP9_ARITH_REFCPU>(w, job, sb, sbx, sby, lane, nb);
+    const int nchunks = fast_sb_setup<A>(w, job, sb, sbx, sby, lane, nb);
     if (lane == 0) general[t] = nchunks < 0 ? 1u : 0u;
     if (nchunks < 0) {
         if (lane == 0) atomicAdd(general + 2 * n_tickets + 1, 1u);   /* k_compact skips when 0 */
@@ -3048,7 +3077,13 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     uint8_t *U = Y + (size_t)W * H;
     uint8_t *V = U + (size_t)CW * CH;
     const size_t coff = (size_t)(sby >> 1) * CW + (sbx >> 1);
-    const PredDst D = { Y + (size_t)sby * W + sbx, U + coff, V + coff, W, CW };
+    const PredDst D = { Y + (size_t)sby * W + sbx, U + coff, V + coff, W, CW,
+                        min(64, W - sbx), min(64, H - sby), min(32, CW - (sbx >> 1)), min(32, CH - (sby >> 1)) };
+    if (A == CVP9_ARITH_SPEC) {
+        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_luma_pass(w, D, job, c0, nchunks, sbx, sby, lane);
+        for (int c0 = 0; c0 < nchunks; c0 += 4) spec_chroma_pass(w, D, job, c0, nchunks, sbx, sby, lane);
+        return;
+    }
     /* two passes of four chunks per iteration; the next iteration's rows
      * are requested before this one's are filtered */
     const int nit = (nchunks + 7) >> 3;
@@ -3079,8 +3114,8 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     }
 }
 
-/* U8: the 8x8 transform through fast_residual_d (inter path 4) */
-template <int MINB, bool U8>
+/* U8: the REFCPU 8x8 transform through fast_residual_d (inter path 4) */
+template <int A, int MINB, bool U8>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_t *__restrict__ jobs,
                                                             const uint32_t *__restrict__ tickets,
                                                             uint32_t n_tickets, const uint32_t *__restrict__ general)
@@ -3097,9 +3132,20 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_
     const int sbx = sbc * 64, sby = sbr * 64;
     int nb;
     /* the same descriptors k_pred checked and packed: packing alone */
-    fast_sb_setup<CVP9_ARITH_REFCPU, false>(w, job, sb, sbx, sby, lane, nb);
+    fast_sb_setup<A, false>(w, job, sb, sbx, sby, lane, nb);
     __syncwarp();
-    fast_refcpu_residual<true, U8>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
+    if (A == CVP9_ARITH_SPEC) {
+        const int W = job.W, H = job.H, CW = job.CW, CH = job.CH;
+        uint8_t *Y = job.out;
+        uint8_t *U = Y + (size_t)W * H;
+        uint8_t *V = U + (size_t)CW * CH;
+        const size_t coff = (size_t)(sby >> 1) * CW + (sbx >> 1);
+        const PredDst D = { Y + (size_t)sby * W + sbx, U + coff, V + coff, W, CW,
+                        min(64, W - sbx), min(64, H - sby), min(32, CW - (sbx >> 1)), min(32, CH - (sby >> 1)) };
+        fast_spec_residual<true>(w, D, job, nb, lane);
+    } else {
+        fast_refcpu_residual<true, U8>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
+    }
     __syncwarp();
     if (lane == 0) {
         __threadfence();
@@ -3633,14 +3679,19 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
             if ((e = cudaMemsetAsync(L->n_general + 1, 0, 4, st)) != cudaSuccess) return (int)e;
             const size_t fs = kFastWarps * sizeof(FastSmem);
             const bool spec = L->arith == CVP9_ARITH_SPEC;
-            if ((L->inter_variant == 3 || L->inter_variant == 4) && !spec) {
-                k_pred<kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
+            if ((L->inter_variant == 3 || L->inter_variant == 4) && spec) {
+                k_pred<CVP9_ARITH_SPEC, kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+                k_resid<CVP9_ARITH_SPEC, kResidMinB, false><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+            } else if (L->inter_variant == 3 || L->inter_variant == 4) {
+                k_pred<CVP9_ARITH_REFCPU, kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
                     L->jobs, L->tickets, L->n_tickets, L->general);
                 if (L->inter_variant == 4)
-                    k_resid<kResidMinB, true><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
+                    k_resid<CVP9_ARITH_REFCPU, kResidMinB, true><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
                         L->jobs, L->tickets, L->n_tickets, L->general);
                 else
-                    k_resid<kResidMinB, false><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
+                    k_resid<CVP9_ARITH_REFCPU, kResidMinB, false><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
                         L->jobs, L->tickets, L->n_tickets, L->general);
             } else if (L->inter_variant == 2) {
                 if (spec) k_inter<CVP9_ARITH_SPEC, 6><<<fg, kFastWarps * 32, fs, st>>>(L->jobs, L->tickets, L->n_tickets, L->general);

@@ -60,9 +60,9 @@ typedef struct {
     int      settled;        /* 1: every knob measured, the fields below hold     */
     int      inter_path;     /* 0 general kernel only, 1 warp-per-SB inter kernel
                               * (96 registers), 2 the same at 80 registers,
-                              * 3 (REFCPU) prediction and residual as two
-                              * kernels at 96 and 64 registers, 4 the same with
-                              * 8x8 TXs walked TX by TX                          */
+                              * 3 prediction and residual as two kernels (64
+                              * registers for the residual), 4 (REFCPU) the
+                              * same with 8x8 TXs walked TX by TX                */
     int      lf_tile_h;      /* loop filter: 16 register strips (8x16 per thread),
                               * 32 shared-memory tiles (64x32 per CTA)           */
     int      half_width;     /* 1: wavefront kernel on half the resident CTAs    */

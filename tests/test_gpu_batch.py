@@ -53,17 +53,18 @@ def test_batch_matches_oracle(profile):
             assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
 
 
-@pytest.mark.parametrize("variant", ["0", "2", "3", "4"])
-def test_every_inter_path_matches_oracle(variant, monkeypatch):
+@pytest.mark.parametrize("profile,variant", [(REFCPU, "0"), (REFCPU, "2"), (REFCPU, "3"), (REFCPU, "4"),
+                                             (SPEC, "0"), (SPEC, "2"), (SPEC, "3")])
+def test_every_inter_path_matches_oracle(profile, variant, monkeypatch):
     """Each fixed inter path the tuner can pick (general kernel only, the
-    80-register k_inter, REFCPU's k_pred + k_resid split) decodes the mixed
-    batch to the oracle's bytes."""
+    80-register k_inter, the k_pred + k_resid split, REFCPU's split walking
+    8x8 TXs per TX) decodes the mixed batch to the oracle's bytes."""
     monkeypatch.setenv("CVP9_AUTOTUNE", "0")
     monkeypatch.setenv("CVP9_INTER_FAST", variant)
-    outs = decode_mix(REFCPU, MIX, 3)
+    outs = decode_mix(profile, MIX, 3)
     for i, (p, w, h, ov) in enumerate(MIX):
         syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
-        orc = OracleStream(REFCPU)
+        orc = OracleStream(profile)
         for f in range(3):
             assert np.array_equal(outs[i][f], orc.decode(syn.frame(f))), "stream %d frame %d" % (i, f)
 
@@ -127,8 +128,8 @@ def test_admission_budget():
 def test_autotune_settles_with_oracle_output(profile):
     """The tuner runs every candidate configuration on real steps: each of
     those steps still decodes to the oracle's bytes, and the bucket settles
-    after all knobs were measured (the inter paths — 3, REFCPU 5 — then
-    filter layout and wavefront width: 5 configurations, REFCPU 7)."""
+    after all knobs were measured (the inter paths — 4, REFCPU 5 — then
+    filter layout and wavefront width: 6 configurations, REFCPU 7)."""
     tuning = []
     frames = 14
     outs = decode_mix(profile, MIX, frames, tuning=tuning)
@@ -140,9 +141,9 @@ def test_autotune_settles_with_oracle_output(profile):
             assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
     assert len(tuning) == 1, tuning
     e = tuning[0]
-    assert e["settled"] == 1 and e["trials"] == (7 if profile == REFCPU else 5), e
+    assert e["settled"] == 1 and e["trials"] == (7 if profile == REFCPU else 6), e
     assert e["best_ms"] > 0 and e["lf_tile_h"] in (16, 32)
-    assert e["inter_path"] in ((0, 1, 2, 3, 4) if profile == REFCPU else (0, 1, 2))
+    assert e["inter_path"] in ((0, 1, 2, 3, 4) if profile == REFCPU else (0, 1, 2, 3))
 
 
 def _pinned_copy(pf, keep):

@@ -77,5 +77,15 @@ def test_refcpu_parity_prediction_residual_split(name, variant, monkeypatch):
 
 
 @pytest.mark.parametrize("name", list(CASES))
+def test_spec_parity_prediction_residual_split(name, monkeypatch):
+    """SPEC through the two-kernel inter path (k_pred into the frame, then
+    k_resid over every plane in place; CVP9_INTER_FAST=3) gives the
+    restatement's bytes on every case, frame edges included (its TXs follow
+    the MI grid past the edge, where nothing may be written)."""
+    monkeypatch.setenv("CVP9_INTER_FAST", "3")
+    run_case(SPEC, *CASES[name])
+
+
+@pytest.mark.parametrize("name", list(CASES))
 def test_spec_parity(name):
     run_case(SPEC, *CASES[name])

@@ -86,7 +86,7 @@ def test_spec_tunes_the_same_knobs(lib):
             break
         if not seen or seen[-1] != cfg:
             seen.append(cfg)
-    assert seen == [(1, 0, 0), (0, 0, 0), (2, 0, 0), (1, 1, 0), (1, 0, 1)]
+    assert seen == [(1, 0, 0), (0, 0, 0), (2, 0, 0), (3, 0, 0), (1, 1, 0), (1, 0, 1)]
     assert step(lib, t, 5, lambda c: 1.0) == (-1, (1, 0, 1))
 
 
