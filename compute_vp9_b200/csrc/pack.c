@@ -85,7 +85,7 @@ static uint32_t *scan_avx2(const int16_t *src, uint32_t m, uint32_t off, uint32_
             out += __builtin_popcount(nz);
         }
     }
-    return scan_scalar(src + k, m - k, off + k, out);
+    return k < m ? scan_scalar(src + k, m - k, off + k, out) : out;
 }
 
 __attribute__((target("avx512f,avx512bw,avx512vl,popcnt")))
@@ -106,7 +106,7 @@ static uint32_t *scan_avx512(const int16_t *src, uint32_t m, uint32_t off, uint3
         _mm512_storeu_si512((void *)out, _mm512_maskz_compress_epi32((__mmask16)(nz >> 16), e1));
         out += __builtin_popcount((unsigned)(nz >> 16));
     }
-    return scan_scalar(src + k, m - k, off + k, out);
+    return k < m ? scan_scalar(src + k, m - k, off + k, out) : out;
 }
 #endif
 
