@@ -90,9 +90,16 @@ class BatchError(RuntimeError):
 
 
 class Batch:
-    """Engine handle. Streams are admitted by HBM budget (open_stream returns
-    None when the budget is full); step() reconstructs one frame per listed
-    stream in one launch chain."""
+    """Engine handle (cvp9_batch_*). Streams are admitted by HBM budget
+    (open_stream returns None when the budget is full); submit() enqueues
+    one frame per listed stream, reconstructed in one launch chain, up to
+    three steps in flight.
+
+    autotune: time the kernel configurations on the first steps of each
+    shape bucket and keep the fastest (tuning() reports them).
+    pack: host-side packing of dense host coefficient arrays before the
+    upload — 0 for steps moving at least 64 MB of them, with the packed
+    share balanced against the link; 1 always; -1 never."""
 
     def __init__(self, device=-1, arith=-1, hbm_budget=0, max_streams=0, use_graphs=1, autotune=1, pack=0):
         from . import cuda_lib
