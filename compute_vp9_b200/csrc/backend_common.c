@@ -121,6 +121,13 @@ int cvp9_env_arith(void)
     return CVP9_ARITH_REFCPU;
 }
 
+int cvp9_filter_supported(int arith, int interp_filter, const char **why)
+{
+    if (arith == CVP9_ARITH_REFCPU || interp_filter == VP9_FILTER_EIGHTTAP) return 1;
+    if (why) *why = "interpolation filter other than EIGHTTAP: the shader profile holds the regular 8-tap table only";
+    return 0;
+}
+
 void cvp9_job_geometry(cvp9_job_t *job, const vp9_parsed_frame_t *pf)
 {
     int W = (int)pf->hdr.width, H = (int)pf->hdr.height;

@@ -49,6 +49,14 @@ int cvp9_env_gather(void);          /* $CVP9_GATHER: 0 uploads whole coefficient
  * overrides the configured value) */
 int cvp9_env_pack(int configured);
 
+/* Whether the profile can reconstruct a frame with this header's
+ * interpolation filter, as the frame's bitstream defines it. REFCPU: every
+ * value (the CPU path, src/decoder/vp9_reconstruct.c:94-131, always
+ * predicts bilinearly and never reads the field). SPEC: EIGHTTAP only (the
+ * shaders hold the regular table alone, shaders/vp9_mc.comp.glsl:40-57).
+ * On 0, *why names the reason for the caller's error text. */
+int cvp9_filter_supported(int arith, int interp_filter, const char **why);
+
 /* Fill the frame-geometry and parameter fields of a job from a parsed
  * frame (inputs, output, refs and scratch pointers are set by the caller). */
 void cvp9_job_geometry(cvp9_job_t *job, const vp9_parsed_frame_t *pf);

@@ -93,7 +93,7 @@ typedef struct {
     cvp9_job_t     *h_jobs; cvp9_job_t *d_jobs; int jobs_cap;
     uint32_t       *d_sb_range; size_t sb_cap;      /* uint32 entries */
     uint32_t       *d_misc; uint32_t *h_misc; int misc_cap;  /* [0] tickets, [1+i] status, [n+1] gathered
-                                                     * bytes, [n+2] malformed packed frames */
+                                                     * bytes, [n+2+i] malformed packed frame i */
     uint32_t       *d_tickets; size_t tickets_cap; uint32_t n_tickets; uint64_t tickets_key;
     uint32_t       *h_tickets; size_t h_tickets_cap;
     uint32_t       *d_fast; size_t fast_cap;    /* inter fast path: flags, tickets, count */
@@ -448,11 +448,11 @@ static uint64_t mix64(uint64_t h, uint64_t v)
 }
 
 /* Status word of job i of a completed slot; a malformed packed upload
- * (bit i % 32 of the unpack error word) reads as a bad block. */
+ * (job i's own unpack error word) reads as a bad block. */
 static uint32_t slot_status(const bslot_t *s, int i)
 {
     uint32_t st = s->h_misc[1 + i];
-    if (s->h_misc[s->n + 2] & (1u << (i & 31))) st |= CVP9_JOB_BAD_BLOCK;
+    if (s->h_misc[s->n + 2 + i]) st |= CVP9_JOB_BAD_BLOCK;
     return st;
 }
 
@@ -595,6 +595,11 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         if (lists ? (lists[i].n && (!lists[i].pos || !lists[i].val)) : (pf->num_coeffs && !pf->coeffs))
             return CVP9_ERR_INVALID_DATA;
         for (int j = 0; j < i; j++) if (sids[j] == sid) return CVP9_ERR_INVALID_DATA;
+        const char *why = NULL;
+        if (!cvp9_filter_supported(b->arith, (int)pf->hdr.interp_filter, &why)) {
+            snprintf(b->err, sizeof(b->err), "stream %d: %s", sid, why);
+            return CVP9_ERR_UNSUPPORTED;
+        }
     }
 
     const uint64_t seq = b->seq + 1;
@@ -726,8 +731,8 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             return err;
         s->jobs_cap = cap;
     }
-    if (s->misc_cap < n + 3) {
-        int cap = (n > b->nst ? n : b->nst) + 3;
+    if (s->misc_cap < 2 * n + 2) {
+        int cap = 2 * (n > b->nst ? n : b->nst) + 2;
         s->misc_cap = 0;
         if ((err = grow_host(b, (void **)&s->h_misc, &s->h_misc_bytes, (size_t)cap * 4)) ||
             (err = grow_dev(b, (void **)&s->d_misc, &s->d_misc_bytes, (size_t)cap * 4)))
@@ -870,10 +875,10 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     BCK(cudaMemcpyAsync(s->d_jobs, s->h_jobs, (size_t)n * sizeof(cvp9_job_t), cudaMemcpyHostToDevice, b->hs),
         "upload jobs");
     s->h2d_bytes += (size_t)n * sizeof(cvp9_job_t);
-    /* the counter of gathered bytes and the unpack error word are cleared
-     * here, on the upload stream; the compute stream's clear of the status
-     * words stops before them */
-    BCK(cudaMemsetAsync(s->d_misc + n + 1, 0, 8, b->hs), "clear upload words");
+    /* the counter of gathered bytes and the per-job unpack error words are
+     * cleared here, on the upload stream; the compute stream's clear of the
+     * status words stops before them */
+    BCK(cudaMemsetAsync(s->d_misc + n + 1, 0, (size_t)(n + 1) * 4, b->hs), "clear upload words");
     s->launches_extra = 0;
     if (any_gather) {
         int grc = cvp9k_launch_gather(s->d_jobs, n, max_blocks, s->d_misc + n + 1, b->hs);
@@ -931,8 +936,9 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
     gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
-    /* k_inter + k_compact, or k_pred + k_resid + k_compact (REFCPU split) */
-    const int split = L.inter_variant >= 3 && b->arith == CVP9_ARITH_REFCPU;
+    /* k_inter + k_compact, or k_pred + k_resid + k_compact (the split, both
+     * profiles: cvp9k_launch_frame dispatches inter paths 3 and 4 to it) */
+    const int split = L.inter_variant >= 3;
     s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
                              (L.general ? (split ? 3 : 2) : 0));
     if (b->use_graphs) {
@@ -999,7 +1005,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         }
     }
     if (ofr != out_frame) free(ofr);
-    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(n + 3) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
+    BCK(cudaMemcpyAsync(s->h_misc, s->d_misc, (size_t)(2 * n + 2) * 4, cudaMemcpyDeviceToHost, b->ds), "status");
     s->d2h_bytes += (size_t)(n + 3) * 4;
     /* ev_end, then the completion callback (so a stamped step is complete
      * for every other query), then ev_cb, which slot reuse waits on so the

@@ -10,8 +10,13 @@
  *     I420 frames (pointer swaps, no copies — the Vulkan backend copies
  *     luma into images, vulkan_backend.c:1310-1354);
  *   - CVP9_CUDA_INFLIGHT slots of pinned staging (inputs, job descriptor,
- *     output frame, status word) so the CPU parse of the next frame overlaps
- *     the GPU work of this one (vulkan_backend.h:36-81).
+ *     status word) so the CPU parse of the next frame overlaps the GPU work
+ *     of this one (vulkan_backend.h:36-81);
+ *   - OUTBUFS pinned output frames, apart from the slots. A delivered
+ *     frame's planes stay untouched for the next two decode calls whatever
+ *     the ring holds, as include/compute_vp9/decoder.h:100-104 promises (the
+ *     Vulkan backend keeps its output in the ring slot, which the very next
+ *     decode reuses when two other frames are still in flight).
  */
 #include "cuda_backend.h"
 #include "backend_common.h"
@@ -25,6 +30,18 @@
 
 #define MAX_DFRAMES 12
 #define WAIT_LIMIT_S 30.0
+/* Output frames needed so that a delivered frame survives two decodes: at a
+ * decode at most two frames are pending, at most four frames entered the
+ * ring since the decode two calls back (two pending then, two decoded since),
+ * plus the new one. */
+#define OUTBUFS (CVP9_CUDA_INFLIGHT + 2)
+
+typedef struct {
+    uint8_t *h;
+    size_t   cap;
+    int      busy;         /* holds a frame still in the ring               */
+    uint64_t free_after;   /* may be reused once this many decodes were made */
+} outbuf_t;
 
 typedef struct {
     uint8_t *dev;
@@ -45,7 +62,7 @@ typedef struct {
     void        *h_coeffs;  size_t h_coeffs_cap;
     cvp9_job_t  *h_job;
     uint32_t    *h_status;
-    uint8_t     *h_out;     size_t h_out_cap;
+    int          out;                  /* output buffer of this frame */
     /* device inputs */
     void        *d_blocks;  size_t d_blocks_cap;
     void        *d_coeffs;  size_t d_coeffs_cap;
@@ -73,6 +90,8 @@ typedef struct {
     int          recon_ctas;
     slot_t       slots[CVP9_CUDA_INFLIGHT];
     int          ring_head, ring_count;
+    outbuf_t     outs[OUTBUFS];
+    uint64_t     decodes;              /* successful decode calls */
     void        *pending_target;       /* device pointer of armed NV12 target */
     uint64_t     pending_target_size;
     float        last_total_ms, last_kernel_ms;
@@ -97,7 +116,6 @@ static void free_slot(slot_t *s)
     cudaFreeHost(s->h_coeffs);
     cudaFreeHost(s->h_job);
     cudaFreeHost(s->h_status);
-    cudaFreeHost(s->h_out);
     cudaFree(s->d_blocks);
     cudaFree(s->d_coeffs);
     cudaFree(s->d_job);
@@ -164,6 +182,7 @@ void cuda_backend_destroy(void *ctx)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int i = 0; i < CVP9_CUDA_INFLIGHT; i++) free_slot(&c->slots[i]);
+    for (int i = 0; i < OUTBUFS; i++) cudaFreeHost(c->outs[i].h);
     for (int i = 0; i < MAX_DFRAMES; i++) cudaFree(c->frames[i].dev);
     free_geometry(c);
     cudaFree(c->d_misc);
@@ -272,6 +291,11 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     if (W <= 0 || H <= 0 || W > 65535 || H > 65535) return CVP9_ERR_INVALID_DATA;
     if (pf->num_blocks && !pf->blocks) return CVP9_ERR_INVALID_DATA;
     if (pf->num_coeffs && !pf->coeffs) return CVP9_ERR_INVALID_DATA;
+    const char *why = NULL;
+    if (!cvp9_filter_supported(c->arith, (int)pf->hdr.interp_filter, &why)) {
+        snprintf(c->last_error, sizeof(c->last_error), "%s", why);
+        return CVP9_ERR_UNSUPPORTED;
+    }
     if (cudaSetDevice(c->device) != cudaSuccess) return CVP9_ERR_GPU;
 
     cvp9_err_t err;
@@ -285,9 +309,14 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     size_t nbb = (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t);
     size_t ncb = (size_t)pf->num_coeffs * sizeof(int16_t);
     size_t outb = nv12_need;
+    int ob = -1;
+    for (int i = 0; i < OUTBUFS && ob < 0; i++)
+        if (!c->outs[i].busy && c->outs[i].free_after <= c->decodes) ob = i;
+    if (ob < 0) return fail(c, cudaErrorMemoryAllocation, "output buffers");
+    outbuf_t *o = &c->outs[ob];
     if ((err = grow_pinned(c, &s->h_blocks, &s->h_blocks_cap, nbb ? nbb : 64)) ||
         (err = grow_pinned(c, &s->h_coeffs, &s->h_coeffs_cap, ncb ? ncb : 64)) ||
-        (err = grow_pinned(c, (void **)&s->h_out, &s->h_out_cap, outb)) ||
+        (err = grow_pinned(c, (void **)&o->h, &o->cap, outb)) ||
         (err = grow_device(c, &s->d_blocks, &s->d_blocks_cap, nbb ? nbb : 64)) ||
         (err = grow_device(c, &s->d_coeffs, &s->d_coeffs_cap, ncb ? ncb : 64)))
         return err;
@@ -362,7 +391,7 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     int lrc = cvp9k_launch_frame(&L, st);
     if (lrc != 0) return fail(c, (cudaError_t)lrc, "launch");
     CK(cudaEventRecord(s->ev_k1, st), "event");
-    CK(cudaMemcpyAsync(s->h_out, c->frames[of].dev, outb, cudaMemcpyDeviceToHost, st), "download frame");
+    CK(cudaMemcpyAsync(o->h, c->frames[of].dev, outb, cudaMemcpyDeviceToHost, st), "download frame");
     CK(cudaMemcpyAsync(s->h_status, c->d_misc, 4, cudaMemcpyDeviceToHost, st), "download status");
     CK(cudaEventRecord(s->ev_end, st), "event");
 
@@ -379,6 +408,9 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     c->pending_target = NULL;
     c->pending_target_size = 0;
     s->pending = 1;
+    s->out = ob;
+    o->busy = 1;
+    c->decodes++;
     s->pts = pts;
     s->w = W;
     s->h = H;
@@ -419,6 +451,9 @@ cvp9_err_t cuda_get_frame(void *ctx, cvp9_frame_info_t *info, int wait)
     s->pending = 0;
     c->ring_head = (c->ring_head + 1) % CVP9_CUDA_INFLIGHT;
     c->ring_count--;
+    outbuf_t *o = &c->outs[s->out];
+    o->busy = 0;
+    o->free_after = c->decodes + 2;     /* untouched by the next two decodes */
 
     float t = 0.f, k = 0.f;
     cudaEventElapsedTime(&t, s->ev_start, s->ev_end);
@@ -442,9 +477,9 @@ cvp9_err_t cuda_get_frame(void *ctx, cvp9_frame_info_t *info, int wait)
     info->height = h;
     info->stride_y = w;
     info->stride_uv = cw;
-    info->plane_y = s->h_out;
-    info->plane_u = s->h_out + (size_t)w * h;
-    info->plane_v = s->h_out + (size_t)w * h + (size_t)cw * ch;
+    info->plane_y = o->h;
+    info->plane_u = o->h + (size_t)w * h;
+    info->plane_v = o->h + (size_t)w * h + (size_t)cw * ch;
     info->pts = s->pts;
     return CVP9_OK;
 }

@@ -3535,7 +3535,7 @@ __global__ void __launch_bounds__(256) k_unpack_coeffs(const cvp9_job_t *__restr
     if (!pk) return;
     const uint32_t nw = job.packed_words, np = nw ? pk[0] : 0u;
     if (1u + 2u * (uint64_t)np > nw) {
-        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(err, 1u << (blockIdx.y & 31));
+        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(err + blockIdx.y, 1u);
         return;
     }
     for (uint32_t p = blockIdx.x; p < np; p += gridDim.x) {
@@ -3547,7 +3547,7 @@ __global__ void __launch_bounds__(256) k_unpack_coeffs(const cvp9_job_t *__restr
         const bool dense = st >> 31;
         const uint64_t words = dense ? ((uint64_t)len + 1) / 2 : cnt;
         if ((s0 & 3u) || (dense && cnt != len) || (!dense && cnt > (len + 1) / 2) || s0 + words > nw) {
-            if (threadIdx.x == 0) atomicOr(err, 1u << (blockIdx.y & 31));
+            if (threadIdx.x == 0) atomicOr(err + blockIdx.y, 1u);
             continue;
         }
         int16_t *dst = const_cast<int16_t *>(job.coeffs) + base;     /* 16-byte aligned */

@@ -60,7 +60,7 @@ int    cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, c
 /* Packed coefficient upload: every job with `packed` set gets its dense
  * coeffs array rebuilt from the pages (entry pages zero-filled, then
  * scattered; dense pages copied). max_pages: most pages of any job; a
- * malformed page of job j sets bit j % 32 of *err (device word). */
+ * malformed page of job j sets err[j] to 1 (device, one word per job). */
 int    cvp9k_launch_unpack(const cvp9_job_t *jobs, int njobs, uint32_t max_pages, uint32_t *err,
                            cudaStream_t stream);
 

@@ -111,6 +111,12 @@ extern "C" cvp9_err_t cuda_reconstruct_noalloc(const vp9_parsed_frame_t *pf,
         return CVP9_ERR_INVALID_DATA;
     }
     if ((pf->num_blocks && !pf->blocks) || (pf->num_coeffs && !pf->coeffs)) return CVP9_ERR_INVALID_DATA;
+    const int a = arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU;
+    const char *why = nullptr;
+    if (!cvp9_filter_supported(a, (int)pf->hdr.interp_filter, &why)) {
+        fprintf(stderr, "[compute-vp9] cuda_reconstruct_noalloc: %s\n", why);
+        return CVP9_ERR_UNSUPPORTED;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || setup_device(dev) != 0) return CVP9_ERR_GPU;
     unsigned char *base = g_scratch_ptr[dev];
@@ -148,7 +154,6 @@ extern "C" cvp9_err_t cuda_reconstruct_noalloc(const vp9_parsed_frame_t *pf,
 
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int a = arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU;
     cvp9k_launch_t L;
     memset(&L, 0, sizeof(L));
     L.jobs = (const cvp9_job_t *)(base + kOffJob);

@@ -5,7 +5,7 @@
  * src/backend/vulkan/vulkan_backend.h:141-163 and are called from the same
  * places in src/decoder/vp9_decoder.c (init 110-119, decode 203-207 and
  * 448-452, get 256-259, dmabuf 286-293, export 295-317, render target
- * 319-325, destroy 131-134). INTEGRATION.md shows the patch.
+ * 319-325, destroy 131-134).
  *
  * Contract (mirrors the Vulkan backend):
  *  - cuda_decode_frame copies everything it needs out of *pf before it
@@ -16,8 +16,9 @@
  *    still on the GPU unless every slot is busy, in which case it blocks;
  *    wait=1 always blocks. CVP9_ERR_UNSUPPORTED when nothing is queued.
  *    Frames come back in submission order. Plane pointers point into
- *    backend-owned pinned memory and stay valid until that slot is reused,
- *    i.e. for at least the next CVP9_CUDA_INFLIGHT-1 decodes.
+ *    backend-owned pinned memory and stay valid for the next two
+ *    cuda_decode_frame calls (include/compute_vp9/decoder.h:100-104),
+ *    however many frames the ring holds when the frame is delivered.
  *  - Errors found on the device (invalid block layout, an expired bounded
  *    wait) are reported by the cuda_get_frame call that delivers the frame:
  *    CVP9_ERR_INVALID_DATA or CVP9_ERR_GPU.
@@ -32,7 +33,9 @@
  * (src/decoder/vp9_decoder.c:224-231) bit for bit; CVP9_CUDA_ARITH_SPEC runs
  * the shader arithmetic (integer butterflies with dequantisation, 8-tap MC
  * on all planes, shader intra rules) with the Vulkan pool rules
- * (refresh_frame_flags, ref_frame_idx). The environment variable
+ * (refresh_frame_flags, ref_frame_idx); the shaders hold only the regular
+ * 8-tap filter, so SPEC returns CVP9_ERR_UNSUPPORTED (from decode) for a
+ * frame whose header asks for another filter. The environment variable
  * CVP9_ARITH=refcpu|spec picks the profile for cuda_backend_init;
  * CVP9_CUDA_DEVICE picks the GPU.
  */

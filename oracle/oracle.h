@@ -12,9 +12,12 @@
  *            vp9_intra_pred.comp.glsl, vp9_loopfilter.comp.glsl and
  *            vp9_nv12_pack.comp.glsl, applied block by block in parse order,
  *            with chroma MC and the all-plane residual written from the VP9
- *            design. The shaders cannot run here (no graphics stack), so this
- *            profile's parity is unpinned except where it coincides with the
- *            REFCPU loop filter.
+ *            design. The shaders cannot run here (no graphics stack); the
+ *            profile is pinned stage by stage to mechanical Python
+ *            translations of the shaders' own functions (inverse transforms,
+ *            luma MC, intra: tests/golden/spec_*.json) and, for the loop
+ *            filter, to the REFCPU one it equals. Chroma MC and the all-plane
+ *            residual have no shader counterpart: unpinned.
  */
 #ifndef CVP9_ORACLE_H
 #define CVP9_ORACLE_H
@@ -57,6 +60,17 @@ void oracle_refcpu_idct2d(const int16_t *in, int16_t *out, int n);
 /* SPEC integer inverse DCT with dequantisation (vp9_idct.comp.glsl:654-789):
  * returns the rounded residual (before the add/clamp). */
 void oracle_spec_idct2d(const int16_t *in, int32_t *out, int n, int q_dc, int q_ac);
+
+/* SPEC intra prediction of one w x h block in place (neighbours read from
+ * the same plane; vp9_intra_pred.comp.glsl:54-109 generalised to w x h). */
+void oracle_spec_intra_block(uint8_t *plane, int w, int h, int stride, int x, int y,
+                             int bw, int bh, int mode);
+
+/* SPEC inter prediction of one block of dst from ref (luma: 1/8-pel MV on
+ * even phases, vp9_mc.comp.glsl:61-110; chroma: the MV as 1/16 chroma pel). */
+void oracle_spec_mc_block(const uint8_t *ref, int rw, int rh, int rstride,
+                          uint8_t *dst, int dw, int dh, int dstride,
+                          int x, int y, int bw, int bh, int mvx, int mvy, int chroma);
 
 /* Loop filter in place on a luma plane: REFCPU (level 0 = off) or SPEC
  * (threshold floored at 1, always on). */

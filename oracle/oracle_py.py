@@ -50,6 +50,10 @@ def oracle_lib():
         lib.oracle_nv12_pack.restype = None
         lib.oracle_refcpu_basis.argtypes = [C.c_void_p]
         lib.oracle_refcpu_basis.restype = None
+        lib.oracle_spec_intra_block.argtypes = [C.c_void_p] + [C.c_int] * 8
+        lib.oracle_spec_intra_block.restype = None
+        lib.oracle_spec_mc_block.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 10
+        lib.oracle_spec_mc_block.restype = None
         lib.oracle_dc_quant.argtypes = [C.c_int]
         lib.oracle_ac_quant.argtypes = [C.c_int]
         _orc = lib
@@ -160,3 +164,22 @@ def nv12_pack(i420, w, h):
     dst = np.empty(_i420_size(w, h), np.uint8)
     oracle_lib().oracle_nv12_pack(src.ctypes.data, dst.ctypes.data, w, h)
     return dst
+
+
+def spec_intra_block(plane, x, y, bw, bh, mode):
+    """SPEC intra prediction of one block; returns the plane after it."""
+    p = np.ascontiguousarray(plane, np.uint8).copy()
+    h, w = p.shape
+    oracle_lib().oracle_spec_intra_block(p.ctypes.data, w, h, w, x, y, bw, bh, mode)
+    return p
+
+
+def spec_mc_block(ref, dst_shape, x, y, bw, bh, mvx, mvy, chroma=0):
+    """SPEC inter prediction of one block from ref into a zeroed plane of
+    dst_shape; returns that plane."""
+    r = np.ascontiguousarray(ref, np.uint8)
+    d = np.zeros(dst_shape, np.uint8)
+    oracle_lib().oracle_spec_mc_block(r.ctypes.data, r.shape[1], r.shape[0], r.shape[1],
+                                      d.ctypes.data, d.shape[1], d.shape[0], d.shape[1],
+                                      x, y, bw, bh, mvx, mvy, chroma)
+    return d

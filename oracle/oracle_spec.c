@@ -458,6 +458,22 @@ static void spec_inter(plane_t dst, plane_t ref, int x, int y, int w, int h,
         }
 }
 
+/* Stage-level entry points (unit tests against the shader translations). */
+void oracle_spec_intra_block(uint8_t *plane, int w, int h, int stride, int x, int y,
+                             int bw, int bh, int mode)
+{
+    plane_t pl = { plane, w, h, stride };
+    spec_intra(pl, x, y, bw, bh, mode);
+}
+
+void oracle_spec_mc_block(const uint8_t *ref, int rw, int rh, int rstride,
+                          uint8_t *dst, int dw, int dh, int dstride,
+                          int x, int y, int bw, int bh, int mvx, int mvy, int chroma)
+{
+    plane_t r = { (uint8_t *)ref, rw, rh, rstride }, d = { dst, dw, dh, dstride };
+    spec_inter(d, r, x, y, bw, bh, mvx, mvy, chroma);
+}
+
 static int max_tx_for(int w, int h)
 {
     int m = w < h ? w : h;

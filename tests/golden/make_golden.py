@@ -20,6 +20,17 @@ spec_idct.json      input/output vectors of the shader inverse transforms,
                     shaders/vp9_idct.comp.glsl's idct4/8/16/32 functions and
                     its main() dequant/shift logic into Python (done here at
                     generation time; only the vectors are committed).
+spec_intra.json     the shader intra predictor (shaders/vp9_intra_pred.comp.glsl
+                    main() and its sample_* helpers, translated statement by
+                    statement by glsl_py.py and run per invocation of a 32x32
+                    workgroup): every block size, the four modes it implements
+                    and two it does not, at the four edge-availability cases;
+                    inputs from tests/golden/vectors.py seeds, outputs as
+                    digests of the predicted plane.
+spec_mc.json        the shader luma motion compensation (shaders/vp9_mc.comp.glsl
+                    main() and fetch_ref, translated the same way, run per
+                    pixel of a 64x48 frame with one MV in every 4x4 cell): all
+                    64 (x, y) phase pairs and MVs far outside the frame.
 """
 import ctypes as C
 import hashlib
@@ -32,8 +43,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("CVP9_REFERENCE", "/root/reference")
+# the reference tree: $CVP9_REFERENCE, else a checkout named "reference"
+# beside this repository
+REF = os.environ.get("CVP9_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
 
 from compute_vp9_b200 import Synth, fnv1a64, synth_config  # noqa: E402
 from compute_vp9_b200.cvp9_ctypes import layout_offsets  # noqa: E402
@@ -136,6 +150,81 @@ def spec_vectors():
     return vecs
 
 
+class _Obj:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def _shader_namespace(shader, functions):
+    """Execute the translated shader functions in a namespace with the GLSL
+    built-ins they use."""
+    import glsl_py
+    src = open(os.path.join(REF, "shaders", shader)).read()
+    code = "".join(glsl_py.translate(src, f) for f in functions)
+
+    def clamp(v, lo, hi):
+        if isinstance(v, tuple):
+            return tuple(min(max(a, b), c) for a, b, c in zip(v, lo, hi))
+        return min(max(v, lo), hi)
+
+    def vec2(*a):
+        return (a[0], a[0]) if len(a) == 1 else tuple(a)
+
+    ns = {"u32": lambda v: int(v) & 0xFFFFFFFF, "i32": lambda v: wrap32(int(v)), "u8": lambda v: int(v) & 0xFF,
+          "clamp": clamp, "vec2": vec2}
+    exec(code, ns)
+    return ns
+
+
+def spec_intra_vectors():
+    from vectors import INTRA_PLANE, digest, intra_cases, plane_bytes
+    ns = _shader_namespace("vp9_intra_pred.comp.glsl", ("sample_above", "sample_left", "sample_top_left", "main"))
+    out = []
+    for case in intra_cases():
+        plane = plane_bytes(case["seed"], INTRA_PLANE)
+        stride = INTRA_PLANE[1]
+        ns["pred"] = plane.reshape(-1).astype(int).tolist()
+        ns["blocks"] = [_Obj(is_intra=1, skip=0, block_size=case["n"], tx_size=0, pred_mode=case["mode"],
+                             qstep=0, coeff_offset=0, dst_stride=stride,
+                             dst_offset=case["y"] * stride + case["x"], qstep_dc=0)]
+        ns["gl_WorkGroupID"] = (0, 0, 0)
+        for py in range(32):
+            for px in range(32):
+                ns["gl_LocalInvocationID"] = (px, py)
+                ns["main"]()
+        got = np.array(ns["pred"], np.uint8).reshape(INTRA_PLANE)
+        out.append(dict(case, digest=digest(got)))
+    return out
+
+
+def spec_mc_vectors():
+    from vectors import MC_PLANE, digest, mc_cases, plane_bytes
+    ns = _shader_namespace("vp9_mc.comp.glsl", ("fetch_ref", "main"))
+    g = open(os.path.join(REF, "shaders/vp9_mc.comp.glsl")).read()
+    m = re.search(r"SUBPEL_FILTER\[16\]\[8\] = int\[16\]\[8\]\((.*?)\);", g, re.S)
+    ns["SUBPEL_FILTER"] = [[int(x) for x in r.split(",")] for r in re.findall(r"int\[8\]\(([^)]*)\)", m.group(1))]
+    h, w = MC_PLANE
+    ns["pc"] = _Obj(frame_width=w, frame_height=h, block_size=0, filter_type=0)
+    out = []
+    for case in mc_cases():
+        ref = plane_bytes(case["seed"], MC_PLANE)
+        tex = _Obj(data=ref)
+
+        def texel_fetch(t, p, lod):
+            return _Obj(r=float(t.data[p[1], p[0]]) / 255.0)
+        ns["texelFetch"] = texel_fetch
+        ns["ref_frames"] = [tex, tex, tex]
+        cells = ((w + 3) // 4) * ((h + 3) // 4)
+        ns["mv"] = [(case["mvx"], case["mvy"], 0, 0)] * cells
+        ns["dst_luma"] = [0] * (w * h)
+        for py in range(h):
+            for px in range(w):
+                ns["gl_GlobalInvocationID"] = (px, py)
+                ns["main"]()
+        out.append(dict(case, digest=digest(np.array(ns["dst_luma"], np.uint8))))
+    return out
+
+
 def main():
     O.build()
     if not O.ref_available():
@@ -153,6 +242,8 @@ def main():
     json.dump({"offsets": list(buf[:k])}, open(os.path.join(HERE, "layout.json"), "w"))
     json.dump(table_hash(), open(os.path.join(HERE, "tables.json"), "w"), indent=1)
     json.dump(spec_vectors(), open(os.path.join(HERE, "spec_idct.json"), "w"))
+    json.dump(spec_intra_vectors(), open(os.path.join(HERE, "spec_intra.json"), "w"), indent=0)
+    json.dump(spec_mc_vectors(), open(os.path.join(HERE, "spec_mc.json"), "w"), indent=0)
     print("golden fixtures written; layout match:", list(buf[:k]) == layout_offsets())
 
 

@@ -9,6 +9,7 @@ import pytest
 from compute_vp9_b200 import CVP9_OK, Synth, synth_config
 from compute_vp9_b200.batch import DEVICE_INPUTS, Batch
 from oracle.oracle_py import REFCPU, SPEC, OracleStream
+from profiles import mix_for
 
 pytestmark = pytest.mark.gpu
 
@@ -23,6 +24,7 @@ MIX = [
 
 def decode_mix(profile, streams, frames, graphs=1, order=None, seeds=None, tuning=None):
     eng = Batch(arith=profile, use_graphs=graphs)
+    streams = mix_for(profile, streams)
     seeds = seeds or [10 + i for i in range(len(streams))]
     syns = [Synth(synth_config(p, w, h, seed=seeds[i], **ov)) for i, (p, w, h, ov) in enumerate(streams)]
     sids = [eng.open_stream(w, h) for (_, w, h, _) in streams]
@@ -45,7 +47,7 @@ def decode_mix(profile, streams, frames, graphs=1, order=None, seeds=None, tunin
 @pytest.mark.parametrize("profile", [REFCPU, SPEC])
 def test_batch_matches_oracle(profile):
     outs = decode_mix(profile, MIX, 4)
-    for i, (p, w, h, ov) in enumerate(MIX):
+    for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX)):
         syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
         orc = OracleStream(profile)
         for f in range(4):
@@ -62,7 +64,7 @@ def test_every_inter_path_matches_oracle(profile, variant, monkeypatch):
     monkeypatch.setenv("CVP9_AUTOTUNE", "0")
     monkeypatch.setenv("CVP9_INTER_FAST", variant)
     outs = decode_mix(profile, MIX, 3)
-    for i, (p, w, h, ov) in enumerate(MIX):
+    for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX)):
         syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
         orc = OracleStream(profile)
         for f in range(3):
@@ -133,7 +135,7 @@ def test_autotune_settles_with_oracle_output(profile):
     tuning = []
     frames = 14
     outs = decode_mix(profile, MIX, frames, tuning=tuning)
-    for i, (p, w, h, ov) in enumerate(MIX):
+    for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX)):
         syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
         orc = OracleStream(profile)
         for f in range(frames):
@@ -171,7 +173,7 @@ def test_pinned_inputs_match_oracle(profile):
     """Page-locked inputs take the direct upload path (REFCPU: the luma-only
     coefficient gather from host memory); every frame equals the oracle."""
     eng = Batch(arith=profile)
-    syns = [Synth(synth_config(p, w, h, seed=30 + i, **ov)) for i, (p, w, h, ov) in enumerate(MIX)]
+    syns = [Synth(synth_config(p, w, h, seed=30 + i, **ov)) for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX))]
     orcs = [OracleStream(profile) for _ in MIX]
     sids = [eng.open_stream(w, h) for (_, w, h, _) in MIX]
     for f in range(4):
@@ -196,7 +198,7 @@ def test_sparse_coefficients_match_oracle(profile, pinned):
     import torch
     from compute_vp9_b200.batch import CoeffList
     eng = Batch(arith=profile)
-    syns = [Synth(synth_config(p, w, h, seed=50 + i, **ov)) for i, (p, w, h, ov) in enumerate(MIX)]
+    syns = [Synth(synth_config(p, w, h, seed=50 + i, **ov)) for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX))]
     orcs = [OracleStream(profile) for _ in MIX]
     sids = [eng.open_stream(w, h) for (_, w, h, _) in MIX]
     for f in range(3):
@@ -233,7 +235,7 @@ def test_packed_coefficients_match_oracle(profile, pinned):
     rebuilt on the device (k_unpack_coeffs) decode to the oracle's bytes,
     from page-locked and from pageable memory, and move fewer bytes."""
     eng = Batch(arith=profile, pack=1)
-    syns = [Synth(synth_config(p, w, h, seed=70 + i, **ov)) for i, (p, w, h, ov) in enumerate(MIX)]
+    syns = [Synth(synth_config(p, w, h, seed=70 + i, **ov)) for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX))]
     orcs = [OracleStream(profile) for _ in MIX]
     sids = [eng.open_stream(w, h) for (_, w, h, _) in MIX]
     for f in range(4):

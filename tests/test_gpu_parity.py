@@ -11,6 +11,7 @@ import pytest
 
 from compute_vp9_b200 import CVP9_OK, CudaBackend, Synth, synth_config
 from oracle.oracle_py import REFCPU, SPEC, OracleStream
+from profiles import overrides_for
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +31,7 @@ CASES = {
 
 
 def run_case(profile, preset, w, h, frames, overrides, seed=11):
-    cfg = synth_config(preset, w, h, seed, **overrides)
+    cfg = synth_config(preset, w, h, seed, **overrides_for(profile, overrides))
     syn = Synth(cfg)
     gpu = CudaBackend(arith=profile)
     orc = OracleStream(profile)

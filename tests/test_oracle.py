@@ -84,3 +84,39 @@ def test_nv12_pack():
     out = O.nv12_pack(np.concatenate([y, u, v]), w, h)
     assert np.array_equal(out[:w * h], y)
     assert np.array_equal(out[w * h::2], u) and np.array_equal(out[w * h + 1::2], v)
+
+
+def _vectors():
+    import sys
+    if GOLD not in sys.path:
+        sys.path.insert(0, GOLD)
+    import vectors
+    return vectors
+
+
+def test_spec_intra_matches_shader_translation():
+    """The restated shader intra predictor equals the shader's own main()
+    (translated statement by statement) on every block size, the modes it
+    implements (DC, V, H, TM), two it falls back on (D45, D207 -> V), and the
+    four edge-availability cases."""
+    V = _vectors()
+    cases = _load("spec_intra.json")
+    assert len(cases) == len(V.INTRA_SIZES) * len(V.INTRA_MODES) * len(V.INTRA_POS)
+    for c in cases:
+        plane = V.plane_bytes(c["seed"], V.INTRA_PLANE)
+        got = O.spec_intra_block(plane, c["x"], c["y"], c["n"], c["n"], c["mode"])
+        assert V.digest(got) == c["digest"], c
+
+
+def test_spec_mc_matches_shader_translation():
+    """The restated luma 8-tap prediction equals the shader's main() and
+    fetch_ref on all 64 phase pairs and on MVs reaching far outside the
+    frame (every fetch clamped)."""
+    V = _vectors()
+    cases = _load("spec_mc.json")
+    assert len(cases) == 72
+    h, w = V.MC_PLANE
+    for c in cases:
+        ref = V.plane_bytes(c["seed"], V.MC_PLANE)
+        got = O.spec_mc_block(ref, (h, w), 0, 0, w, h, c["mvx"], c["mvy"], 0)
+        assert V.digest(got) == c["digest"], c

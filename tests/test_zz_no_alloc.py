@@ -45,12 +45,16 @@ def _device_frame(pf, keep):
     return d
 
 
+# 352x288 runs the tiled loop filter; 353x289 (8k+1 in both directions) the
+# frame-wide one; 251x131 has odd luma and chroma sizes on the tiled path.
+@pytest.mark.parametrize("size", [(352, 288), (353, 289), (251, 131)])
 @pytest.mark.parametrize("arith", [0, 1])
-def test_noalloc_two_calls_match_existing_entry_point(arith):
+def test_noalloc_two_calls_match_existing_entry_point(arith, size):
     import torch
     fn = _bind()
-    w, h = 352, 288
-    syn = Synth(synth_config(2, w, h, seed=21, gop=60, intra_in_inter=0.1))
+    w, h = size
+    # the shader profile (arith 1) reconstructs regular-filter frames only
+    syn = Synth(synth_config(2, w, h, seed=21, gop=60, intra_in_inter=0.1, interp_filter=0))
 
     be = CudaBackend(arith=arith)
     want = []
