@@ -347,6 +347,14 @@ static void emit_block(emit_ctx_t *e, int x, int y, int w, int h)
         b->mv[0][1] = (int16_t)rng_range(r, -range8, range8);
     }
     b->ref_frame[1] = 0;
+    if (!intra && c->compound_prob > 0 && rng_unit(r) < c->compound_prob) {
+        /* second reference: another of LAST/GOLDEN/ALTREF, its own MV */
+        int second = rng_range(r, 1, 2);
+        b->ref_frame[1] = (uint8_t)(1 + (b->ref_frame[0] - 1 + second) % 3);
+        int range8 = c->mv_range_px * 8;
+        b->mv[1][0] = (int16_t)rng_range(r, -range8, range8);
+        b->mv[1][1] = (int16_t)rng_range(r, -range8, range8);
+    }
     b->skip = (uint8_t)(c->skip_prob > 0 && rng_unit(r) < c->skip_prob);
     b->coeff_offset = pf->num_coeffs;
 

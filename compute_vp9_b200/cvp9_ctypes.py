@@ -180,6 +180,7 @@ class SynthConfig(C.Structure):
         ("intra_in_inter", C.c_double),
         ("skip_prob", C.c_double),
         ("log2_tile_cols", C.c_int),
+        ("compound_prob", C.c_double),
     ]
 
 

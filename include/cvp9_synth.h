@@ -42,6 +42,7 @@ typedef struct {
     double   intra_in_inter;   /* share of intra blocks inside inter frames      */
     double   skip_prob;        /* share of skip blocks                           */
     int      log2_tile_cols;   /* >0: blocks emitted tile-column major           */
+    double   compound_prob;    /* share of inter blocks with a second reference  */
 } cvp9_synth_config_t;
 
 /* Workload presets: 1 = plain 720p stream (every SB split to 8x8, TX 8x8,

@@ -18,6 +18,9 @@
  *            luma MC, intra: tests/golden/spec_*.json) and, for the loop
  *            filter, to the REFCPU one it equals. Chroma MC and the all-plane
  *            residual have no shader counterpart: unpinned.
+ *   FULL   — SPEC completed to the VP9 specification where the reference is
+ *            a skeleton (oracle_full.c): unpinned, no VP9 decoder or
+ *            conformance stream is present to pin it.
  */
 #ifndef CVP9_ORACLE_H
 #define CVP9_ORACLE_H
@@ -28,7 +31,7 @@
 extern "C" {
 #endif
 
-enum { ORACLE_REFCPU = 0, ORACLE_SPEC = 1 };
+enum { ORACLE_REFCPU = 0, ORACLE_SPEC = 1, ORACLE_FULL = 2 };
 
 /* A frame owned by the oracle: I420, stride = width (vp9_frame.c:8-34). */
 typedef struct {
@@ -44,6 +47,14 @@ int  oracle_refcpu_reconstruct(const vp9_parsed_frame_t *pf,
 
 /* SPEC: whole-frame reconstruction from the pool slots (8). */
 int  oracle_spec_reconstruct(const vp9_parsed_frame_t *pf,
+                             const oracle_frame_t *const pool[8],
+                             oracle_frame_t *out);
+
+/* FULL: the shader profile completed to the VP9 specification where the
+ * reference is a skeleton (oracle_full.c). Returns 0 for frames the profile
+ * does not take (sizes not multiples of 8, a SWITCHABLE filter on an inter
+ * frame, references of another size). */
+int  oracle_full_reconstruct(const vp9_parsed_frame_t *pf,
                              const oracle_frame_t *const pool[8],
                              oracle_frame_t *out);
 
@@ -71,6 +82,24 @@ void oracle_spec_intra_block(uint8_t *plane, int w, int h, int stride, int x, in
 void oracle_spec_mc_block(const uint8_t *ref, int rw, int rh, int rstride,
                           uint8_t *dst, int dw, int dh, int dstride,
                           int x, int y, int bw, int bh, int mvx, int mvy, int chroma);
+
+/* The shader 1-D inverse DCT, n = 4, 8, 16 or 32 (32-bit wrap). */
+void oracle_idct1d(int n, const int *in, int *out);
+
+/* FULL residual of one n x n TX: dequantised (32x32 halved toward zero),
+ * rows then columns, tx_type 0 DCT, 1 ADST down the columns, 2 ADST along
+ * the rows, 3 both; Walsh-Hadamard for 4x4 when lossless. */
+void oracle_full_itx2d(const int16_t *in, int32_t *out, int n, int tx_type, int lossless,
+                       int q_dc, int q_ac);
+
+/* FULL inter prediction of one block (compound: averaged with ref1). */
+void oracle_full_mc_block(const uint8_t *ref0, const uint8_t *ref1, int rw, int rh, int rstride,
+                          uint8_t *dst, int dw, int dh, int dstride, int x, int y, int bw, int bh,
+                          int mv0x, int mv0y, int mv1x, int mv1y, int compound, int filter, int chroma);
+
+/* FULL intra prediction of one n x n TX in place (VP9 edge rules). */
+void oracle_full_intra_tx(uint8_t *plane, int pw, int ph, int stride, int x0, int y0, int n,
+                          int mode, int have_top, int have_left, int have_right);
 
 /* Loop filter in place on a luma plane: REFCPU (level 0 = off) or SPEC
  * (threshold floored at 1, always on). */

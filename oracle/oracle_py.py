@@ -2,7 +2,7 @@
 tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, never by the
 product package.
 
-    OracleStream(profile)   the restatement in oracle/*.c (REFCPU or SPEC)
+    OracleStream(profile)   the restatement in oracle/*.c (REFCPU, SPEC or FULL)
     RefStream()             the reference's own vp9_reconstruct_frame compiled
                             from its sources (oracle/_ref), REFCPU only
 """
@@ -18,6 +18,7 @@ REF_LIB = os.path.join(HERE, "_ref", "libvp9ref.so")
 
 REFCPU = 0
 SPEC = 1
+FULL = 2
 
 _orc = None
 _ref = None
@@ -54,6 +55,13 @@ def oracle_lib():
         lib.oracle_spec_intra_block.restype = None
         lib.oracle_spec_mc_block.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 10
         lib.oracle_spec_mc_block.restype = None
+        lib.oracle_full_itx2d.argtypes = [C.c_void_p, C.c_void_p] + [C.c_int] * 5
+        lib.oracle_full_itx2d.restype = None
+        lib.oracle_full_mc_block.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p] + \
+            [C.c_int] * 14
+        lib.oracle_full_mc_block.restype = None
+        lib.oracle_full_intra_tx.argtypes = [C.c_void_p] + [C.c_int] * 10
+        lib.oracle_full_intra_tx.restype = None
         lib.oracle_dc_quant.argtypes = [C.c_int]
         lib.oracle_ac_quant.argtypes = [C.c_int]
         _orc = lib
@@ -182,4 +190,30 @@ def spec_mc_block(ref, dst_shape, x, y, bw, bh, mvx, mvy, chroma=0):
     oracle_lib().oracle_spec_mc_block(r.ctypes.data, r.shape[1], r.shape[0], r.shape[1],
                                       d.ctypes.data, d.shape[1], d.shape[0], d.shape[1],
                                       x, y, bw, bh, mvx, mvy, chroma)
+    return d
+
+
+def full_itx2d(coeffs, tx_type, q_dc, q_ac, lossless=0):
+    n = coeffs.shape[0]
+    x = np.ascontiguousarray(coeffs, np.int16)
+    out = np.empty((n, n), np.int32)
+    oracle_lib().oracle_full_itx2d(x.ctypes.data, out.ctypes.data, n, tx_type, lossless, q_dc, q_ac)
+    return out
+
+
+def full_intra_tx(plane, x0, y0, n, mode, have_top, have_left, have_right):
+    """FULL intra prediction of one TX; returns the plane after it."""
+    p = np.ascontiguousarray(plane, np.uint8).copy()
+    h, w = p.shape
+    oracle_lib().oracle_full_intra_tx(p.ctypes.data, w, h, w, x0, y0, n, mode, have_top, have_left, have_right)
+    return p
+
+
+def full_mc_block(ref0, ref1, dst_shape, x, y, bw, bh, mv0, mv1=(0, 0), compound=0, filt=0, chroma=0):
+    r0 = np.ascontiguousarray(ref0, np.uint8)
+    r1 = np.ascontiguousarray(ref1 if ref1 is not None else ref0, np.uint8)
+    d = np.zeros(dst_shape, np.uint8)
+    oracle_lib().oracle_full_mc_block(r0.ctypes.data, r1.ctypes.data, r0.shape[1], r0.shape[0], r0.shape[1],
+                                      d.ctypes.data, d.shape[1], d.shape[0], d.shape[1], x, y, bw, bh,
+                                      mv0[0], mv0[1], mv1[0], mv1[1], compound, filt, chroma)
     return d

@@ -336,7 +336,7 @@ static void idct32(const int *in, int *out)
     }
 }
 
-static void idct1d(int n, const int *in, int *out)
+void oracle_idct1d(int n, const int *in, int *out)
 {
     int tmp[32];
     memcpy(tmp, in, (size_t)n * sizeof(int));
@@ -356,11 +356,11 @@ void oracle_spec_idct2d(const int16_t *in, int32_t *out, int n, int q_dc, int q_
     int col[32], res[32];
     for (int c = 0; c < n; c++) {
         for (int r = 0; r < n; r++) col[r] = (int)in[r * n + c] * ((r == 0 && c == 0) ? q_dc : q_ac);
-        idct1d(n, col, res);
+        oracle_idct1d(n, col, res);
         for (int r = 0; r < n; r++) buf[r][c] = res[r];
     }
     for (int r = 0; r < n; r++) {
-        idct1d(n, buf[r], res);
+        oracle_idct1d(n, buf[r], res);
         for (int c = 0; c < n; c++) buf[r][c] = res[c];
     }
     int sh = n == 4 ? 4 : (n == 8 ? 5 : 6);

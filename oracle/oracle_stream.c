@@ -5,7 +5,7 @@
  * Pool rules:
  *   REFCPU — src/decoder/vp9_decoder.c:224-231: a key frame is copied into
  *            all 8 slots, any other frame into slot 0 only.
- *   SPEC   — src/backend/vulkan/vulkan_backend.c:1312-1354: the slots set in
+ *   SPEC, FULL — src/backend/vulkan/vulkan_backend.c:1312-1354: the slots set in
  *            refresh_frame_flags (0 means 0x01) take the new frame; here all
  *            three planes, where the Vulkan skeleton copies luma only.
  */
@@ -53,6 +53,7 @@ int oracle_stream_decode(oracle_stream_t *s, const vp9_parsed_frame_t *pf, uint8
 
     oracle_frame_t out = {0};
     int ok = s->profile == ORACLE_SPEC ? oracle_spec_reconstruct(pf, refs, &out)
+           : s->profile == ORACLE_FULL ? oracle_full_reconstruct(pf, refs, &out)
                                        : oracle_refcpu_reconstruct(pf, refs, &out);
     if (!ok) return 0;
 
@@ -64,7 +65,7 @@ int oracle_stream_decode(oracle_stream_t *s, const vp9_parsed_frame_t *pf, uint8
         memcpy(out_i420 + ny + nc, out.v, nc);
     }
 
-    if (s->profile == ORACLE_SPEC) {
+    if (s->profile != ORACLE_REFCPU) {
         unsigned refresh = pf->hdr.refresh_frame_flags ? pf->hdr.refresh_frame_flags : 0x01u;
         for (int i = 0; i < 8; i++)
             if (refresh & (1u << i)) copy_frame(&s->slot[i], &out);

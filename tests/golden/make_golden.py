@@ -12,9 +12,11 @@ spec_frames.json    the same for the SPEC restatement (oracle/), so its output
                     is frozen against accidental change.
 layout.json         sizeof/offsetof of the boundary structs as the reference
                     headers compile them.
-tables.json         SHA-256 of the quantiser tables and the regular 8-tap
-                    filter as the reference sources spell them
-                    (src/decoder/vp9_dequant.h:12-60, shaders/vp9_mc.comp.glsl:40-57).
+tables.json         SHA-256 of the quantiser tables, the regular 8-tap filter and
+                    the intra-mode -> transform-type map as the reference
+                    sources spell them (src/decoder/vp9_dequant.h:12-60,
+                    shaders/vp9_mc.comp.glsl:40-57,
+                    src/decoder/vp9_default_probs.h:1728).
 spec_idct.json      input/output vectors of the shader inverse transforms,
                     computed by a mechanical translation of
                     shaders/vp9_idct.comp.glsl's idct4/8/16/32 functions and
@@ -80,7 +82,11 @@ def table_hash():
     m = re.search(r"SUBPEL_FILTER\[16\]\[8\] = int\[16\]\[8\]\((.*?)\);", g, re.S)
     rows = re.findall(r"int\[8\]\(([^)]*)\)", m.group(1))
     filt = [[int(x) for x in r.split(",")] for r in rows]
+    d = open(os.path.join(REF, "src/decoder/vp9_default_probs.h")).read()
+    m = re.search(r"vp9_intra_mode_to_tx_type\[10\] = \{([^}]*)\}", d)
+    txt = [int(x) for x in m.group(1).split(",")]
     return {
+        "intra_tx_type_sha256": hashlib.sha256(np.array(txt, np.int32).tobytes()).hexdigest(),
         "dc_q_sha256": hashlib.sha256(np.array(vals[0], np.int32).tobytes()).hexdigest(),
         "ac_q_sha256": hashlib.sha256(np.array(vals[1], np.int32).tobytes()).hexdigest(),
         "subpel_regular_sha256": hashlib.sha256(np.array(filt, np.int32).tobytes()).hexdigest(),

@@ -253,3 +253,25 @@ def test_packed_coefficients_match_oracle(profile, pinned):
         assert 0 < st.h2d_bytes < dense
         assert st.kernel_launches >= 1
     eng.close()
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_launch_count_follows_inter_path(profile, monkeypatch):
+    """kernel_launches counts the inter path's kernels in both profiles:
+    k_inter + k_compact (path 1) or k_pred + k_resid + k_compact (path 3)
+    on top of the general chain (path 0)."""
+    monkeypatch.setenv("CVP9_AUTOTUNE", "0")
+    counts = {}
+    for variant in ("0", "1", "3"):
+        monkeypatch.setenv("CVP9_INTER_FAST", variant)
+        eng = Batch(arith=profile, use_graphs=0)
+        p, w, h, ov = mix_for(profile, [MIX[1]])[0]
+        syn = Synth(synth_config(p, w, h, seed=10, **ov))
+        sid = eng.open_stream(w, h)
+        for f in range(2):
+            eng.submit([sid], [syn.frame(f)], [f])
+            assert eng.wait() == CVP9_OK, eng.last_error()
+        counts[variant] = eng.stats().kernel_launches
+        eng.close()
+    assert counts["1"] - counts["0"] == 2, counts
+    assert counts["3"] - counts["0"] == 3, counts

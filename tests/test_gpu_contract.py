@@ -22,9 +22,9 @@ import numpy as np
 import pytest
 
 from compute_vp9_b200 import (CVP9_ERR_AGAIN, CVP9_ERR_INVALID_DATA, CVP9_ERR_UNSUPPORTED, CVP9_OK,
-                              CudaBackend, DmabufFrame, ExportBuffer, FrameInfo, Synth, cuda_lib,
+                              CudaBackend, DmabufFrame, ExportBuffer, Synth, cuda_lib,
                               i420_size, synth_config)
-from compute_vp9_b200.batch import Batch
+from compute_vp9_b200.batch import Batch, BatchError
 from oracle.oracle_py import REFCPU, SPEC, OracleStream, nv12_pack
 from profiles import overrides_for
 
@@ -118,7 +118,6 @@ def test_inflight_ring(profile):
     want = [orc.decode(syn.frame(f)) for f in range(8)]
 
     # empty ring
-    info = FrameInfo()
     assert gpu.get_frame(wait=0)[0] == CVP9_ERR_UNSUPPORTED
     assert gpu.get_frame(wait=1)[0] == CVP9_ERR_UNSUPPORTED
 
@@ -174,7 +173,9 @@ def test_spec_rejects_filters_it_does_not_hold(filt):
 
     eng = Batch(arith=SPEC)
     sid = eng.open_stream(w, h)
-    assert eng.submit([sid], [syn.frame(0)], [0]) == CVP9_ERR_UNSUPPORTED
+    with pytest.raises(BatchError) as e:
+        eng.submit([sid], [syn.frame(0)], [0])
+    assert e.value.code == CVP9_ERR_UNSUPPORTED
     assert "filter" in eng.last_error()
     eng.close()
 

@@ -59,6 +59,9 @@ def test_tables_match_reference():
     assert len(taps) == 128
     assert hashlib.sha256(np.array(taps, np.int32).reshape(16, 8).tobytes()).hexdigest() == \
         want["subpel_regular_sha256"]
+    m = re.search(r"CVP9_INTRA_TX_TYPE_INIT \{([^}]*)\}", text)
+    txt = [int(x) for x in m.group(1).split(",")]
+    assert hashlib.sha256(np.array(txt, np.int32).tobytes()).hexdigest() == want["intra_tx_type_sha256"]
 
 
 def test_dct_basis_identical_to_oracle():
