@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 from .cvp9_ctypes import (  # noqa: F401
-    ARITH_REFCPU, ARITH_SPEC, CVP9_ERR_AGAIN, CVP9_ERR_GPU, CVP9_ERR_INVALID_DATA,
+    ARITH_FULL, ARITH_REFCPU, ARITH_SPEC, CVP9_ERR_AGAIN, CVP9_ERR_GPU, CVP9_ERR_INVALID_DATA,
     CVP9_ERR_UNSUPPORTED, CVP9_OK, ERR_NAMES, BlockInfo, DmabufFrame, ExportBuffer,
     FrameHeader, FrameInfo, MV, ParsedFrame, SynthConfig, i420_size, layout_offsets,
 )

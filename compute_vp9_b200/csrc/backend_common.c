@@ -64,7 +64,7 @@ int cvp9_device_setup(int device)
 int cvp9_recon_ctas_per_sm(int device, int arith)
 {
     if (device < 0 || device >= MAX_DEVICES) return 1;
-    int v = g_ctas[device][arith == CVP9_ARITH_SPEC ? 1 : 0];
+    int v = g_ctas[device][arith != CVP9_ARITH_REFCPU ? 1 : 0];    /* FULL runs the SPEC kernel */
     return v > 0 ? v : 1;
 }
 
@@ -118,14 +118,44 @@ int cvp9_env_arith(void)
 {
     const char *e = getenv("CVP9_ARITH");
     if (e && (strcmp(e, "spec") == 0 || strcmp(e, "SPEC") == 0)) return CVP9_ARITH_SPEC;
+    if (e && (strcmp(e, "full") == 0 || strcmp(e, "FULL") == 0)) return CVP9_ARITH_FULL;
     return CVP9_ARITH_REFCPU;
 }
 
 int cvp9_filter_supported(int arith, int interp_filter, const char **why)
 {
     if (arith == CVP9_ARITH_REFCPU || interp_filter == VP9_FILTER_EIGHTTAP) return 1;
-    if (why) *why = "interpolation filter other than EIGHTTAP: the shader profile holds the regular 8-tap table only";
+    if (arith == CVP9_ARITH_FULL && interp_filter >= 0 && interp_filter <= VP9_FILTER_BILINEAR) return 1;
+    if (why) *why = arith == CVP9_ARITH_FULL
+        ? "SWITCHABLE interpolation filter: the parsed block record carries no per-block filter"
+        : "interpolation filter other than EIGHTTAP: the shader profile holds the regular 8-tap table only";
     return 0;
+}
+
+int cvp9_frame_supported(int arith, const vp9_parsed_frame_t *pf, const char **why)
+{
+    const int inter = pf->hdr.frame_type != VP9_FRAME_KEY && !pf->hdr.intra_only;
+    if (arith == CVP9_ARITH_FULL && ((pf->hdr.width & 7) || (pf->hdr.height & 7))) {
+        if (why) *why = "the VP9 profile takes frames whose sizes are multiples of 8";
+        return 0;
+    }
+    /* intra frames carry no filter; only inter frames are held to it */
+    return inter ? cvp9_filter_supported(arith, (int)pf->hdr.interp_filter, why) : 1;
+}
+
+void cvp9_job_full(cvp9_job_t *job, const vp9_parsed_frame_t *pf)
+{
+    const vp9_frame_header_t *h = &pf->hdr;
+    const int q = h->base_qindex;
+    const int inter = h->frame_type != VP9_FRAME_KEY && !h->intra_only;
+    job->full = 1;
+    job->q_dc = cvp9_dc_q(q + h->y_dc_delta_q);
+    job->q_ac = cvp9_ac_q(q);
+    job->q_dc_uv = cvp9_dc_q(q + h->uv_dc_delta_q);
+    job->q_ac_uv = cvp9_ac_q(q + h->uv_ac_delta_q);
+    job->lossless = (uint8_t)(q == 0 && h->y_dc_delta_q == 0 && h->uv_dc_delta_q == 0 && h->uv_ac_delta_q == 0);
+    job->interp_filter = (uint8_t)(inter ? (h->interp_filter & 3) : 0);
+    job->log2_tile_cols = h->log2_tile_cols;
 }
 
 void cvp9_job_geometry(cvp9_job_t *job, const vp9_parsed_frame_t *pf)
@@ -177,6 +207,9 @@ void cvp9_tuner_init(cvp9_tuner_t *t, int arith, int enabled, cvp9_tcfg_t fixed)
     t->arith = arith;
     t->enabled = enabled;
     t->fixed = fixed;
+    /* FULL: every superblock goes through the general kernel and the VP9
+     * loop filter has one layout; only the wavefront width is tuned */
+    if (arith == CVP9_ARITH_FULL) { t->fixed.inter = 0; t->fixed.lf32 = 0; }
 }
 
 static int same_cfg(cvp9_tcfg_t a, cvp9_tcfg_t b)
@@ -194,7 +227,7 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
              * kernel alone, k_inter at 80 registers, the two-kernel split
              * and (REFCPU) the split walking 8x8 TXs per TX */
             static const int8_t alts[4] = { 0, 2, 3, 4 };
-            if (e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 3)) {
+            if (t->arith != CVP9_ARITH_FULL && e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 3)) {
                 e->cur = e->best;
                 e->cur.inter = alts[e->idx - 1];
                 break;
@@ -202,7 +235,7 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
             e->stage = 1;
             e->idx = 0;
         } else if (e->stage == 1) {
-            if (e->idx == 1) { e->cur = e->best; e->cur.lf32 = 1; break; }
+            if (e->idx == 1 && t->arith != CVP9_ARITH_FULL) { e->cur = e->best; e->cur.lf32 = 1; break; }
             e->stage = 2;
             e->idx = 0;
         } else if (e->stage == 2) {

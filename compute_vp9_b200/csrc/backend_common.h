@@ -35,7 +35,7 @@ int cvp9_tickets_on_diagonal(int sb_cols, int sb_rows, int job, int d, uint32_t 
 int cvp9_dc_q(int qindex);
 int cvp9_ac_q(int qindex);
 
-/* Environment knobs: $CVP9_CUDA_DEVICE, $CVP9_ARITH (refcpu|spec),
+/* Environment knobs: $CVP9_CUDA_DEVICE, $CVP9_ARITH (refcpu|spec|full),
  * $CVP9_INTER_FAST (warp-per-superblock inter path: 0 off, 1 the
  * 96-register kernel, 2 the 80-register kernel, 3 the two-kernel split,
  * k_pred + k_resid, 4 (REFCPU) the split with 8x8 TXs walked per TX;
@@ -56,6 +56,15 @@ int cvp9_env_pack(int configured);
  * shaders hold the regular table alone, shaders/vp9_mc.comp.glsl:40-57).
  * On 0, *why names the reason for the caller's error text. */
 int cvp9_filter_supported(int arith, int interp_filter, const char **why);
+
+/* Whether the profile takes this frame: the filter rule above on inter
+ * frames; FULL also wants both sizes multiples of 8 (its transform and
+ * loop-filter edges then end inside the frame, as the MI grid does). */
+int cvp9_frame_supported(int arith, const vp9_parsed_frame_t *pf, const char **why);
+
+/* The FULL profile's fields of a job: per-plane quantiser steps with the
+ * header's delta_q values, lossless, the frame's filter, the tile columns. */
+void cvp9_job_full(cvp9_job_t *job, const vp9_parsed_frame_t *pf);
 
 /* Fill the frame-geometry and parameter fields of a job from a parsed
  * frame (inputs, output, refs and scratch pointers are set by the caller). */

@@ -48,6 +48,8 @@ typedef struct {
     int32_t   W, H;
     int       n_sb;
     uint32_t *d_sb_done;
+    uint32_t *d_mi_map;         /* FULL loop filter: mode info per 8x8 MI   */
+    size_t    mi_cap;           /* its entries                              */
     uint32_t  epoch;
     bframe_t  f[MAXF];
     int       ref_slot[8];
@@ -168,7 +170,9 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     cvp9_batch_t *b = calloc(1, sizeof(*b));
     if (!b) return CVP9_ERR_NOMEM;
     b->device = (cfg && cfg->device >= 0) ? cfg->device : cvp9_env_device();
-    b->arith = (cfg && cfg->arith >= 0) ? (cfg->arith ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU) : cvp9_env_arith();
+    b->arith = (cfg && cfg->arith >= 0) ? (cfg->arith == 2 ? CVP9_ARITH_FULL : cfg->arith ? CVP9_ARITH_SPEC
+                                                                                : CVP9_ARITH_REFCPU)
+                                        : cvp9_env_arith();
     b->budget = (cfg && cfg->hbm_budget) ? cfg->hbm_budget : 150ull * 1000 * 1000 * 1000;
     b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
     b->use_graphs = cfg ? cfg->use_graphs : 1;
@@ -231,6 +235,7 @@ static void free_stream(cvp9_batch_t *b, bstream_t *s)
 {
     for (int i = 0; i < MAXF; i++) arena_free(&b->dev, s->f[i].dev, s->f[i].cap);
     arena_free(&b->dev, s->d_sb_done, (size_t)s->sb_cap * 4);
+    arena_free(&b->dev, s->d_mi_map, s->mi_cap * 4);
     arena_free(&b->pin, s->h_out[0], s->h_out_cap[0]);
     arena_free(&b->pin, s->h_out[1], s->h_out_cap[1]);
     memset(s, 0, sizeof(*s));
@@ -318,6 +323,23 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
     if (cudaMemsetAsync(s->d_sb_done, 0, (size_t)n_sb * 4, b->cs) != cudaSuccess) {
         free_stream(b, s);
         return CVP9_ERR_NOMEM;
+    }
+    if (b->arith == CVP9_ARITH_FULL) {
+        const size_t nmi = (size_t)((w + 7) / 8) * ((h + 7) / 8);
+        if (s->mi_cap < nmi) {
+            arena_free(&b->dev, s->d_mi_map, s->mi_cap * 4);
+            s->d_mi_map = (uint32_t *)arena_alloc(&b->dev, nmi * 4);
+            s->mi_cap = s->d_mi_map ? nmi : 0;
+            if (!s->d_mi_map) {
+                free_stream(b, s);
+                return CVP9_ERR_NOMEM;
+            }
+        }
+        /* entries carry the frame epoch, which restarts with the stream */
+        if (cudaMemsetAsync(s->d_mi_map, 0, nmi * 4, b->cs) != cudaSuccess) {
+            free_stream(b, s);
+            return CVP9_ERR_NOMEM;
+        }
     }
     /* both download buffers now, so no pinned allocation happens per step */
     {
@@ -596,10 +618,20 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             return CVP9_ERR_INVALID_DATA;
         for (int j = 0; j < i; j++) if (sids[j] == sid) return CVP9_ERR_INVALID_DATA;
         const char *why = NULL;
-        if (!cvp9_filter_supported(b->arith, (int)pf->hdr.interp_filter, &why)) {
+        if (!cvp9_frame_supported(b->arith, pf, &why)) {
             snprintf(b->err, sizeof(b->err), "stream %d: %s", sid, why);
             return CVP9_ERR_UNSUPPORTED;
         }
+        if (b->arith == CVP9_ARITH_FULL && pf->hdr.frame_type != VP9_FRAME_KEY && !pf->hdr.intra_only)
+            for (int k = 0; k < 3; k++) {
+                const bstream_t *st = &b->st[sid];
+                int f = st->ref_slot[pf->hdr.ref_frame_idx[k] & 7];
+                if (f >= 0 && (st->f[f].w != st->W || st->f[f].h != st->H)) {
+                    snprintf(b->err, sizeof(b->err), "stream %d: reference of another size "
+                             "(scaled motion compensation is not built)", sid);
+                    return CVP9_ERR_UNSUPPORTED;
+                }
+            }
     }
 
     const uint64_t seq = b->seq + 1;
@@ -614,7 +646,9 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     b->submit_pack_ms = 0.f;
 
     /* sizes */
+    const int full = b->arith == CVP9_ARITH_FULL;
     size_t in_bytes = 0, n_sb = 0;
+    int max_sbr = 0;
     int max_blocks = 0, max_mi = 0, lf_tx = 0, lf_ty = 0, lf_sx = 0, lf_sy = 0;
     int flat_w = 0, flat_h = 0, flat_nv = 0;
     int maxd = 0;
@@ -649,6 +683,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         }
         int d = (st->W + 63) / 64 + (st->H + 63) / 64 - 1;
         if (d > maxd) maxd = d;
+        if ((st->H + 63) / 64 > max_sbr) max_sbr = (st->H + 63) / 64;
         key = mix64(key, ((uint64_t)st->W << 32) | (uint64_t)st->H);
     }
 
@@ -731,8 +766,8 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             return err;
         s->jobs_cap = cap;
     }
-    if (s->misc_cap < 2 * n + 2) {
-        int cap = 2 * (n > b->nst ? n : b->nst) + 2;
+    if (s->misc_cap < 2 * n + 3) {
+        int cap = 2 * (n > b->nst ? n : b->nst) + 3;
         s->misc_cap = 0;
         if ((err = grow_host(b, (void **)&s->h_misc, &s->h_misc_bytes, (size_t)cap * 4)) ||
             (err = grow_dev(b, (void **)&s->d_misc, &s->d_misc_bytes, (size_t)cap * 4)))
@@ -839,6 +874,11 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         cvp9_job_t *job = &s->h_jobs[i];
         memset(job, 0, sizeof(*job));
         cvp9_job_geometry(job, pf);
+        if (full) {
+            cvp9_job_full(job, pf);
+            job->mi_map = st->d_mi_map;
+            job->lf_tiled = 0;                  /* the VP9 filter replaces the others */
+        }
         if (job->lf_tiled && !tc.lf32 && !(st->W & 3)) job->lf_tiled = 2;   /* register strips */
         any_tile |= job->lf_tiled == 1;
         any_strip |= job->lf_tiled == 2;
@@ -906,7 +946,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     memset(&L, 0, sizeof(L));
     L.jobs = s->d_jobs;
     L.njobs = n;
-    L.arith = b->arith;
+    L.arith = full ? CVP9_ARITH_SPEC : b->arith;
     L.max_blocks = max_blocks;
     L.scan_ctas = (max_mi + 255) / 256;
     L.tickets = s->d_tickets;
@@ -930,17 +970,25 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     L.flat_lf_max_w = flat_w;
     L.flat_lf_max_h = flat_h;
     L.flat_nv12 = flat_nv;
+    if (full) {
+        L.full = 1;
+        L.lf_counter = s->d_misc + 2 * (size_t)n + 2;
+        L.lf_tickets = (uint32_t)(n * max_sbr);
+        L.lf_ctas = b->resident_ctas;
+    }
     for (int k = 0; k < 4; k++) L.ev[k] = s->ev_kern[k];
     uint64_t gkey = mix64(mix64(mix64(key, (uint64_t)(uintptr_t)s->d_jobs), (uint64_t)(uintptr_t)s->d_sb_range),
                           mix64((uint64_t)(uintptr_t)s->d_misc, (uint64_t)(uintptr_t)s->d_tickets));
     gkey = mix64(gkey, ((uint64_t)L.scan_ctas << 32) | (uint64_t)L.recon_ctas);
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
     gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
+    gkey = mix64(gkey, ((uint64_t)L.full << 32) | (uint64_t)L.lf_tickets);
     /* k_inter + k_compact, or k_pred + k_resid + k_compact (the split, both
      * profiles: cvp9k_launch_frame dispatches inter paths 3 and 4 to it) */
     const int split = L.inter_variant >= 3;
-    s->launches = (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
-                             (L.general ? (split ? 3 : 2) : 0));
+    s->launches = full ? (uint32_t)(2 * (L.scan_ctas > 0) + 1 + 1)     /* scan, mode info, recon, VP9 filter */
+                       : (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
+                                    (L.general ? (split ? 3 : 2) : 0));
     if (b->use_graphs) {
         if (!s->graph || s->graph_key != gkey) {
             if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = NULL; }
@@ -948,6 +996,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             BCK(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal), "graph capture");
             cudaMemsetAsync(s->d_sb_range, 0, n_sb * 16, b->cs);
             cudaMemsetAsync(s->d_misc, 0, (size_t)(n + 1) * 4, b->cs);
+            if (full) cudaMemsetAsync(L.lf_counter, 0, 4, b->cs);
             int lrc = cvp9k_launch_frame(&L, b->cs);
             cudaError_t ce = cudaStreamEndCapture(b->cs, &g);
             if (lrc != 0 || ce != cudaSuccess) {
@@ -966,6 +1015,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     } else {
         BCK(cudaMemsetAsync(s->d_sb_range, 0, n_sb * 16, b->cs), "clear sb_range");
         BCK(cudaMemsetAsync(s->d_misc, 0, (size_t)(n + 1) * 4, b->cs), "clear status");
+        if (full) BCK(cudaMemsetAsync(L.lf_counter, 0, 4, b->cs), "clear filter tickets");
         int lrc = cvp9k_launch_frame(&L, b->cs);
         if (lrc != 0) return bfail(b, (cudaError_t)lrc, "launch");
     }
@@ -995,7 +1045,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         st->last_seq = seq;
         /* pool update, as the per-stream backend does */
         const vp9_parsed_frame_t *pf = pfs[i];
-        if (b->arith == CVP9_ARITH_SPEC) {
+        if (b->arith != CVP9_ARITH_REFCPU) {
             unsigned refresh = pf->hdr.refresh_frame_flags ? pf->hdr.refresh_frame_flags : 0x01u;
             for (int r = 0; r < 8; r++) if (refresh & (1u << r)) set_ref(st, r, ofr[i]);
         } else if (pf->hdr.frame_type == VP9_FRAME_KEY) {

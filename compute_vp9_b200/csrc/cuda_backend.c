@@ -81,9 +81,10 @@ typedef struct {
     /* per-geometry scratch */
     uint32_t    *d_sb_range;           /* 4 * n_sb, zeroed per frame    */
     uint32_t    *d_sb_done;            /* n_sb                          */
-    uint32_t    *d_misc;               /* [0] status, [1] ticket counter */
+    uint32_t    *d_misc;               /* [0] status, [1] ticket counter, [2] filter tickets */
     uint32_t    *d_tickets;
     uint32_t    *d_fast;               /* inter fast path: general flags, tickets, count */
+    uint32_t    *d_mi_map;             /* FULL loop filter: mode info per 8x8 MI          */
     cvp9_tuner_t tuner;                /* kernel configuration per frame size */
     int          resident_ctas;
     uint32_t     n_tickets;
@@ -128,7 +129,8 @@ static void free_geometry(cuctx_t *c)
     cudaFree(c->d_sb_done);
     cudaFree(c->d_tickets);
     cudaFree(c->d_fast);
-    c->d_sb_range = c->d_sb_done = c->d_tickets = c->d_fast = NULL;
+    cudaFree(c->d_mi_map);
+    c->d_sb_range = c->d_sb_done = c->d_tickets = c->d_fast = c->d_mi_map = NULL;
     c->n_tickets = 0;
 }
 
@@ -141,7 +143,8 @@ cvp9_err_t cuda_backend_init_ex(void **out, const cuda_backend_options_t *opt)
     cuctx_t *c = calloc(1, sizeof(*c));
     if (!c) return CVP9_ERR_NOMEM;
     c->device = (opt && opt->device >= 0) ? opt->device : cvp9_env_device();
-    c->arith = (opt && opt->arith >= 0) ? (opt->arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU)
+    c->arith = (opt && opt->arith >= 0) ? (opt->arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC
+                                           : opt->arith == CVP9_CUDA_ARITH_FULL ? CVP9_ARITH_FULL : CVP9_ARITH_REFCPU)
                                         : cvp9_env_arith();
     {
         cvp9_tcfg_t fixed = { (int8_t)cvp9_env_inter_fast(), 0, 0 };
@@ -207,6 +210,11 @@ static cvp9_err_t set_geometry(cuctx_t *c, int32_t W, int32_t H)
     CK(cudaMemset(c->d_sb_done, 0, (size_t)c->n_sb * 4), "clear sb_done");
     CK(cudaMalloc((void **)&c->d_tickets, (size_t)c->n_sb * 4), "alloc tickets");
     CK(cudaMalloc((void **)&c->d_fast, (size_t)(2 * c->n_sb + 2) * 4), "alloc fast-path scratch");
+    if (c->arith == CVP9_ARITH_FULL) {
+        size_t nmi = (size_t)((W + 7) / 8) * ((H + 7) / 8);
+        CK(cudaMalloc((void **)&c->d_mi_map, nmi * 4), "alloc mode-info map");
+        CK(cudaMemset(c->d_mi_map, 0, nmi * 4), "clear mode-info map");
+    }
     uint32_t *t = malloc((size_t)c->n_sb * 4);
     if (!t) return CVP9_ERR_NOMEM;
     uint32_t n = 0;
@@ -292,10 +300,20 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     if (pf->num_blocks && !pf->blocks) return CVP9_ERR_INVALID_DATA;
     if (pf->num_coeffs && !pf->coeffs) return CVP9_ERR_INVALID_DATA;
     const char *why = NULL;
-    if (!cvp9_filter_supported(c->arith, (int)pf->hdr.interp_filter, &why)) {
+    if (!cvp9_frame_supported(c->arith, pf, &why)) {
         snprintf(c->last_error, sizeof(c->last_error), "%s", why);
         return CVP9_ERR_UNSUPPORTED;
     }
+    if (c->arith == CVP9_ARITH_FULL && pf->hdr.frame_type != VP9_FRAME_KEY && !pf->hdr.intra_only)
+        for (int k = 0; k < 3; k++) {
+            int f = c->ref_slot[pf->hdr.ref_frame_idx[k] & 7];
+            if (f >= 0 && (c->frames[f].w != W || c->frames[f].h != H)) {
+                snprintf(c->last_error, sizeof(c->last_error),
+                         "reference %d is %dx%d: scaled motion compensation is not built", k,
+                         (int)c->frames[f].w, (int)c->frames[f].h);
+                return CVP9_ERR_UNSUPPORTED;
+            }
+        }
     if (cudaSetDevice(c->device) != cudaSuccess) return CVP9_ERR_GPU;
 
     cvp9_err_t err;
@@ -330,6 +348,11 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     cvp9_job_t *job = s->h_job;
     memset(job, 0, sizeof(*job));
     cvp9_job_geometry(job, pf);
+    const int full = c->arith == CVP9_ARITH_FULL;
+    if (full) {
+        cvp9_job_full(job, pf);
+        job->mi_map = c->d_mi_map;
+    }
     cvp9_tcfg_t tc;
     s->tune_idx = cvp9_tuner_pick(&c->tuner, cvp9_tune_key(c->arith, 1, (uint64_t)c->n_sb), 1, &tc);
     s->tune_cfg = tc;
@@ -357,14 +380,14 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     if (ncb) CK(cudaMemcpyAsync(s->d_coeffs, s->h_coeffs, ncb, cudaMemcpyHostToDevice, st), "upload coeffs");
     CK(cudaMemcpyAsync(s->d_job, job, sizeof(*job), cudaMemcpyHostToDevice, st), "upload job");
     CK(cudaMemsetAsync(c->d_sb_range, 0, (size_t)c->n_sb * 16, st), "clear sb_range");
-    CK(cudaMemsetAsync(c->d_misc, 0, 8, st), "clear status");
+    CK(cudaMemsetAsync(c->d_misc, 0, 12, st), "clear status");
     CK(cudaEventRecord(s->ev_k0, st), "event");
 
     cvp9k_launch_t L;
     memset(&L, 0, sizeof(L));
     L.jobs = s->d_job;
     L.njobs = 1;
-    L.arith = c->arith;
+    L.arith = full ? CVP9_ARITH_SPEC : c->arith;
     L.max_blocks = (int)pf->num_blocks;
     L.tickets = c->d_tickets;
     L.n_tickets = c->n_tickets;
@@ -377,7 +400,13 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
         L.n_general = c->d_fast + 2 * c->n_sb;
         L.inter_variant = tc.inter;
     }
-    if (job->lf_tiled == 2) {
+    if (full) {
+        L.full = 1;
+        L.lf_counter = c->d_misc + 2;
+        L.lf_tickets = (uint32_t)c->sb_rows;
+        L.lf_ctas = c->sb_rows;
+        L.full_nv12_max_px = job->nv12 ? W * H : 0;
+    } else if (job->lf_tiled == 2) {
         L.lf_strips_x = ((W + 4 + 7) / 8 + 127) / 128;
         L.lf_strips_y = (H + 4 + 15) / 16;
     } else if (job->lf_tiled) {
@@ -396,7 +425,7 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     CK(cudaEventRecord(s->ev_end, st), "event");
 
     /* reference pool update (host bookkeeping; stream order protects reuse) */
-    if (c->arith == CVP9_ARITH_SPEC) {
+    if (c->arith != CVP9_ARITH_REFCPU) {
         unsigned refresh = pf->hdr.refresh_frame_flags ? pf->hdr.refresh_frame_flags : 0x01u;
         for (int i = 0; i < 8; i++) if (refresh & (1u << i)) set_ref(c, i, of);
     } else if (pf->hdr.frame_type == VP9_FRAME_KEY) {

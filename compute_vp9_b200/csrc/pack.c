@@ -216,7 +216,7 @@ int64_t cvp9_pack_coeffs(int arith, const vp9_parsed_frame_t *pf, uint32_t *out,
     k.np = (uint32_t)(((uint64_t)n + PAGE_LEN - 1) >> PAGE_SHIFT);
     k.start = align4(1u + 2u * k.np);
     out[0] = k.np;
-    if (arith == CVP9_ARITH_SPEC) {
+    if (arith != CVP9_ARITH_REFCPU) {     /* SPEC and FULL read every plane */
         pack_range(&k, 0, n);
     } else {
         /* each block's luma TX span, as k_gather_luma moves it */

@@ -58,6 +58,10 @@ constexpr long long kSpinLimit = 1ll << 20;   /* ~0.25 s of polling */
 
 __constant__ double c_dct[16 + 64 + 256 + 1024];      /* N = 4, 8, 16, 32 */
 __constant__ int c_subpel[16][8] = CVP9_SUBPEL_REGULAR_INIT;
+/* FULL: the frame header's filter, interp_filter 0..3 */
+__constant__ int c_subpel4[4][16][8] = { CVP9_SUBPEL_REGULAR_INIT, CVP9_SUBPEL_SMOOTH_INIT,
+                                         CVP9_SUBPEL_SHARP_INIT, CVP9_SUBPEL_BILINEAR_INIT };
+__constant__ uint8_t c_tx_type[10] = CVP9_INTRA_TX_TYPE_INIT;
 /* the same taps as signed bytes, taps 0-3 and 4-7 in two words, for dp4a
  * (phase 0's 128 does not fit a byte: callers take the centre sample for
  * it, which is what its filter computes); uploaded by cvp9k_configure */
@@ -297,11 +301,14 @@ struct BlkS {
     uint8_t  ref0;
     uint8_t  ptxl[3];       /* residual TX log2-4 per plane                */
     uint8_t  pnx[3];        /* residual TXs per row per plane              */
-    uint8_t  pad;
+    uint8_t  ref1;          /* FULL: second reference of a compound block  */
     uint16_t pnt[3];        /* residual TX count per plane                 */
     int16_t  mvx, mvy;
+    int16_t  mv1x, mv1y;    /* FULL: its MV                                */
     uint32_t coeff;
 };
+/* BlkS.flags: 1 intra, 2 skip, 4 FULL intra (one warp predicts and
+ * reconstructs the block TX by TX; no residual items) */
 
 struct ReconSmem {
     union {
@@ -351,6 +358,33 @@ __device__ __forceinline__ int max_tx_for(int w, int h)
  * REFCPU: luma only, counts from the frame-clamped size
  * (vp9_reconstruct.c:336-347). SPEC: every plane in the tile parser's layout
  * (vp9_kf_tile.c:320-396): coded area clipped at the MI-aligned frame edge. */
+/* The tile parser's TX layout of one plane of a block (vp9_kf_tile.c:
+ * 320-396): TX size, TXs per row and per column over the coded area clipped
+ * at the MI-aligned frame edge, and the plane block width (sub-8x8 blocks
+ * code a whole 8x8, chroma at least 4x4). */
+__device__ __forceinline__ void plane_layout(const BlkS &b, const cvp9_job_t &job, int gx, int gy, int p,
+                                             int &tx, int &nx, int &ny, int &pbw)
+{
+    int sub8 = b.w < 8 || b.h < 8;
+    int ew = sub8 ? 8 : b.w, eh = sub8 ? 8 : b.h;
+    int mi_col = gx >> 3, mi_row = gy >> 3;
+    int ss = p > 0;
+    int pw = ss ? ew / 2 : ew, ph = ss ? eh / 2 : eh;
+    pw = pw < 4 ? 4 : pw;
+    ph = ph < 4 ? 4 : ph;
+    tx = b.txl;
+    if (ss) { int mt = max_tx_for(pw, ph); tx = sub8 ? 0 : (tx > mt ? mt : tx); }
+    int t4 = 1 << tx;
+    int o4x = (mi_col * 2) >> ss, o4y = (mi_row * 2) >> ss;
+    int mw = pw / 4, mh = ph / 4;
+    int lim_w = ((job.mi_cols * 2) >> ss) - o4x, lim_h = ((job.mi_rows * 2) >> ss) - o4y;
+    if (mw > lim_w) mw = lim_w;
+    if (mh > lim_h) mh = lim_h;
+    nx = mw > 0 ? (mw + t4 - 1) / t4 : 0;
+    ny = mh > 0 ? (mh + t4 - 1) / t4 : 0;
+    pbw = pw;
+}
+
 template <int A>
 __device__ void residual_layout(BlkS &b, const cvp9_job_t &job, int gx, int gy)
 {
@@ -365,24 +399,9 @@ __device__ void residual_layout(BlkS &b, const cvp9_job_t &job, int gx, int gy)
         b.pnx[0] = (uint8_t)nx;
         b.pnt[0] = (uint16_t)(nx * ny);
     } else {
-        int sub8 = b.w < 8 || b.h < 8;
-        int ew = sub8 ? 8 : b.w, eh = sub8 ? 8 : b.h;
-        int mi_col = gx >> 3, mi_row = gy >> 3;
         for (int p = 0; p < 3; p++) {
-            int ss = p > 0;
-            int pw = ss ? ew / 2 : ew, ph = ss ? eh / 2 : eh;
-            pw = pw < 4 ? 4 : pw;
-            ph = ph < 4 ? 4 : ph;
-            int tx = b.txl;
-            if (ss) { int mt = max_tx_for(pw, ph); tx = sub8 ? 0 : (tx > mt ? mt : tx); }
-            int t4 = 1 << tx;
-            int o4x = (mi_col * 2) >> ss, o4y = (mi_row * 2) >> ss;
-            int mw = pw / 4, mh = ph / 4;
-            int lim_w = ((job.mi_cols * 2) >> ss) - o4x, lim_h = ((job.mi_rows * 2) >> ss) - o4y;
-            if (mw > lim_w) mw = lim_w;
-            if (mh > lim_h) mh = lim_h;
-            int nx = mw > 0 ? (mw + t4 - 1) / t4 : 0;
-            int ny = mh > 0 ? (mh + t4 - 1) / t4 : 0;
+            int tx, nx, ny, pbw;
+            plane_layout(b, job, gx, gy, p, tx, nx, ny, pbw);
             b.ptxl[p] = (uint8_t)tx;
             b.pnx[p] = (uint8_t)nx;
             b.pnt[p] = (uint16_t)(nx * ny);
@@ -392,6 +411,7 @@ __device__ void residual_layout(BlkS &b, const cvp9_job_t &job, int gx, int gy)
 
 __device__ __forceinline__ int block_items(const BlkS &b)
 {
+    if (b.flags & 4) return 0;      /* FULL intra: reconstructed by its prediction warp */
     return b.pnt[0] * (4 << b.ptxl[0]) + b.pnt[1] * (4 << b.ptxl[1]) + b.pnt[2] * (4 << b.ptxl[2]);
 }
 
@@ -681,23 +701,22 @@ __device__ __forceinline__ void fill_chunk(ReconSmem &s, int v, int lx0, int ly0
     if (r < clh && c < clw) TC(s, p, cx0 + c, cy0 + r) = (uint8_t)v;
 }
 
-/* SPEC inter prediction of one chunk: regular 8-tap on luma (even phases of
- * the 1/8-pel MV) and chroma (1/16 chroma pel), every fetch clamped into the
- * reference plane, horizontal pass rounded and clipped to 8 bits before the
- * vertical pass (vp9_mc.comp.glsl:61-110). */
-__device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
-                                 int lx0, int ly0, int lw, int lh,
-                                 int cx0, int cy0, int clw, int clh, int warp, int lane)
+/* SPEC inter prediction of one chunk from one reference: 8-tap on luma
+ * (even phases of the 1/8-pel MV) and chroma (1/16 chroma pel), every fetch
+ * clamped into the reference plane, horizontal pass rounded and clipped to 8
+ * bits before the vertical pass (vp9_mc.comp.glsl:61-110). F: the filter
+ * (the regular one under SPEC). avg: round-average into the tile (the
+ * second prediction of a FULL compound block). */
+__device__ void spec_inter_pass(ReconSmem &s, const cvp9_ref_t &R, int mvx, int mvy, const int (*F)[8], bool avg,
+                                int sbx, int sby, int lx0, int ly0, int lw, int lh,
+                                int cx0, int cy0, int clw, int clh, int warp, int lane)
 {
-    const cvp9_ref_t &R = s.jc.ref[s.jc.ref_slot_of[clampi((int)b.ref0 - 1, 0, 2)] & 7];
     const uint8_t *rp = R.plane;
-    if (!rp) { fill_chunk(s, 128, lx0, ly0, lw, lh, cx0, cy0, clw, clh, lane); return; }
     const int rw = R.w, rh = R.h;
     const int rcs = (rw + 1) >> 1;
     const uint8_t *ru = rp + (size_t)rw * rh;
     const uint8_t *rv = ru + (size_t)rcs * ((rh + 1) >> 1);
     uint8_t *st = s.stage[warp];
-    const int mvx = b.mvx, mvy = b.mvy;
         /* luma: (lw+7) x (lh+7) window at pitch 16; H pass into 15 x 8 */
         int bx = sbx + lx0 + (mvx >> 3), by = sby + ly0 + (mvy >> 3);
         int fx = (mvx & 7) << 1, fy = (mvy & 7) << 1;
@@ -720,7 +739,7 @@ __device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
             int r = i / lw, c = i - r * lw;
             int acc = 0;
 #pragma unroll
-            for (int t = 0; t < 8; t++) acc += c_subpel[fx][t] * sy_[r * 16 + c + t];
+            for (int t = 0; t < 8; t++) acc += F[fx][t] * sy_[r * 16 + c + t];
             hy[r * 8 + c] = (uint8_t)clampi((acc + 64) >> 7, 0, 255);
         }
         for (int i = lane; i < 2 * (clh + 7) * clw; i += 32) {
@@ -730,7 +749,7 @@ __device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
             const uint8_t *src = pl ? sv : su;
             int acc = 0;
 #pragma unroll
-            for (int t = 0; t < 8; t++) acc += c_subpel[cfx][t] * src[r * 12 + c + t];
+            for (int t = 0; t < 8; t++) acc += F[cfx][t] * src[r * 12 + c + t];
             (pl ? hv : hu)[r * 4 + c] = (uint8_t)clampi((acc + 64) >> 7, 0, 255);
         }
         __syncwarp();
@@ -743,10 +762,11 @@ __device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
             } else {
                 int acc = 0;
 #pragma unroll
-                for (int t = 0; t < 8; t++) acc += c_subpel[fy][t] * hy[(r + t) * 8 + c];
+                for (int t = 0; t < 8; t++) acc += F[fy][t] * hy[(r + t) * 8 + c];
                 v = clampi((acc + 64) >> 7, 0, 255);
             }
-            TY(s, lx0 + c, ly0 + r) = (uint8_t)v;
+            uint8_t &d = TY(s, lx0 + c, ly0 + r);
+            d = (uint8_t)(avg ? ((int)d + v + 1) >> 1 : v);
         }
         {
             int p = 1 + (lane >> 4), r = (lane >> 2) & 3, c = lane & 3;
@@ -758,13 +778,35 @@ __device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
                     const uint8_t *h = p == 1 ? hu : hv;
                     int acc = 0;
 #pragma unroll
-                    for (int t = 0; t < 8; t++) acc += c_subpel[cfy][t] * h[(r + t) * 4 + c];
+                    for (int t = 0; t < 8; t++) acc += F[cfy][t] * h[(r + t) * 4 + c];
                     v = clampi((acc + 64) >> 7, 0, 255);
                 }
-                TC(s, p, cx0 + c, cy0 + r) = (uint8_t)v;
+                uint8_t &d = TC(s, p, cx0 + c, cy0 + r);
+                d = (uint8_t)(avg ? ((int)d + v + 1) >> 1 : v);
             }
         }
         __syncwarp();
+}
+
+/* SPEC inter prediction of one chunk; FULL also takes the header's filter
+ * and averages in a second reference's prediction (compound blocks). A
+ * missing first reference predicts flat 128; a missing second one leaves
+ * the single prediction. */
+__device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
+                                 int lx0, int ly0, int lw, int lh,
+                                 int cx0, int cy0, int clw, int clh, int warp, int lane)
+{
+    const cvp9_job_t &job = s.jc;
+    const cvp9_ref_t &R = job.ref[job.ref_slot_of[clampi((int)b.ref0 - 1, 0, 2)] & 7];
+    if (!R.plane) { fill_chunk(s, 128, lx0, ly0, lw, lh, cx0, cy0, clw, clh, lane); return; }
+    const int (*F)[8] = job.full ? c_subpel4[job.interp_filter & 3] : c_subpel;
+    spec_inter_pass(s, R, b.mvx, b.mvy, F, false, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh, warp, lane);
+    if (b.ref1) {
+        const cvp9_ref_t &R1 = job.ref[job.ref_slot_of[clampi((int)b.ref1 - 1, 0, 2)] & 7];
+        if (R1.plane)
+            spec_inter_pass(s, R1, b.mv1x, b.mv1y, F, true, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh,
+                            warp, lane);
+    }
 }
 
 /* ── Residual: one item = one TX column (pass 1) or one TX row (pass 2) ── */
@@ -907,6 +949,333 @@ __device__ __forceinline__ void spec_row(ReconSmem &s, int i, const TxRef &t)
         int r = ((int)((unsigned)v[j].v + (1u << (sh - 1)))) >> sh;
         uint8_t &px = t.plane == 0 ? TY(s, t.px0 + j, t.py0 + i) : TC(s, t.plane, t.px0 + j, t.py0 + i);
         px = (uint8_t)clampi((int)px + r, 0, 255);
+    }
+}
+
+/* ── FULL profile: ADST and WHT, rows-then-columns residual, per-TX intra ── */
+
+/* sin(k*pi/9) * 2/3 * sqrt(2) in Q14, the 4-point ADST multipliers */
+enum : int { KS1 = 5283, KS2 = 9929, KS3 = 13377, KS4 = 15212 };
+
+/* 1-D inverse ADSTs in place, 32-bit wrap and Q14 rounding as the DCTs. */
+__device__ __forceinline__ void iadst4(wi *x)
+{
+    wi a = x[0] * KS1 + x[2] * KS4 + x[3] * KS2;
+    wi b = x[0] * KS2 - x[2] * KS1 - x[3] * KS4;
+    wi c = (x[0] - x[2] + x[3]) * KS3;
+    wi d = x[1] * KS3;
+    x[0] = RS(a + d); x[1] = RS(b + d); x[2] = RS(c); x[3] = RS(a + b - d);
+}
+
+__device__ __forceinline__ void rot(wi x, wi y, int ca, int cb, wi &o0, wi &o1)
+{
+    o0 = x * ca + y * cb;
+    o1 = x * cb - y * ca;
+}
+
+__device__ __forceinline__ void iadst8(wi *in)
+{
+    wi x0 = in[7], x1 = in[0], x2 = in[5], x3 = in[2], x4 = in[3], x5 = in[4], x6 = in[1], x7 = in[6];
+    wi s0, s1, s2, s3, s4, s5, s6, s7;
+    rot(x0, x1, K2, K30, s0, s1);
+    rot(x2, x3, K10, K22, s2, s3);
+    rot(x4, x5, K18, K14, s4, s5);
+    rot(x6, x7, K26, K6, s6, s7);
+    x0 = RS(s0 + s4); x1 = RS(s1 + s5); x2 = RS(s2 + s6); x3 = RS(s3 + s7);
+    x4 = RS(s0 - s4); x5 = RS(s1 - s5); x6 = RS(s2 - s6); x7 = RS(s3 - s7);
+    s4 = x4 * K8 + x5 * K24;
+    s5 = x4 * K24 - x5 * K8;
+    s6 = x7 * K8 - x6 * K24;
+    s7 = x6 * K8 + x7 * K24;
+    s0 = x0 + x2; s1 = x1 + x3; s2 = x0 - x2; s3 = x1 - x3;
+    x4 = RS(s4 + s6); x5 = RS(s5 + s7); x6 = RS(s4 - s6); x7 = RS(s5 - s7);
+    x2 = RS((s2 + s3) * K16);
+    x3 = RS((s2 - s3) * K16);
+    wi y6 = RS((x6 + x7) * K16), y7 = RS((x6 - x7) * K16);
+    in[0] = s0; in[1] = -x4; in[2] = y6; in[3] = -x2;
+    in[4] = x3; in[5] = -y7; in[6] = x5; in[7] = -s1;
+}
+
+__device__ __forceinline__ void iadst16(wi *in)
+{
+    wi x[16], s[16];
+    x[0] = in[15]; x[1] = in[0]; x[2] = in[13]; x[3] = in[2]; x[4] = in[11]; x[5] = in[4];
+    x[6] = in[9]; x[7] = in[6]; x[8] = in[7]; x[9] = in[8]; x[10] = in[5]; x[11] = in[10];
+    x[12] = in[3]; x[13] = in[12]; x[14] = in[1]; x[15] = in[14];
+    rot(x[0], x[1], K1, K31, s[0], s[1]);
+    rot(x[2], x[3], K5, K27, s[2], s[3]);
+    rot(x[4], x[5], K9, K23, s[4], s[5]);
+    rot(x[6], x[7], K13, K19, s[6], s[7]);
+    rot(x[8], x[9], K17, K15, s[8], s[9]);
+    rot(x[10], x[11], K21, K11, s[10], s[11]);
+    rot(x[12], x[13], K25, K7, s[12], s[13]);
+    rot(x[14], x[15], K29, K3, s[14], s[15]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) { x[k] = RS(s[k] + s[k + 8]); x[k + 8] = RS(s[k] - s[k + 8]); }
+#pragma unroll
+    for (int k = 0; k < 8; k++) s[k] = x[k];
+    s[8] = x[8] * K4 + x[9] * K28;
+    s[9] = x[8] * K28 - x[9] * K4;
+    s[10] = x[10] * K20 + x[11] * K12;
+    s[11] = x[10] * K12 - x[11] * K20;
+    s[12] = x[13] * K4 - x[12] * K28;
+    s[13] = x[12] * K4 + x[13] * K28;
+    s[14] = x[15] * K20 - x[14] * K12;
+    s[15] = x[14] * K20 + x[15] * K12;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        x[k] = s[k] + s[k + 4];
+        x[k + 4] = s[k] - s[k + 4];
+        x[k + 8] = RS(s[k + 8] + s[k + 12]);
+        x[k + 12] = RS(s[k + 8] - s[k + 12]);
+    }
+#pragma unroll
+    for (int g = 0; g < 16; g += 8) {
+        s[g + 0] = x[g + 0]; s[g + 1] = x[g + 1]; s[g + 2] = x[g + 2]; s[g + 3] = x[g + 3];
+        s[g + 4] = x[g + 4] * K8 + x[g + 5] * K24;
+        s[g + 5] = x[g + 4] * K24 - x[g + 5] * K8;
+        s[g + 6] = x[g + 7] * K8 - x[g + 6] * K24;
+        s[g + 7] = x[g + 6] * K8 + x[g + 7] * K24;
+        x[g + 0] = s[g + 0] + s[g + 2];
+        x[g + 1] = s[g + 1] + s[g + 3];
+        x[g + 2] = s[g + 0] - s[g + 2];
+        x[g + 3] = s[g + 1] - s[g + 3];
+        x[g + 4] = RS(s[g + 4] + s[g + 6]);
+        x[g + 5] = RS(s[g + 5] + s[g + 7]);
+        x[g + 6] = RS(s[g + 4] - s[g + 6]);
+        x[g + 7] = RS(s[g + 5] - s[g + 7]);
+    }
+    wi t2 = RS(-((x[2] + x[3]) * K16)), t3 = RS((x[2] - x[3]) * K16);
+    wi t6 = RS((x[6] + x[7]) * K16), t7 = RS((x[7] - x[6]) * K16);
+    wi t10 = RS((x[10] + x[11]) * K16), t11 = RS((x[11] - x[10]) * K16);
+    wi t14 = RS(-((x[14] + x[15]) * K16)), t15 = RS((x[14] - x[15]) * K16);
+    in[0] = x[0];  in[1] = -x[8];  in[2] = x[12];  in[3] = -x[4];
+    in[4] = t6;    in[5] = t14;    in[6] = t10;    in[7] = t2;
+    in[8] = t3;    in[9] = t11;    in[10] = t15;   in[11] = t7;
+    in[12] = x[5]; in[13] = -x[13]; in[14] = x[9]; in[15] = -x[1];
+}
+
+/* 4-point inverse Walsh-Hadamard (lossless frames); the row pass first
+ * undoes the quantiser step 4 with a shift. */
+__device__ __forceinline__ void iwht4(wi *x, bool rows)
+{
+    wi a = x[0], c = x[1], d = x[2], b = x[3];
+    if (rows) { a = wi(a.v >> 2); c = wi(c.v >> 2); d = wi(d.v >> 2); b = wi(b.v >> 2); }
+    a = a + c; d = d - b;
+    wi e = wi((a - d).v >> 1);
+    b = e - b; c = e - c;
+    a = a - b; d = d + c;
+    x[0] = a; x[1] = b; x[2] = c; x[3] = d;
+}
+
+template <int N>
+__device__ __forceinline__ void itx1(wi *v, bool adst)
+{
+    if (N == 4 && adst) iadst4(v);
+    else if (N == 8 && adst) iadst8(v);
+    else if (N == 16 && adst) iadst16(v);
+    else idct_n(v, N);
+}
+
+/* FULL pass 1 on TX row i: dequantise (the plane's steps, DC at [0][0];
+ * 32x32 values halved toward zero) and transform along the row (DCT, or
+ * ADST when row_adst; WHT when lossless) into the temp rows. Returns
+ * whether the row had a nonzero coefficient. */
+template <int N>
+__device__ __forceinline__ bool full_row(ReconSmem &s, const int16_t *X, int i, int plane, int px0, int py0,
+                                         int qdc, int qac, bool lossless, bool row_adst)
+{
+    wi v[N];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        int c = X[i * N + k];
+        any |= c != 0;
+        int d = c * ((i == 0 && k == 0) ? qdc : qac);
+        v[k] = wi(N == 32 ? d / 2 : d);
+    }
+    if (any) {
+        if (N == 4 && lossless) iwht4(v, true);
+        else itx1<N>(v, row_adst);
+    }
+#pragma unroll
+    for (int k = 0; k < N; k++) *spec_temp(s, plane, px0 + k, py0 + i) = any ? v[k].v : 0;
+    return any;
+}
+
+/* FULL pass 2 on TX column j: transform down the column, final rounding
+ * shift 4/5/6/6 (none after the WHT), add and clamp into the tile. */
+template <int N>
+__device__ __forceinline__ void full_col(ReconSmem &s, int j, int plane, int px0, int py0, bool lossless,
+                                         bool col_adst)
+{
+    wi v[N];
+#pragma unroll
+    for (int k = 0; k < N; k++) v[k] = wi(*spec_temp(s, plane, px0 + j, py0 + k));
+    const bool wht = N == 4 && lossless;
+    if (wht) iwht4(v, false);
+    else itx1<N>(v, col_adst);
+    const int sh = N == 4 ? 4 : (N == 8 ? 5 : 6);
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        int r = wht ? v[k].v : ((int)((unsigned)v[k].v + (1u << (sh - 1)))) >> sh;
+        uint8_t &px = plane == 0 ? TY(s, px0 + j, py0 + k) : TC(s, plane, px0 + j, py0 + k);
+        px = (uint8_t)clampi((int)px + r, 0, 255);
+    }
+}
+
+/* First MI column of the tile column holding mi_col (VP9 tile offsets). */
+__device__ __forceinline__ int full_tile_start(int mi_col, int mi_cols, int log2_tile_cols)
+{
+    const int sb_cols = (mi_cols + 7) >> 3;
+    int start = 0;
+    for (int t = 1; t < (1 << log2_tile_cols); t++) {
+        int o = ((t * sb_cols) >> log2_tile_cols) << 3;
+        if (o > mi_cols) o = mi_cols;
+        if (o <= mi_col) start = o;
+    }
+    return start;
+}
+
+__device__ __forceinline__ uint8_t &TP(ReconSmem &s, int p, int x, int y)
+{
+    return p == 0 ? TY(s, x, y) : TC(s, p, x, y);
+}
+
+#define FAVG2(a, b) (((a) + (b) + 1) >> 1)
+#define FAVG3(a, b, c) (((a) + 2 * (b) + (c) + 2) >> 2)
+
+/* One sample of a VP9 intra predictor from the TX's edges: above[-1..2n-1]
+ * (above[-1] the corner), left[0..n-1]. */
+__device__ __forceinline__ int full_pred(int mode, int r, int c, int n, const uint8_t *above, const uint8_t *left,
+                                         int dc)
+{
+    switch (mode) {
+    case 1: return above[c];
+    case 2: return left[r];
+    case 3: {
+        const int k = r + c;
+        return k + 2 < 2 * n ? FAVG3(above[k], above[k + 1], above[k + 2]) : above[2 * n - 1];
+    }
+    case 4: {
+        const int t = c - r;
+        auto e = [&](int u) -> int { return u >= 0 ? above[u] : (u == -1 ? above[-1] : left[-u - 2]); };
+        return FAVG3(e(t - 2), e(t - 1), e(t));
+    }
+    case 5: {
+        const int k = min(r >> 1, c), rr = r - 2 * k, cc = c - k;
+        if (rr == 0) return FAVG2(above[cc - 1], above[cc]);
+        if (rr == 1) return cc == 0 ? FAVG3(left[0], above[-1], above[0]) : FAVG3(above[cc - 2], above[cc - 1], above[cc]);
+        return rr == 2 ? FAVG3(above[-1], left[0], left[1]) : FAVG3(left[rr - 3], left[rr - 2], left[rr - 1]);
+    }
+    case 6: {
+        const int k = min(r, c >> 1), rr = r - k, cc = c - 2 * k;
+        if (cc == 0) return rr == 0 ? FAVG2(above[-1], left[0]) : FAVG2(left[rr - 1], left[rr]);
+        if (cc == 1) return rr == 0 ? FAVG3(left[0], above[-1], above[0])
+                          : rr == 1 ? FAVG3(above[-1], left[0], left[1]) : FAVG3(left[rr - 2], left[rr - 1], left[rr]);
+        return FAVG3(above[cc - 3], above[cc - 2], above[cc - 1]);
+    }
+    case 7: {
+        const int k = r + (c >> 1);
+        auto L = [&](int i) -> int { return left[i < n ? i : n - 1]; };
+        return (c & 1) ? FAVG3(L(k), L(k + 1), L(k + 2)) : FAVG2(L(k), L(k + 1));
+    }
+    case 8: {
+        const int k = (r >> 1) + c;
+        return (r & 1) ? FAVG3(above[k], above[k + 1], above[k + 2]) : FAVG2(above[k], above[k + 1]);
+    }
+    case 9: return clampi((int)left[r] + (int)above[c] - (int)above[-1], 0, 255);
+    default: return dc;
+    }
+}
+
+/* FULL intra prediction of one n x n TX at tile position (lx, ly) of plane
+ * p, plane position (X0, Y0) in a plane of pw x ph samples: VP9 edge rules
+ * (127 above / 129 left when unavailable, above-right only for a 4x4 TX
+ * with have_right, samples past the plane's right or bottom edge repeating
+ * the last one inside). One warp; `edge` is the warp's scratch. */
+__device__ void full_intra_tx(ReconSmem &s, int p, int lx, int ly, int X0, int Y0, int pw, int ph, int n,
+                              int mode, bool have_top, bool have_left, bool have_right, uint8_t *edge, int lane)
+{
+    uint8_t *above = edge + 1, *left = edge + 80;
+    if (have_top) {
+        const int want = n + ((n == 4 && have_right) ? 4 : 0);
+        const int cnt = min(want, pw - X0);
+        for (int i = lane; i < 2 * n; i += 32) above[i] = TP(s, p, lx + (i < cnt ? i : cnt - 1), ly - 1);
+        if (lane == 0) above[-1] = have_left ? TP(s, p, lx - 1, ly - 1) : (uint8_t)129;
+    } else {
+        for (int i = lane; i < 2 * n + 1; i += 32) edge[i] = 127;
+    }
+    for (int i = lane; i < n; i += 32) left[i] = have_left ? TP(s, p, lx - 1, ly + min(i, ph - 1 - Y0)) : (uint8_t)129;
+    __syncwarp();
+    int dc = 128;
+    if (mode == 0) {
+        const unsigned sa = __reduce_add_sync(0xffffffffu, lane < n ? (unsigned)above[lane] : 0u);
+        const unsigned sl = __reduce_add_sync(0xffffffffu, lane < n ? (unsigned)left[lane] : 0u);
+        if (have_top && have_left) dc = (int)((sa + sl + (unsigned)n) / (unsigned)(2 * n));
+        else if (have_top) dc = (int)((sa + (unsigned)n / 2) / (unsigned)n);
+        else if (have_left) dc = (int)((sl + (unsigned)n / 2) / (unsigned)n);
+    }
+    const int lg = n == 4 ? 2 : n == 8 ? 3 : n == 16 ? 4 : 5;
+    for (int idx = lane; idx < n * n; idx += 32) {
+        const int r = idx >> lg, c = idx & (n - 1);
+        TP(s, p, lx + c, ly + r) = (uint8_t)full_pred(mode, r, c, n, above, left, dc);
+    }
+    __syncwarp();
+}
+
+/* FULL residual of one n x n TX by one warp (lane = row, then column). */
+template <int N>
+__device__ void full_tx_warp(ReconSmem &s, const int16_t *X, int p, int lx, int ly, int qdc, int qac,
+                             bool lossless, int tx_type, int lane)
+{
+    bool any = false;
+    if (lane < N) any = full_row<N>(s, X, lane, p, lx, ly, qdc, qac, lossless, tx_type == 2 || tx_type == 3);
+    any = __any_sync(0xffffffffu, any);
+    __syncwarp();
+    if (any && lane < N) full_col<N>(s, lane, p, lx, ly, lossless, tx_type == 1 || tx_type == 3);
+    __syncwarp();
+}
+
+/* FULL intra block, one warp: for each plane, each TX in raster order is
+ * predicted from the reconstructed samples around it and gets its residual
+ * before the next TX is predicted (the VP9 decoding order). */
+__device__ void full_intra_block(ReconSmem &s, const BlkS &b, int sbx, int sby, bool staged, unsigned c_base,
+                                 int warp, int lane)
+{
+    const cvp9_job_t &job = s.jc;
+    const int gx = sbx + b.x, gy = sby + b.y;
+    const int mi_col = gx >> 3, mi_row = gy >> 3;
+    const bool left_ok = mi_col > full_tile_start(mi_col, job.mi_cols, job.log2_tile_cols);
+    uint8_t *edge = s.stage[warp];
+    uint64_t off = b.coeff;
+    for (int p = 0; p < 3; p++) {
+        int txl, nx, ny, pbw;
+        plane_layout(b, job, gx, gy, p, txl, nx, ny, pbw);
+        const int n = 4 << txl;
+        const int mode = p ? (b.uvmode > 9 ? 0 : b.uvmode) : (b.ymode > 9 ? 0 : b.ymode);
+        const int tx_type = (p == 0 && !job.lossless && txl < 3 && b.ymode < 10) ? c_tx_type[b.ymode] : 0;
+        const int pw = p ? job.CW : job.W, ph = p ? job.CH : job.H;
+        const int ox = p ? (b.x >> 1) : b.x, oy = p ? (b.y >> 1) : b.y;
+        const int gox = p ? (gx >> 1) : gx, goy = p ? (gy >> 1) : gy;
+        const int qdc = p ? job.q_dc_uv : job.q_dc, qac = p ? job.q_ac_uv : job.q_ac;
+        for (int ty = 0; ty < ny; ty++)
+            for (int tx = 0; tx < nx; tx++) {
+                const int lx = ox + tx * n, ly = oy + ty * n;
+                full_intra_tx(s, p, lx, ly, gox + tx * n, goy + ty * n, pw, ph, n, mode,
+                              ty > 0 || mi_row > 0, tx > 0 || left_ok, (tx + 1) * n < pbw, edge, lane);
+                if (b.flags & 2) continue;
+                const uint64_t co = off + (uint64_t)(ty * nx + tx) * (uint64_t)(n * n);
+                if (co + (uint64_t)(n * n) > (uint64_t)job.num_coeffs) continue;
+                const int16_t *X = staged ? s.coef + (co - c_base) : job.coeffs + co;
+                switch (txl) {
+                case 0: full_tx_warp<4>(s, X, p, lx, ly, qdc, qac, job.lossless, tx_type, lane); break;
+                case 1: full_tx_warp<8>(s, X, p, lx, ly, qdc, qac, job.lossless, tx_type, lane); break;
+                case 2: full_tx_warp<16>(s, X, p, lx, ly, qdc, qac, job.lossless, tx_type, lane); break;
+                default: full_tx_warp<32>(s, X, p, lx, ly, qdc, qac, job.lossless, 0, lane); break;
+                }
+            }
+        if (!(b.flags & 2)) off += (uint64_t)(nx * ny) * (uint64_t)(n * n);
     }
 }
 
@@ -1153,7 +1522,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
             mb.ref0 = g.ref_frame[0];
             mb.mvx = g.mv[0][0];
             mb.mvy = g.mv[0][1];
+            mb.ref1 = 0;
+            mb.mv1x = g.mv[1][0];
+            mb.mv1y = g.mv[1][1];
             mb.coeff = g.coeff_offset;
+            if (A == CVP9_ARITH_SPEC && job.full) {
+                /* the block's whole MI for a sub-8x8 block (one MV, one
+                 * mode); a second reference; intra blocks TX by TX */
+                if (g.width < 8 || g.height < 8) {
+                    mb.cw = (uint8_t)min(8, job.W - (int)g.x);
+                    mb.ch = (uint8_t)min(8, job.H - (int)g.y);
+                }
+                if (!g.is_intra) mb.ref1 = g.ref_frame[1];
+                else mb.flags |= 4;
+            }
             residual_layout<A>(mb, job, g.x, g.y);
             s.blk[tid] = mb;
             my_intra = g.is_intra != 0;
@@ -1381,6 +1763,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                 }
             }
         }
+        /* FULL intra blocks read their coefficients during prediction */
+        if (A == CVP9_ARITH_SPEC && job.full) cp_async_wait_all();
         __syncthreads();
 
         /* 5. levels */
@@ -1434,7 +1818,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                 for (int chk = chk0 + warp; chk < chk1; chk += kWarps) {
                     ChunkP c = chunk_params(s, chk);
                     const BlkS &b = *c.b;
-                    if (b.flags & 1)
+                    if (b.flags & 4) {
+                        /* FULL intra: the warp of the block's first chunk
+                         * does the whole block, TX by TX */
+                        if (c.lx0 == b.x && c.ly0 == b.y) full_intra_block(s, b, sbx, sby, staged, c_base, warp, lane);
+                    } else if (b.flags & 1)
                         predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, c.lx0, c.ly0, c.lw, c.lh,
                                                c.cx0, c.cy0, c.clw, c.clh, lane);
                     else
@@ -1460,6 +1848,17 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                     case 2: refcpu_col<16>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
                     default: refcpu_col<32>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
                     }
+                } else if (job.full) {
+                    /* FULL inter residual (DCT): rows first, item j = row j */
+                    const int qdc = t.plane ? job.q_dc_uv : job.q_dc, qac = t.plane ? job.q_ac_uv : job.q_ac;
+                    bool any;
+                    switch (t.txl) {
+                    case 0: any = full_row<4>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+                    case 1: any = full_row<8>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+                    case 2: any = full_row<16>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+                    default: any = full_row<32>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+                    }
+                    if (any) atomicOr(&s.txmask[t.mask_idx], 1u);
                 } else {
                     switch (t.txl) {
                     case 0: spec_col<4>(s, X, j, t, job.q_dc, job.q_ac); break;
@@ -1485,6 +1884,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                     case 1: refcpu_row<8>(s, i, t.px0, t.py0, mask, M); break;
                     case 2: refcpu_row<16>(s, i, t.px0, t.py0, mask, M); break;
                     default: refcpu_row<32>(s, i, t.px0, t.py0, mask, M); break;
+                    }
+                } else if (job.full) {
+                    /* item i = column i */
+                    switch (t.txl) {
+                    case 0: full_col<4>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+                    case 1: full_col<8>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+                    case 2: full_col<16>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+                    default: full_col<32>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
                     }
                 } else {
                     switch (t.txl) {
@@ -3445,10 +3852,264 @@ __global__ void k_lf_flat_v(const cvp9_job_t *__restrict__ jobs, int refcpu)
     filter4(Y + base - 2, Y + base - 1, Y + base, Y + base + 1, thr);
 }
 
+/* ── FULL profile: the VP9 loop filter ───────────────────────────────────
+ *
+ * k_lf_mimap records, per 8x8 MI, what the filter needs of the block that
+ * covers it: luma and chroma TX size, whether it is a skipped inter block,
+ * and the MI's offset inside the block (bits 0-1, 2-3, 4, 5-7, 8-10), tagged
+ * with the frame's epoch in the high half so that entries of earlier frames
+ * read as "no block". k_lf_full then filters superblock by superblock in the
+ * VP9 order: every vertical edge of a superblock (each row left to right),
+ * then its horizontal edges (each column top to bottom), superblocks in
+ * raster order. A CTA takes a superblock row (ticket) and walks it left to
+ * right; superblock (r, c) starts once row r-1 has finished (r-1, c+1), the
+ * last one whose filtering reaches the samples (r, c) reads. Each
+ * superblock is filtered in shared memory with an 8-sample halo above and
+ * to the left, which its first edges modify. */
+__global__ void __launch_bounds__(256) k_lf_mimap(const cvp9_job_t *__restrict__ jobs)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    if (!job.full || !job.mi_map) return;
+    const uint32_t tag = (job.epoch & 0xFFFFu) << 16;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < job.num_blocks; i += gridDim.x * blockDim.x) {
+        const vp9_macroblock_info_t b = job.blocks[i];
+        if (b.x >= job.W || b.y >= job.H || b.tx_size > 3 || b.width < 4 || b.height < 4) continue;
+        const bool sub8 = b.width < 8 || b.height < 8;
+        const int bw = sub8 ? 8 : b.width, bh = sub8 ? 8 : b.height;
+        const int uvw = bw / 2 < 4 ? 4 : bw / 2, uvh = bh / 2 < 4 ? 4 : bh / 2;
+        const int txuv = sub8 ? 0 : min((int)b.tx_size, max_tx_for(uvw, uvh));
+        const uint32_t info = tag | (uint32_t)b.tx_size | ((uint32_t)txuv << 2) |
+                              ((uint32_t)(b.skip && !b.is_intra) << 4);
+        const int mc = b.x >> 3, mr = b.y >> 3;
+        const int nc = min((bw + 7) >> 3, job.mi_cols - mc), nr = min((bh + 7) >> 3, job.mi_rows - mr);
+        for (int r = 0; r < nr; r++)
+            for (int c = 0; c < nc; c++)
+                job.mi_map[(size_t)(mr + r) * job.mi_cols + mc + c] = info | ((uint32_t)c << 5) | ((uint32_t)r << 8);
+    }
+}
+
+struct LfThr { int lim, mblim, hev; };
+
+/* Filter across one edge: q0 at s[0], p0 at s[-st]; fs = widest filter
+ * allowed there (4, 8 or 16), narrowed by the flatness tests. */
+__device__ __forceinline__ void lf_edge_full(uint8_t *s, int st, int fs, LfThr th)
+{
+    auto P = [&](int i) -> int { return s[(-i - 1) * st]; };
+    auto Q = [&](int i) -> int { return s[i * st]; };
+    const int p3 = P(3), p2 = P(2), p1 = P(1), p0 = P(0), q0 = Q(0), q1 = Q(1), q2 = Q(2), q3 = Q(3);
+    const bool mask = abs(p3 - p2) <= th.lim && abs(p2 - p1) <= th.lim && abs(p1 - p0) <= th.lim &&
+                      abs(q1 - q0) <= th.lim && abs(q2 - q1) <= th.lim && abs(q3 - q2) <= th.lim &&
+                      abs(p0 - q0) * 2 + abs(p1 - q1) / 2 <= th.mblim;
+    if (!mask) return;
+    const bool flat = fs >= 8 && abs(p1 - p0) <= 1 && abs(q1 - q0) <= 1 && abs(p2 - p0) <= 1 &&
+                      abs(q2 - q0) <= 1 && abs(p3 - p0) <= 1 && abs(q3 - q0) <= 1;
+    bool flat2 = false;
+    if (fs == 16 && flat) {
+        flat2 = true;
+#pragma unroll
+        for (int i = 4; i < 8; i++) flat2 &= abs(P(i) - p0) <= 1 && abs(Q(i) - q0) <= 1;
+    }
+    if (flat2) {
+        int v[16], o[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) { v[7 - i] = P(i); v[8 + i] = Q(i); }
+#pragma unroll
+        for (int k = 1; k < 15; k++) {
+            int acc = v[k];
+#pragma unroll
+            for (int t = k - 7; t <= k + 7; t++) acc += v[t < 0 ? 0 : (t > 15 ? 15 : t)];
+            o[k] = (acc + 8) >> 4;
+        }
+#pragma unroll
+        for (int k = 1; k < 15; k++) s[(k - 8) * st] = (uint8_t)o[k];
+    } else if (flat) {
+        int v[8], o[8];
+#pragma unroll
+        for (int i = 0; i < 4; i++) { v[3 - i] = P(i); v[4 + i] = Q(i); }
+#pragma unroll
+        for (int k = 1; k < 7; k++) {
+            int acc = v[k];
+#pragma unroll
+            for (int t = k - 3; t <= k + 3; t++) acc += v[t < 0 ? 0 : (t > 7 ? 7 : t)];
+            o[k] = (acc + 4) >> 3;
+        }
+#pragma unroll
+        for (int k = 1; k < 7; k++) s[(k - 4) * st] = (uint8_t)o[k];
+    } else {
+        auto sc8 = [](int v) { return v < -128 ? -128 : (v > 127 ? 127 : v); };
+        const int ps1 = p1 - 128, ps0 = p0 - 128, qs0 = q0 - 128, qs1 = q1 - 128;
+        const bool hev = abs(p1 - p0) > th.hev || abs(q1 - q0) > th.hev;
+        int f = hev ? sc8(ps1 - qs1) : 0;
+        f = sc8(f + 3 * (qs0 - ps0));
+        const int f1 = sc8(f + 4) >> 3, f2 = sc8(f + 3) >> 3;
+        s[0] = (uint8_t)(sc8(qs0 - f1) + 128);
+        s[-st] = (uint8_t)(sc8(ps0 + f2) + 128);
+        if (!hev) {
+            const int f3 = (f1 + 1) >> 1;
+            s[st] = (uint8_t)(sc8(qs1 - f3) + 128);
+            s[-2 * st] = (uint8_t)(sc8(ps1 + f3) + 128);
+        }
+    }
+}
+
+/* Filter size of the edge on the left (dir 0) or top (dir 1) of 8x8 unit
+ * (ux, uy) of a plane, 0 for none; inner: the 4x4 edge 4 samples in is
+ * filtered too. Chroma units take the block at their top-left MI. */
+__device__ __forceinline__ int lf_unit_edge(const cvp9_job_t &job, int plane, int ux, int uy, int dir, bool &inner)
+{
+    const int ss = plane > 0;
+    const uint32_t e = job.mi_map[(size_t)(uy << ss) * job.mi_cols + (ux << ss)];
+    const uint32_t info = (e >> 16) == (job.epoch & 0xFFFFu) ? (e & 0xFFFFu) : 0u;
+    const int tx = ss ? (int)((info >> 2) & 3u) : (int)(info & 3u);
+    const bool skipi = (info >> 4) & 1u;
+    const int pos = (int)(dir ? (info >> 8) & 7u : (info >> 5) & 7u) * (ss ? 4 : 8);
+    const int u = dir ? uy : ux, edge = u * 8;
+    const bool half = ss && ((u << 1) + 1 >= (dir ? job.mi_rows : job.mi_cols));
+    inner = tx == 0 && !skipi && !half;
+    if (edge == 0) return 0;
+    const bool block_edge = pos == 0, tx_edge = (pos & ((4 << tx) - 1)) == 0;
+    if (!block_edge && !(tx_edge && !skipi)) return 0;
+    int fs = tx == 0 ? 4 : (tx == 1 ? 8 : 16);
+    if (fs == 4 && (edge & 31) == 0) fs = 8;
+    if (fs == 16 && half) fs = 8;
+    return fs;
+}
+
+constexpr int kLfY = 72, kLfC = 40;      /* window pitches: 8-sample halo + superblock */
+
+__device__ bool wait_at_least(const unsigned *flag, unsigned v)
+{
+    for (long long it = 0; it < kSpinLimit; it++) {
+        if (ld_acquire(flag) >= v) return true;
+        __nanosleep(it < 64 ? 32 : 256);
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ jobs, int njobs,
+                                                uint32_t n_tickets, uint32_t *counter)
+{
+    __shared__ __align__(16) uint8_t wy[kLfY * kLfY];
+    __shared__ __align__(16) uint8_t wc[2][kLfC * kLfC];
+    __shared__ int s_ticket;
+    const int tid = threadIdx.x;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_ticket = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int t = s_ticket;
+        if (t >= (int)n_tickets) return;
+        const cvp9_job_t &job = jobs[t % njobs];
+        const int row = t / njobs;
+        if (!job.full || row >= job.sb_rows || job.lf_level == 0) continue;
+        LfThr th;
+        {
+            const int level = job.lf_level, sharp = job.lf_sharpness;
+            int bil = level >> ((sharp > 0) + (sharp > 4));
+            if (sharp > 0 && bil > 9 - sharp) bil = 9 - sharp;
+            if (bil < 1) bil = 1;
+            th.lim = bil;
+            th.mblim = 2 * (level + 2) + bil;
+            th.hev = level >> 4;
+        }
+        const int W = job.W, H = job.H, CW = job.CW, CH = job.CH;
+        uint8_t *Y = job.out;
+        uint8_t *U = Y + (size_t)W * H;
+        uint8_t *V = U + (size_t)CW * CH;
+        unsigned *prog_prev = row > 0 ? job.sb_range + 4 * (size_t)(row - 1) * job.sb_cols + 3 : nullptr;
+        unsigned *prog = job.sb_range + 4 * (size_t)row * job.sb_cols + 3;
+        for (int c = 0; c < job.sb_cols; c++) {
+            if (prog_prev && tid == 0) {
+                const unsigned need = (unsigned)min(c + 2, job.sb_cols);
+                if (!wait_at_least(prog_prev, need)) atomicOr(job.status, (unsigned)CVP9_JOB_TIMEOUT);
+            }
+            __syncthreads();
+            const int X0 = c * 64, Y0 = row * 64, XC = c * 32, YC = row * 32;
+            /* load the windows (4-byte words: W and the window origins are
+             * multiples of 8, so every word is inside one row) */
+            for (int i = tid; i < kLfY * (kLfY / 4); i += 128) {
+                const int r = i / (kLfY / 4), w4 = i - r * (kLfY / 4);
+                const int gy = Y0 - 8 + r, gx = X0 - 8 + 4 * w4;
+                if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+                    *reinterpret_cast<uint32_t *>(&wy[r * kLfY + 4 * w4]) =
+                        __ldcg(reinterpret_cast<const unsigned int *>(Y + (size_t)gy * W + gx));
+            }
+            for (int i = tid; i < 2 * kLfC * (kLfC / 4); i += 128) {
+                const int pl = i >= kLfC * (kLfC / 4);
+                const int k = pl ? i - kLfC * (kLfC / 4) : i;
+                const int r = k / (kLfC / 4), w4 = k - r * (kLfC / 4);
+                const int gy = YC - 8 + r, gx = XC - 8 + 4 * w4;
+                if (gy >= 0 && gy < CH && gx >= 0 && gx < CW)
+                    *reinterpret_cast<uint32_t *>(&wc[pl][r * kLfC + 4 * w4]) =
+                        __ldcg(reinterpret_cast<const unsigned int *>((pl ? V : U) + (size_t)gy * CW + gx));
+            }
+            __syncthreads();
+            /* vertical edges: a thread per row (64 luma, 32 + 32 chroma) */
+            {
+                const int p = tid < 64 ? 0 : (tid < 96 ? 1 : 2);
+                const int r = p == 0 ? tid : (tid - 32 - 32 * p);
+                const int sz = p ? 32 : 64, pw = p ? CW : W, ph = p ? CH : H;
+                const int gy = (p ? YC : Y0) + r, gx0 = p ? XC : X0;
+                uint8_t *row_p = p == 0 ? &wy[(8 + r) * kLfY + 8] : &wc[p - 1][(8 + r) * kLfC + 8];
+                if (gy < ph)
+                    for (int x = 0; x < sz && gx0 + x < pw; x += 8) {
+                        bool inner;
+                        const int fs = lf_unit_edge(job, p, (gx0 + x) >> 3, gy >> 3, 0, inner);
+                        if (fs) lf_edge_full(row_p + x, 1, fs, th);
+                        if (inner && gx0 + x + 4 < pw) lf_edge_full(row_p + x + 4, 1, 4, th);
+                    }
+            }
+            __syncthreads();
+            /* horizontal edges: a thread per column */
+            {
+                const int p = tid < 64 ? 0 : (tid < 96 ? 1 : 2);
+                const int x = p == 0 ? tid : (tid - 32 - 32 * p);
+                const int sz = p ? 32 : 64, pw = p ? CW : W, ph = p ? CH : H;
+                const int gx = (p ? XC : X0) + x, gy0 = p ? YC : Y0;
+                const int pitch = p ? kLfC : kLfY;
+                uint8_t *col_p = p == 0 ? &wy[8 * kLfY + 8 + x] : &wc[p - 1][8 * kLfC + 8 + x];
+                if (gx < pw)
+                    for (int y = 0; y < sz && gy0 + y < ph; y += 8) {
+                        bool inner;
+                        const int fs = lf_unit_edge(job, p, gx >> 3, (gy0 + y) >> 3, 1, inner);
+                        if (fs) lf_edge_full(col_p + y * pitch, pitch, fs, th);
+                        if (inner && gy0 + y + 4 < ph) lf_edge_full(col_p + (y + 4) * pitch, pitch, 4, th);
+                    }
+            }
+            __syncthreads();
+            /* write back: the superblock's rows with the left halo, and the
+             * halo rows above over the superblock's columns */
+            for (int i = tid; i < kLfY * (kLfY / 4); i += 128) {
+                const int r = i / (kLfY / 4), w4 = i - r * (kLfY / 4);
+                if (r < 8 && w4 < 2) continue;                  /* the corner: untouched */
+                const int gy = Y0 - 8 + r, gx = X0 - 8 + 4 * w4;
+                if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+                    *reinterpret_cast<uint32_t *>(Y + (size_t)gy * W + gx) =
+                        *reinterpret_cast<const uint32_t *>(&wy[r * kLfY + 4 * w4]);
+            }
+            for (int i = tid; i < 2 * kLfC * (kLfC / 4); i += 128) {
+                const int pl = i >= kLfC * (kLfC / 4);
+                const int k = pl ? i - kLfC * (kLfC / 4) : i;
+                const int r = k / (kLfC / 4), w4 = k - r * (kLfC / 4);
+                if (r < 8 && w4 < 2) continue;
+                const int gy = YC - 8 + r, gx = XC - 8 + 4 * w4;
+                if (gy >= 0 && gy < CH && gx >= 0 && gx < CW)
+                    *reinterpret_cast<uint32_t *>((pl ? V : U) + (size_t)gy * CW + gx) =
+                        *reinterpret_cast<const uint32_t *>(&wc[pl][r * kLfC + 4 * w4]);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                st_release(prog, (unsigned)(c + 1));
+            }
+        }
+    }
+}
+
 __global__ void k_nv12_pack(const cvp9_job_t *__restrict__ jobs)
 {
     const cvp9_job_t &job = jobs[blockIdx.y];
-    if (job.lf_tiled || !job.nv12) return;
+    if ((job.lf_tiled && !job.full) || !job.nv12) return;
     size_t ny = (size_t)job.W * job.H, nc = (size_t)job.CW * job.CH;
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ny) job.nv12[i] = job.out[i];
@@ -3665,6 +4326,7 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
         int gx = L->scan_ctas > 0 ? L->scan_ctas : (L->max_blocks + 255) / 256;
         dim3 g((unsigned)gx, (unsigned)L->njobs);
         k_scan_blocks<<<g, 256, 0, st>>>(L->jobs);
+        if (L->full) k_lf_mimap<<<g, 256, 0, st>>>(L->jobs);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     if ((e = mark(L->ev[1], st, capturing)) != cudaSuccess) return (int)e;
@@ -3715,6 +4377,18 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     if ((e = mark(L->ev[2], st, capturing)) != cudaSuccess) return (int)e;
+    if (L->full) {
+        if (L->lf_tickets > 0 && L->lf_counter) {
+            const int grid = L->lf_ctas > 0 && L->lf_ctas < (int)L->lf_tickets ? L->lf_ctas : (int)L->lf_tickets;
+            k_lf_full<<<grid, 128, 0, st>>>(L->jobs, L->njobs, L->lf_tickets, L->lf_counter);
+        }
+        if (L->full_nv12_max_px > 0) {
+            long long n = L->full_nv12_max_px;
+            k_nv12_pack<<<dim3((unsigned)((n + 255) / 256), (unsigned)L->njobs), 256, 0, st>>>(L->jobs);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+        return (int)mark(L->ev[3], st, capturing);
+    }
     if (L->lf_tiles_x > 0 && L->lf_tiles_y > 0) {
         /* lf_tiles_y counts 64-row tiles; 32-row tiles need twice as many
          * (one more covers the 4-row shift) */

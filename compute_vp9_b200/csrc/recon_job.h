@@ -18,7 +18,11 @@
 extern "C" {
 #endif
 
-enum { CVP9_ARITH_REFCPU = 0, CVP9_ARITH_SPEC = 1 };
+/* Arithmetic profiles. FULL runs the SPEC kernels with job.full set: the
+ * shader arithmetic completed to the VP9 specification where the reference
+ * is a skeleton (compound prediction, every frame-level filter, per-TX
+ * directional intra with ADST, the VP9 loop filter). */
+enum { CVP9_ARITH_REFCPU = 0, CVP9_ARITH_SPEC = 1, CVP9_ARITH_FULL = 2 };
 
 /* Job status bits, written by the kernels, read back with the frame. */
 enum {
@@ -61,6 +65,14 @@ typedef struct {
     uint32_t        packed_words;   /* packed upload (cvp9_pack_coeffs): its words  */
     const uint32_t *packed;         /* (device), expanded into coeffs by
                                      * k_unpack_coeffs; NULL: none                  */
+    /* FULL profile (full != 0) */
+    uint32_t *mi_map;               /* per 8x8 MI: loop-filter mode info, tagged
+                                     * with the frame's epoch (k_lf_mimap)          */
+    int32_t  q_dc_uv, q_ac_uv;      /* chroma quantiser steps (q_dc, q_ac: luma)     */
+    uint8_t  full;
+    uint8_t  interp_filter;         /* 0 regular, 1 smooth, 2 sharp, 3 bilinear      */
+    uint8_t  lossless;              /* 4x4 Walsh-Hadamard residual                  */
+    uint8_t  log2_tile_cols;        /* intra left edges end at tile columns         */
 } cvp9_job_t;
 
 #ifdef __cplusplus

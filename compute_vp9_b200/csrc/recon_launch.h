@@ -39,6 +39,14 @@ typedef struct {
     uint32_t        *general_tickets;
     uint32_t        *n_general;
     int              inter_variant;  /* 0: default, 1: 96-register k_inter, 2: 80-register */
+    /* FULL profile (jobs with full set; arith SPEC): k_lf_mimap after the
+     * scan, the VP9 loop filter k_lf_full after the reconstruction instead
+     * of the other filters, then the NV12 pack of armed targets. */
+    int              full;
+    uint32_t        *lf_counter;   /* device word, zeroed before the launch      */
+    uint32_t         lf_tickets;   /* njobs * (most superblock rows of a job)    */
+    int              lf_ctas;      /* grid of k_lf_full                          */
+    int              full_nv12_max_px;  /* > 0: largest W*H of a job with a target */
     cudaEvent_t      ev[4];        /* optional: before scan, recon, filter; after */
 } cvp9k_launch_t;
 

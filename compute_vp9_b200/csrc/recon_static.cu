@@ -111,9 +111,13 @@ extern "C" cvp9_err_t cuda_reconstruct_noalloc(const vp9_parsed_frame_t *pf,
         return CVP9_ERR_INVALID_DATA;
     }
     if ((pf->num_blocks && !pf->blocks) || (pf->num_coeffs && !pf->coeffs)) return CVP9_ERR_INVALID_DATA;
+    if (arith == CVP9_CUDA_ARITH_FULL) {
+        fprintf(stderr, "[compute-vp9] cuda_reconstruct_noalloc: takes the REFCPU and SPEC profiles\n");
+        return CVP9_ERR_UNSUPPORTED;
+    }
     const int a = arith == CVP9_CUDA_ARITH_SPEC ? CVP9_ARITH_SPEC : CVP9_ARITH_REFCPU;
     const char *why = nullptr;
-    if (!cvp9_filter_supported(a, (int)pf->hdr.interp_filter, &why)) {
+    if (!cvp9_frame_supported(a, pf, &why)) {
         fprintf(stderr, "[compute-vp9] cuda_reconstruct_noalloc: %s\n", why);
         return CVP9_ERR_UNSUPPORTED;
     }

@@ -31,6 +31,7 @@ VP9_FRAME_NON_KEY = 1
 
 ARITH_REFCPU = 0
 ARITH_SPEC = 1
+ARITH_FULL = 2
 
 
 class FrameHeader(C.Structure):

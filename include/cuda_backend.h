@@ -34,10 +34,17 @@
  * the shader arithmetic (integer butterflies with dequantisation, 8-tap MC
  * on all planes, shader intra rules) with the Vulkan pool rules
  * (refresh_frame_flags, ref_frame_idx); the shaders hold only the regular
- * 8-tap filter, so SPEC returns CVP9_ERR_UNSUPPORTED (from decode) for a
- * frame whose header asks for another filter. The environment variable
- * CVP9_ARITH=refcpu|spec picks the profile for cuda_backend_init;
- * CVP9_CUDA_DEVICE picks the GPU.
+ * 8-tap filter, so SPEC returns CVP9_ERR_UNSUPPORTED (from decode) for an
+ * inter frame whose header asks for another filter. CVP9_CUDA_ARITH_FULL is
+ * SPEC completed to the VP9 specification where the reference is a
+ * skeleton: compound prediction, the smooth/sharp/bilinear filters, intra
+ * prediction per transform block with the directional modes, ADST (and the
+ * Walsh-Hadamard transform of lossless frames), the header's delta_q values,
+ * and the VP9 loop filter; it returns CVP9_ERR_UNSUPPORTED for sizes that
+ * are not multiples of 8, a SWITCHABLE filter on an inter frame (the parsed
+ * block record has no per-block filter) and references of another size.
+ * The environment variable CVP9_ARITH=refcpu|spec|full picks the profile for
+ * cuda_backend_init; CVP9_CUDA_DEVICE picks the GPU.
  */
 #ifndef CVP9_CUDA_BACKEND_H
 #define CVP9_CUDA_BACKEND_H
@@ -53,6 +60,7 @@ extern "C" {
 typedef enum {
     CVP9_CUDA_ARITH_REFCPU = 0,
     CVP9_CUDA_ARITH_SPEC   = 1,
+    CVP9_CUDA_ARITH_FULL   = 2,
 } cvp9_cuda_arith_t;
 
 typedef struct {

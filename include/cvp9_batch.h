@@ -37,7 +37,7 @@ typedef struct cvp9_batch cvp9_batch_t;
 
 typedef struct {
     int      device;         /* CUDA ordinal; -1: $CVP9_CUDA_DEVICE or 0         */
-    int      arith;          /* 0 REFCPU, 1 SPEC; -1: $CVP9_ARITH or REFCPU       */
+    int      arith;          /* 0 REFCPU, 1 SPEC, 2 FULL; -1: $CVP9_ARITH or REFCPU */
     uint64_t hbm_budget;     /* bytes of stream state to admit; 0: 150 GB         */
     int      max_streams;    /* 0: 1024                                          */
     int      use_graphs;     /* replay the kernel chain from per-bucket graphs    */

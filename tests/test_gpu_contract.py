@@ -163,18 +163,23 @@ def test_inflight_ring(profile):
 
 @pytest.mark.parametrize("filt", [1, 2, 3, 4])
 def test_spec_rejects_filters_it_does_not_hold(filt):
+    """Inter frames only: a key frame carries no filter."""
     w, h = 192, 128
     gpu = CudaBackend(arith=SPEC)
-    syn = Synth(synth_config(2, w, h, 3, gop=2, interp_filter=filt))
-    assert gpu.decode(syn.frame(0), 0) == CVP9_ERR_UNSUPPORTED
+    syn = Synth(synth_config(2, w, h, 3, gop=4, interp_filter=filt))
+    assert gpu.decode(syn.frame(0), 0) == CVP9_OK, gpu.last_error()
+    assert gpu.get_frame(wait=1)[0] == CVP9_OK
+    assert gpu.decode(syn.frame(1), 1) == CVP9_ERR_UNSUPPORTED
     assert "filter" in gpu.last_error()
     assert gpu.get_frame(wait=1)[0] == CVP9_ERR_UNSUPPORTED     # nothing queued
     gpu.close()
 
     eng = Batch(arith=SPEC)
     sid = eng.open_stream(w, h)
+    eng.submit([sid], [syn.frame(0)], [0])
+    assert eng.wait() == CVP9_OK
     with pytest.raises(BatchError) as e:
-        eng.submit([sid], [syn.frame(0)], [0])
+        eng.submit([sid], [syn.frame(1)], [1])
     assert e.value.code == CVP9_ERR_UNSUPPORTED
     assert "filter" in eng.last_error()
     eng.close()
