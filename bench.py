@@ -8,17 +8,24 @@ Workload (one step): one frame of each of 64 independent 1920x1080 8-bit
 4:2:0 streams (seeds 0..63), content as in the reference's synthetic
 benchmark shape — every 64x64 superblock split to 8x8 blocks, 8x8 DCT, q60,
 ~5% Laplacian coefficients (|v| <= 512), MVs uniform +-64 px in 1/8 pel from
-LAST, loop-filter level 32. Frame 0 of every stream is intra; the timed
-steps are inter frames. Each stream cycles through 8 distinct parsed frames
-(frame 0, then 1..7 repeated); the reference chain keeps evolving, so every
-step is real decode work. Per-step inputs (~460 MB) and outputs (~200 MB)
-exceed the 126 MB L2, so no flush is needed between steps.
+LAST, loop-filter level 32. A key (intra) frame every GOP steps (default
+100: the reference benchmark's stream has frame 0 intra of 100 frames), inter
+frames between; the default 100 timed steps hold one key step. Each stream
+cycles through 8 distinct parsed frames (the key frame, then 1..7 repeated);
+the reference chain keeps evolving, so every step is real decode work.
+Per-step inputs (~460 MB) and outputs (~200 MB) exceed the 126 MB L2, so no
+flush is needed between steps.
 
-value  — device-resident: parsed frames already in HBM, K steps timed with
-         CUDA events on the engine's streams, max over ranks.
-e2e    — the same K steps through cvp9_batch_submit with the parsed frames in
-         pinned host memory: upload, kernels and the download of every
-         reconstructed frame inside the timed region.
+value        device-resident: parsed frames already in HBM, K GOP-shaped
+             steps timed with CUDA events on the engine's streams, max over
+             ranks; value_inter / value_key time inter or key steps alone.
+e2e          the same K steps through cvp9_batch_submit with the parsed
+             frames in pinned host memory: upload, kernels and the download
+             of every reconstructed frame inside the timed region; every
+             stream's final frame is then checked against the reference's
+             own compiled reconstruction.
+value_spec   the same steps in the shader arithmetic; value_full the VP9
+             (FULL) profile on mixed block/TX/filter content.
 Single-stream figures come from the plain per-stream path on stream 0.
 Each rank decodes its own 64 streams (weak scaling, no data-path collective).
 """
@@ -43,13 +50,18 @@ DISTINCT = 8
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--gop", type=int, default=100,
+                    help="key frame every GOP steps (the reference benchmark's stream: frame 0 intra of 100)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--streams", type=int, default=64)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
-    ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec"])
+    ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec", "full"])
+    ap.add_argument("--no-spec", action="store_true", help="skip the shader-arithmetic leg")
+    ap.add_argument("--no-full", action="store_true", help="skip the VP9 (FULL) leg")
+    ap.add_argument("--no-capacity", action="store_true", help="skip the serving capacity sweep")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-single", action="store_true", help="skip the single-stream leg")
     ap.add_argument("--no-graphs", action="store_true")
@@ -62,7 +74,14 @@ def parse():
     return ap.parse_args()
 
 
-def step_frame(t):
+def step_frame(t, mode="inter", gop=100):
+    """Distinct parsed frame used at step t. "gop": a key frame every `gop`
+    steps (t % gop == 0), inter frames between; "inter": the key frame at
+    t = 0 only; "key": key frames only."""
+    if mode == "key":
+        return 0
+    if mode == "gop":
+        t %= gop
     return 0 if t == 0 else 1 + (t - 1) % (DISTINCT - 1)
 
 
@@ -115,11 +134,14 @@ class Workload:
     optional device copy. pfs_host[s][f] / pfs_dev[s][f] are ParsedFrame
     structs whose arrays live in those arenas."""
 
-    def __init__(self, streams, w, h, device_copy=True, seeds=None, preset=1, overrides=None):
+    def __init__(self, streams, w, h, device_copy=True, seeds=None, preset=1, overrides=None, gop=100):
         import numpy as np
         import torch
         from compute_vp9_b200 import ParsedFrame, Synth, synth_config
         self.S, self.w, self.h = streams, w, h
+        self.gop, self.mode = gop, "gop"
+        self.seeds = list(seeds) if seeds is not None else list(range(streams))
+        self.preset, self.overrides = preset, dict(overrides or {})
         t0 = time.time()
         # pass 1: generate and measure
         frames = []
@@ -242,12 +264,15 @@ class Workload:
                 lr.append(CoeffList(pos.size, base + op, base + ov))
             self.lists.append(lr)
 
+    def frame_of(self, t):
+        return step_frame(t, self.mode, self.gop)
+
     def step_lists(self, t):
-        f = step_frame(t)
+        f = self.frame_of(t)
         return [self.lists[s][f] for s in range(self.S)]
 
     def step_pfs(self, t, device):
-        f = step_frame(t)
+        f = self.frame_of(t)
         src = self.pfs_dev if device else self.pfs_host
         return [C.pointer(src[s][f]) for s in range(self.S)]
 
@@ -255,7 +280,7 @@ class Workload:
         """Algorithmic bytes of one step: recon write 1.5*W*H, reference read
         1.5*W*H on inter frames, 4 bytes per nonzero coefficient read, 32 per
         block descriptor (no NV12 target armed)."""
-        f = step_frame(t)
+        f = self.frame_of(t)
         px = self.w * self.h
         inter = 1 if f != 0 else 0
         tot = 0
@@ -322,25 +347,29 @@ class ClockSampler:
 
 # ── legs ─────────────────────────────────────────────────────────────────────
 
-def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False, record=None,
-                pack=0):
-    """K timed steps of all streams; returns (ms, per-step stats list, latencies).
+def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False, pack=0,
+                final=False):
+    """K timed steps of all streams in the workload's schedule (wl.mode).
     The engine's tuner first settles this shape's kernel configuration on
-    untimed steps (a few per candidate); `tuned` receives its choice."""
+    untimed steps; `tuned` receives its choice. Returns a dict: ms (timed
+    region), stats (last timed step), prof (per-phase device times of three
+    more steps), lat (host latencies), seq (the step indices submitted, in
+    order) and, with final=True, outs: every stream's frame after one more
+    step that downloads its outputs (the bit-exactness check replays seq)."""
     import torch
     from compute_vp9_b200.batch import DEVICE_INPUTS, NO_OUTPUT, Batch
     eng = Batch(arith=arith, use_graphs=1 if graphs else 0, autotune=1, pack=pack)
     sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
     assert all(s is not None for s in sids), "admission refused"
     flags = (DEVICE_INPUTS | NO_OUTPUT) if device_inputs else 0
+    seq = []
 
-    def submit(t):
-        if record is not None:
-            record.append(t)
+    def submit(t, fl=None):
+        seq.append(t)
         if sparse:
             eng.submit_sparse(sids, wl.step_pfs(t, False), wl.step_lists(t), [t] * wl.S, flags)
         else:
-            eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags)
+            eng.submit(sids, wl.step_pfs(t, device_inputs), [t] * wl.S, flags if fl is None else fl)
     for t in range(40):
         submit(t)
         assert eng.wait() == 0, eng.last_error()
@@ -368,41 +397,77 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None,
     last = eng.stats()
     # per-kernel device times: a few more steps, each waited for
     prof = []
-    for t in range(warmup + steps, warmup + steps + 3):
+    t_next = warmup + steps
+    for t in range(t_next, t_next + 3):
         submit(t)
         eng.wait()
         st = eng.stats()
         prof.append((st.scan_ms, st.recon_ms, st.filter_ms, st.kernels_ms, st.step_ms))
-    if record is not None and not device_inputs:
-        rc, arr = eng.get_frame_array(sids[0])
-        record_out = arr if rc == 0 else None
-    else:
-        record_out = None
+    t_next += 3
+    outs = None
+    if final:
+        submit(t_next, DEVICE_INPUTS if device_inputs else 0)
+        assert eng.wait() == 0, eng.last_error()
+        outs = []
+        for sid in sids:
+            rc, arr = eng.get_frame_array(sid)
+            outs.append(arr if rc == 0 else None)
     eng.close()
-    if record is not None:
-        record.append(record_out)
-    return ms, last, prof, [x for x in lat if x is not None]
+    return {"ms": ms, "stats": last, "prof": prof, "lat": [x for x in lat if x is not None],
+            "seq": seq, "outs": outs}
+
+
+def check_parity(wl, seq, outs, profile, streams, threads):
+    """Replay each listed stream's submitted sequence on the CPU (from its
+    last key frame, which refreshes every reference slot) and compare the
+    final frame byte for byte. REFCPU replays through the reference's own
+    compiled reconstruction (oracle/_ref) when it is built, otherwise and for
+    SPEC/FULL through the restatement. Returns the JSON record."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.oracle_py import FULL, REFCPU, SPEC, OracleStream, RefStream, ref_available
+    use_ref = profile == REFCPU and ref_available()
+    frames = [wl.frame_of(t) for t in seq]
+    start = max(i for i, f in enumerate(frames) if f == 0)
+
+    def one(s):
+        chk = RefStream() if use_ref else OracleStream(profile)
+        want = None
+        for f in frames[start:]:
+            want = chk.decode(C.pointer(wl.pfs_host[s][f]))
+        chk.close()
+        return outs[s] is not None and bool((want == outs[s]).all())
+
+    with ThreadPoolExecutor(max(1, min(threads, len(streams)))) as ex:
+        ok = list(ex.map(one, streams))
+    return {"streams_checked": len(streams), "streams_bit_exact": int(sum(ok)),
+            "frames_replayed_per_stream": len(frames) - start,
+            "checked": "final frame of each checked stream after the run's %d submitted steps, replayed "
+                       "on the CPU from the last key frame" % len(frames),
+            "against": "oracle/_ref (the reference's vp9_reconstruct_frame)" if use_ref
+                       else "oracle restatement (%s)" % {REFCPU: "REFCPU", SPEC: "SPEC", FULL: "FULL"}[profile],
+            "bit_exact": all(ok)}
 
 
 def run_single_plain(wl, frames, arith):
-    """Plain per-stream backend (the drop-in ABI) on stream 0, host inputs."""
+    """Plain per-stream backend (the drop-in ABI) on stream 0, host inputs,
+    frames in the workload's schedule."""
     from compute_vp9_b200 import CVP9_OK, CudaBackend
     be = CudaBackend(arith=arith)
     # warm-up: key frame + the frames the backend's tuner measures on
     warm = 14
     for t in range(warm):
-        assert be.decode(C.pointer(wl.pfs_host[0][step_frame(t)]), t) == CVP9_OK
+        assert be.decode(C.pointer(wl.pfs_host[0][wl.frame_of(t)]), t) == CVP9_OK
         rc, _ = be.get_frame(1)
         assert rc == CVP9_OK, be.last_error()
     t0 = time.perf_counter()
     pending = 0
     for t in range(warm, warm + frames):
-        rc = be.decode(C.pointer(wl.pfs_host[0][step_frame(t)]), t)
+        rc = be.decode(C.pointer(wl.pfs_host[0][wl.frame_of(t)]), t)
         if rc == -6:  # ring full: deliver the oldest, then resubmit
             r2, _ = be.get_frame(1)
             assert r2 == CVP9_OK
             pending -= 1
-            rc = be.decode(C.pointer(wl.pfs_host[0][step_frame(t)]), t)
+            rc = be.decode(C.pointer(wl.pfs_host[0][wl.frame_of(t)]), t)
         assert rc == CVP9_OK, be.last_error()
         pending += 1
     while pending:
@@ -493,7 +558,7 @@ def reference_arm(args, ws, rank):
     from concurrent.futures import ThreadPoolExecutor
     from oracle import oracle_py as O
     kind = "reference" if O.ref_available() else "port"
-    wl = Workload(args.streams, args.width, args.height, device_copy=False)
+    wl = Workload(args.streams, args.width, args.height, device_copy=False, gop=args.gop)
     cores = host_cores()
     threads = min(cores, wl.S)
     mk = (lambda: O.RefStream()) if kind == "reference" else (lambda: O.OracleStream(O.REFCPU))
@@ -501,7 +566,7 @@ def reference_arm(args, ws, rank):
 
     def one(args_):
         s, t = args_
-        streams[s].decode(C.pointer(wl.pfs_host[s][step_frame(t)]))
+        streams[s].decode(C.pointer(wl.pfs_host[s][wl.frame_of(t)]))
 
     with ThreadPoolExecutor(threads) as ex:
         for t in range(args.warmup):
@@ -530,12 +595,26 @@ def workload_config(args):
     return {
         "workload": "batched: %d x %dx%d 8-bit 4:2:0 streams, one frame per stream per step "
                     "(8x8 blocks, TX 8x8, q60, 5%% coeffs, +-64 px MVs from LAST, LF 32; "
-                    "seeds 0..%d; %d distinct parsed frames per stream, cycled)"
-                    % (args.streams, args.width, args.height, args.streams - 1, DISTINCT),
-        "streams_per_gpu": args.streams, "width": args.width, "height": args.height,
+                    "seeds 0..%d; a key frame every %d steps, inter frames between; %d distinct parsed "
+                    "frames per stream, cycled)"
+                    % (args.streams, args.width, args.height, args.streams - 1, args.gop, DISTINCT),
+        "streams_per_gpu": args.streams, "width": args.width, "height": args.height, "gop": args.gop,
         "arith": args.arith, "l2": "per-step inputs+outputs exceed L2 (no flush needed)",
         "parallelism": "streams sharded per GPU (replicas, no collective)",
     }
+
+
+def px_rate(wl, steps, ms, ws=1):
+    return ws * wl.S * wl.w * wl.h * steps / (ms / 1000.0) / 1e6
+
+
+def leg_roofline(wl, r, steps, warmup, peak):
+    """Achieved algorithmic GB/s of the recon phase of the three profiling
+    steps after the timed region, and its fraction of the peak."""
+    recon_ms = statistics.mean(p[1] for p in r["prof"])
+    alg = statistics.mean(wl.alg_bytes(t) for t in range(warmup + steps, warmup + steps + 3))
+    ach = alg / (recon_ms / 1000.0) / 1e9
+    return {"recon_ms": recon_ms, "alg_bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak}
 
 
 def main():
@@ -550,75 +629,89 @@ def main():
     import torch
     torch.cuda.set_device(local)
     os.environ.setdefault("CVP9_CUDA_DEVICE", str(local))
-    from compute_vp9_b200 import ARITH_REFCPU, ARITH_SPEC
-    arith = ARITH_SPEC if args.arith == "spec" else ARITH_REFCPU
+    from compute_vp9_b200 import ARITH_FULL, ARITH_REFCPU, ARITH_SPEC
+    from oracle.oracle_py import FULL, REFCPU, SPEC
+    arith = {"spec": ARITH_SPEC, "full": ARITH_FULL}.get(args.arith, ARITH_REFCPU)
+    oracle_profile = {ARITH_SPEC: SPEC, ARITH_FULL: FULL}.get(arith, REFCPU)
     wl = Workload(args.streams, args.width, args.height, device_copy=True,
-                  seeds=rank_seeds(rank, args.streams))
+                  seeds=rank_seeds(rank, args.streams), gop=args.gop)
     px_step = wl.S * wl.w * wl.h
+    graphs = not args.no_graphs
+    peak, peak_kind = read_peaks()
+    cores = host_cores()
 
+    # device-resident legs: the GOP-shaped sequence (the headline), inter
+    # steps only and key steps only
     clocks = ClockSampler(int(os.environ.get("CVP9_NVSMI_INDEX", str(local))))
     tuned = []
     with clocks:
-        ms_dev, st_dev, prof, _ = run_batched(wl, args.steps, args.warmup, arith, True,
-                                              not args.no_graphs, ws, tuned)
-    ms_dev = allreduce_max(ws, ms_dev)
-    value = ws * px_step * args.steps / (ms_dev / 1000.0) / 1e6
+        wl.mode = "gop"
+        R = run_batched(wl, args.steps, args.warmup, arith, True, graphs, ws, tuned)
+        wl.mode = "inter"
+        Ri = run_batched(wl, args.steps, args.warmup, arith, True, graphs, ws)
+        wl.mode = "key"
+        key_steps = min(args.steps, 12)
+        Rk = run_batched(wl, key_steps, args.warmup, arith, True, graphs, ws)
+    wl.mode = "gop"
+    ms_dev = allreduce_max(ws, R["ms"])
+    value = px_rate(wl, args.steps, ms_dev, ws)
+    ms_int = allreduce_max(ws, Ri["ms"])
+    ms_key = allreduce_max(ws, Rk["ms"])
+    timed_keys = sum(1 for t in range(args.warmup, args.warmup + args.steps) if wl.frame_of(t) == 0)
 
-    seq0 = []
-    ms_e2e, st_e2e, _, lat = run_batched(wl, args.steps, args.warmup, arith, False,
-                                         not args.no_graphs, ws, record=seq0)
-    ms_e2e = allreduce_max(ws, ms_e2e)
-    e2e = ws * px_step * args.steps / (ms_e2e / 1000.0) / 1e6
+    # end to end through the public API from page-locked host arrays, every
+    # frame downloaded; its final frames are checked against the reference
+    E = run_batched(wl, args.steps, args.warmup, arith, False, graphs, ws, final=True)
+    ms_e2e = allreduce_max(ws, E["ms"])
+    e2e = px_rate(wl, args.steps, ms_e2e, ws)
 
     # the same without host-side coefficient packing (dense arrays over PCIe)
-    ms_np, st_np, _, _ = run_batched(wl, args.steps, args.warmup, arith, False,
-                                     not args.no_graphs, ws, pack=-1)
-    ms_np = allreduce_max(ws, ms_np)
-    e2e_np = ws * px_step * args.steps / (ms_np / 1000.0) / 1e6
+    Enp = run_batched(wl, args.steps, args.warmup, arith, False, graphs, ws, pack=-1)
+    ms_np = allreduce_max(ws, Enp["ms"])
+    e2e_np = px_rate(wl, args.steps, ms_np, ws)
 
     # the same, coefficients as (index, value) lists (cvp9_batch_submit_sparse)
     wl.build_sparse()
-    ms_sp, st_sp, _, _ = run_batched(wl, args.steps, args.warmup, arith, False,
-                                     not args.no_graphs, ws, sparse=True)
-    ms_sp = allreduce_max(ws, ms_sp)
-    e2e_sp = ws * px_step * args.steps / (ms_sp / 1000.0) / 1e6
+    Esp = run_batched(wl, args.steps, args.warmup, arith, False, graphs, ws, sparse=True)
+    ms_sp = allreduce_max(ws, Esp["ms"])
+    e2e_sp = px_rate(wl, args.steps, ms_sp, ws)
+
+    # the shader arithmetic on the same workload (regular filter, as the
+    # shaders hold), device-resident
+    Rs = None
+    if not args.no_spec and arith != ARITH_SPEC:
+        Rs = run_batched(wl, args.steps, args.warmup, ARITH_SPEC, True, graphs, ws, final=True)
+        Rs["ms"] = allreduce_max(ws, Rs["ms"])
 
     out = None
     if rank == 0:
-        recon_ms = statistics.mean(p[1] for p in prof)
-        alg = statistics.mean(wl.alg_bytes(t) for t in range(args.warmup + args.steps,
-                                                               args.warmup + args.steps + 3))
-        peak, peak_kind = read_peaks()
-        achieved = alg / (recon_ms / 1000.0) / 1e9
+        main_rf = leg_roofline(wl, R, args.steps, args.warmup, peak)
+        recon_ms, alg, achieved = main_rf["recon_ms"], main_rf["alg_bytes_per_launch"], main_rf["achieved_gbs"]
         split = bool(tuned) and tuned[0].get("inter_path") in (3, 4)
         traffic = read_traffic(split)
+        parity = check_parity(wl, E["seq"], E["outs"], oracle_profile, list(range(wl.S)), cores)
+        value_spec = None
+        if Rs is not None:
+            value_spec = {"value": px_rate(wl, args.steps, Rs["ms"], ws), "unit": UNIT,
+                          "ms_per_step": Rs["ms"] / args.steps,
+                          "roofline": leg_roofline(wl, Rs, args.steps, args.warmup, peak),
+                          "parity": check_parity(wl, Rs["seq"], Rs["outs"], SPEC, list(range(min(16, wl.S))),
+                                                 cores),
+                          "what": "the same GOP-shaped device-resident steps in the shader arithmetic "
+                                  "(8-tap MC, integer butterflies on every plane)"}
         single = None
         if not args.no_single:
-            one = Workload(1, args.width, args.height, device_copy=True)
-            ms1, _, prof1, _ = run_batched(one, 60, args.warmup, arith, True, not args.no_graphs, 1)
-            single_dev = one.w * one.h * 60 / (ms1 / 1000.0) / 1e6
-            plain_e2e, plain_kern = run_single_plain(one, 60, arith)
+            one = Workload(1, args.width, args.height, device_copy=True, gop=args.gop)
+            r1 = run_batched(one, args.gop, args.warmup, arith, True, graphs, 1)
+            single_dev = px_rate(one, args.gop, r1["ms"])
+            plain_e2e, plain_kern = run_single_plain(one, args.gop, arith)
             single = {"value": single_dev, "e2e_plain_backend": plain_e2e, "unit": UNIT,
                       "kernel_ms_per_frame": plain_kern,
-                      "workload": "stream 0 alone, %dx%d; value device-resident, e2e through "
-                                  "cuda_decode_frame/cuda_get_frame with host inputs" % (one.w, one.h)}
-        # bit-exactness of the timed run: stream 0's last frame against the
-        # CPU reference (REFCPU: the reference's own code when built here,
-        # else the restatement) replaying the same frame sequence
-        parity = None
-        if not args.no_parity and seq0 and seq0[-1] is not None:
-            from oracle.oracle_py import REFCPU, SPEC, OracleStream, RefStream, ref_available
-            use_ref = arith == ARITH_REFCPU and ref_available()
-            chk = RefStream() if use_ref else OracleStream(SPEC if arith == ARITH_SPEC else REFCPU)
-            want = None
-            for t in seq0[:-1]:
-                want = chk.decode(C.pointer(wl.pfs_host[0][step_frame(t)]))
-            chk.close()
-            parity = {"checked": "stream 0, final frame after %d frames of the e2e run" % (len(seq0) - 1),
-                      "against": "oracle/_ref (the reference's vp9_reconstruct_frame)" if use_ref
-                                 else "oracle restatement",
-                      "bit_exact": bool(want is not None and (want == seq0[-1]).all())}
+                      "workload": "stream 0 alone, %dx%d, %d frames holding one key frame; value "
+                                  "device-resident, e2e through cuda_decode_frame/cuda_get_frame with host "
+                                  "inputs" % (one.w, one.h, args.gop)}
         serving = None
+        capacity = None
         if not args.no_serve:
             from compute_vp9_b200 import serve
             sv = serve.run(streams=256, rate=2.0, frames=120, fps=30.0, speed=args.serve_speed,
@@ -630,54 +723,78 @@ def main():
                        "mean_batch": sv["mean_batch"], "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
                        "value": sv["mpx_per_s"], "unit": UNIT, "admission_waits": sv["admission_waits"],
                        "latency": "frame due -> its planes in host memory"}
+            if not args.no_capacity:
+                capacity = serve.capacity_sweep(arith=arith)
         cpu = None
         if not args.no_cpu:
-            v, kind, cores, sample = cpu_leg(wl, host_cores())
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
-        launches_per_step = int(st_dev.kernel_launches)
-        # the batched step again on the other single-stream config's
-        # statistics (blocks 8-64, TX 4x4-32x32, 2-20% coefficients, +-128 px
-        # MVs from LAST/GOLDEN/ALTREF, GOP 60 with intra on key frames only)
+            v, kind, cthreads, sample = cpu_leg(wl, cores)
+            cpu = {"value": v, "unit": UNIT, "cores": cthreads, "kind": kind, "sample": sample}
+        launches_per_step = int(R["stats"].kernel_launches)
+        lat = E["lat"]
+        # configs[1]-style content (blocks 8-64, TX 4x4-32x32 weighted
+        # 30/30/25/15, 2-20% coefficients, +-128 px MVs over LAST/GOLDEN/
+        # ALTREF, filters uniform over regular/smooth/sharp, GOP 60): REFCPU
+        # and the VP9 (FULL) profile
         mixed = None
-        if not args.no_mixed:
+        value_full = None
+        if not args.no_mixed or not args.no_full:
             n_steps = args.steps
             del wl
             wl = None
             wl2 = Workload(args.streams, args.width, args.height, device_copy=True,
-                           seeds=rank_seeds(rank, args.streams), preset=2, overrides={"intra_in_inter": 0.0})
-            tuned2 = []
-            ms2, _, prof2, _ = run_batched(wl2, n_steps, args.warmup, arith, True, not args.no_graphs, 1, tuned2)
-            v2 = wl2.S * wl2.w * wl2.h * n_steps / (ms2 / 1000.0) / 1e6
-            r2 = statistics.mean(p[1] for p in prof2)
-            a2 = statistics.mean(wl2.alg_bytes(t) for t in range(args.warmup + n_steps, args.warmup + n_steps + 3))
-            mixed = {"workload": "%d x %dx%d streams, blocks 8-64 (rectangular partitions), TX 4x4..32x32 "
-                                 "weighted 30/30/25/15, 2-20%% coefficients, +-128 px MVs over LAST/GOLDEN/"
-                                 "ALTREF, GOP 60, intra on key frames only; device-resident inputs"
-                                 % (wl2.S, wl2.w, wl2.h),
-                     "value": v2, "unit": UNIT, "ms_per_step": ms2 / n_steps, "recon_ms": r2,
-                     "roofline_frac": (a2 / (r2 / 1000.0) / 1e9) / peak,
-                     "tuning": [{k: e[k] for k in ("inter_path", "lf_tile_h", "half_width")} for e in tuned2]}
+                           seeds=rank_seeds(rank, args.streams), preset=2, gop=60)
+            wdesc = ("%d x %dx%d streams, blocks 8-64 (rectangular partitions), TX 4x4..32x32 weighted "
+                     "30/30/25/15, 2-20%% coefficients, +-128 px MVs over LAST/GOLDEN/ALTREF, filter "
+                     "uniform over regular/smooth/sharp, a key frame every 60 steps; device-resident inputs"
+                     % (wl2.S, wl2.w, wl2.h))
+            if not args.no_mixed:
+                tuned2 = []
+                r2 = run_batched(wl2, n_steps, args.warmup, ARITH_REFCPU, True, graphs, 1, tuned2)
+                rf2 = leg_roofline(wl2, r2, n_steps, args.warmup, peak)
+                mixed = {"workload": wdesc, "value": px_rate(wl2, n_steps, r2["ms"]), "unit": UNIT,
+                         "ms_per_step": r2["ms"] / n_steps, "recon_ms": rf2["recon_ms"],
+                         "roofline_frac": rf2["frac"], "arith": "refcpu",
+                         "tuning": [{k: e[k] for k in ("inter_path", "lf_tile_h", "half_width")} for e in tuned2]}
+            if not args.no_full:
+                rf = run_batched(wl2, n_steps, args.warmup, ARITH_FULL, True, graphs, 1, final=True)
+                value_full = {"workload": wdesc, "value": px_rate(wl2, n_steps, rf["ms"]), "unit": UNIT,
+                              "ms_per_step": rf["ms"] / n_steps,
+                              "roofline": leg_roofline(wl2, rf, n_steps, args.warmup, peak),
+                              "kernels_ms_per_step": {"scan": statistics.mean(p[0] for p in rf["prof"]),
+                                                      "recon": statistics.mean(p[1] for p in rf["prof"]),
+                                                      "filter": statistics.mean(p[2] for p in rf["prof"])},
+                              "parity": check_parity(wl2, rf["seq"], rf["outs"], FULL, [0, 1], cores),
+                              "what": "the VP9 completion of the shader profile (compound, all frame "
+                                      "filters, per-TX directional intra + ADST, the VP9 loop filter); "
+                                      "parity against its from-spec restatement (unpinned)"}
             del wl2
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded parsed-frame streams)",
-            "config": workload_config(args),
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(st_e2e.h2d_bytes),
-                    "d2h_bytes_per_step": int(st_e2e.d2h_bytes),
+            "config": dict(workload_config(args), timed_key_steps=timed_keys),
+            "value_inter": {"value": ws * px_step * args.steps / (ms_int / 1000.0) / 1e6, "unit": UNIT,
+                            "ms_per_step": ms_int / args.steps, "what": "inter steps only"},
+            "value_key": {"value": ws * px_step * key_steps / (ms_key / 1000.0) / 1e6, "unit": UNIT,
+                          "ms_per_step": ms_key / key_steps, "steps": key_steps,
+                          "recon_ms": statistics.mean(p[1] for p in Rk["prof"]),
+                          "what": "key (intra) steps only: every superblock through the wavefront kernel"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(E["stats"].h2d_bytes),
+                    "d2h_bytes_per_step": int(E["stats"].d2h_bytes),
                     "ms_per_step": ms_e2e / args.steps,
-                    "packed_frames_per_step": int(st_e2e.packed_frames),
-                    "host_pack_ms_per_step": float(st_e2e.submit_pack_ms),
+                    "packed_frames_per_step": int(E["stats"].packed_frames),
+                    "host_pack_ms_per_step": float(E["stats"].submit_pack_ms),
                     "what": "cvp9_batch_submit from page-locked host arrays in the parser's dense layout; "
-                            "the engine packs coefficients on host threads inside the timed region"},
+                            "the engine packs coefficients on host threads inside the timed region; the "
+                            "same GOP-shaped sequence"},
             "e2e_without_packing": {"value": e2e_np, "unit": UNIT,
-                                    "h2d_bytes_per_step": int(st_np.h2d_bytes),
-                                    "d2h_bytes_per_step": int(st_np.d2h_bytes),
+                                    "h2d_bytes_per_step": int(Enp["stats"].h2d_bytes),
+                                    "d2h_bytes_per_step": int(Enp["stats"].d2h_bytes),
                                     "ms_per_step": ms_np / args.steps},
             "e2e_sparse_input": {"value": e2e_sp, "unit": UNIT,
-                                 "h2d_bytes_per_step": int(st_sp.h2d_bytes),
-                                 "d2h_bytes_per_step": int(st_sp.d2h_bytes),
+                                 "h2d_bytes_per_step": int(Esp["stats"].h2d_bytes),
+                                 "d2h_bytes_per_step": int(Esp["stats"].d2h_bytes),
                                  "ms_per_step": ms_sp / args.steps,
                                  "what": "as e2e, with each frame's coefficients handed over as (index, "
                                          "value) lists through cvp9_batch_submit_sparse (built before "
@@ -693,18 +810,22 @@ def main():
                          "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s",
                          "alg_bytes_per_launch": alg, "launch_ms": recon_ms},
-            "kernels_ms_per_step": {"scan": statistics.mean(p[0] for p in prof),
-                                    "recon": recon_ms, "filter": statistics.mean(p[2] for p in prof)},
+            "kernels_ms_per_step": {"scan": statistics.mean(p[0] for p in R["prof"]),
+                                    "recon": recon_ms, "filter": statistics.mean(p[2] for p in R["prof"])},
             "gpu_launches": launches_per_step * args.steps,
             "tuning": [{k: e[k] for k in ("settled", "inter_path", "lf_tile_h", "half_width", "trials",
                                           "best_ms")} for e in tuned],
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "parity": parity,
+            "value_spec": value_spec,
             "value_mixed_content": mixed,
+            "value_full": value_full,
             "single_stream": single,
             "serving": serving,
+            "serving_capacity": capacity,
             "batched_vs_single": (value / single["value"]) if single else None,
+            "batched_vs_single_e2e": (e2e / single["e2e_plain_backend"]) if single else None,
         }
     barrier(ws)
     if rank == 0:

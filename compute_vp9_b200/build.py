@@ -81,8 +81,11 @@ def build(force=False, oracle=False, verbose_ptxas=False):
 
 def build_oracle():
     """Compile oracle/ (restatements) and, where the reference tree is present,
-    oracle/_ref (the reference's own CPU reconstruction built from source)."""
+    oracle/_ref (the reference's own CPU reconstruction built from source) and
+    the drop-in harness (the reference library with the CUDA branch,
+    integration/)."""
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    _run(["make", "-s", "-C", os.path.join(ROOT, "integration")])
 
 
 if __name__ == "__main__":

@@ -122,3 +122,21 @@ def test_a_challenger_needs_a_clear_win(lib):
         if idx < 0:
             break
     assert step(lib, t, 9, lambda c: 1.0) == (-1, (1, 0, 0))
+
+
+def test_full_tunes_only_the_wavefront_width(lib):
+    """FULL sends every superblock through the general kernel and has one
+    loop-filter layout: whatever the fixed configuration asks, the inter path
+    stays 0 and only the wavefront width is tried."""
+    t = make(lib, arith=2, fixed=(1, 1, 0))
+    seen = []
+    for _ in range(20):
+        idx, cfg = step(lib, t, 9, lambda c: 1.0 - 0.2 * c[2])
+        if idx < 0:
+            break
+        if not seen or seen[-1] != cfg:
+            seen.append(cfg)
+    assert seen == [(0, 0, 0), (0, 0, 1)]
+    assert step(lib, t, 9, lambda c: 1.0) == (-1, (0, 0, 1))
+    t = make(lib, arith=2, enabled=0, fixed=(3, 1, 0))
+    assert step(lib, t, 1, lambda c: 1.0) == (-1, (0, 0, 0))
