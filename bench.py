@@ -687,7 +687,7 @@ def main():
     if rank == 0:
         main_rf = leg_roofline(wl, R, args.steps, args.warmup, peak)
         recon_ms, alg, achieved = main_rf["recon_ms"], main_rf["alg_bytes_per_launch"], main_rf["achieved_gbs"]
-        split = bool(tuned) and tuned[0].get("inter_path") in (3, 4)
+        split = bool(tuned) and tuned[0].get("inter_path") in (3, 4, 5)
         traffic = read_traffic(split)
         parity = check_parity(wl, E["seq"], E["outs"], oracle_profile, list(range(wl.S)), cores)
         value_spec = None

@@ -110,7 +110,7 @@ int cvp9_env_autotune(void)
 int cvp9_env_inter_fast(void)
 {
     const char *e = getenv("CVP9_INTER_FAST");
-    if (e && *e >= '0' && *e <= '4' && !e[1]) return *e - '0';
+    if (e && *e >= '0' && *e <= '5' && !e[1]) return *e - '0';
     return 1;
 }
 
@@ -225,9 +225,11 @@ static void tune_advance(cvp9_tuner_t *t, cvp9_tbucket_t *e)
         if (e->stage == 0) {
             /* inter path: the default was candidate 0; then the general
              * kernel alone, k_inter at 80 registers, the two-kernel split
-             * and (REFCPU) the split walking 8x8 TXs per TX */
-            static const int8_t alts[4] = { 0, 2, 3, 4 };
-            if (t->arith != CVP9_ARITH_FULL && e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 4 : 3)) {
+             * and (REFCPU) the split walking 8x8 TXs per TX, and that split
+             * with superblocks of 8x8 TXs only in a residual kernel of their
+             * own */
+            static const int8_t alts[5] = { 0, 2, 3, 4, 5 };
+            if (t->arith != CVP9_ARITH_FULL && e->idx <= (t->arith == CVP9_ARITH_REFCPU ? 5 : 3)) {
                 e->cur = e->best;
                 e->cur.inter = alts[e->idx - 1];
                 break;

@@ -38,8 +38,9 @@ int cvp9_ac_q(int qindex);
 /* Environment knobs: $CVP9_CUDA_DEVICE, $CVP9_ARITH (refcpu|spec|full),
  * $CVP9_INTER_FAST (warp-per-superblock inter path: 0 off, 1 the
  * 96-register kernel, 2 the 80-register kernel, 3 the two-kernel split,
- * k_pred + k_resid, 4 (REFCPU) the split with 8x8 TXs walked per TX;
- * default 1). */
+ * k_pred + k_resid, 4 (REFCPU) the split with 8x8 TXs walked per TX,
+ * 5 (REFCPU) path 4 with 8x8-only superblocks in a residual kernel of
+ * their own; default 1). */
 int cvp9_env_device(void);
 int cvp9_env_arith(void);
 int cvp9_env_inter_fast(void);
@@ -91,7 +92,8 @@ double cvp9_now(void);
 
 typedef struct {
     int8_t inter;      /* 0 general kernel only, 1 k_inter (96 registers), 2 k_inter (80),
-                        * 3 k_pred + k_resid, 4 REFCPU: the same, 8x8 TXs walked per TX */
+                        * 3 k_pred + k_resid, 4 REFCPU: the same, 8x8 TXs walked per TX,
+                        * 5 REFCPU: 4 with 8x8-only superblocks in their own residual kernel */
     int8_t lf32;       /* loop filter in 64x32 shared-memory tiles instead of
                         * 8x16 register strips */
     int8_t half;       /* wavefront kernel on half the resident CTAs */

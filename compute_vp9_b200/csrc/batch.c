@@ -985,10 +985,10 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     gkey = mix64(gkey, ((uint64_t)L.full << 32) | (uint64_t)L.lf_tickets);
     /* k_inter + k_compact, or k_pred + k_resid + k_compact (the split, both
      * profiles: cvp9k_launch_frame dispatches inter paths 3 and 4 to it) */
-    const int split = L.inter_variant >= 3;
+    const int split = L.inter_variant >= 3;     /* path 5: one more residual kernel */
     s->launches = full ? (uint32_t)(2 * (L.scan_ctas > 0) + 1 + 1)     /* scan, mode info, recon, VP9 filter */
                        : (uint32_t)((L.scan_ctas > 0) + 1 + any_tile + any_strip + (flat_w > 0 ? 2 : 0) +
-                                    (L.general ? (split ? 3 : 2) : 0));
+                                    (L.general ? (split ? 3 + (L.inter_variant == 5 && L.arith == CVP9_ARITH_REFCPU) : 2) : 0));
     if (b->use_graphs) {
         if (!s->graph || s->graph_key != gkey) {
             if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = NULL; }

@@ -3039,7 +3039,7 @@ __device__ int fast_sb_setup(S &w, const cvp9_job_t &job, int sb, int sbx, int s
  * (measured faster on both 8x8-only and mixed content; an unrolled
  * union-of-columns form, tried before it, cut instructions on 8x8 content
  * but its code size cost more on mixed TX sizes). */
-template <bool GLOBAL, bool U8, class S>
+template <bool GLOBAL, bool U8, class S, bool ONLY8 = false>
 __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_job_t &job, int nb, int lane)
 {
     unsigned sizes = 0;
@@ -3067,14 +3067,19 @@ __device__ void fast_refcpu_residual(S &w, uint8_t *dst, int pitch, const cvp9_j
         if (lane < nb) { w.txoff[lane] = (uint16_t)e0; for (int c = 0; c < cnt[0]; c++) w.txblk[e0 + c] = (uint8_t)lane; }
         if (lane + 32 < nb) { w.txoff[lane + 32] = (uint16_t)e1; for (int c = 0; c < cnt[1]; c++) w.txblk[e1 + c] = (uint8_t)(lane + 32); }
         __syncwarp();
-        switch (txl) {
-        case 0: fast_residual<4, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
-        case 1:
-            if (U8) fast_residual_d<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
-            else fast_residual<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
-            break;
-        case 2: fast_residual<16, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
-        default: fast_residual<32, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+        if (ONLY8) {
+            /* the caller took superblocks whose TXs are all 8x8 */
+            fast_residual_d<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
+        } else {
+            switch (txl) {
+            case 0: fast_residual<4, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+            case 1:
+                if (U8) fast_residual_d<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
+                else fast_residual<8, GLOBAL>(w, dst, pitch, job, ntx, lane);
+                break;
+            case 2: fast_residual<16, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+            default: fast_residual<32, GLOBAL>(w, dst, pitch, job, ntx, lane); break;
+            }
         }
         __syncwarp();
     }
@@ -3455,9 +3460,11 @@ static_assert(offsetof(ResidSmem, coef) % 16 == 0, "coefficient rows are written
  * registers (20 warps), residual at 64 (32 warps, some spilled); measured
  * best of 5..8 each on 64 x 1080p steps (1.016 ms against 1.028 for 80/64
  * and 1.10 for 80/80). */
-constexpr int kPredMinB = 5, kResidMinB = 8;
+constexpr int kPredMinB = 5, kResidMinB = 8, kResid8MinB = 8;
 
-template <int A, int MINB>
+/* MARK (REFCPU inter path 5): a taken superblock with a TX other than 8x8
+ * is marked 2 instead of 0, for k_resid's PART 2. */
+template <int A, int MINB, bool MARK = false>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t *__restrict__ jobs,
                                                            const uint32_t *__restrict__ tickets,
                                                            uint32_t n_tickets, uint32_t *__restrict__ general)
@@ -3474,7 +3481,17 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
     const int sbx = sbc * 64, sby = sbr * 64;
     int nb;
     const int nchunks = fast_sb_setup<A>(w, job, sb, sbx, sby, lane, nb);
-    if (lane == 0) general[t] = nchunks < 0 ? 1u : 0u;
+    unsigned mark = 0u;
+    if (MARK && nchunks >= 0) {
+        unsigned sizes = 0u;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int i = lane + 32 * r;
+            if (i < nb && !fb_skip(w.blk[i])) sizes |= 1u << fb_txl(w.blk[i]);
+        }
+        mark = (__reduce_or_sync(0xffffffffu, sizes) & ~2u) ? 2u : 0u;
+    }
+    if (lane == 0) general[t] = nchunks < 0 ? 1u : mark;
     if (nchunks < 0) {
         if (lane == 0) atomicAdd(general + 2 * n_tickets + 1, 1u);   /* k_compact skips when 0 */
         return;
@@ -3522,7 +3539,11 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_pred(const cvp9_job_t
 }
 
 /* U8: the REFCPU 8x8 transform through fast_residual_d (inter path 4) */
-template <int A, int MINB, bool U8>
+/* PART 0: every superblock k_pred took (general[t] == 0); with k_pred
+ * marking TX sizes (inter path 5, REFCPU), PART 1 takes the superblocks
+ * whose TXs are all 8x8 (general[t] == 0) with only the 8x8 transform in its
+ * code, PART 2 the others (general[t] == 2). */
+template <int A, int MINB, bool U8, int PART = 0>
 __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_t *__restrict__ jobs,
                                                             const uint32_t *__restrict__ tickets,
                                                             uint32_t n_tickets, const uint32_t *__restrict__ general)
@@ -3531,7 +3552,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     ResidSmem &w = reinterpret_cast<ResidSmem *>(smem_raw)[warp];
     const uint32_t t = blockIdx.x * kFastWarps + warp;
-    if (t >= n_tickets || general[t]) return;    /* general superblocks: k_recon */
+    if (t >= n_tickets || general[t] != (PART == 2 ? 2u : 0u)) return;    /* general superblocks: k_recon */
     const uint32_t code = __ldg(tickets + t);
     const cvp9_job_t &job = jobs[code >> 20];
     const int sb = (int)(code & 0xFFFFFu);
@@ -3551,7 +3572,8 @@ __global__ void __launch_bounds__(kFastWarps * 32, MINB) k_resid(const cvp9_job_
                         min(64, W - sbx), min(64, H - sby), min(32, CW - (sbx >> 1)), min(32, CH - (sby >> 1)) };
         fast_spec_residual<true>(w, D, job, nb, lane);
     } else {
-        fast_refcpu_residual<true, U8>(w, job.out + (size_t)sby * job.W + sbx, job.W, job, nb, lane);
+        fast_refcpu_residual<true, U8, ResidSmem, PART == 1>(w, job.out + (size_t)sby * job.W + sbx, job.W, job,
+                                                             nb, lane);
     }
     __syncwarp();
     if (lane == 0) {
@@ -3576,7 +3598,7 @@ __global__ void __launch_bounds__(1024) k_compact(const uint32_t *__restrict__ t
     const uint32_t per = (n + 1023u) / 1024u;
     const uint32_t b = min(n, (uint32_t)tid * per), e = min(n, b + per);
     uint32_t c = 0;
-    for (uint32_t i = b; i < e; i++) c += general[i] != 0u;
+    for (uint32_t i = b; i < e; i++) c += general[i] == 1u;
     uint32_t x = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -3597,7 +3619,7 @@ __global__ void __launch_bounds__(1024) k_compact(const uint32_t *__restrict__ t
     __syncthreads();
     uint32_t pos = x - c + (wid ? wsum[wid - 1] : 0u);
     for (uint32_t i = b; i < e; i++)
-        if (general[i]) out[pos++] = tickets[i];
+        if (general[i] == 1u) out[pos++] = tickets[i];
     if (tid == 1023) *count = pos;
 }
 
@@ -4341,11 +4363,22 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
             if ((e = cudaMemsetAsync(L->n_general + 1, 0, 4, st)) != cudaSuccess) return (int)e;
             const size_t fs = kFastWarps * sizeof(FastSmem);
             const bool spec = L->arith == CVP9_ARITH_SPEC;
-            if ((L->inter_variant == 3 || L->inter_variant == 4) && spec) {
+            if (L->inter_variant >= 3 && spec) {       /* SPEC has one split (3; 4 and 5 are REFCPU forms) */
                 k_pred<CVP9_ARITH_SPEC, kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
                     L->jobs, L->tickets, L->n_tickets, L->general);
                 k_resid<CVP9_ARITH_SPEC, kResidMinB, false><<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(
                     L->jobs, L->tickets, L->n_tickets, L->general);
+            } else if (L->inter_variant == 5) {
+                /* REFCPU: k_pred marks superblocks with TXs other than 8x8;
+                 * the 8x8-only residual kernel carries no larger transform */
+                k_pred<CVP9_ARITH_REFCPU, kPredMinB, true><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
+                    L->jobs, L->tickets, L->n_tickets, L->general);
+                k_resid<CVP9_ARITH_REFCPU, kResid8MinB, true, 1>
+                    <<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(L->jobs, L->tickets, L->n_tickets,
+                                                                               L->general);
+                k_resid<CVP9_ARITH_REFCPU, kResidMinB, true, 2>
+                    <<<fg, kFastWarps * 32, kFastWarps * sizeof(ResidSmem), st>>>(L->jobs, L->tickets, L->n_tickets,
+                                                                               L->general);
             } else if (L->inter_variant == 3 || L->inter_variant == 4) {
                 k_pred<CVP9_ARITH_REFCPU, kPredMinB><<<fg, kFastWarps * 32, kFastWarps * sizeof(PredSmem), st>>>(
                     L->jobs, L->tickets, L->n_tickets, L->general);

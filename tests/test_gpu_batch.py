@@ -55,7 +55,7 @@ def test_batch_matches_oracle(profile):
             assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
 
 
-@pytest.mark.parametrize("profile,variant", [(REFCPU, "0"), (REFCPU, "2"), (REFCPU, "3"), (REFCPU, "4"),
+@pytest.mark.parametrize("profile,variant", [(REFCPU, "0"), (REFCPU, "2"), (REFCPU, "3"), (REFCPU, "4"), (REFCPU, "5"),
                                              (SPEC, "0"), (SPEC, "2"), (SPEC, "3")])
 def test_every_inter_path_matches_oracle(profile, variant, monkeypatch):
     """Each fixed inter path the tuner can pick (general kernel only, the
@@ -130,8 +130,8 @@ def test_admission_budget():
 def test_autotune_settles_with_oracle_output(profile):
     """The tuner runs every candidate configuration on real steps: each of
     those steps still decodes to the oracle's bytes, and the bucket settles
-    after all knobs were measured (the inter paths — 4, REFCPU 5 — then
-    filter layout and wavefront width: 6 configurations, REFCPU 7)."""
+    after all knobs were measured (the inter paths — 4, REFCPU 6 — then
+    filter layout and wavefront width: 6 configurations, REFCPU 8)."""
     tuning = []
     frames = 14
     outs = decode_mix(profile, MIX, frames, tuning=tuning)
@@ -143,9 +143,9 @@ def test_autotune_settles_with_oracle_output(profile):
             assert np.array_equal(outs[i][f], want), "stream %d frame %d" % (i, f)
     assert len(tuning) == 1, tuning
     e = tuning[0]
-    assert e["settled"] == 1 and e["trials"] == (7 if profile == REFCPU else 6), e
+    assert e["settled"] == 1 and e["trials"] == (8 if profile == REFCPU else 6), e
     assert e["best_ms"] > 0 and e["lf_tile_h"] in (16, 32)
-    assert e["inter_path"] in ((0, 1, 2, 3, 4) if profile == REFCPU else (0, 1, 2, 3))
+    assert e["inter_path"] in ((0, 1, 2, 3, 4, 5) if profile == REFCPU else (0, 1, 2, 3))
 
 
 def _pinned_copy(pf, keep):
@@ -262,7 +262,7 @@ def test_launch_count_follows_inter_path(profile, monkeypatch):
     on top of the general chain (path 0)."""
     monkeypatch.setenv("CVP9_AUTOTUNE", "0")
     counts = {}
-    for variant in ("0", "1", "3"):
+    for variant in ("0", "1", "3", "5"):
         monkeypatch.setenv("CVP9_INTER_FAST", variant)
         eng = Batch(arith=profile, use_graphs=0)
         p, w, h, ov = mix_for(profile, [MIX[1]])[0]
@@ -275,3 +275,5 @@ def test_launch_count_follows_inter_path(profile, monkeypatch):
         eng.close()
     assert counts["1"] - counts["0"] == 2, counts
     assert counts["3"] - counts["0"] == 3, counts
+    # path 5 adds the second residual kernel under REFCPU; SPEC runs its split
+    assert counts["5"] - counts["0"] == (4 if profile == REFCPU else 3), counts

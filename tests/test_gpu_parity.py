@@ -67,12 +67,13 @@ def test_parity_without_inter_fast_path(name, profile, monkeypatch):
     run_case(profile, *CASES[name])
 
 
-@pytest.mark.parametrize("variant", ["3", "4"])
+@pytest.mark.parametrize("variant", ["3", "4", "5"])
 @pytest.mark.parametrize("name", list(CASES))
 def test_refcpu_parity_prediction_residual_split(name, variant, monkeypatch):
     """REFCPU's two-kernel inter path (k_pred into the frame, then k_resid in
-    place; CVP9_INTER_FAST=3, and 4 walking 8x8 TXs per TX) gives
-    the oracle's bytes on every case."""
+    place; CVP9_INTER_FAST=3, 4 walking 8x8 TXs per TX, 5 with superblocks
+    of 8x8 TXs only in a residual kernel of their own) gives the oracle's
+    bytes on every case."""
     monkeypatch.setenv("CVP9_INTER_FAST", variant)
     run_case(REFCPU, *CASES[name])
 
