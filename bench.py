@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--no-parity", action="store_true", help="skip the bit-exactness check of the e2e run")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the second batched run on mixed block/TX-size content")
+    ap.add_argument("--leg", default=None, choices=["gop", "inter", "key", "mixed"],
+                    help="run one device-resident leg alone and print its timing (profiler captures); "
+                         "mixed = the mixed block/TX-size content, GOP 60")
+    ap.add_argument("--no-tune", action="store_true", help="with --leg: the tuner off (default kernels)")
     ap.add_argument("--serve-speed", type=float, default=4.0,
                     help="pacing compression of the serving run (1 = the config's real time)")
     return ap.parse_args()
@@ -348,7 +352,7 @@ class ClockSampler:
 # ── legs ─────────────────────────────────────────────────────────────────────
 
 def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None, sparse=False, pack=0,
-                final=False):
+                final=False, tune=True):
     """K timed steps of all streams in the workload's schedule (wl.mode).
     The engine's tuner first settles this shape's kernel configuration on
     untimed steps; `tuned` receives its choice. Returns a dict: ms (timed
@@ -358,7 +362,7 @@ def run_batched(wl, steps, warmup, arith, device_inputs, graphs, ws, tuned=None,
     step that downloads its outputs (the bit-exactness check replays seq)."""
     import torch
     from compute_vp9_b200.batch import DEVICE_INPUTS, NO_OUTPUT, Batch
-    eng = Batch(arith=arith, use_graphs=1 if graphs else 0, autotune=1, pack=pack)
+    eng = Batch(arith=arith, use_graphs=1 if graphs else 0, autotune=1 if tune else 0, pack=pack)
     sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
     assert all(s is not None for s in sids), "admission refused"
     flags = (DEVICE_INPUTS | NO_OUTPUT) if device_inputs else 0
@@ -617,9 +621,46 @@ def leg_roofline(wl, r, steps, warmup, peak):
     return {"recon_ms": recon_ms, "alg_bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak}
 
 
+def leg_only(args, ws, rank, local):
+    """One device-resident leg alone, for profiler captures: the tuner's
+    settling steps (unless --no-tune), W warm-up steps, K timed steps and
+    three profiling steps of the named schedule; prints one JSON line."""
+    import torch
+    torch.cuda.set_device(local)
+    os.environ.setdefault("CVP9_CUDA_DEVICE", str(local))
+    from compute_vp9_b200 import ARITH_FULL, ARITH_REFCPU, ARITH_SPEC
+    arith = {"spec": ARITH_SPEC, "full": ARITH_FULL}.get(args.arith, ARITH_REFCPU)
+    preset, gop, mode, ov = 1, args.gop, args.leg, {}
+    if args.leg == "mixed":
+        preset, gop, mode, ov = 2, 60, "gop", {"intra_in_inter": 0.0}
+        if arith == ARITH_SPEC:
+            ov["interp_filter"] = 0          # the shader profile holds the regular filter only
+    wl = Workload(args.streams, args.width, args.height, device_copy=True,
+                  seeds=rank_seeds(rank, args.streams), preset=preset, overrides=ov, gop=gop)
+    wl.mode = mode
+    tuned = []
+    r = run_batched(wl, args.steps, args.warmup, arith, True, not args.no_graphs, ws, tuned,
+                    tune=not args.no_tune)
+    ms = allreduce_max(ws, r["ms"])
+    if rank == 0:
+        print(json.dumps({"leg": args.leg, "arith": args.arith, "streams": wl.S, "width": wl.w, "height": wl.h,
+                          "steps": args.steps, "value": px_rate(wl, args.steps, ms, ws), "unit": UNIT,
+                          "ms_per_step": ms / args.steps,
+                          "kernels_ms": {k: statistics.mean(p[i] for p in r["prof"])
+                                         for i, k in enumerate(("scan", "recon", "filter", "all", "step"))},
+                          "tuning": [{k: e[k] for k in ("inter_path", "lf_tile_h", "half_width")}
+                                     for e in tuned]}), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
+    if args.leg:
+        leg_only(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         reference_arm(args, ws, rank)
         if ws > 1:
@@ -742,7 +783,8 @@ def main():
             del wl
             wl = None
             wl2 = Workload(args.streams, args.width, args.height, device_copy=True,
-                           seeds=rank_seeds(rank, args.streams), preset=2, gop=60)
+                           seeds=rank_seeds(rank, args.streams), preset=2, gop=60,
+                           overrides={"intra_in_inter": 0.0})
             wdesc = ("%d x %dx%d streams, blocks 8-64 (rectangular partitions), TX 4x4..32x32 weighted "
                      "30/30/25/15, 2-20%% coefficients, +-128 px MVs over LAST/GOLDEN/ALTREF, filter "
                      "uniform over regular/smooth/sharp, a key frame every 60 steps; device-resident inputs"

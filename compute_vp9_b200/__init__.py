@@ -30,9 +30,9 @@ EXPORTED_SYMBOLS = [
     "cuda_backend_last_error", "cuda_backend_selftest_wait_limit",
     "cvp9_batch_create", "cvp9_batch_destroy", "cvp9_batch_stream_bytes",
     "cvp9_batch_open_stream", "cvp9_batch_close_stream", "cvp9_batch_submit",
-    "cvp9_batch_wait", "cvp9_batch_poll", "cvp9_batch_get_frame", "cvp9_batch_stats",
+    "cvp9_batch_wait", "cvp9_batch_poll", "cvp9_batch_get_frame", "cvp9_batch_get_frame_at", "cvp9_batch_stats",
     "cvp9_batch_last_error", "cvp9_batch_timer_start", "cvp9_batch_timer_stop",
-    "cvp9_batch_last_seq", "cvp9_batch_step_latency", "cvp9_batch_tune_count",
+    "cvp9_batch_last_seq", "cvp9_batch_step_latency", "cvp9_batch_step_timeline", "cvp9_batch_tune_count",
     "cvp9_batch_tune_entry", "cvp9_batch_submit_sparse", "cvp9_pack_bound_words",
     "cvp9_pack_coeffs",
 ]

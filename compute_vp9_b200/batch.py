@@ -56,6 +56,7 @@ def _bind(lib):
     lib.cvp9_batch_wait.argtypes = [vp]
     lib.cvp9_batch_poll.argtypes = [vp]
     lib.cvp9_batch_get_frame.argtypes = [vp, C.c_int, C.POINTER(FrameInfo)]
+    lib.cvp9_batch_get_frame_at.argtypes = [vp, C.c_int, C.c_uint64, C.POINTER(FrameInfo)]
     lib.cvp9_batch_stats.argtypes = [vp, C.POINTER(BatchStats)]
     lib.cvp9_batch_last_error.argtypes = [vp]
     lib.cvp9_batch_last_error.restype = C.c_char_p
@@ -64,6 +65,7 @@ def _bind(lib):
     lib.cvp9_batch_last_seq.argtypes = [vp]
     lib.cvp9_batch_last_seq.restype = C.c_uint64
     lib.cvp9_batch_step_latency.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double)]
+    lib.cvp9_batch_step_timeline.argtypes = [vp, C.c_uint64, C.POINTER(C.c_float)]
     lib.cvp9_pack_bound_words.argtypes = [C.c_uint32]
     lib.cvp9_pack_bound_words.restype = C.c_size_t
     lib.cvp9_pack_coeffs.argtypes = [C.c_int, C.POINTER(ParsedFrame), vp, C.c_size_t]
@@ -160,6 +162,19 @@ class Batch:
         n = i420_size(info.width, info.height)
         return rc, np.ctypeslib.as_array(info.plane_y, shape=(n,)).copy()
 
+    def get_frame_at(self, sid, seq):
+        """The frame stream `sid` got from step `seq` (cvp9_batch_get_frame_at)."""
+        info = FrameInfo()
+        rc = self._lib.cvp9_batch_get_frame_at(self._h, sid, seq, C.byref(info))
+        return rc, info
+
+    def get_frame_array_at(self, sid, seq):
+        rc, info = self.get_frame_at(sid, seq)
+        if rc != CVP9_OK:
+            return rc, None
+        n = i420_size(info.width, info.height)
+        return rc, np.ctypeslib.as_array(info.plane_y, shape=(n,)).copy()
+
     def stats(self):
         st = BatchStats()
         self._lib.cvp9_batch_stats(self._h, C.byref(st))
@@ -197,6 +212,14 @@ class Batch:
         ms = C.c_double()
         rc = self._lib.cvp9_batch_step_latency(self._h, seq, C.byref(ms))
         return ms.value if rc == CVP9_OK else None
+
+    def step_timeline(self, seq):
+        """Device timeline of completed step `seq` after timer_start: ms to
+        its (upload start, upload end, kernels start, kernels end, download
+        end), or None."""
+        t = (C.c_float * 5)()
+        rc = self._lib.cvp9_batch_step_timeline(self._h, seq, t)
+        return tuple(t) if rc == CVP9_OK else None
 
     def close(self):
         if self._h:

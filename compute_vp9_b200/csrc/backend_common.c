@@ -114,6 +114,12 @@ int cvp9_env_inter_fast(void)
     return 1;
 }
 
+int cvp9_env_recon_warp(void)
+{
+    const char *e = getenv("CVP9_RECON_WARP");
+    return !(e && e[0] == '0' && !e[1]);
+}
+
 int cvp9_env_arith(void)
 {
     const char *e = getenv("CVP9_ARITH");

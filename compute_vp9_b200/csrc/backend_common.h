@@ -45,6 +45,7 @@ int cvp9_env_device(void);
 int cvp9_env_arith(void);
 int cvp9_env_inter_fast(void);
 int cvp9_env_autotune(void);        /* $CVP9_AUTOTUNE: 0 turns tuning off */
+int cvp9_env_recon_warp(void);      /* $CVP9_RECON_WARP: 0 keeps every k_recon level CTA-wide */
 int cvp9_env_gather(void);          /* $CVP9_GATHER: 0 uploads whole coefficient arrays */
 /* coefficient packing: -1 never, 0 large steps, 1 always ($CVP9_PACK=0|1
  * overrides the configured value) */

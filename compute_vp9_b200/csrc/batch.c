@@ -30,6 +30,9 @@
 
 #define BSLOTS 3
 #define MAXF 12
+/* Host output buffers per stream: up to two other steps in flight holding
+ * the stream, the two newest completed frames, and the new one. */
+#define OUTR (BSLOTS + 2)
 #define WAIT_LIMIT_S 60.0
 #define ALIGN_UP(x, a) (((x) + (a) - 1) / (a) * (a))
 #define LAT_RING 4096
@@ -54,11 +57,14 @@ typedef struct {
     bframe_t  f[MAXF];
     int       ref_slot[8];
     uint64_t  reserved;
-    uint8_t  *h_out[2];
-    size_t    h_out_cap[2];
-    int32_t   out_w[2], out_h[2];
-    int64_t   out_pts[2];
-    uint64_t  out_seq[2];
+    /* host output ring: the newest step's frame, frames of steps still in
+     * flight and the two newest completed ones are never overwritten */
+    uint8_t  *h_out[OUTR];
+    size_t    h_out_cap[OUTR];
+    int32_t   out_w[OUTR], out_h[OUTR];
+    int64_t   out_pts[OUTR];
+    uint64_t  out_seq[OUTR];      /* step that downloads into it, 0 none       */
+    uint32_t  out_status[OUTR];   /* that step's status word for this stream   */
     int       latest;           /* output buffer of the newest step, -1 none */
     uint64_t  last_seq;         /* newest step that included this stream     */
     uint32_t  last_status;
@@ -75,6 +81,7 @@ typedef struct {
     size_t      at[IN_N];  /* byte offsets in d_in */
     const void *gsrc;      /* REFCPU gather source: device view of page-locked coefficients */
     unsigned    staged;    /* bit k: array k goes through the pinned staging buffer */
+    int         outk;      /* host output buffer of the frame's stream, -1 none */
 } bfin_t;
 typedef struct { const void *src; size_t off, n; } bdirect_t;
 
@@ -130,6 +137,11 @@ struct cvp9_batch {
     double       lat_submit[LAT_RING];
     volatile double lat_done[LAT_RING];
     uint64_t     lat_seq[LAT_RING];
+    /* device timeline of recent steps, ms after the timer's start event:
+     * upload start, upload end, kernels start, kernels end, download end */
+    float        tl[LAT_RING][5];
+    uint64_t     tl_seq[LAT_RING];
+    int          t0_set;
     float        submit_pack_ms, submit_wait_ms;   /* the last submit's host time */
     cvp9_batch_stats_t last;
     arena_t      dev;        /* device buffers: frames, flags, step inputs      */
@@ -236,8 +248,7 @@ static void free_stream(cvp9_batch_t *b, bstream_t *s)
     for (int i = 0; i < MAXF; i++) arena_free(&b->dev, s->f[i].dev, s->f[i].cap);
     arena_free(&b->dev, s->d_sb_done, (size_t)s->sb_cap * 4);
     arena_free(&b->dev, s->d_mi_map, s->mi_cap * 4);
-    arena_free(&b->pin, s->h_out[0], s->h_out_cap[0]);
-    arena_free(&b->pin, s->h_out[1], s->h_out_cap[1]);
+    for (int k = 0; k < OUTR; k++) arena_free(&b->pin, s->h_out[k], s->h_out_cap[k]);
     memset(s, 0, sizeof(*s));
 }
 
@@ -341,7 +352,9 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
             return CVP9_ERR_NOMEM;
         }
     }
-    /* both download buffers now, so no pinned allocation happens per step */
+    /* two download buffers now, so a stream that is in at most one step at a
+     * time never allocates pinned memory on a step; the rest of the ring is
+     * taken when steps holding the stream overlap */
     {
         size_t fb = frame_bytes((int32_t)w, (int32_t)h);
         for (int k = 0; k < 2; k++) {
@@ -360,6 +373,7 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
     s->n_sb = n_sb;
     s->epoch = 0;
     for (int i = 0; i < MAXF; i++) { s->f[i].users = 0; s->f[i].d2h_seq = 0; }
+    for (int k = 0; k < OUTR; k++) { s->out_seq[k] = 0; s->out_status[k] = 0; }
     s->latest = -1;
     s->last_seq = 0;
     s->last_status = 0;
@@ -499,9 +513,20 @@ static void complete_slot(cvp9_batch_t *b, bslot_t *s)
     b->last.recon_ms = r;
     b->last.filter_ms = f;
     cvp9_tuner_report(&b->tuner, s->tune_idx, s->tune_cfg, k);
+    if (b->t0_set) {
+        cudaEvent_t ev[5] = { s->ev_start, s->ev_h2d, s->ev_k0, s->ev_k1, s->ev_end };
+        float *tl = b->tl[s->seq % LAT_RING];
+        for (int i = 0; i < 5; i++)
+            if (cudaEventElapsedTime(&tl[i], b->ev_t0, ev[i]) != cudaSuccess) tl[i] = 0.f;
+        b->tl_seq[s->seq % LAT_RING] = s->seq;
+    }
     for (int i = 0; i < s->n; i++) {
         bstream_t *st = &b->st[s->sids[i]];
-        if (st->open && st->last_seq == s->seq) st->last_status = slot_status(s, i);
+        if (!st->open) continue;
+        const uint32_t w = slot_status(s, i);
+        if (st->last_seq == s->seq) st->last_status = w;
+        for (int k = 0; k < OUTR; k++)
+            if (st->out_seq[k] == s->seq) st->out_status[k] = w;
     }
     if (s->seq > b->done_seq) b->done_seq = s->seq;
     s->busy = 0;
@@ -539,6 +564,30 @@ static const void *mapped_ptr(const void *p)
     struct cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return NULL; }
     return a.type == cudaMemoryTypeHost ? a.devicePointer : NULL;
+}
+
+/* Host output buffer for the stream's frame of the step being submitted:
+ * not one a step still in flight downloads into, and not one of the two
+ * newest completed frames (a delivered frame stays valid until the stream's
+ * second next step completes). An allocated buffer is preferred; with at
+ * most two other steps in flight (the slot being reused has completed) one
+ * of the OUTR entries is always free. */
+static int pick_out(const cvp9_batch_t *b, const bstream_t *st, size_t fb)
+{
+    uint64_t n1 = 0, n2 = 0;
+    for (int k = 0; k < OUTR; k++) {
+        uint64_t q = st->out_seq[k];
+        if (!q || q > b->done_seq) continue;
+        if (q > n1) { n2 = n1; n1 = q; } else if (q > n2) n2 = q;
+    }
+    int empty = -1;
+    for (int k = 0; k < OUTR; k++) {
+        uint64_t q = st->out_seq[k];
+        if (q && (q > b->done_seq || q == n1 || q == n2)) continue;
+        if (st->h_out[k] && st->h_out_cap[k] >= fb) return k;
+        if (empty < 0) empty = k;
+    }
+    return empty;
 }
 
 /* Per-frame bookkeeping of a slot for steps of up to n frames. */
@@ -694,6 +743,22 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     int any_tile = 0, any_strip = 0;
 
     if ((err = slot_frames(s, n))) return err;
+
+    /* host output buffers, chosen (and any missing one taken from the
+     * pinned arena) before anything of the step is queued */
+    for (int i = 0; i < n; i++) {
+        bstream_t *st = &b->st[sids[i]];
+        s->fin[i].outk = -1;
+        if (!want_out) continue;
+        const size_t fb = frame_bytes(st->W, st->H);
+        const int k = pick_out(b, st, fb);
+        if (k < 0) {
+            snprintf(b->err, sizeof(b->err), "stream %d: no free output buffer", sids[i]);
+            return CVP9_ERR_NOMEM;
+        }
+        if ((err = grow_host(b, (void **)&st->h_out[k], &st->h_out_cap[k], fb))) return err;
+        s->fin[i].outk = k;
+    }
 
     /* Large steps of dense host arrays: pack the coefficients on the host
      * pool (the PCIe link, not the host, bounds such a step) */
@@ -957,6 +1022,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         L.recon_ctas = (int)s->n_tickets < width ? (int)s->n_tickets : width;
     }
     L.lf_tile_h = tc.lf32 ? 32 : 64;
+    L.warp_levels = cvp9_env_recon_warp();
     if (tc.inter) {
         L.general = s->d_fast;
         L.general_tickets = s->d_fast + s->n_tickets;
@@ -983,6 +1049,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     gkey = mix64(gkey, (uint64_t)(uintptr_t)L.general);
     gkey = mix64(gkey, ((uint64_t)L.inter_variant << 16) | (uint64_t)L.lf_tile_h);
     gkey = mix64(gkey, ((uint64_t)L.full << 32) | (uint64_t)L.lf_tickets);
+    gkey = mix64(gkey, (uint64_t)L.warp_levels);
     /* k_inter + k_compact, or k_pred + k_resid + k_compact (the split, both
      * profiles: cvp9k_launch_frame dispatches inter paths 3 and 4 to it) */
     const int split = L.inter_variant >= 3;     /* path 5: one more residual kernel */
@@ -1027,12 +1094,8 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     for (int i = 0; i < n; i++) {
         bstream_t *st = &b->st[sids[i]];
         if (want_out) {
-            int par = st->latest < 0 ? 0 : (st->latest ^ 1);
-            size_t fb = frame_bytes(st->W, st->H);
-            if ((err = grow_host(b, (void **)&st->h_out[par], &st->h_out_cap[par], fb))) {
-                if (ofr != out_frame) free(ofr);
-                return err;
-            }
+            const int par = s->fin[i].outk;
+            const size_t fb = frame_bytes(st->W, st->H);
             BCK(cudaMemcpyAsync(st->h_out[par], st->f[ofr[i]].dev, fb, cudaMemcpyDeviceToHost, b->ds), "download");
             s->d2h_bytes += fb;
             st->f[ofr[i]].d2h_seq = seq;
@@ -1040,6 +1103,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             st->out_h[par] = st->H;
             st->out_pts[par] = pts ? pts[i] : 0;
             st->out_seq[par] = seq;
+            st->out_status[par] = 0;
             st->latest = par;
         }
         st->last_seq = seq;
@@ -1109,37 +1173,56 @@ int cvp9_batch_poll(cvp9_batch_t *b)
     return 1;
 }
 
-cvp9_err_t cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *info)
+/* Planes of output buffer k of stream sid, once the step downloading into
+ * it has completed (AGAIN while it runs). */
+static cvp9_err_t deliver(cvp9_batch_t *b, int sid, int k, cvp9_frame_info_t *info)
 {
-    if (!b || !info || sid < 0 || sid >= b->max_streams || !b->st[sid].open) return CVP9_ERR_INVALID_DATA;
     bstream_t *st = &b->st[sid];
-    if (st->latest < 0) return CVP9_ERR_UNSUPPORTED;
-    int par = st->latest;
-    if (st->out_seq[par] > b->done_seq) {
-        bslot_t *s = &b->slot[st->out_seq[par] % BSLOTS];
-        if (s->busy && s->seq == st->out_seq[par]) {
+    if (st->out_seq[k] > b->done_seq) {
+        bslot_t *s = &b->slot[st->out_seq[k] % BSLOTS];
+        if (s->busy && s->seq == st->out_seq[k]) {
             /* the frame and the status words have landed once ev_end is done */
             cudaError_t e = cudaEventQuery(s->ev_end);
             if (e == cudaErrorNotReady) return CVP9_ERR_AGAIN;
             if (e != cudaSuccess) return bfail(b, e, "step completion");
             for (int i = 0; i < s->n; i++)
-                if (s->sids[i] == sid) st->last_status = slot_status(s, i);
+                if (s->sids[i] == sid) {
+                    st->out_status[k] = slot_status(s, i);
+                    if (st->last_seq == s->seq) st->last_status = st->out_status[k];
+                }
             if (cudaEventQuery(s->ev_cb) == cudaSuccess) complete_slot(b, s);
         }
     }
-    if (st->last_status & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) return CVP9_ERR_INVALID_DATA;
-    if (st->last_status & CVP9_JOB_TIMEOUT) return CVP9_ERR_GPU;
-    uint32_t w = (uint32_t)st->out_w[par], h = (uint32_t)st->out_h[par];
+    const uint32_t status = st->out_status[k];
+    if (status & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) return CVP9_ERR_INVALID_DATA;
+    if (status & CVP9_JOB_TIMEOUT) return CVP9_ERR_GPU;
+    uint32_t w = (uint32_t)st->out_w[k], h = (uint32_t)st->out_h[k];
     uint32_t cw = (w + 1) / 2, ch = (h + 1) / 2;
     info->width = w;
     info->height = h;
     info->stride_y = w;
     info->stride_uv = cw;
-    info->plane_y = st->h_out[par];
-    info->plane_u = st->h_out[par] + (size_t)w * h;
-    info->plane_v = st->h_out[par] + (size_t)w * h + (size_t)cw * ch;
-    info->pts = st->out_pts[par];
+    info->plane_y = st->h_out[k];
+    info->plane_u = st->h_out[k] + (size_t)w * h;
+    info->plane_v = st->h_out[k] + (size_t)w * h + (size_t)cw * ch;
+    info->pts = st->out_pts[k];
     return CVP9_OK;
+}
+
+cvp9_err_t cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *info)
+{
+    if (!b || !info || sid < 0 || sid >= b->max_streams || !b->st[sid].open) return CVP9_ERR_INVALID_DATA;
+    if (b->st[sid].latest < 0) return CVP9_ERR_UNSUPPORTED;
+    return deliver(b, sid, b->st[sid].latest, info);
+}
+
+cvp9_err_t cvp9_batch_get_frame_at(cvp9_batch_t *b, int sid, uint64_t seq, cvp9_frame_info_t *info)
+{
+    if (!b || !info || sid < 0 || sid >= b->max_streams || !b->st[sid].open || seq == 0) return CVP9_ERR_INVALID_DATA;
+    const bstream_t *st = &b->st[sid];
+    for (int k = 0; k < OUTR; k++)
+        if (st->out_seq[k] == seq) return deliver(b, sid, k, info);
+    return CVP9_ERR_INVALID_DATA;
 }
 
 cvp9_err_t cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *out)
@@ -1167,6 +1250,7 @@ cvp9_err_t cvp9_batch_timer_start(cvp9_batch_t *b)
     if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
     /* the next step's upload (hs) starts after this event */
     BCK(cudaEventRecord(b->ev_t0, b->hs), "timer");
+    b->t0_set = 1;
     return CVP9_OK;
 }
 
@@ -1201,6 +1285,15 @@ cvp9_err_t cvp9_batch_step_latency(cvp9_batch_t *b, uint64_t seq, double *ms)
     double d = b->lat_done[seq % LAT_RING];
     if (d == 0.0) return CVP9_ERR_AGAIN;
     *ms = 1000.0 * (d - b->lat_submit[seq % LAT_RING]);
+    return CVP9_OK;
+}
+
+cvp9_err_t cvp9_batch_step_timeline(cvp9_batch_t *b, uint64_t seq, float t[5])
+{
+    if (!b || !t || seq == 0 || seq > b->seq || b->seq - seq >= LAT_RING || !b->t0_set) return CVP9_ERR_INVALID_DATA;
+    if (seq > b->done_seq) return CVP9_ERR_AGAIN;
+    if (b->tl_seq[seq % LAT_RING] != seq) return CVP9_ERR_INVALID_DATA;
+    memcpy(t, b->tl[seq % LAT_RING], 5 * sizeof(float));
     return CVP9_OK;
 }
 

@@ -394,6 +394,7 @@ cvp9_err_t cuda_decode_frame(void *ctx, const vp9_parsed_frame_t *pf, int64_t pt
     L.ticket_counter = c->d_misc + 1;
     L.recon_ctas = tc.half ? (c->recon_ctas + 1) / 2 : c->recon_ctas;
     L.lf_tile_h = tc.lf32 ? 32 : 64;
+    L.warp_levels = cvp9_env_recon_warp();
     if (tc.inter) {
         L.general = c->d_fast;
         L.general_tickets = c->d_fast + c->n_sb;

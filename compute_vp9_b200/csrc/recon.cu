@@ -323,6 +323,8 @@ struct ReconSmem {
     cvp9_job_t jc;                               /* this ticket's job           */
     BlkS     blk[kMaxBlocks];
     unsigned long long lvl_cnt[kMaxBlocks + 1];
+    uint8_t  lvl_big[kMaxBlocks + 1];            /* level holds a block that is
+                                                  * not a small intra block    */
     uint32_t txmask[256 + 64 + 64];              /* per-TX column-nonzero bits  */
     uint16_t cell[256];                          /* owner block + 1 per 4x4     */
     uint16_t lvl[kMaxBlocks];
@@ -1279,6 +1281,81 @@ __device__ void full_intra_block(ReconSmem &s, const BlkS &b, int sbx, int sby, 
     }
 }
 
+/* The two transform passes of one residual item (a TX column, then a TX
+ * row; FULL: a row, then a column) of block b, item index `item` inside the
+ * block. Pass 1 reads the coefficients (staged span or global), pass 2 adds
+ * the residual into the tile. */
+template <int A>
+__device__ __forceinline__ void item_pass1(ReconSmem &s, const BlkS &b, int item, bool staged, unsigned c_base)
+{
+    const cvp9_job_t &job = s.jc;
+    int j;
+    TxRef t = locate_item(b, item, &j);
+    if (t.coeff + (uint64_t)(t.n * t.n) > (uint64_t)job.num_coeffs) return;
+    const int16_t *X = staged ? s.coef + (t.coeff - c_base) : job.coeffs + t.coeff;
+    if (A == CVP9_ARITH_REFCPU) {
+        const double *M = dct_basis(t.txl);
+        switch (t.txl) {
+        case 0: refcpu_col<4>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+        case 1: refcpu_col<8>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+        case 2: refcpu_col<16>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+        default: refcpu_col<32>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
+        }
+    } else if (job.full) {
+        /* FULL inter residual (DCT): rows first, item j = row j */
+        const int qdc = t.plane ? job.q_dc_uv : job.q_dc, qac = t.plane ? job.q_ac_uv : job.q_ac;
+        bool any;
+        switch (t.txl) {
+        case 0: any = full_row<4>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+        case 1: any = full_row<8>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+        case 2: any = full_row<16>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+        default: any = full_row<32>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
+        }
+        if (any) atomicOr(&s.txmask[t.mask_idx], 1u);
+    } else {
+        switch (t.txl) {
+        case 0: spec_col<4>(s, X, j, t, job.q_dc, job.q_ac); break;
+        case 1: spec_col<8>(s, X, j, t, job.q_dc, job.q_ac); break;
+        case 2: spec_col<16>(s, X, j, t, job.q_dc, job.q_ac); break;
+        default: spec_col<32>(s, X, j, t, job.q_dc, job.q_ac); break;
+        }
+    }
+}
+
+template <int A>
+__device__ __forceinline__ void item_pass2(ReconSmem &s, const BlkS &b, int item)
+{
+    const cvp9_job_t &job = s.jc;
+    int i;
+    TxRef t = locate_item(b, item, &i);
+    unsigned mask = s.txmask[t.mask_idx];
+    if (!mask) return;
+    if (A == CVP9_ARITH_REFCPU) {
+        const double *M = dct_basis(t.txl);
+        switch (t.txl) {
+        case 0: refcpu_row<4>(s, i, t.px0, t.py0, mask, M); break;
+        case 1: refcpu_row<8>(s, i, t.px0, t.py0, mask, M); break;
+        case 2: refcpu_row<16>(s, i, t.px0, t.py0, mask, M); break;
+        default: refcpu_row<32>(s, i, t.px0, t.py0, mask, M); break;
+        }
+    } else if (job.full) {
+        /* item i = column i */
+        switch (t.txl) {
+        case 0: full_col<4>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+        case 1: full_col<8>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+        case 2: full_col<16>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+        default: full_col<32>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
+        }
+    } else {
+        switch (t.txl) {
+        case 0: spec_row<4>(s, i, t); break;
+        case 1: spec_row<8>(s, i, t); break;
+        case 2: spec_row<16>(s, i, t); break;
+        default: spec_row<32>(s, i, t); break;
+        }
+    }
+}
+
 /* ── Synchronisation helpers ────────────────────────────────────────────── */
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
@@ -1446,7 +1523,7 @@ template <int A>
 __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restrict__ jobs,
                                                    const uint32_t *__restrict__ tickets,
                                                    uint32_t n_tickets, uint32_t *ticket_counter,
-                                                   const uint32_t *__restrict__ n_dev)
+                                                   const uint32_t *__restrict__ n_dev, int warp_levels)
 {
     /* with the inter fast path the general ticket count is known on the device */
     if (n_dev) n_tickets = *n_dev;
@@ -1488,7 +1565,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
         }
         for (int i = tid; i < 256 + 128; i += kThreads) s.txmask[i] = 0;
         for (int i = tid; i < 256; i += kThreads) s.cell[i] = 0;
-        for (int i = tid; i <= kMaxBlocks; i += kThreads) s.lvl_cnt[i] = 0ull;
+        for (int i = tid; i <= kMaxBlocks; i += kThreads) { s.lvl_cnt[i] = 0ull; s.lvl_big[i] = 0; }
         if (tid == 0) { s.nlev = 1; s.nb = nb; s.c_lo = 0xFFFFFFFFu; s.c_hi = 0u; }
         __syncthreads();
 
@@ -1666,6 +1743,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
         if (tid < nb) {
             my_lvl = s.lvl[tid];
             atomicMax(&s.nlev, my_lvl + 1);
+            /* small intra block: a warp predicts and transforms it alone */
+            if (!my_intra || nit > 32 || nch > 4) s.lvl_big[my_lvl] = 1;
             old = atomicAdd(&s.lvl_cnt[my_lvl], (1ull << 40) | ((unsigned long long)nch << 20) |
                                                     (unsigned long long)nit);
         }
@@ -1763,12 +1842,43 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                 }
             }
         }
-        /* FULL intra blocks read their coefficients during prediction */
-        if (A == CVP9_ARITH_SPEC && job.full) cp_async_wait_all();
+        /* FULL intra blocks, and the warp-per-block levels, read their
+         * coefficients during the prediction phase */
+        const bool warp_lv = warp_levels && any_intra;
+        if ((A == CVP9_ARITH_SPEC && job.full) || warp_lv) cp_async_wait_all();
         __syncthreads();
 
         /* 5. levels */
         for (int L = 0; L < nlev && nb > 0; L++) {
+            if (warp_lv && !s.lvl_big[L]) {
+                /* every block of the level is a small intra block: a warp
+                 * per block predicts it and runs both transform passes on its
+                 * lanes; one CTA barrier for the level instead of three */
+                for (int pos = s.base_blk[L] + warp; pos < s.base_blk[L + 1]; pos += kWarps) {
+                    const BlkS &b = s.blk[s.order[pos]];
+                    if (b.flags & 4) {
+                        full_intra_block(s, b, sbx, sby, staged, c_base, warp, lane);
+                        continue;
+                    }
+                    for (int chk = s.chunk_off[pos]; chk < s.chunk_off[pos + 1]; chk++) {
+                        const ChunkP c = chunk_params(s, chk);
+                        predict_intra_chunk<A>(s, b, sbx + b.x, sby + b.y, c.lx0, c.ly0, c.lw, c.lh,
+                                               c.cx0, c.cy0, c.clw, c.clh, lane);
+                    }
+                    __syncwarp();
+                    const int n_it = s.item_off[pos + 1] - s.item_off[pos];
+                    for (int k = lane; k < n_it; k += 32) item_pass1<A>(s, b, k, staged, c_base);
+                    __syncwarp();
+                    for (int k = lane; k < n_it; k += 32) item_pass2<A>(s, b, k);
+                    __syncwarp();
+                }
+                __syncthreads();
+                if (seq) {
+                    for (int i = tid; i < 256 + 128; i += kThreads) s.txmask[i] = 0;
+                    __syncthreads();
+                }
+                continue;
+            }
             /* phase P: prediction, warp per 8x8 chunk. REFCPU stages the
              * windows of up to kRound chunks per warp with async copies into
              * the (idle) transform buffer, waits once, then computes them. */
@@ -1835,72 +1945,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
             /* phase P': first transform pass, thread per TX column */
             for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
                 const int lo = s.item_blk[it];
-                const BlkS &b = s.blk[s.order[lo]];
-                int j;
-                TxRef t = locate_item(b, it - s.item_off[lo], &j);
-                if (t.coeff + (uint64_t)(t.n * t.n) > (uint64_t)job.num_coeffs) continue;
-                const int16_t *X = staged ? s.coef + (t.coeff - c_base) : job.coeffs + t.coeff;
-                if (A == CVP9_ARITH_REFCPU) {
-                    const double *M = dct_basis(t.txl);
-                    switch (t.txl) {
-                    case 0: refcpu_col<4>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
-                    case 1: refcpu_col<8>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
-                    case 2: refcpu_col<16>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
-                    default: refcpu_col<32>(s, X, j, t.px0, t.py0, t.mask_idx, M); break;
-                    }
-                } else if (job.full) {
-                    /* FULL inter residual (DCT): rows first, item j = row j */
-                    const int qdc = t.plane ? job.q_dc_uv : job.q_dc, qac = t.plane ? job.q_ac_uv : job.q_ac;
-                    bool any;
-                    switch (t.txl) {
-                    case 0: any = full_row<4>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
-                    case 1: any = full_row<8>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
-                    case 2: any = full_row<16>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
-                    default: any = full_row<32>(s, X, j, t.plane, t.px0, t.py0, qdc, qac, job.lossless, false); break;
-                    }
-                    if (any) atomicOr(&s.txmask[t.mask_idx], 1u);
-                } else {
-                    switch (t.txl) {
-                    case 0: spec_col<4>(s, X, j, t, job.q_dc, job.q_ac); break;
-                    case 1: spec_col<8>(s, X, j, t, job.q_dc, job.q_ac); break;
-                    case 2: spec_col<16>(s, X, j, t, job.q_dc, job.q_ac); break;
-                    default: spec_col<32>(s, X, j, t, job.q_dc, job.q_ac); break;
-                    }
-                }
+                item_pass1<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], staged, c_base);
             }
             __syncthreads();
             /* phase Q: second pass + residual add, thread per TX row */
             for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
                 const int lo = s.item_blk[it];
-                const BlkS &b = s.blk[s.order[lo]];
-                int i;
-                TxRef t = locate_item(b, it - s.item_off[lo], &i);
-                unsigned mask = s.txmask[t.mask_idx];
-                if (!mask) continue;
-                if (A == CVP9_ARITH_REFCPU) {
-                    const double *M = dct_basis(t.txl);
-                    switch (t.txl) {
-                    case 0: refcpu_row<4>(s, i, t.px0, t.py0, mask, M); break;
-                    case 1: refcpu_row<8>(s, i, t.px0, t.py0, mask, M); break;
-                    case 2: refcpu_row<16>(s, i, t.px0, t.py0, mask, M); break;
-                    default: refcpu_row<32>(s, i, t.px0, t.py0, mask, M); break;
-                    }
-                } else if (job.full) {
-                    /* item i = column i */
-                    switch (t.txl) {
-                    case 0: full_col<4>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
-                    case 1: full_col<8>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
-                    case 2: full_col<16>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
-                    default: full_col<32>(s, i, t.plane, t.px0, t.py0, job.lossless, false); break;
-                    }
-                } else {
-                    switch (t.txl) {
-                    case 0: spec_row<4>(s, i, t); break;
-                    case 1: spec_row<8>(s, i, t); break;
-                    case 2: spec_row<16>(s, i, t); break;
-                    default: spec_row<32>(s, i, t); break;
-                    }
-                }
+                item_pass2<A>(s, s.blk[s.order[lo]], it - s.item_off[lo]);
             }
             __syncthreads();
             if (seq) {
@@ -4398,14 +4449,18 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
             k_compact<<<1, 1024, 0, st>>>(L->tickets, L->general, L->n_tickets, L->general_tickets, L->n_general);
             if (spec)
                 k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->general_tickets, L->n_tickets,
-                                                                        L->ticket_counter, L->n_general);
+                                                                        L->ticket_counter, L->n_general,
+                                                                        L->warp_levels);
             else
                 k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->general_tickets, L->n_tickets,
-                                                                          L->ticket_counter, L->n_general);
+                                                                          L->ticket_counter, L->n_general,
+                                                                          L->warp_levels);
         } else if (L->arith == CVP9_ARITH_SPEC) {
-            k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter, nullptr);
+            k_recon<CVP9_ARITH_SPEC><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter,
+                                                                    nullptr, L->warp_levels);
         } else {
-            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter, nullptr);
+            k_recon<CVP9_ARITH_REFCPU><<<grid, kThreads, smem, st>>>(L->jobs, L->tickets, L->n_tickets, L->ticket_counter,
+                                                                      nullptr, L->warp_levels);
         }
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;

@@ -39,6 +39,7 @@ typedef struct {
     uint32_t        *general_tickets;
     uint32_t        *n_general;
     int              inter_variant;  /* 0: default, 1: 96-register k_inter, 2: 80-register */
+    int              warp_levels;    /* k_recon: levels of small intra blocks a warp per block */
     /* FULL profile (jobs with full set; arith SPEC): k_lf_mimap after the
      * scan, the VP9 loop filter k_lf_full after the reconstruction instead
      * of the other filters, then the NV12 pack of armed targets. */

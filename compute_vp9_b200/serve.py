@@ -9,7 +9,10 @@ admitted as soon as a finished stream frees its reservation. Every loop
 iteration gathers the frames that are due from all admitted streams — new
 arrivals join the very next step — and reconstructs them in one engine step;
 up to three steps are in flight (the engine's step slots), so frames that
-become due while the GPU works go into the next step. While a step is in
+become due while the GPU works go into the next step, also when the same
+stream's previous frame is still in one of the steps in flight (the engine
+keeps an output buffer per step in flight and delivers each frame by its
+step, cvp9_batch_get_frame_at). While a step is in
 flight, due frames are held back until the oldest of them has waited
 `hold_ms` (or a full batch is ready), so that steps carry many streams; an
 idle GPU takes due frames at once. Latency of a frame = time its
@@ -175,7 +178,7 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
                 px += st.size[0] * st.size[1]
                 st.done_frames += 1
                 if verify_hook is not None:
-                    rc, arr = eng.get_frame_array(st.sid)
+                    rc, arr = eng.get_frame_array_at(st.sid, seq)
                     verify_hook(st.req, fi, arr if rc == CVP9_OK else None)
                 if st.done_frames == st.frames:
                     eng.close_stream(st.sid)
@@ -200,10 +203,10 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
             st.admit_time = max(st.arrival, tn)
             active.append(st)
         waiting = still
-        # gather due frames (one per stream per step)
-        busy = {id(st) for _, items, _ in inflight for st, _, _ in items}
-        ready = [st for st in active if st.next_frame < st.frames and st.due(st.next_frame) <= tn
-                 and id(st) not in busy]
+        # gather due frames (one per stream per step; a stream whose previous
+        # frame is still in flight joins the next step all the same, since
+        # steps run in submission order on the device)
+        ready = [st for st in active if st.next_frame < st.frames and st.due(st.next_frame) <= tn]
         if ready and inflight and len(ready) < max_batch and hold_ms > 0:
             # the GPU is busy: let the step fill up until the oldest due frame
             # has waited hold_ms

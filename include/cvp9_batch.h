@@ -171,6 +171,14 @@ int         cvp9_batch_poll(cvp9_batch_t *b);
  * still running, CVP9_ERR_UNSUPPORTED if it has none on the host). */
 cvp9_err_t  cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *info);
 
+/* The frame stream `sid` got from step `seq` (a value of
+ * cvp9_batch_last_seq after the submit that held it): AGAIN while that step
+ * runs, INVALID_DATA if the stream was not in it, the step produced no
+ * output for it, or its buffer has since been reused (after the stream's
+ * second next step completed). A stream may sit in several steps in flight
+ * at once; this reads each of their frames in turn. */
+cvp9_err_t  cvp9_batch_get_frame_at(cvp9_batch_t *b, int sid, uint64_t seq, cvp9_frame_info_t *info);
+
 cvp9_err_t  cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *st);
 
 /* Device timer over whole steps: start records an event ahead of the next
@@ -187,6 +195,14 @@ uint64_t    cvp9_batch_last_seq(cvp9_batch_t *b);
  * landing in host memory (CVP9_ERR_AGAIN while it runs; the most recent
  * 4096 steps are kept). */
 cvp9_err_t  cvp9_batch_step_latency(cvp9_batch_t *b, uint64_t seq, double *ms);
+
+/* Device timeline of a completed step `seq` (recent 4096 steps, after a
+ * cvp9_batch_timer_start): milliseconds from the timer's start event to its
+ * upload start, upload end, kernels start, kernels end and download end
+ * (negative for events recorded before the start event). AGAIN while it
+ * runs. Shows how consecutive steps overlap on the copy and compute
+ * streams. */
+cvp9_err_t  cvp9_batch_step_timeline(cvp9_batch_t *b, uint64_t seq, float t[5]);
 
 /* Tuner buckets in use, and a copy of bucket i (0 <= i < count). */
 int         cvp9_batch_tune_count(cvp9_batch_t *b);

@@ -133,7 +133,7 @@ def test_autotune_settles_with_oracle_output(profile):
     after all knobs were measured (the inter paths — 4, REFCPU 6 — then
     filter layout and wavefront width: 6 configurations, REFCPU 8)."""
     tuning = []
-    frames = 14
+    frames = 22
     outs = decode_mix(profile, MIX, frames, tuning=tuning)
     for i, (p, w, h, ov) in enumerate(mix_for(profile, MIX)):
         syn = Synth(synth_config(p, w, h, seed=10 + i, **ov))
@@ -277,3 +277,51 @@ def test_launch_count_follows_inter_path(profile, monkeypatch):
     assert counts["3"] - counts["0"] == 3, counts
     # path 5 adds the second residual kernel under REFCPU; SPEC runs its split
     assert counts["5"] - counts["0"] == (4 if profile == REFCPU else 3), counts
+
+
+@pytest.mark.parametrize("profile", [REFCPU, SPEC])
+def test_stream_in_several_steps_in_flight(profile):
+    """One stream submitted in consecutive steps without waiting (three in
+    flight, next to a second stream that skips every other step): each
+    frame is read back by its step (cvp9_batch_get_frame_at) and equals the
+    oracle's; a step without the stream reports INVALID_DATA, and a frame
+    stays readable until the stream's second next step has completed."""
+    from compute_vp9_b200 import CVP9_ERR_AGAIN, CVP9_ERR_INVALID_DATA
+    streams = mix_for(profile, [(2, 352, 288, {"gop": 4}), (1, 320, 192, {})])
+    syns = [Synth(synth_config(p, w, h, seed=40 + i, **ov)) for i, (p, w, h, ov) in enumerate(streams)]
+    orcs = [OracleStream(profile) for _ in streams]
+    eng = Batch(arith=profile)
+    sids = [eng.open_stream(w, h) for (_, w, h, _) in streams]
+    frames = 9
+    seqs = []                                  # (step seq, [stream indices])
+    nxt = [0, 0]
+    for t in range(frames):
+        idx = [0] if t % 2 else [0, 1]
+        eng.submit([sids[i] for i in idx], [syns[i].frame(nxt[i]) for i in idx], [nxt[i] for i in idx])
+        seqs.append((eng.last_seq(), [(i, nxt[i]) for i in idx]))
+        for i in idx:
+            nxt[i] += 1
+        if t >= 2:
+            # read the frames of the step submitted two steps ago, while the
+            # two newer steps holding the same stream may still run
+            q, items = seqs[t - 2]
+            for i, f in items:
+                rc, arr = eng.get_frame_array_at(sids[i], q)
+                while rc == CVP9_ERR_AGAIN:
+                    rc, arr = eng.get_frame_array_at(sids[i], q)
+                assert rc == CVP9_OK, (rc, eng.last_error())
+                assert np.array_equal(arr, orcs[i].decode(syns[i].frame(f))), "stream %d frame %d" % (i, f)
+            if 1 not in [i for i, _ in items]:
+                assert eng.get_frame_at(sids[1], q)[0] == CVP9_ERR_INVALID_DATA
+    assert eng.wait() == CVP9_OK, eng.last_error()
+    for q, items in seqs[frames - 2:]:
+        for i, f in items:
+            rc, arr = eng.get_frame_array_at(sids[i], q)
+            assert rc == CVP9_OK
+            assert np.array_equal(arr, orcs[i].decode(syns[i].frame(f)))
+    # stream 0 was in every step: the frame of step seqs[-3] is its third
+    # newest, whose second next step has completed, so its buffer may be
+    # reused; the two newest stay readable
+    assert eng.get_frame_at(sids[0], seqs[-1][0])[0] == CVP9_OK
+    assert eng.get_frame_at(sids[0], seqs[-2][0])[0] == CVP9_OK
+    eng.close()

@@ -47,3 +47,36 @@ def test_served_frames_match_alone(profile):
     assert out["admission_waits"] > 0           # the budget made streams wait
     assert out["max_batch"] > 1                 # frames of several streams shared a step
     assert out["p99_ms"] is not None
+
+
+@pytest.mark.parametrize("profile", [REFCPU])
+def test_served_stream_pipelines_its_frames(profile):
+    """Frames due faster than a step completes: a stream's next frame joins
+    the next step while its previous one is still in flight, and every frame
+    still equals the oracle's."""
+    pool = serve.FramePool(SIZES, distinct=4, gop=6)
+    orcs = {}
+    sizes_of = {}
+    orig = serve.Stream.__init__
+
+    def capture(self, req, size, *a):
+        orig(self, req, size, *a)
+        sizes_of[req] = size
+    serve.Stream.__init__ = capture
+
+    def hook(req, fi, arr):
+        assert arr is not None, "frame not delivered"
+        o = orcs.setdefault(req, OracleStream(profile))
+        want = o.decode(__import__("ctypes").pointer(pool.frame(sizes_of[req], fi)))
+        assert np.array_equal(arr, want), "stream %d frame %d" % (req, fi)
+
+    trace = []
+    try:
+        out = serve.run(streams=3, rate=1000.0, frames=30, fps=20000.0, speed=1.0, arith=profile, seed=5,
+                        pool=pool, verify_hook=hook, sizes=SIZES, weights=[1, 1, 1], trace=trace, hold_ms=0)
+    finally:
+        serve.Stream.__init__ = orig
+    assert out["frames"] == 3 * 30
+    done = {(r[0], r[3]): r[6] for r in trace}
+    overlapped = sum(1 for r in trace if (r[0], r[3] - 1) in done and r[5] < done[(r[0], r[3] - 1)])
+    assert overlapped > 0, "no stream had two frames in flight"
