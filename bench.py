@@ -69,9 +69,11 @@ def parse():
     ap.add_argument("--no-parity", action="store_true", help="skip the bit-exactness check of the e2e run")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the second batched run on mixed block/TX-size content")
-    ap.add_argument("--leg", default=None, choices=["gop", "inter", "key", "mixed"],
+    ap.add_argument("--leg", default=None, choices=["gop", "inter", "key", "mixed", "link"],
                     help="run one device-resident leg alone and print its timing (profiler captures); "
-                         "mixed = the mixed block/TX-size content, GOP 60")
+                         "mixed = the mixed block/TX-size content, GOP 60; link = the PCIe copy probe "
+                         "(each direction alone and both at once, as single copies and as the "
+                         "per-frame pieces of a 64 x 1080p step)")
     ap.add_argument("--no-tune", action="store_true", help="with --leg: the tuner off (default kernels)")
     ap.add_argument("--serve-speed", type=float, default=4.0,
                     help="pacing compression of the serving run (1 = the config's real time)")
@@ -621,6 +623,62 @@ def leg_roofline(wl, r, steps, warmup, peak):
     return {"recon_ms": recon_ms, "alg_bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak}
 
 
+def link_probe(local):
+    """PCIe host<->device throughput on this GPU: H2D alone, D2H alone and
+    both at once on two streams, for one large copy per direction and for
+    the sizes of a 64 x 1080p step (packed inputs up, I420 frames down) as
+    single copies and as per-frame pieces. CUDA events; best of 4."""
+    import torch
+    torch.cuda.set_device(local)
+    MB = 1 << 20
+    big = 256 * MB
+    h_up = torch.empty(big, dtype=torch.uint8, pin_memory=True)
+    h_dn = torch.empty(big, dtype=torch.uint8, pin_memory=True)
+    d_up = torch.empty(big, dtype=torch.uint8, device="cuda")
+    d_dn = torch.empty(big, dtype=torch.uint8, device="cuda")
+    s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def pieces(n, piece):
+        return [(o, min(piece, n - o)) for o in range(0, n, piece)]
+
+    def run(up, dn):
+        best = None
+        for r in range(5):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            s_up.wait_stream(torch.cuda.current_stream())
+            s_dn.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s_dn):
+                for o, n in dn:
+                    h_dn[o:o + n].copy_(d_dn[o:o + n], non_blocking=True)
+            with torch.cuda.stream(s_up):
+                for o, n in up:
+                    d_up[o:o + n].copy_(h_up[o:o + n], non_blocking=True)
+            torch.cuda.current_stream().wait_stream(s_up)
+            torch.cuda.current_stream().wait_stream(s_dn)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if r and (best is None or ms < best):
+                best = ms
+        return best
+
+    UP, DN, FB = 102400000, 199065600, 3110400
+    cases = [("one 256 MB copy each way", pieces(big, big), pieces(big, big)),
+             ("a 64x1080p step, one copy each way", pieces(UP, UP), pieces(DN, DN)),
+             ("a 64x1080p step, per-frame pieces (0.8 MB up, 3.1 MB down)", pieces(UP, 800000), pieces(DN, FB)),
+             ("a 64x1080p step, 8 MB pieces", pieces(UP, 8 * MB), pieces(DN, 8 * MB))]
+    out = []
+    for name, up, dn in cases:
+        bu, bd = sum(n for _, n in up), sum(n for _, n in dn)
+        tu, td, tb = run(up, []), run([], dn), run(up, dn)
+        out.append({"case": name, "up_MB": bu / 1e6, "down_MB": bd / 1e6, "up_GBps": bu / tu / 1e6,
+                    "down_GBps": bd / td / 1e6, "both_ms": tb, "serial_ms": tu + td, "max_ms": max(tu, td),
+                    "both_GBps": (bu + bd) / tb / 1e6})
+    print(json.dumps({"leg": "link", "cases": out}), flush=True)
+
+
 def leg_only(args, ws, rank, local):
     """One device-resident leg alone, for profiler captures: the tuner's
     settling steps (unless --no-tune), W warm-up steps, K timed steps and
@@ -655,6 +713,13 @@ def leg_only(args, ws, rank, local):
 def main():
     args = parse()
     ws, rank, local = dist_setup()
+    if args.leg == "link":
+        if rank == 0:
+            link_probe(local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.leg:
         leg_only(args, ws, rank, local)
         if ws > 1:

@@ -29,7 +29,7 @@ EXPORTED_SYMBOLS = [
     "cuda_set_render_target", "cuda_backend_init_ex", "cuda_backend_last_timing",
     "cuda_backend_last_error", "cuda_backend_selftest_wait_limit",
     "cvp9_batch_create", "cvp9_batch_destroy", "cvp9_batch_stream_bytes",
-    "cvp9_batch_open_stream", "cvp9_batch_close_stream", "cvp9_batch_submit",
+    "cvp9_batch_open_stream", "cvp9_batch_close_stream", "cvp9_batch_reserve", "cvp9_batch_submit",
     "cvp9_batch_wait", "cvp9_batch_poll", "cvp9_batch_get_frame", "cvp9_batch_get_frame_at", "cvp9_batch_stats",
     "cvp9_batch_last_error", "cvp9_batch_timer_start", "cvp9_batch_timer_stop",
     "cvp9_batch_last_seq", "cvp9_batch_step_latency", "cvp9_batch_step_timeline", "cvp9_batch_tune_count",

@@ -33,7 +33,8 @@ class BatchStats(C.Structure):
                 ("graph_replays", C.c_int), ("kernel_launches", C.c_uint32),
                 ("scan_ms", C.c_float), ("recon_ms", C.c_float), ("filter_ms", C.c_float),
                 ("packed_frames", C.c_uint32), ("submit_pack_ms", C.c_float),
-                ("submit_wait_ms", C.c_float)]
+                ("submit_wait_ms", C.c_float), ("submit_stage_ms", C.c_float), ("dev_held_bytes", C.c_uint64),
+                ("host_held_bytes", C.c_uint64)]
 
 
 def _bind(lib):
@@ -50,6 +51,7 @@ def _bind(lib):
     lib.cvp9_batch_stream_bytes.restype = C.c_uint64
     lib.cvp9_batch_open_stream.argtypes = [vp, C.c_uint32, C.c_uint32]
     lib.cvp9_batch_close_stream.argtypes = [vp, C.c_int]
+    lib.cvp9_batch_reserve.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_int]
     lib.cvp9_batch_submit.argtypes = [vp, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.POINTER(ParsedFrame)), C.POINTER(C.c_int64),
                                       C.c_uint32]
@@ -118,6 +120,13 @@ class Batch:
     def open_stream(self, w, h):
         sid = self._lib.cvp9_batch_open_stream(self._h, w, h)
         return sid if sid >= 0 else None
+
+    def reserve(self, w, h, nstreams):
+        """Take device and pinned memory now for `nstreams` streams of w x h
+        (cvp9_batch_reserve), so that opening them later allocates nothing."""
+        rc = self._lib.cvp9_batch_reserve(self._h, w, h, nstreams)
+        if rc != CVP9_OK:
+            raise BatchError(rc, "cvp9_batch_reserve", self.last_error())
 
     def close_stream(self, sid):
         rc = self._lib.cvp9_batch_close_stream(self._h, sid)

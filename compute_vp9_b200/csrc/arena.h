@@ -168,4 +168,17 @@ static void arena_destroy(arena_t *a)
     memset(a, 0, sizeof(*a));
 }
 
+/* Make at least n bytes free (one new chunk for what is missing); the
+ * chunk is then carved like any other. Returns -1 when the driver refuses. */
+static int arena_reserve(arena_t *a, size_t n)
+{
+    const size_t free_b = a->held - a->used;
+    if (free_b >= n) return 0;
+    const size_t need = arena_round(n - free_b);
+    void *p = arena_alloc(a, need);
+    if (!p) return -1;
+    arena_free(a, p, need);
+    return 0;
+}
+
 #endif /* CVP9_ARENA_H */

@@ -30,6 +30,8 @@
 
 #define BSLOTS 3
 #define MAXF 12
+/* steps of at least this many frames send their inputs as one staged copy */
+#define COALESCE_MIN_FRAMES 8
 /* Host output buffers per stream: up to two other steps in flight holding
  * the stream, the two newest completed frames, and the new one. */
 #define OUTR (BSLOTS + 2)
@@ -57,10 +59,10 @@ typedef struct {
     bframe_t  f[MAXF];
     int       ref_slot[8];
     uint64_t  reserved;
-    /* host output ring: the newest step's frame, frames of steps still in
-     * flight and the two newest completed ones are never overwritten */
-    uint8_t  *h_out[OUTR];
-    size_t    h_out_cap[OUTR];
+    /* the stream's frames of its recent steps: where each landed in the
+     * engine's per-step output areas */
+    uint8_t  *h_out[OUTR];        /* planes in output area out_area[k]         */
+    int       out_area[OUTR];
     int32_t   out_w[OUTR], out_h[OUTR];
     int64_t   out_pts[OUTR];
     uint64_t  out_seq[OUTR];      /* step that downloads into it, 0 none       */
@@ -81,7 +83,8 @@ typedef struct {
     size_t      at[IN_N];  /* byte offsets in d_in */
     const void *gsrc;      /* REFCPU gather source: device view of page-locked coefficients */
     unsigned    staged;    /* bit k: array k goes through the pinned staging buffer */
-    int         outk;      /* host output buffer of the frame's stream, -1 none */
+    int         outk;      /* output record of the frame's stream, -1 none */
+    size_t      out_off;   /* the frame's offset in the step's output staging and area */
 } bfin_t;
 typedef struct { const void *src; size_t off, n; } bdirect_t;
 
@@ -95,6 +98,9 @@ typedef struct {
     uint8_t        *h_in;   size_t h_in_cap;
     uint32_t       *h_pack; size_t h_pack_cap;     /* packed coefficients (pinned) */
     bfin_t         *fin; bdirect_t *direct;        /* per frame / per array of the step */
+    bdirect_t      *stg; int stg_cap;              /* pieces copied into h_in on the host pool */
+    uint8_t        *d_out; size_t d_out_cap;       /* the step's frames side by side (device) */
+    size_t          out_total;                     /* their bytes, 256-aligned each */
     int64_t        *pk_words; size_t *pk_off;     /* packed words (-1: not packed), offset in h_pack */
     int             fin_cap;
     uint32_t        packed;                     /* frames uploaded packed */
@@ -131,6 +137,9 @@ struct cvp9_batch {
     uint64_t     seq;        /* steps submitted */
     uint64_t     done_seq;   /* every step <= done_seq is complete */
     int          graph_replays;
+    int          coalesce;   /* stage page-locked inputs of large steps: 1 always, 0 never,
+                              * -1 when the step packs nothing ($CVP9_COALESCE) */
+    int          collect;    /* download a step's frames in one copy ($CVP9_DL_COLLECT=0: one each) */
     int          resident_ctas;
     cudaEvent_t  ev_t0, ev_t1;
     /* host-clock submit and completion time of recent steps */
@@ -140,9 +149,16 @@ struct cvp9_batch {
     /* device timeline of recent steps, ms after the timer's start event:
      * upload start, upload end, kernels start, kernels end, download end */
     float        tl[LAT_RING][5];
+    /* per-step output areas (page-locked): step q downloads its frames into
+     * area q % OUTR in one copy; area_seq says which step's frames it holds */
+    uint8_t     *h_area[OUTR];
+    size_t       h_area_cap[OUTR];
+    uint64_t     area_seq[OUTR];
+    size_t       out_reserve;  /* output bytes of one step the reservations cover */
     uint64_t     tl_seq[LAT_RING];
     int          t0_set;
     float        submit_pack_ms, submit_wait_ms;   /* the last submit's host time */
+    float        submit_stage_ms;
     cvp9_batch_stats_t last;
     arena_t      dev;        /* device buffers: frames, flags, step inputs      */
     arena_t      pin;        /* pinned host buffers: downloads, job tables      */
@@ -166,11 +182,11 @@ uint64_t cvp9_batch_stream_bytes(uint32_t w, uint32_t h)
 {
     /* reference frames (LAST, GOLDEN, ALTREF, a stale key frame), the frame
      * being written, two whose downloads are in flight; SB flags; per-step
-     * inputs x BSLOTS: the dense coefficient array (2 bytes per sample), its
-     * packed form (at most as large) and the blocks */
+     * buffers x BSLOTS: the dense coefficient array (2 bytes per sample), its
+     * packed form (at most as large), the blocks and the output staging */
     uint64_t fb = frame_bytes((int32_t)w, (int32_t)h);
     uint64_t nsb = (uint64_t)((w + 63) / 64) * ((h + 63) / 64);
-    return 7 * fb + nsb * 20 + BSLOTS * (4 * fb + (uint64_t)((w + 7) / 8) * ((h + 7) / 8) * 32);
+    return 7 * fb + nsb * 20 + BSLOTS * (5 * fb + (uint64_t)((w + 7) / 8) * ((h + 7) / 8) * 32);
 }
 
 cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
@@ -189,6 +205,12 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     b->max_streams = (cfg && cfg->max_streams > 0) ? cfg->max_streams : 1024;
     b->use_graphs = cfg ? cfg->use_graphs : 1;
     b->gather = b->arith == CVP9_ARITH_REFCPU && cvp9_env_gather();
+    {
+        const char *e = getenv("CVP9_COALESCE");
+        b->coalesce = (e && e[0] == '1') ? 1 : (e && e[0] == '0') ? 0 : -1;
+        e = getenv("CVP9_DL_COLLECT");
+        b->collect = !(e && e[0] == '0');
+    }
     b->pack = cvp9_env_pack(cfg ? cfg->pack : 0);
     b->pack_q = 16;
     {
@@ -248,7 +270,6 @@ static void free_stream(cvp9_batch_t *b, bstream_t *s)
     for (int i = 0; i < MAXF; i++) arena_free(&b->dev, s->f[i].dev, s->f[i].cap);
     arena_free(&b->dev, s->d_sb_done, (size_t)s->sb_cap * 4);
     arena_free(&b->dev, s->d_mi_map, s->mi_cap * 4);
-    for (int k = 0; k < OUTR; k++) arena_free(&b->pin, s->h_out[k], s->h_out_cap[k]);
     memset(s, 0, sizeof(*s));
 }
 
@@ -272,6 +293,7 @@ void cvp9_batch_destroy(cvp9_batch_t *b)
         free(s->sids);
         free(s->fin);
         free(s->direct);
+        free(s->stg);
         free(s->pk_words);
         free(s->pk_off);
     }
@@ -301,8 +323,7 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
         bstream_t *c = &b->st[i];
         if (c->open) continue;
         /* smallest closed slot whose buffers fit */
-        if (c->d_sb_done && c->sb_cap >= n_sb && c->h_out_cap[0] >= fb_need &&
-            (sid < 0 || c->sb_cap < b->st[sid].sb_cap)) sid = i;
+        if (c->d_sb_done && c->sb_cap >= n_sb && (sid < 0 || c->sb_cap < b->st[sid].sb_cap)) sid = i;
         if (fresh < 0 && !c->d_sb_done) fresh = i;
     }
     if (sid < 0) sid = fresh;
@@ -350,22 +371,6 @@ int cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t w, uint32_t h)
         if (cudaMemsetAsync(s->d_mi_map, 0, nmi * 4, b->cs) != cudaSuccess) {
             free_stream(b, s);
             return CVP9_ERR_NOMEM;
-        }
-    }
-    /* two download buffers now, so a stream that is in at most one step at a
-     * time never allocates pinned memory on a step; the rest of the ring is
-     * taken when steps holding the stream overlap */
-    {
-        size_t fb = frame_bytes((int32_t)w, (int32_t)h);
-        for (int k = 0; k < 2; k++) {
-            if (s->h_out_cap[k] >= fb) continue;
-            arena_free(&b->pin, s->h_out[k], s->h_out_cap[k]);
-            s->h_out[k] = (uint8_t *)arena_alloc(&b->pin, fb);
-            s->h_out_cap[k] = s->h_out[k] ? fb : 0;
-            if (!s->h_out[k]) {
-                free_stream(b, s);
-                return CVP9_ERR_NOMEM;
-            }
         }
     }
     s->W = (int32_t)w;
@@ -566,13 +571,11 @@ static const void *mapped_ptr(const void *p)
     return a.type == cudaMemoryTypeHost ? a.devicePointer : NULL;
 }
 
-/* Host output buffer for the stream's frame of the step being submitted:
- * not one a step still in flight downloads into, and not one of the two
- * newest completed frames (a delivered frame stays valid until the stream's
- * second next step completes). An allocated buffer is preferred; with at
- * most two other steps in flight (the slot being reused has completed) one
- * of the OUTR entries is always free. */
-static int pick_out(const cvp9_batch_t *b, const bstream_t *st, size_t fb)
+/* Entry of the stream's output record for the step being submitted: not
+ * one of a step still in flight, and not one of the two newest completed
+ * frames. With at most two other steps in flight (the slot being reused has
+ * completed) one of the OUTR entries is always free. */
+static int pick_out(const cvp9_batch_t *b, const bstream_t *st)
 {
     uint64_t n1 = 0, n2 = 0;
     for (int k = 0; k < OUTR; k++) {
@@ -580,14 +583,12 @@ static int pick_out(const cvp9_batch_t *b, const bstream_t *st, size_t fb)
         if (!q || q > b->done_seq) continue;
         if (q > n1) { n2 = n1; n1 = q; } else if (q > n2) n2 = q;
     }
-    int empty = -1;
     for (int k = 0; k < OUTR; k++) {
         uint64_t q = st->out_seq[k];
         if (q && (q > b->done_seq || q == n1 || q == n2)) continue;
-        if (st->h_out[k] && st->h_out_cap[k] >= fb) return k;
-        if (empty < 0) empty = k;
+        return k;
     }
-    return empty;
+    return -1;
 }
 
 /* Per-frame bookkeeping of a slot for steps of up to n frames. */
@@ -622,6 +623,17 @@ static void pack_task(void *ctx, int i)
     j->words[i] = pf->num_coeffs ? cvp9_pack_coeffs(j->arith, pf, j->base + j->off[i],
                                                     cvp9_pack_bound_words(pf->num_coeffs))
                                  : -1;
+}
+
+/* Staging runs on the host pool too: piece k of the step's staged arrays
+ * (src -> h_in + off, at most STAGE_PIECE bytes). */
+#define STAGE_PIECE (4u << 20)
+typedef struct { uint8_t *h_in; const bdirect_t *pc; } stage_job_t;
+
+static void stage_task(void *ctx, int k)
+{
+    const stage_job_t *j = (const stage_job_t *)ctx;
+    memcpy(j->h_in + j->pc[k].off, j->pc[k].src, j->pc[k].n);
 }
 
 static void CUDART_CB step_done_cb(void *p)
@@ -693,6 +705,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     const double waited_ms = (b->lat_submit[seq % LAT_RING] - tw0) * 1e3;
     b->submit_wait_ms = (float)waited_ms;
     b->submit_pack_ms = 0.f;
+    b->submit_stage_ms = 0.f;
 
     /* sizes */
     const int full = b->arith == CVP9_ARITH_FULL;
@@ -744,20 +757,29 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
 
     if ((err = slot_frames(s, n))) return err;
 
-    /* host output buffers, chosen (and any missing one taken from the
-     * pinned arena) before anything of the step is queued */
+    /* outputs: each frame's place in the step's staging buffer and in the
+     * step's output area (taken from the arenas before anything of the step
+     * is queued); the area last held step seq - OUTR, long complete */
+    s->out_total = 0;
     for (int i = 0; i < n; i++) {
         bstream_t *st = &b->st[sids[i]];
         s->fin[i].outk = -1;
         if (!want_out) continue;
-        const size_t fb = frame_bytes(st->W, st->H);
-        const int k = pick_out(b, st, fb);
+        const int k = pick_out(b, st);
         if (k < 0) {
-            snprintf(b->err, sizeof(b->err), "stream %d: no free output buffer", sids[i]);
+            snprintf(b->err, sizeof(b->err), "stream %d: no free output record", sids[i]);
             return CVP9_ERR_NOMEM;
         }
-        if ((err = grow_host(b, (void **)&st->h_out[k], &st->h_out_cap[k], fb))) return err;
         s->fin[i].outk = k;
+        s->fin[i].out_off = s->out_total;
+        s->out_total += ALIGN_UP(frame_bytes(st->W, st->H), 256);
+    }
+    if (s->out_total) {
+        const int a = (int)(seq % OUTR);
+        if ((b->collect && (err = grow_dev(b, (void **)&s->d_out, &s->d_out_cap, s->out_total))) ||
+            (err = grow_host(b, (void **)&b->h_area[a], &b->h_area_cap[a], s->out_total)))
+            return err;
+        b->area_seq[a] = seq;
     }
 
     /* Large steps of dense host arrays: pack the coefficients on the host
@@ -801,8 +823,18 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
 
     /* how each host array travels: the gather kernel (REFCPU coefficients in
      * page-locked memory), direct DMA (page-locked), or the pinned staging
-     * buffer (pageable); coefficient regions the device fills get no copy */
+     * buffer (pageable); coefficient regions the device fills get no copy.
+     * A step of many frames that packed nothing also stages its page-locked
+     * block records and list arrays, so that its upload is one large copy:
+     * the PCIe link runs both directions at once best for large copies (two
+     * of ~100 MB each way move in 3.8 ms together, as 0.8 MB and 3.1 MB
+     * pieces in 5.1 ms; a 64x1080p step of coefficient lists 6.4 -> 5.2 ms).
+     * A step that packs does not: its host threads already use the host
+     * memory bandwidth that the staging copy would take (packed 64x1080p:
+     * 6.7 ms unstaged, 8.1 ms staged). $CVP9_COALESCE=0|1 forces either. */
     int any_staged = 0;
+    const int coalesce = !dev_in && n >= COALESCE_MIN_FRAMES &&
+                         (b->coalesce > 0 || (b->coalesce < 0 && !any_packed));
     for (int i = 0; i < n && !dev_in; i++) {
         const vp9_parsed_frame_t *pf = pfs[i];
         bfin_t *f = &s->fin[i];
@@ -810,10 +842,11 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         f->gsrc = NULL;
         f->staged = 0;
         if (b->gather && !lists && !packed && pf->num_coeffs && pf->num_blocks) f->gsrc = mapped_ptr(pf->coeffs);
-        if (pf->num_blocks && !is_pinned(pf->blocks)) f->staged |= 1u << IN_BLOCKS;
+        if (pf->num_blocks && (coalesce || !is_pinned(pf->blocks))) f->staged |= 1u << IN_BLOCKS;
         if (!lists && !packed && !f->gsrc && pf->num_coeffs && !is_pinned(pf->coeffs)) f->staged |= 1u << IN_COEFFS;
-        if (lists && lists[i].n && !is_pinned(lists[i].pos)) f->staged |= 1u << IN_POS;
-        if (lists && lists[i].n && !is_pinned(lists[i].val)) f->staged |= 1u << IN_VAL;
+        if (lists && lists[i].n && (coalesce || !is_pinned(lists[i].pos))) f->staged |= 1u << IN_POS;
+        if (lists && lists[i].n && (coalesce || !is_pinned(lists[i].val))) f->staged |= 1u << IN_VAL;
+        if (packed && coalesce) f->staged |= 1u << IN_PACKED;
         any_staged |= f->staged != 0;
     }
     if (!dev_in && in_bytes) {
@@ -872,7 +905,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
      * unpacked coefficients) get space only */
     s->h2d_bytes = 0;
     BCK(cudaEventRecord(s->ev_start, b->hs), "event");
-    int any_gather = 0, ndirect = 0;
+    int any_gather = 0, ndirect = 0, npieces = 0;
     size_t off = 0, staged_end = 0;
     for (int phase = 0; phase < 2 && !dev_in; phase++) {
         for (int i = 0; i < n; i++) {
@@ -892,7 +925,21 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
                 f->at[k] = off;
                 if (len[k] && copied[k]) {
                     if (stg) {
-                        cvp9_parallel_memcpy(s->h_in + off, src[k], len[k]);
+                        /* pieces of at most STAGE_PIECE bytes, copied below */
+                        const int np = (int)((len[k] + STAGE_PIECE - 1) / STAGE_PIECE);
+                        if (npieces + np > s->stg_cap) {
+                            int cap = 2 * (npieces + np) + 64;
+                            bdirect_t *q = (bdirect_t *)realloc(s->stg, (size_t)cap * sizeof(bdirect_t));
+                            if (!q) return CVP9_ERR_NOMEM;
+                            s->stg = q;
+                            s->stg_cap = cap;
+                        }
+                        for (size_t o = 0; o < len[k]; o += STAGE_PIECE) {
+                            s->stg[npieces].src = (const uint8_t *)src[k] + o;
+                            s->stg[npieces].off = off + o;
+                            s->stg[npieces].n = len[k] - o < STAGE_PIECE ? len[k] - o : STAGE_PIECE;
+                            npieces++;
+                        }
                     } else {
                         s->direct[ndirect].src = src[k];
                         s->direct[ndirect].off = off;
@@ -905,6 +952,12 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
             any_gather |= phase == 1 && f->gsrc != NULL;
         }
         if (phase == 0) staged_end = off;
+    }
+    if (npieces) {
+        stage_job_t sj = { s->h_in, s->stg };
+        const double ts0 = cvp9_now();
+        cvp9_parallel_for(npieces, stage_task, &sj);
+        b->submit_stage_ms = (float)((cvp9_now() - ts0) * 1e3);
     }
     cudaError_t ue = cudaSuccess;
     if (staged_end) {
@@ -952,6 +1005,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         job->coeffs = dev_in ? pf->coeffs : (const int16_t *)(s->d_in + f->at[IN_COEFFS]);
         job->out = st->f[of].dev;
         job->nv12 = NULL;
+        job->dl = (s->fin[i].outk >= 0 && b->collect) ? s->d_out + s->fin[i].out_off : NULL;
         for (int r = 0; r < 8; r++) {
             int f = st->ref_slot[r];
             if (f >= 0) {
@@ -1088,16 +1142,39 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     }
     BCK(cudaEventRecord(s->ev_k1, b->cs), "event");
 
-    /* downloads */
+    /* downloads: the frames side by side in the staging buffer (one kernel),
+     * then one copy into the step's output area */
     BCK(cudaStreamWaitEvent(b->ds, s->ev_k1, 0), "wait kernels");
     s->d2h_bytes = 0;
+    const int area = (int)(seq % OUTR);
+    if (s->out_total && !b->collect) {
+        for (int i = 0; i < n; i++) {
+            const bstream_t *st = &b->st[sids[i]];
+            BCK(cudaMemcpyAsync(b->h_area[area] + s->fin[i].out_off, st->f[ofr[i]].dev, frame_bytes(st->W, st->H),
+                                cudaMemcpyDeviceToHost, b->ds), "download");
+            s->d2h_bytes += frame_bytes(st->W, st->H);
+        }
+    } else if (s->out_total) {
+        size_t max_fb = 0;
+        for (int i = 0; i < n; i++) {
+            const size_t fb = frame_bytes(b->st[sids[i]].W, b->st[sids[i]].H);
+            if (fb > max_fb) max_fb = fb;
+        }
+        int crc = cvp9k_launch_collect(s->d_jobs, n, max_fb, b->ds);
+        if (crc != 0) {
+            if (ofr != out_frame) free(ofr);
+            return bfail(b, (cudaError_t)crc, "output collection");
+        }
+        s->launches_extra++;
+        BCK(cudaMemcpyAsync(b->h_area[area], s->d_out, s->out_total, cudaMemcpyDeviceToHost, b->ds), "download");
+        s->d2h_bytes += s->out_total;
+    }
     for (int i = 0; i < n; i++) {
         bstream_t *st = &b->st[sids[i]];
         if (want_out) {
             const int par = s->fin[i].outk;
-            const size_t fb = frame_bytes(st->W, st->H);
-            BCK(cudaMemcpyAsync(st->h_out[par], st->f[ofr[i]].dev, fb, cudaMemcpyDeviceToHost, b->ds), "download");
-            s->d2h_bytes += fb;
+            st->h_out[par] = b->h_area[area] + s->fin[i].out_off;
+            st->out_area[par] = area;
             st->f[ofr[i]].d2h_seq = seq;
             st->out_w[par] = st->W;
             st->out_h[par] = st->H;
@@ -1193,6 +1270,8 @@ static cvp9_err_t deliver(cvp9_batch_t *b, int sid, int k, cvp9_frame_info_t *in
             if (cudaEventQuery(s->ev_cb) == cudaSuccess) complete_slot(b, s);
         }
     }
+    /* the output area has since taken a newer step's frames */
+    if (b->area_seq[st->out_area[k]] != st->out_seq[k]) return CVP9_ERR_INVALID_DATA;
     const uint32_t status = st->out_status[k];
     if (status & (CVP9_JOB_BAD_BLOCK | CVP9_JOB_BAD_ORDER | CVP9_JOB_TOO_MANY)) return CVP9_ERR_INVALID_DATA;
     if (status & CVP9_JOB_TIMEOUT) return CVP9_ERR_GPU;
@@ -1225,6 +1304,44 @@ cvp9_err_t cvp9_batch_get_frame_at(cvp9_batch_t *b, int sid, uint64_t seq, cvp9_
     return CVP9_ERR_INVALID_DATA;
 }
 
+cvp9_err_t cvp9_batch_reserve(cvp9_batch_t *b, uint32_t w, uint32_t h, int nstreams)
+{
+    if (!b || w == 0 || h == 0 || w > 65535 || h > 65535 || nstreams <= 0) return CVP9_ERR_INVALID_DATA;
+    if (cudaSetDevice(b->device) != cudaSuccess) return CVP9_ERR_GPU;
+    const uint64_t fb = frame_bytes((int32_t)w, (int32_t)h);
+    /* the output areas and staging buffers are resized below: no step may
+     * still use them */
+    for (int k = 0; k < BSLOTS; k++) {
+        cvp9_err_t e = wait_slot(b, &b->slot[k]);
+        if (e != CVP9_OK) return e;
+    }
+    /* device: the admission unit per stream covers its frames and its share
+     * of the step buffers (the output staging with the arena's headroom on
+     * top); host: one frame per stream of slack for the step's staging and
+     * packing buffers; then every output area and staging buffer sized for
+     * a step holding all reserved streams at once */
+    const uint64_t dev = (uint64_t)nstreams * (cvp9_batch_stream_bytes(w, h) + 2 * fb);
+    const uint64_t pin = (uint64_t)nstreams * fb;
+    if (arena_reserve(&b->dev, (size_t)(b->dev.held - b->dev.used + dev)) != 0) {
+        snprintf(b->err, sizeof(b->err), "device arena: no memory to reserve %llu bytes", (unsigned long long)dev);
+        return CVP9_ERR_NOMEM;
+    }
+    if (arena_reserve(&b->pin, (size_t)(b->pin.held - b->pin.used + pin)) != 0) {
+        snprintf(b->err, sizeof(b->err), "pinned arena: no memory to reserve %llu bytes", (unsigned long long)pin);
+        return CVP9_ERR_NOMEM;
+    }
+    b->out_reserve += (size_t)nstreams * ALIGN_UP(fb, 256);
+    cvp9_err_t err;
+    for (int a = 0; a < OUTR; a++) {
+        if (b->h_area[a] && b->h_area_cap[a] >= b->out_reserve) continue;
+        b->area_seq[a] = 0;                    /* its frames, if any, are gone */
+        if ((err = grow_host(b, (void **)&b->h_area[a], &b->h_area_cap[a], b->out_reserve))) return err;
+    }
+    for (int k = 0; k < BSLOTS && b->collect; k++)
+        if ((err = grow_dev(b, (void **)&b->slot[k].d_out, &b->slot[k].d_out_cap, b->out_reserve))) return err;
+    return CVP9_OK;
+}
+
 cvp9_err_t cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *out)
 {
     if (!b || !out) return CVP9_ERR_INVALID_DATA;
@@ -1236,6 +1353,9 @@ cvp9_err_t cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *out)
     out->graph_replays = b->graph_replays;
     out->submit_pack_ms = b->submit_pack_ms;
     out->submit_wait_ms = b->submit_wait_ms;
+    out->submit_stage_ms = b->submit_stage_ms;
+    out->dev_held_bytes = b->dev.held;
+    out->host_held_bytes = b->pin.held;
     return CVP9_OK;
 }
 

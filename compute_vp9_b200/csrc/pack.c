@@ -202,6 +202,69 @@ static void pack_range(packer_t *k, uint64_t a, uint64_t e)
     }
 }
 
+#if defined(__x86_64__)
+/* The REFCPU block walk with the AVX-512 scan inlined: every luma span the
+ * reconstruction reads is a whole number of 4x4 TXs (16 coefficients), so
+ * it goes in vectors of 32 and at most one of 16, each stored whole and
+ * advanced by its mask's popcount (no branch on the data; a store past the
+ * entries is overwritten by later entries or the page padding, as in
+ * scan_avx512). Spans that cross a page, would outgrow it or end at a
+ * clipped array take the general path. Same words as the general walk. */
+__attribute__((target("avx512f,avx512bw,avx512vl,popcnt")))
+static int pack_refcpu_avx512(packer_t *k, const vp9_parsed_frame_t *pf)
+{
+    const __m512i lane = _mm512_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15);
+    const int W = (int)pf->hdr.width, H = (int)pf->hdr.height;
+    const uint32_t n = k->n;
+    uint64_t last = 0;
+    for (uint32_t i = 0; i < pf->num_blocks; i++) {
+        const vp9_macroblock_info_t *b = &pf->blocks[i];
+        if (b->skip || b->tx_size > 3 || (int)b->x >= W || (int)b->y >= H) continue;
+        const int sh = 2 + b->tx_size;
+        const int cw = b->width < W - b->x ? b->width : W - b->x;
+        const int ch = b->height < H - b->y ? b->height : H - b->y;
+        const uint64_t a = b->coeff_offset;
+        uint64_t e = a + ((uint64_t)((cw >> sh) * (ch >> sh)) << (2 * sh));
+        if (e > n) e = n;
+        if (a >= e) continue;
+        if (a < last) return -1;
+        last = e;
+        const uint32_t m = (uint32_t)(e - a);
+        if ((a >> PAGE_SHIFT) != k->p || ((e - 1) >> PAGE_SHIFT) != k->p || k->dense || (m & 15) ||
+            m > (page_len(k, k->p) + 1) / 2 - k->count) {
+            pack_range(k, a, e);
+            continue;
+        }
+        const int16_t *src = k->src + a;
+        uint32_t off = (uint32_t)(a - ((uint64_t)k->p << PAGE_SHIFT));
+        uint32_t *o = k->out + k->start + k->count;
+        uint32_t j = 0;
+        for (; j + 32 <= m; j += 32) {
+            const __m512i v = _mm512_loadu_si512((const void *)(src + j));
+            const __mmask32 nz = _mm512_test_epi16_mask(v, v);
+            const __m512i base = _mm512_add_epi32(_mm512_set1_epi32((int)(off + j)), lane);
+            const __m512i e0 = _mm512_or_si512(_mm512_slli_epi32(_mm512_cvtepi16_epi32(_mm512_castsi512_si256(v)), 16), base);
+            const __m512i e1 = _mm512_or_si512(_mm512_slli_epi32(_mm512_cvtepi16_epi32(_mm512_extracti64x4_epi64(v, 1)), 16),
+                                               _mm512_add_epi32(base, _mm512_set1_epi32(16)));
+            _mm512_storeu_si512((void *)o, _mm512_maskz_compress_epi32((__mmask16)nz, e0));
+            o += __builtin_popcount((unsigned)(nz & 0xffffu));
+            _mm512_storeu_si512((void *)o, _mm512_maskz_compress_epi32((__mmask16)(nz >> 16), e1));
+            o += __builtin_popcount((unsigned)(nz >> 16));
+        }
+        if (j < m) {
+            const __m256i v = _mm256_loadu_si256((const __m256i *)(src + j));
+            const __mmask16 nz = _mm256_test_epi16_mask(v, v);
+            const __m512i e0 = _mm512_or_si512(_mm512_slli_epi32(_mm512_cvtepi16_epi32(v), 16),
+                                               _mm512_add_epi32(_mm512_set1_epi32((int)(off + j)), lane));
+            _mm512_storeu_si512((void *)o, _mm512_maskz_compress_epi32(nz, e0));
+            o += __builtin_popcount((unsigned)nz);
+        }
+        k->count = (uint32_t)(o - (k->out + k->start));
+    }
+    return 0;
+}
+#endif
+
 int64_t cvp9_pack_coeffs(int arith, const vp9_parsed_frame_t *pf, uint32_t *out, size_t cap_words)
 {
     if (!pf || !out) return -1;
@@ -218,9 +281,14 @@ int64_t cvp9_pack_coeffs(int arith, const vp9_parsed_frame_t *pf, uint32_t *out,
     out[0] = k.np;
     if (arith != CVP9_ARITH_REFCPU) {     /* SPEC and FULL read every plane */
         pack_range(&k, 0, n);
+    } else if (pf->num_blocks && !pf->blocks) {
+        return -1;
+#if defined(__x86_64__)
+    } else if (g_scan == scan_avx512) {
+        if (pack_refcpu_avx512(&k, pf) != 0) return -1;
+#endif
     } else {
         /* each block's luma TX span, as k_gather_luma moves it */
-        if (pf->num_blocks && !pf->blocks) return -1;
         const int W = (int)pf->hdr.width, H = (int)pf->hdr.height;
         uint64_t last = 0;
         for (uint32_t i = 0; i < pf->num_blocks; i++) {

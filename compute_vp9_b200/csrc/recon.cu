@@ -4329,6 +4329,36 @@ int cvp9k_launch_unpack(const cvp9_job_t *jobs, int njobs, uint32_t max_pages, u
     return (int)cudaGetLastError();
 }
 
+/* One job per blockIdx.y; 16-byte streaming copies (both ends are
+ * 256-byte aligned arena ranges), the tail bytewise. */
+__global__ void __launch_bounds__(256) k_collect(const cvp9_job_t *__restrict__ jobs)
+{
+    const cvp9_job_t &job = jobs[blockIdx.y];
+    uint8_t *dst = job.dl;
+    if (!dst) return;
+    const uint8_t *src = job.out;
+    const size_t n = (size_t)job.W * job.H + 2 * (size_t)job.CW * job.CH;
+    const size_t n16 = n >> 4;
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+    for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < n16; i += (size_t)gridDim.x * 256)
+        __stcs(d4 + i, __ldcs(s4 + i));
+    if (blockIdx.x == 0)
+        for (size_t i = (n16 << 4) + threadIdx.x; i < n; i += 256) dst[i] = src[i];
+}
+
+int cvp9k_launch_collect(const cvp9_job_t *jobs, int njobs, size_t max_bytes, cudaStream_t st)
+{
+    if (njobs <= 0 || !max_bytes) return 0;
+    /* about four CTAs per SM in all, at least one per 256 KB of a frame */
+    size_t gx = (max_bytes + (256u << 10) - 1) >> 18;
+    const size_t want = (size_t)(4 * 148 + njobs - 1) / (size_t)njobs;
+    if (gx > want) gx = want;
+    if (gx < 1) gx = 1;
+    k_collect<<<dim3((unsigned)gx, (unsigned)njobs), 256, 0, st>>>(jobs);
+    return (int)cudaGetLastError();
+}
+
 int cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, uint32_t *bytes, cudaStream_t st)
 {
     if (njobs <= 0 || max_blocks <= 0) return 0;
@@ -4368,6 +4398,35 @@ int cvp9k_configure(void)
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_REFCPU, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_SPEC, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_SPEC, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    /* Load every kernel the launcher can pick now. With lazy module loading
+     * (the CUDA 12 default) a kernel's code is loaded at its first launch,
+     * which stalls the device for tens of milliseconds; the tuner's first
+     * trial of an inter path would otherwise take that stall inside a
+     * serving step. */
+    const void *fns[] = {
+        (const void *)k_scan_blocks, (const void *)k_lf_mimap, (const void *)k_compact,
+        (const void *)k_recon<CVP9_ARITH_REFCPU>, (const void *)k_recon<CVP9_ARITH_SPEC>,
+        (const void *)k_inter<CVP9_ARITH_REFCPU, 5>, (const void *)k_inter<CVP9_ARITH_REFCPU, 6>,
+        (const void *)k_inter<CVP9_ARITH_SPEC, 5>, (const void *)k_inter<CVP9_ARITH_SPEC, 6>,
+        (const void *)k_pred<CVP9_ARITH_SPEC, kPredMinB>, (const void *)k_pred<CVP9_ARITH_REFCPU, kPredMinB>,
+        (const void *)k_pred<CVP9_ARITH_REFCPU, kPredMinB, true>,
+        (const void *)k_resid<CVP9_ARITH_SPEC, kResidMinB, false>,
+        (const void *)k_resid<CVP9_ARITH_REFCPU, kResidMinB, true>,
+        (const void *)k_resid<CVP9_ARITH_REFCPU, kResidMinB, false>,
+        (const void *)k_resid<CVP9_ARITH_REFCPU, kResid8MinB, true, 1>,
+        (const void *)k_resid<CVP9_ARITH_REFCPU, kResidMinB, true, 2>,
+        (const void *)k_lf_full, (const void *)k_nv12_pack,
+        (const void *)k_loopfilter<CVP9_ARITH_SPEC, 32>, (const void *)k_loopfilter<CVP9_ARITH_REFCPU, 32>,
+        (const void *)k_loopfilter<CVP9_ARITH_SPEC, 64>, (const void *)k_loopfilter<CVP9_ARITH_REFCPU, 64>,
+        (const void *)k_lf_strip<CVP9_ARITH_SPEC>, (const void *)k_lf_strip<CVP9_ARITH_REFCPU>,
+        (const void *)k_lf_flat_h, (const void *)k_lf_flat_v,
+        (const void *)k_gather_luma, (const void *)k_scatter_coeffs, (const void *)k_unpack_coeffs,
+        (const void *)k_collect,
+    };
+    for (size_t i = 0; i < sizeof(fns) / sizeof(fns[0]); i++) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, fns[i]) != cudaSuccess) return -1;
+    }
     return 0;
 }
 

@@ -73,6 +73,10 @@ typedef struct {
     uint8_t  interp_filter;         /* 0 regular, 1 smooth, 2 sharp, 3 bilinear      */
     uint8_t  lossless;              /* 4x4 Walsh-Hadamard residual                  */
     uint8_t  log2_tile_cols;        /* intra left edges end at tile columns         */
+    /* batch engine download */
+    uint8_t *dl;                    /* the step's contiguous output staging
+                                     * (device): k_collect copies `out` here;
+                                     * NULL: no download                           */
 } cvp9_job_t;
 
 #ifdef __cplusplus

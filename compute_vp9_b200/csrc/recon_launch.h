@@ -73,6 +73,11 @@ int    cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, c
 int    cvp9k_launch_unpack(const cvp9_job_t *jobs, int njobs, uint32_t max_pages, uint32_t *err,
                            cudaStream_t stream);
 
+/* Output collection of a batch step: every job with `dl` set gets its
+ * I420 frame (`out`, W*H + 2*CW*CH bytes) copied to `dl`, so that the step's
+ * frames leave the device in one copy. max_bytes: the largest frame. */
+int    cvp9k_launch_collect(const cvp9_job_t *jobs, int njobs, size_t max_bytes, cudaStream_t stream);
+
 /* Enqueue the chain on `stream`; returns the cudaError_t of the first
  * failing call (0 on success). */
 int    cvp9k_launch_frame(const cvp9k_launch_t *launch, cudaStream_t stream);

@@ -122,8 +122,10 @@ INFLIGHT = 3      # step slots of the engine (csrc/batch.c BSLOTS)
 
 def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9,
         arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None,
-        trace=None, hold_ms=4.0):
+        trace=None, hold_ms=4.0, reserve_streams=32):
     """Serve a Poisson arrival of `streams` streams; returns a summary dict.
+    reserve_streams: device and pinned memory for that many concurrent
+    streams (in the size mix) is taken before the clock starts.
     verify_hook(stream_req, frame_index, planes) receives every delivered
     frame (used by the tests to check bit-exactness in the mix). If `trace` is
     a list, one tuple (stream, width, height, frame_index, due_s, submit_s,
@@ -133,8 +135,19 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
     weights = weights or WEIGHTS
     pool = pool or FramePool(sizes)
     # the set of streams changes from step to step, so kernels are launched
-    # directly rather than replayed from per-shape graphs
-    eng = Batch(arith=arith, hbm_budget=int(hbm_budget), use_graphs=0)
+    # directly rather than replayed from per-shape graphs. No host-side
+    # coefficient packing: it runs on the submitting thread and its first
+    # use pins a buffer of the step's size (tens of ms inside one step); a
+    # serving step is small enough that its coefficients cross PCIe in
+    # about a millisecond as they are
+    eng = Batch(arith=arith, hbm_budget=int(hbm_budget), use_graphs=0, pack=-1)
+    # memory for the expected peak of concurrent streams, taken before the
+    # clock starts: a burst of arrivals must not wait for the driver to pin
+    # host memory or grow device memory
+    if reserve_streams:
+        tot = float(sum(weights))
+        for (w, h), wt in zip(sizes, weights):
+            eng.reserve(w, h, max(1, int(math.ceil(reserve_streams * wt / tot))))
     # schedule in scaled time
     t = 0.0
     pending = []
@@ -255,7 +268,7 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
     }
 
 
-def capacity_sweep(arith=0, speeds=(8, 12, 16, 24, 32, 40, 48, 64), p99_budget_ms=33.0, hold_ms=4.0,
+def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 24, 32, 48, 64), p99_budget_ms=33.0, hold_ms=4.0,
                    seed=1, pool=None):
     """Highest pacing compression of the serving mix whose p99 frame latency
     stays within the budget: each speed runs the whole 256-stream schedule

@@ -19,10 +19,12 @@
  *    returns.
  *  - CVP9_BATCH_DEVICE_INPUTS: pf->blocks and pf->coeffs are device pointers
  *    on the engine's GPU, read by the step's kernels.
- *  - outputs: cvp9_batch_get_frame returns pinned host planes of the
- *    stream's most recent completed frame, valid until that stream's second
- *    next step completes. With CVP9_BATCH_NO_OUTPUT the frame stays on the
- *    device only (it still becomes the stream's reference).
+ *  - outputs: a step's frames leave the device in one copy, into one of
+ *    five page-locked output areas used in turn. cvp9_batch_get_frame returns
+ *    planes of the stream's most recent frame, valid until the fifth step
+ *    after the one that produced it is submitted; after that the call
+ *    answers CVP9_ERR_INVALID_DATA. With CVP9_BATCH_NO_OUTPUT the frame stays
+ *    on the device only (it still becomes the stream's reference).
  */
 #ifndef CVP9_BATCH_H
 #define CVP9_BATCH_H
@@ -91,6 +93,9 @@ typedef struct {
     uint32_t packed_frames;  /* frames of that step uploaded packed              */
     float    submit_pack_ms; /* host time the last submit spent packing          */
     float    submit_wait_ms; /* and waiting for a free step slot                 */
+    float    submit_stage_ms;/* and copying inputs into the staging buffer       */
+    uint64_t dev_held_bytes; /* device memory the engine holds from the driver   */
+    uint64_t host_held_bytes;/* page-locked host memory it holds                 */
 } cvp9_batch_stats_t;
 
 cvp9_err_t  cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out);
@@ -102,6 +107,16 @@ uint64_t    cvp9_batch_stream_bytes(uint32_t width, uint32_t height);
 /* Admit a stream: returns its id (>= 0), or CVP9_ERR_NOMEM when the HBM
  * budget or the stream limit would be exceeded (retry after a close). */
 int         cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t width, uint32_t height);
+
+/* Take device and page-locked memory from the driver now for `nstreams`
+ * streams of width x height (their frames, output ring and step buffers),
+ * so that opening and decoding that many streams later allocates nothing
+ * from the driver: pinning host memory costs about 0.4 ms per MB and
+ * device allocations can wait for the device, both on a serving loop's
+ * critical path. The step output areas and staging buffers are sized for a
+ * step holding every reserved stream at once (steps in flight are waited
+ * for first). Admission (the HBM budget) is unchanged. Calls add up. */
+cvp9_err_t  cvp9_batch_reserve(cvp9_batch_t *b, uint32_t width, uint32_t height, int nstreams);
 cvp9_err_t  cvp9_batch_close_stream(cvp9_batch_t *b, int sid);
 
 /* Enqueue one step: frame pfs[i] for stream sids[i] (each stream at most
@@ -174,9 +189,9 @@ cvp9_err_t  cvp9_batch_get_frame(cvp9_batch_t *b, int sid, cvp9_frame_info_t *in
 /* The frame stream `sid` got from step `seq` (a value of
  * cvp9_batch_last_seq after the submit that held it): AGAIN while that step
  * runs, INVALID_DATA if the stream was not in it, the step produced no
- * output for it, or its buffer has since been reused (after the stream's
- * second next step completed). A stream may sit in several steps in flight
- * at once; this reads each of their frames in turn. */
+ * output for it, or its output area has since been given to a newer step
+ * (five steps later). A stream may sit in several steps in flight at once;
+ * this reads each of their frames in turn. */
 cvp9_err_t  cvp9_batch_get_frame_at(cvp9_batch_t *b, int sid, uint64_t seq, cvp9_frame_info_t *info);
 
 cvp9_err_t  cvp9_batch_stats(cvp9_batch_t *b, cvp9_batch_stats_t *st);

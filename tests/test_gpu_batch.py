@@ -284,8 +284,9 @@ def test_stream_in_several_steps_in_flight(profile):
     """One stream submitted in consecutive steps without waiting (three in
     flight, next to a second stream that skips every other step): each
     frame is read back by its step (cvp9_batch_get_frame_at) and equals the
-    oracle's; a step without the stream reports INVALID_DATA, and a frame
-    stays readable until the stream's second next step has completed."""
+    oracle's; a step without the stream reports INVALID_DATA, the two newest
+    frames stay readable, and a frame whose output area went to a step five
+    later reports INVALID_DATA."""
     from compute_vp9_b200 import CVP9_ERR_AGAIN, CVP9_ERR_INVALID_DATA
     streams = mix_for(profile, [(2, 352, 288, {"gop": 4}), (1, 320, 192, {})])
     syns = [Synth(synth_config(p, w, h, seed=40 + i, **ov)) for i, (p, w, h, ov) in enumerate(streams)]
@@ -319,9 +320,40 @@ def test_stream_in_several_steps_in_flight(profile):
             rc, arr = eng.get_frame_array_at(sids[i], q)
             assert rc == CVP9_OK
             assert np.array_equal(arr, orcs[i].decode(syns[i].frame(f)))
-    # stream 0 was in every step: the frame of step seqs[-3] is its third
-    # newest, whose second next step has completed, so its buffer may be
-    # reused; the two newest stay readable
+    # the two newest frames stay readable; the first step's output area has
+    # been given to step 6, so its frames are gone
     assert eng.get_frame_at(sids[0], seqs[-1][0])[0] == CVP9_OK
     assert eng.get_frame_at(sids[0], seqs[-2][0])[0] == CVP9_OK
+    assert eng.get_frame_at(sids[0], seqs[0][0])[0] == CVP9_ERR_INVALID_DATA
+    eng.close()
+
+
+def test_reserve_takes_memory_up_front():
+    """After cvp9_batch_reserve for six streams, opening four of them and
+    running steps that hold each stream in several steps in flight takes
+    nothing more from the driver (device or page-locked memory), and the
+    frames still equal the oracle's."""
+    eng = Batch(arith=REFCPU)
+    eng.reserve(320, 192, 6)
+    st0 = eng.stats()
+    held = (st0.dev_held_bytes, st0.host_held_bytes)
+    assert held[0] > 0 and held[1] > 0
+    syns = [Synth(synth_config(1, 320, 192, seed=70 + i)) for i in range(4)]
+    orcs = [OracleStream(REFCPU) for _ in range(4)]
+    sids = [eng.open_stream(320, 192) for _ in range(4)]
+    seqs = []
+    for f in range(8):
+        eng.submit(sids, [s.frame(f) for s in syns], [f] * 4)
+        seqs.append(eng.last_seq())
+    assert eng.wait() == CVP9_OK, eng.last_error()
+    st = eng.stats()
+    assert (st.dev_held_bytes, st.host_held_bytes) == held
+    for f in range(8):
+        for i in range(4):
+            want = orcs[i].decode(syns[i].frame(f))
+            if f >= 6:          # the two newest frames of each stream stay readable
+                rc, arr = eng.get_frame_array_at(sids[i], seqs[f])
+                assert rc == CVP9_OK and np.array_equal(arr, want)
+    for sid in sids:
+        eng.close_stream(sid)
     eng.close()
