@@ -30,8 +30,10 @@
 
 #define BSLOTS 3
 #define MAXF 12
-/* steps of at least this many frames send their inputs as one staged copy */
-#define COALESCE_MIN_FRAMES 8
+/* steps of at least this many frames send their inputs as one staged copy
+ * (smaller steps have few copies, and a serving step's submit latency
+ * counts: staging took a 9-frame step's submit from 0.3 to 1.1 ms) */
+#define COALESCE_MIN_FRAMES 32
 /* Host output buffers per stream: up to two other steps in flight holding
  * the stream, the two newest completed frames, and the new one. */
 #define OUTR (BSLOTS + 2)
@@ -824,7 +826,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     /* how each host array travels: the gather kernel (REFCPU coefficients in
      * page-locked memory), direct DMA (page-locked), or the pinned staging
      * buffer (pageable); coefficient regions the device fills get no copy.
-     * A step of many frames that packed nothing also stages its page-locked
+     * A step of many frames (COALESCE_MIN_FRAMES) that packed nothing also stages its page-locked
      * block records and list arrays, so that its upload is one large copy:
      * the PCIe link runs both directions at once best for large copies (two
      * of ~100 MB each way move in 3.8 ms together, as 0.8 MB and 3.1 MB
@@ -833,6 +835,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
      * memory bandwidth that the staging copy would take (packed 64x1080p:
      * 6.7 ms unstaged, 8.1 ms staged). $CVP9_COALESCE=0|1 forces either. */
     int any_staged = 0;
+    size_t stage_bytes = 0;
     const int coalesce = !dev_in && n >= COALESCE_MIN_FRAMES &&
                          (b->coalesce > 0 || (b->coalesce < 0 && !any_packed));
     for (int i = 0; i < n && !dev_in; i++) {
@@ -848,9 +851,17 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         if (lists && lists[i].n && (coalesce || !is_pinned(lists[i].val))) f->staged |= 1u << IN_VAL;
         if (packed && coalesce) f->staged |= 1u << IN_PACKED;
         any_staged |= f->staged != 0;
+        /* the staging buffer holds the staged arrays only (the regions the
+         * device fills, and the directly copied arrays, live on the device) */
+        const size_t len[IN_N] = { (size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t),
+                                   (size_t)pf->num_coeffs * sizeof(int16_t),
+                                   lists ? (size_t)lists[i].n * 4 : 0, lists ? (size_t)lists[i].n * 2 : 0,
+                                   packed ? (size_t)s->pk_words[i] * 4 : 0 };
+        for (int k = 0; k < IN_N; k++)
+            if ((f->staged >> k) & 1) stage_bytes += ALIGN_UP(len[k], 256);
     }
     if (!dev_in && in_bytes) {
-        if ((any_staged && (err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, in_bytes))) ||
+        if ((any_staged && (err = grow_host(b, (void **)&s->h_in, &s->h_in_cap, stage_bytes))) ||
             (err = grow_dev(b, (void **)&s->d_in, &s->d_in_cap, in_bytes)))
             return err;
     }

@@ -122,7 +122,7 @@ INFLIGHT = 3      # step slots of the engine (csrc/batch.c BSLOTS)
 
 def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9,
         arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None,
-        trace=None, hold_ms=4.0, reserve_streams=32):
+        trace=None, hold_ms=1.0, reserve_streams=32):
     """Serve a Poisson arrival of `streams` streams; returns a summary dict.
     reserve_streams: device and pinned memory for that many concurrent
     streams (in the size mix) is taken before the clock starts.
@@ -268,7 +268,7 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
     }
 
 
-def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 24, 32, 48, 64), p99_budget_ms=33.0, hold_ms=4.0,
+def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 24, 32, 48, 64), p99_budget_ms=33.0, hold_ms=1.0,
                    seed=1, pool=None):
     """Highest pacing compression of the serving mix whose p99 frame latency
     stays within the budget: each speed runs the whole 256-stream schedule
@@ -304,7 +304,7 @@ def main():
     ap.add_argument("--speed", type=float, default=1.0, help="pacing compression (1 = real time)")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec", "full"])
-    ap.add_argument("--hold-ms", type=float, default=4.0,
+    ap.add_argument("--hold-ms", type=float, default=1.0,
                     help="while a step is in flight, hold due frames this long to batch them")
     ap.add_argument("--sweep", action="store_true", help="capacity sweep over pacing speeds")
     a = ap.parse_args()
