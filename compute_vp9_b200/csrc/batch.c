@@ -715,7 +715,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     int max_sbr = 0;
     int max_blocks = 0, max_mi = 0, lf_tx = 0, lf_ty = 0, lf_sx = 0, lf_sy = 0;
     int flat_w = 0, flat_h = 0, flat_nv = 0;
-    int maxd = 0;
+    int maxd = 0, wave = 0;      /* wave: superblocks on the step's widest diagonals */
     uint64_t key = mix64(0, (uint64_t)n);
     for (int i = 0; i < n; i++) {
         const vp9_parsed_frame_t *pf = pfs[i];
@@ -747,6 +747,10 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         }
         int d = (st->W + 63) / 64 + (st->H + 63) / 64 - 1;
         if (d > maxd) maxd = d;
+        {
+            const int sc = (st->W + 63) / 64, sr = (st->H + 63) / 64;
+            wave += sc < sr ? sc : sr;
+        }
         if ((st->H + 63) / 64 > max_sbr) max_sbr = (st->H + 63) / 64;
         key = mix64(key, ((uint64_t)st->W << 32) | (uint64_t)st->H);
     }
@@ -1083,7 +1087,13 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
     L.n_tickets = s->n_tickets;
     L.ticket_counter = s->d_misc;
     {
-        const int width = tc.half ? (b->resident_ctas + 1) / 2 : b->resident_ctas;
+        int width = tc.half ? (b->resident_ctas + 1) / 2 : b->resident_ctas;
+        /* at most twice the wavefront's width: a CTA beyond that only holds
+         * a ticket whose neighbours are not done and spins on them, keeping
+         * SM slots from work that could run beside this step (a 2160p key
+         * frame is 34 superblocks wide; 64 1080p frames are 1088) */
+        const int cap = 2 * wave > 32 ? 2 * wave : 32;
+        if (width > cap) width = cap;
         L.recon_ctas = (int)s->n_tickets < width ? (int)s->n_tickets : width;
     }
     L.lf_tile_h = tc.lf32 ? 32 : 64;

@@ -1657,6 +1657,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                     if (atomicCAS(&s.cell[cy * 16 + cx], (uint16_t)0, (uint16_t)(tid + 1)) != 0) overlap = true;
         }
         const int any_intra = __syncthreads_or(my_intra);
+        const int any_inter = __syncthreads_or(tid < nb && !my_intra);
         const int any_overlap = __syncthreads_or(overlap);
 
         /* stage the SB's coefficient span in shared memory with 16-byte loads
@@ -1847,6 +1848,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
         const bool warp_lv = warp_levels && any_intra;
         if ((A == CVP9_ARITH_SPEC && job.full) || warp_lv) cp_async_wait_all();
         __syncthreads();
+        /* REFCPU, every block intra and no two blocks overlapping: the first
+         * transform pass reads coefficients only, so every TX's runs here at
+         * once, on all threads, into its own place of the SB-wide temp (no
+         * inter prediction stages reference windows there); the levels then
+         * predict and run the second pass only */
+        const bool pre1 = A == CVP9_ARITH_REFCPU && warp_lv && !any_inter && !seq;
+        if (pre1) {
+            const int n_items = min((int)s.base_item[nlev], kMaxItems);   /* <= 1024: disjoint luma TXs */
+            for (int it = tid; it < n_items; it += kThreads) {
+                const int lo = s.item_blk[it];
+                item_pass1<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], staged, c_base);
+            }
+            __syncthreads();
+        }
 
         /* 5. levels */
         for (int L = 0; L < nlev && nb > 0; L++) {
@@ -1867,8 +1882,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                     }
                     __syncwarp();
                     const int n_it = s.item_off[pos + 1] - s.item_off[pos];
-                    for (int k = lane; k < n_it; k += 32) item_pass1<A>(s, b, k, staged, c_base);
-                    __syncwarp();
+                    if (!pre1) {
+                        for (int k = lane; k < n_it; k += 32) item_pass1<A>(s, b, k, staged, c_base);
+                        __syncwarp();
+                    }
                     for (int k = lane; k < n_it; k += 32) item_pass2<A>(s, b, k);
                     __syncwarp();
                 }
@@ -1943,11 +1960,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
             cp_async_wait_all();     /* the SB's coefficient span */
             __syncthreads();
             /* phase P': first transform pass, thread per TX column */
-            for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
-                const int lo = s.item_blk[it];
-                item_pass1<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], staged, c_base);
+            if (!pre1) {
+                for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
+                    const int lo = s.item_blk[it];
+                    item_pass1<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], staged, c_base);
+                }
+                __syncthreads();
             }
-            __syncthreads();
             /* phase Q: second pass + residual add, thread per TX row */
             for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
                 const int lo = s.item_blk[it];

@@ -3,22 +3,24 @@
     python -m compute_vp9_b200.serve [--streams 256] [--rate 2] [--speed 1]
 
 Streams arrive as a Poisson process; each carries `frames` frames paced at
-`fps`. A stream is admitted when the engine's HBM budget has room
-(cvp9_batch_open_stream); otherwise it waits in the admission queue and is
-admitted as soon as a finished stream frees its reservation. Every loop
-iteration gathers the frames that are due from all admitted streams — new
-arrivals join the very next step — and reconstructs them in one engine step;
-up to three steps are in flight (the engine's step slots), so frames that
-become due while the GPU works go into the next step, also when the same
-stream's previous frame is still in one of the steps in flight (the engine
-keeps an output buffer per step in flight and delivers each frame by its
-step, cvp9_batch_get_frame_at). While a step is in
+`fps`. A stream is admitted while the HBM budget has room (the engines'
+per-stream reservation, cvp9_batch_stream_bytes); otherwise it waits in the
+admission queue and is admitted as soon as a finished stream frees its
+reservation. Streams are spread over `engines` batch engines side by side on
+the GPU (each with its own copy and compute streams), the least loaded
+first, and stay on theirs. Every loop iteration gathers the frames that are
+due from each engine's admitted streams — new arrivals join the very next
+step — and reconstructs them in one step of that engine; up to three steps
+per engine are in flight, so frames that become due while the GPU works go
+into the next step, also when the same stream's previous frame is still in
+one of the steps in flight (the engine keeps each step's frames and delivers
+them by step, cvp9_batch_get_frame_at). While an engine has a step in
 flight, due frames are held back until the oldest of them has waited
 `hold_ms` (or a full batch is ready), so that steps carry many streams; an
-idle GPU takes due frames at once. Latency of a frame = time its
-reconstructed planes reach host memory minus the time it became due. `speed` compresses the
-arrival and pacing schedule (20 = twenty times faster than real time) so a
-run fits in seconds; the GPU work per frame is unchanged.
+idle engine takes due frames at once. Latency of a frame = time its
+reconstructed planes reach host memory minus the time it became due. `speed`
+compresses the arrival and pacing schedule (20 = twenty times faster than
+real time) so a run fits in seconds; the GPU work per frame is unchanged.
 
 Resolution mix, GOP and content follow the serving workload: 640x360,
 1280x720, 1920x1080 and 3840x2160 streams in ratio 4:3:2:1, 8-bit 4:2:0,
@@ -108,6 +110,7 @@ class Stream:
         self.frames = frames
         self.fps = fps
         self.sid = None
+        self.lane = None          # the engine that admitted it
         self.admit_time = None
         self.next_frame = 0
         self.done_frames = 0
@@ -122,14 +125,19 @@ INFLIGHT = 3      # step slots of the engine (csrc/batch.c BSLOTS)
 
 def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9,
         arith=0, seed=1, max_batch=256, pool=None, verify_hook=None, sizes=None, weights=None,
-        trace=None, hold_ms=1.0, reserve_streams=32):
+        trace=None, hold_ms=1.0, reserve_streams=32, engines=2):
     """Serve a Poisson arrival of `streams` streams; returns a summary dict.
+    engines: batch engines side by side on the GPU (each with its own copy
+    and compute streams and three steps in flight); a stream stays on the
+    engine that admitted it, so one engine's long step (a 2160p key frame is
+    a ~6 ms wavefront that fills few SMs) does not hold up the others.
     reserve_streams: device and pinned memory for that many concurrent
-    streams (in the size mix) is taken before the clock starts.
-    verify_hook(stream_req, frame_index, planes) receives every delivered
-    frame (used by the tests to check bit-exactness in the mix). If `trace` is
-    a list, one tuple (stream, width, height, frame_index, due_s, submit_s,
-    done_s, step_seq, step_frames) per delivered frame is appended to it."""
+    streams (in the size mix, split over the engines) is taken before the
+    clock starts. verify_hook(stream_req, frame_index, planes) receives every
+    delivered frame (used by the tests to check bit-exactness in the mix). If
+    `trace` is a list, one tuple (stream, width, height, frame_index, due_s,
+    submit_s, done_s, step_seq, step_frames, engine) per delivered frame is
+    appended to it."""
     rng = random.Random(seed)
     sizes = sizes or SIZES
     weights = weights or WEIGHTS
@@ -139,15 +147,18 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
     # coefficient packing: it runs on the submitting thread and its first
     # use pins a buffer of the step's size (tens of ms inside one step); a
     # serving step is small enough that its coefficients cross PCIe in
-    # about a millisecond as they are
-    eng = Batch(arith=arith, hbm_budget=int(hbm_budget), use_graphs=0, pack=-1)
+    # about a millisecond as they are. Admission is against one HBM budget
+    # for all engines, kept here.
+    engs = [Batch(arith=arith, hbm_budget=int(hbm_budget), use_graphs=0, pack=-1) for _ in range(engines)]
     # memory for the expected peak of concurrent streams, taken before the
     # clock starts: a burst of arrivals must not wait for the driver to pin
     # host memory or grow device memory
     if reserve_streams:
         tot = float(sum(weights))
-        for (w, h), wt in zip(sizes, weights):
-            eng.reserve(w, h, max(1, int(math.ceil(reserve_streams * wt / tot))))
+        for eng in engs:
+            for (w, h), wt in zip(sizes, weights):
+                eng.reserve(w, h, max(1, int(math.ceil(reserve_streams * wt / tot / engines))))
+    need = {sz: engs[0].stream_bytes(*sz) for sz in sizes}
     # schedule in scaled time
     t = 0.0
     pending = []
@@ -157,7 +168,9 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
         pending.append(Stream(i, size, t, frames, fps * speed))
     waiting = []          # arrived, not admitted (HBM budget)
     active = []
-    inflight = []         # (seq, [(stream, frame_index, due_time)])
+    inflight = [[] for _ in engs]   # per engine: (seq, [(stream, frame_index, due_time)], submit_s)
+    load = [0] * engines            # pixels of each engine's active streams
+    reserved = 0
     lat = []
     px = 0
     steps = 0
@@ -168,26 +181,22 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
     def now():
         return time.perf_counter() - t0
 
-    def reap(block):
-        """Deliver finished steps in order; a step is finished once the
-        engine's completion callback stamped it (host time at which its
-        frames landed in host memory)."""
-        nonlocal px
-        while inflight:
-            seq, items, t_sub = inflight[0]
+    def reap(k):
+        """Deliver engine k's finished steps in order (a step is finished once
+        the engine's completion callback stamped it: host time at which its
+        frames landed in host memory); returns how many."""
+        nonlocal px, reserved
+        eng, got = engs[k], 0
+        while inflight[k]:
+            seq, items, t_sub = inflight[k][0]
             ms = eng.step_latency_ms(seq)
             if ms is None:
-                if not block:
-                    return
-                if eng.poll() < 0:
-                    raise RuntimeError("step failed: %s" % eng.last_error())
-                time.sleep(0.0001)
-                continue
+                break
             tdone = t_sub + ms / 1000.0
             for st, fi, due in items:
                 lat.append(1000.0 * (tdone - due))
                 if trace is not None:
-                    trace.append((st.req, st.size[0], st.size[1], fi, due, t_sub, tdone, seq, len(items)))
+                    trace.append((st.req, st.size[0], st.size[1], fi, due, t_sub, tdone, seq, len(items), k))
                 px += st.size[0] * st.size[1]
                 st.done_frames += 1
                 if verify_hook is not None:
@@ -196,42 +205,54 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
                 if st.done_frames == st.frames:
                     eng.close_stream(st.sid)
                     st.sid = None
-            inflight.pop(0)
+                    load[k] -= st.size[0] * st.size[1]
+                    reserved -= need[st.size]
+            inflight[k].pop(0)
+            got += 1
+        if got:
             active[:] = [s for s in active if s.done_frames < s.frames]
-            block = False
+        return got
 
-    while pending or waiting or active or inflight:
+    while pending or waiting or active or any(inflight):
         tn = now()
         while pending and pending[0].arrival <= tn:
             waiting.append(pending.pop(0))
-        # admission by HBM budget, first come first served
+        # admission by HBM budget, first come first served, onto the engine
+        # with the fewest active pixels
         still = []
         for st in waiting:
-            sid = eng.open_stream(*st.size)
+            sid = None
+            if reserved + need[st.size] <= hbm_budget:
+                for k in sorted(range(engines), key=lambda e: load[e]):
+                    sid = engs[k].open_stream(*st.size)
+                    if sid is not None:
+                        break
             if sid is None:
                 still.append(st)
                 rejected += 1
                 continue
-            st.sid = sid
+            st.sid, st.lane = sid, k
             st.admit_time = max(st.arrival, tn)
+            load[k] += st.size[0] * st.size[1]
+            reserved += need[st.size]
             active.append(st)
         waiting = still
-        # gather due frames (one per stream per step; a stream whose previous
-        # frame is still in flight joins the next step all the same, since
-        # steps run in submission order on the device)
-        ready = [st for st in active if st.next_frame < st.frames and st.due(st.next_frame) <= tn]
-        if ready and inflight and len(ready) < max_batch and hold_ms > 0:
-            # the GPU is busy: let the step fill up until the oldest due frame
-            # has waited hold_ms
-            oldest = min(st.due(st.next_frame) for st in ready)
-            if tn - oldest < hold_ms / 1000.0:
-                if len(inflight) < INFLIGHT:
-                    ms = eng.step_latency_ms(inflight[0][0])
-                    if ms is None:
-                        time.sleep(min(0.0002, max(0.0, oldest + hold_ms / 1000.0 - tn)))
-                        continue
-                ready = []
-        if ready and len(inflight) < INFLIGHT:
+        # gather due frames per engine (one per stream per step; a stream
+        # whose previous frame is still in flight joins the next step all the
+        # same, since an engine runs its steps in submission order)
+        submitted = False
+        for k, eng in enumerate(engs):
+            if len(inflight[k]) >= INFLIGHT:
+                continue
+            ready = [st for st in active if st.lane == k and st.next_frame < st.frames and
+                     st.due(st.next_frame) <= tn]
+            if not ready:
+                continue
+            if inflight[k] and len(ready) < max_batch and hold_ms > 0:
+                # the engine is busy: let the step fill up until the oldest
+                # due frame has waited hold_ms
+                if tn - min(st.due(st.next_frame) for st in ready) < hold_ms / 1000.0:
+                    continue
             ready = ready[:max_batch]
             items = [(st, st.next_frame, st.due(st.next_frame)) for st in ready]
             t_sub = now()
@@ -239,12 +260,19 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
                        [st.next_frame for st in ready])
             for st in ready:
                 st.next_frame += 1
-            inflight.append((eng.last_seq(), items, t_sub))
+            inflight[k].append((eng.last_seq(), items, t_sub))
             steps += 1
             batch_sizes.append(len(ready))
+            submitted = True
+        if submitted:
             continue
-        if inflight:
-            reap(block=len(inflight) >= INFLIGHT or not ready and not pending and not waiting)
+        if sum(reap(k) for k in range(engines)):
+            continue
+        if any(inflight):
+            for eng in engs:
+                if eng.poll() < 0:
+                    raise RuntimeError("step failed: %s" % eng.last_error())
+            time.sleep(0.0001)
             continue
         # idle until the next due frame or arrival
         nxt = [st.due(st.next_frame) for st in active if st.next_frame < st.frames]
@@ -253,11 +281,12 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
         if nxt:
             time.sleep(max(0.0, min(nxt) - now()))
     wall = now()
-    eng.close()
+    for eng in engs:
+        eng.close()
     lat.sort()
     return {
         "sizes": [list(x) for x in sizes], "weights": list(weights),
-        "streams": streams, "frames_per_stream": frames, "speed": speed,
+        "streams": streams, "frames_per_stream": frames, "speed": speed, "engines": engines,
         "frames": len(lat), "steps": steps,
         "mean_batch": statistics.mean(batch_sizes) if batch_sizes else 0,
         "max_batch": max(batch_sizes) if batch_sizes else 0,
@@ -268,8 +297,8 @@ def run(streams=256, rate=2.0, frames=120, fps=30.0, speed=1.0, hbm_budget=150e9
     }
 
 
-def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 24, 32, 48, 64), p99_budget_ms=33.0, hold_ms=1.0,
-                   seed=1, pool=None):
+def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 20, 24, 32, 48), p99_budget_ms=33.0, hold_ms=1.0,
+                   seed=1, pool=None, engines=2):
     """Highest pacing compression of the serving mix whose p99 frame latency
     stays within the budget: each speed runs the whole 256-stream schedule
     compressed that many times; returns every run and the best."""
@@ -278,7 +307,7 @@ def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 24, 32, 48, 64), p99_budget_ms
     best = None
     over = 0
     for sp in speeds:
-        r = run(speed=sp, arith=arith, seed=seed, pool=pool, hold_ms=hold_ms)
+        r = run(speed=sp, arith=arith, seed=seed, pool=pool, hold_ms=hold_ms, engines=engines)
         runs.append({"speed": sp, "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "value": r["mpx_per_s"],
                      "mean_batch": r["mean_batch"], "steps": r["steps"]})
         if r["p99_ms"] is not None and r["p99_ms"] <= p99_budget_ms:
@@ -288,7 +317,7 @@ def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 24, 32, 48, 64), p99_budget_ms
             over += 1
             if over >= 2:
                 break
-    return {"p99_budget_ms": p99_budget_ms, "hold_ms": hold_ms, "runs": runs,
+    return {"p99_budget_ms": p99_budget_ms, "hold_ms": hold_ms, "engines": engines, "runs": runs,
             "capacity": best, "unit": "Mpixel/s",
             "what": "serving mix (256 streams, Poisson 2/s, 360p/720p/1080p/2160p 4:3:2:1, 120 frames, "
                     "GOP 60) with arrivals and 30 fps pacing compressed by `speed`; capacity = the highest "
@@ -307,12 +336,14 @@ def main():
     ap.add_argument("--hold-ms", type=float, default=1.0,
                     help="while a step is in flight, hold due frames this long to batch them")
     ap.add_argument("--sweep", action="store_true", help="capacity sweep over pacing speeds")
+    ap.add_argument("--engines", type=int, default=2, help="batch engines side by side on the GPU")
     a = ap.parse_args()
     arith = {"refcpu": 0, "spec": 1, "full": 2}[a.arith]
     if a.sweep:
-        out = capacity_sweep(arith=arith, hold_ms=a.hold_ms)
+        out = capacity_sweep(arith=arith, hold_ms=a.hold_ms, engines=a.engines)
     else:
-        out = run(a.streams, a.rate, a.frames, a.fps, a.speed, a.budget_gb * 1e9, arith, hold_ms=a.hold_ms)
+        out = run(a.streams, a.rate, a.frames, a.fps, a.speed, a.budget_gb * 1e9, arith, hold_ms=a.hold_ms,
+                  engines=a.engines)
     print(json.dumps(out))
 
 
