@@ -1848,12 +1848,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
         const bool warp_lv = warp_levels && any_intra;
         if ((A == CVP9_ARITH_SPEC && job.full) || warp_lv) cp_async_wait_all();
         __syncthreads();
-        /* REFCPU, every block intra and no two blocks overlapping: the first
-         * transform pass reads coefficients only, so every TX's runs here at
-         * once, on all threads, into its own place of the SB-wide temp (no
-         * inter prediction stages reference windows there); the levels then
+        /* Every block intra and no two blocks overlapping (REFCPU, or SPEC
+         * without the FULL completion, whose intra blocks reconstruct TX by
+         * TX in their prediction warp): the first transform pass reads
+         * coefficients only, so every TX's runs here at once, on all
+         * threads, into its own place of the SB-wide temp (no inter
+         * prediction stages reference windows there); the levels then
          * predict and run the second pass only */
-        const bool pre1 = A == CVP9_ARITH_REFCPU && warp_lv && !any_inter && !seq;
+        const bool pre1 = (A == CVP9_ARITH_REFCPU || !job.full) && warp_lv && !any_inter && !seq;
         if (pre1) {
             const int n_items = min((int)s.base_item[nlev], kMaxItems);   /* <= 1024: disjoint luma TXs */
             for (int it = tid; it < n_items; it += kThreads) {
