@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec", "full"])
     ap.add_argument("--no-spec", action="store_true", help="skip the shader-arithmetic leg")
     ap.add_argument("--no-full", action="store_true", help="skip the VP9 (FULL) leg")
-    ap.add_argument("--no-capacity", action="store_true", help="skip the serving capacity sweep")
+    ap.add_argument("--no-capacity", action="store_true", help="skip the serving capacity sweeps")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-single", action="store_true", help="skip the single-stream leg")
     ap.add_argument("--no-graphs", action="store_true")
@@ -818,6 +818,7 @@ def main():
                                   "inputs" % (one.w, one.h, args.gop)}
         serving = None
         capacity = None
+        capacity_streams = None
         if not args.no_serve:
             from compute_vp9_b200 import serve
             sv = serve.run(streams=256, rate=2.0, frames=120, fps=30.0, speed=args.serve_speed,
@@ -831,6 +832,7 @@ def main():
                        "latency": "frame due -> its planes in host memory"}
             if not args.no_capacity:
                 capacity = serve.capacity_sweep(arith=arith)
+                capacity_streams = serve.stream_capacity_sweep(arith=arith)
         cpu = None
         if not args.no_cpu:
             v, kind, cthreads, sample = cpu_leg(wl, cores)
@@ -931,6 +933,7 @@ def main():
             "single_stream": single,
             "serving": serving,
             "serving_capacity": capacity,
+            "serving_capacity_streams": capacity_streams,
             "batched_vs_single": (value / single["value"]) if single else None,
             "batched_vs_single_e2e": (e2e / single["e2e_plain_backend"]) if single else None,
         }

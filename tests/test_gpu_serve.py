@@ -80,3 +80,36 @@ def test_served_stream_pipelines_its_frames(profile):
     done = {(r[0], r[3]): r[6] for r in trace}
     overlapped = sum(1 for r in trace if (r[0], r[3] - 1) in done and r[5] < done[(r[0], r[3] - 1)])
     assert overlapped > 0, "no stream had two frames in flight"
+
+
+def test_live_streams_batched_over_two_engines():
+    """Real-time pacing with many streams live, due frames held also while
+    an engine is idle, two engines: steps carry several streams, and every
+    frame still equals the stream's oracle decode."""
+    profile = REFCPU
+    pool = serve.FramePool(SIZES, distinct=4, gop=6)
+    orcs = {}
+    sizes_of = {}
+    orig = serve.Stream.__init__
+
+    def capture(self, req, size, *a):
+        orig(self, req, size, *a)
+        sizes_of[req] = size
+    serve.Stream.__init__ = capture
+
+    def hook(req, fi, arr):
+        assert arr is not None, "frame not delivered"
+        o = orcs.setdefault(req, OracleStream(profile))
+        want = o.decode(__import__("ctypes").pointer(pool.frame(sizes_of[req], fi)))
+        assert np.array_equal(arr, want), "stream %d frame %d" % (req, fi)
+
+    trace = []
+    try:
+        out = serve.run(streams=12, rate=400.0, frames=8, fps=200.0, speed=1.0, arith=profile, seed=6, pool=pool,
+                        verify_hook=hook, sizes=SIZES, weights=[1, 1, 1], trace=trace, hold_ms=4.0,
+                        hold_idle=True, engines=2, max_batch=6)
+    finally:
+        serve.Stream.__init__ = orig
+    assert out["frames"] == 12 * 8 and out["engines"] == 2
+    assert {r[9] for r in trace} == {0, 1}, "both engines served streams"
+    assert out["max_batch"] > 1 and out["max_batch"] <= 6
