@@ -130,6 +130,7 @@ struct cvp9_batch {
     int          gather;     /* REFCPU: luma-only coefficient upload by kernel */
     int          pack;       /* host coefficient packing: -1 never, 0 large steps, 1 always */
     int          pack_q;     /* large steps: frames packed, in 16ths of the step (0..16) */
+    int          pack_fixed; /* $CVP9_PACK_SHARE=0..16 pins pack_q (-1: the feedback sets it) */
     cvp9_tuner_t tuner;      /* kernel configuration per shape bucket */
     uint64_t     budget, reserved;
     cudaStream_t cs, hs, ds;
@@ -215,6 +216,12 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     }
     b->pack = cvp9_env_pack(cfg ? cfg->pack : 0);
     b->pack_q = 16;
+    {
+        const char *e = getenv("CVP9_PACK_SHARE");
+        b->pack_fixed = (e && *e) ? atoi(e) : -1;
+        if (b->pack_fixed > 16) b->pack_fixed = 16;
+        if (b->pack_fixed >= 0) b->pack_q = b->pack_fixed;
+    }
     {
         cvp9_tcfg_t fixed = { (int8_t)cvp9_env_inter_fast(), 0, 0 };
         cvp9_tuner_init(&b->tuner, b->arith, cfg && cfg->autotune && cvp9_env_autotune(), fixed);
@@ -801,7 +808,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         if (b->pack == 1) {
             npack = n;
         } else if (cb >= PACK_AUTO_BYTES) {
-            b->pack_q = cvp9_pack_share_update(b->pack_q, pipelined, waited_ms);
+            if (b->pack_fixed < 0) b->pack_q = cvp9_pack_share_update(b->pack_q, pipelined, waited_ms);
             npack = (b->pack_q * n + 8) / 16;
         }
         if (npack) {
