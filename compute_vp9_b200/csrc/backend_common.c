@@ -39,6 +39,7 @@ void cvp9_build_dct_basis(double *out)
 static pthread_mutex_t g_setup_lock = PTHREAD_MUTEX_INITIALIZER;
 static int g_setup_done[MAX_DEVICES];
 static int g_ctas[MAX_DEVICES][2];
+static int g_lf_ctas[MAX_DEVICES];
 
 int cvp9_device_setup(int device)
 {
@@ -54,6 +55,7 @@ int cvp9_device_setup(int device)
         } else {
             g_ctas[device][0] = cvp9k_recon_ctas_per_sm(CVP9_ARITH_REFCPU);
             g_ctas[device][1] = cvp9k_recon_ctas_per_sm(CVP9_ARITH_SPEC);
+            g_lf_ctas[device] = cvp9k_lf_full_ctas_per_sm();
             g_setup_done[device] = 1;
         }
     }
@@ -66,6 +68,12 @@ int cvp9_recon_ctas_per_sm(int device, int arith)
     if (device < 0 || device >= MAX_DEVICES) return 1;
     int v = g_ctas[device][arith != CVP9_ARITH_REFCPU ? 1 : 0];    /* FULL runs the SPEC kernel */
     return v > 0 ? v : 1;
+}
+
+int cvp9_lf_full_ctas_per_sm(int device)
+{
+    if (device < 0 || device >= MAX_DEVICES) return 1;
+    return g_lf_ctas[device] > 0 ? g_lf_ctas[device] : 1;
 }
 
 int cvp9_tickets_on_diagonal(int sb_cols, int sb_rows, int job, int d, uint32_t *out)

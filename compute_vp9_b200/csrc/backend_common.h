@@ -20,6 +20,8 @@ int cvp9_device_setup(int device);
 
 /* Resident reconstruction CTAs per SM for the profile (after setup). */
 int cvp9_recon_ctas_per_sm(int device, int arith);
+/* The same for the VP9 loop filter kernel (superblock-row tickets). */
+int  cvp9_lf_full_ctas_per_sm(int device);
 
 /* The basis of the reference's float64 inverse DCT, N = 4, 8, 16, 32
  * concatenated (16 + 64 + 256 + 1024 doubles), built with the expression of

@@ -144,6 +144,7 @@ struct cvp9_batch {
                               * -1 when the step packs nothing ($CVP9_COALESCE) */
     int          collect;    /* download a step's frames in one copy ($CVP9_DL_COLLECT=0: one each) */
     int          resident_ctas;
+    int          lf_full_ctas;   /* k_lf_full CTAs resident on the device */
     cudaEvent_t  ev_t0, ev_t1;
     /* host-clock submit and completion time of recent steps */
     double       lat_submit[LAT_RING];
@@ -232,6 +233,7 @@ cvp9_err_t cvp9_batch_create(const cvp9_batch_config_t *cfg, cvp9_batch_t **out)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     b->resident_ctas = sms * cvp9_recon_ctas_per_sm(b->device, b->arith);
+    b->lf_full_ctas = sms * cvp9_lf_full_ctas_per_sm(b->device);
     {
         /* chunk sizes scale with the budget: 2 GB device / 256 MB pinned at
          * the 150 GB default; the first chunk of each is taken now */
@@ -1122,7 +1124,7 @@ static cvp9_err_t submit_impl(cvp9_batch_t *b, int n, const int *sids, const vp9
         L.full = 1;
         L.lf_counter = s->d_misc + 2 * (size_t)n + 2;
         L.lf_tickets = (uint32_t)(n * max_sbr);
-        L.lf_ctas = b->resident_ctas;
+        L.lf_ctas = b->lf_full_ctas;   /* as many as fit: rows wait only on rows taken earlier */
     }
     for (int k = 0; k < 4; k++) L.ev[k] = s->ev_kern[k];
     uint64_t gkey = mix64(mix64(mix64(key, (uint64_t)(uintptr_t)s->d_jobs), (uint64_t)(uintptr_t)s->d_sb_range),

@@ -4451,6 +4451,12 @@ int cvp9k_configure(void)
     return 0;
 }
 
+int cvp9k_lf_full_ctas_per_sm(void)
+{
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lf_full, 128, 0) == cudaSuccess ? n : -1;
+}
+
 int cvp9k_recon_ctas_per_sm(int arith)
 {
     int n = 0;

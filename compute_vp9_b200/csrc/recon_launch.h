@@ -55,6 +55,8 @@ size_t cvp9k_recon_smem_bytes(void);
 int    cvp9k_upload_dct_basis(const double *basis, int count);
 int    cvp9k_configure(void);
 int    cvp9k_recon_ctas_per_sm(int arith);
+/* CTAs of k_lf_full (128 threads, static shared memory) resident per SM. */
+int    cvp9k_lf_full_ctas_per_sm(void);
 /* REFCPU upload of the coefficients the reconstruction reads — each block's
  * luma TXs — straight from page-locked host memory into jobs[j].coeffs, for
  * every job with coeffs_src set; adds the bytes moved to *bytes (device).
