@@ -900,6 +900,42 @@ __device__ __forceinline__ void refcpu_row(ReconSmem &s, int i, int px0, int py0
     }
 }
 
+/* REFCPU pass 2 without the add: row i's rounded, saturated residual
+ * (the same operations as refcpu_row) into res, the SB's 64x64 luma grid,
+ * for the level that predicts the TX's block to add. */
+template <int N>
+__device__ __forceinline__ void refcpu_row_res(ReconSmem &s, int i, int px0, int py0, unsigned mask,
+                                               const double *M, int16_t *res)
+{
+    double acc[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) acc[j] = 0.0;
+    while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1;
+        double t = s.temp.d[(py0 + i) * kTempPitch + px0 + k];
+#pragma unroll
+        for (int j = 0; j < N; j++) acc[j] = __dadd_rn(acc[j], __dmul_rn(t, M[k * N + j]));
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        double v = acc[j];
+        int r = __double2int_rz(__dadd_rn(v, v >= 0.0 ? 0.5 : -0.5));
+        res[(py0 + i) * 64 + px0 + j] = (int16_t)clampi(r, -32768, 32767);
+    }
+}
+
+/* The add and clamp of refcpu_row, from res. */
+template <int N>
+__device__ __forceinline__ void refcpu_add_res(ReconSmem &s, int i, int px0, int py0, const int16_t *res)
+{
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        uint8_t &px = TY(s, px0 + j, py0 + i);
+        px = (uint8_t)clampi((int)px + res[(py0 + i) * 64 + px0 + j], 0, 255);
+    }
+}
+
 __device__ __forceinline__ void idct_n(wi *x, int n)
 {
     if (n == 4) idct4(x);
@@ -1353,6 +1389,39 @@ __device__ __forceinline__ void item_pass2(ReconSmem &s, const BlkS &b, int item
         case 2: spec_row<16>(s, i, t); break;
         default: spec_row<32>(s, i, t); break;
         }
+    }
+}
+
+/* REFCPU item passes that keep the residual apart from the prediction:
+ * item_pass2_res computes row `item` of its TX into res, item_add_res adds
+ * it to the predicted pixels (TXs without coefficients have neither). */
+template <int A>
+__device__ __forceinline__ void item_pass2_res(ReconSmem &s, const BlkS &b, int item, int16_t *res)
+{
+    int i;
+    TxRef t = locate_item(b, item, &i);
+    unsigned mask = s.txmask[t.mask_idx];
+    if (!mask) return;
+    const double *M = dct_basis(t.txl);
+    switch (t.txl) {
+    case 0: refcpu_row_res<4>(s, i, t.px0, t.py0, mask, M, res); break;
+    case 1: refcpu_row_res<8>(s, i, t.px0, t.py0, mask, M, res); break;
+    case 2: refcpu_row_res<16>(s, i, t.px0, t.py0, mask, M, res); break;
+    default: refcpu_row_res<32>(s, i, t.px0, t.py0, mask, M, res); break;
+    }
+}
+
+template <int A>
+__device__ __forceinline__ void item_add_res(ReconSmem &s, const BlkS &b, int item, const int16_t *res)
+{
+    int i;
+    TxRef t = locate_item(b, item, &i);
+    if (!s.txmask[t.mask_idx]) return;
+    switch (t.txl) {
+    case 0: refcpu_add_res<4>(s, i, t.px0, t.py0, res); break;
+    case 1: refcpu_add_res<8>(s, i, t.px0, t.py0, res); break;
+    case 2: refcpu_add_res<16>(s, i, t.px0, t.py0, res); break;
+    default: refcpu_add_res<32>(s, i, t.px0, t.py0, res); break;
     }
 }
 
@@ -1856,6 +1925,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
          * prediction stages reference windows there); the levels then
          * predict and run the second pass only */
         const bool pre1 = (A == CVP9_ARITH_REFCPU || !job.full) && warp_lv && !any_inter && !seq;
+        /* REFCPU goes further: the second pass does not read the prediction
+         * either (the residual is rounded and saturated on its own before
+         * the add), so it runs here too, into a 64x64 int16 grid over the
+         * coefficient staging (spent once the first pass has read it); a
+         * level then predicts its blocks and adds their residual */
+        const bool pre2 = A == CVP9_ARITH_REFCPU && pre1;
+        int16_t *const res = s.coef;
         if (pre1) {
             const int n_items = min((int)s.base_item[nlev], kMaxItems);   /* <= 1024: disjoint luma TXs */
             for (int it = tid; it < n_items; it += kThreads) {
@@ -1863,6 +1939,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                 item_pass1<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], staged, c_base);
             }
             __syncthreads();
+            if (pre2) {
+                for (int it = tid; it < n_items; it += kThreads) {
+                    const int lo = s.item_blk[it];
+                    item_pass2_res<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], res);
+                }
+                __syncthreads();
+            }
         }
 
         /* 5. levels */
@@ -1888,7 +1971,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
                         for (int k = lane; k < n_it; k += 32) item_pass1<A>(s, b, k, staged, c_base);
                         __syncwarp();
                     }
-                    for (int k = lane; k < n_it; k += 32) item_pass2<A>(s, b, k);
+                    if (pre2) {
+                        for (int k = lane; k < n_it; k += 32) item_add_res<A>(s, b, k, res);
+                    } else {
+                        for (int k = lane; k < n_it; k += 32) item_pass2<A>(s, b, k);
+                    }
                     __syncwarp();
                 }
                 __syncthreads();
@@ -1972,7 +2059,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
             /* phase Q: second pass + residual add, thread per TX row */
             for (int it = s.base_item[L] + tid; it < s.base_item[L + 1]; it += kThreads) {
                 const int lo = s.item_blk[it];
-                item_pass2<A>(s, s.blk[s.order[lo]], it - s.item_off[lo]);
+                if (pre2) item_add_res<A>(s, s.blk[s.order[lo]], it - s.item_off[lo], res);
+                else item_pass2<A>(s, s.blk[s.order[lo]], it - s.item_off[lo]);
             }
             __syncthreads();
             if (seq) {
