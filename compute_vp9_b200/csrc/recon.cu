@@ -1774,15 +1774,27 @@ __global__ void __launch_bounds__(kThreads, 3) k_recon(const cvp9_job_t *__restr
         if (seq) {
             if (tid < nb) s.lvl[tid] = (uint16_t)tid;
         } else if (any_intra) {
+            /* longest-path levels. A block's dependencies all have lower
+             * indices, so the warps settle their 32 blocks in index order:
+             * warp w relaxes its blocks (warp syncs only) until none
+             * changes, the earlier warps' levels being final, then one CTA
+             * barrier hands over to warp w + 1 */
             volatile uint16_t *vl = s.lvl;
-            for (;;) {
-                bool changed = false;
-                if (tid < nb && ndeps) {
-                    int L = 0;
-                    for (int k = 0; k < ndeps; k++) { int v = vl[deps[k]] + 1; L = v > L ? v : L; }
-                    if (L != vl[tid]) { vl[tid] = (uint16_t)L; changed = true; }
+            const int nw = (nb + 31) >> 5;
+            for (int w = 0; w < nw; w++) {
+                if (warp == w) {
+                    for (int it = 0; it <= 32; it++) {   /* settles in at most 32 passes: a DAG in index order */
+                        bool changed = false;
+                        if (tid < nb && ndeps) {
+                            int L = 0;
+                            for (int k = 0; k < ndeps; k++) { int v = vl[deps[k]] + 1; L = v > L ? v : L; }
+                            if (L != vl[tid]) { vl[tid] = (uint16_t)L; changed = true; }
+                        }
+                        __syncwarp();
+                        if (!__any_sync(0xffffffffu, changed)) break;
+                    }
                 }
-                if (!__syncthreads_or(changed)) break;
+                __syncthreads();
             }
         }
         __syncthreads();
