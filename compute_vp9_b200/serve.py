@@ -326,7 +326,7 @@ def capacity_sweep(arith=0, speeds=(4, 8, 12, 16, 20, 24, 32, 48), p99_budget_ms
                     "speed whose p99 (frame due -> planes in host memory) is within the budget"}
 
 
-def stream_capacity_sweep(arith=0, concurrency=(64, 128, 192, 256, 320), p99_budget_ms=33.0, hold_ms=8.0,
+def stream_capacity_sweep(arith=0, concurrency=(64, 128, 192, 224, 240, 256), p99_budget_ms=33.0, hold_ms=8.0,
                           seed=1, pool=None, engines=2, max_batch=48):
     """Most concurrent 30 fps streams of the serving mix whose p99 frame
     latency stays within the budget. Pacing stays real time; the arrival
