@@ -34,8 +34,10 @@
  * (smaller steps have few copies, and a serving step's submit latency
  * counts: staging took a 9-frame step's submit from 0.3 to 1.1 ms) */
 #define COALESCE_MIN_FRAMES 32
-/* Host output buffers per stream: up to two other steps in flight holding
- * the stream, the two newest completed frames, and the new one. */
+/* Page-locked output areas (step q downloads into area q % OUTR), and the
+ * records each stream keeps of where its recent frames landed: up to two
+ * other steps in flight holding the stream, the two newest completed
+ * frames, and the new one. */
 #define OUTR (BSLOTS + 2)
 #define WAIT_LIMIT_S 60.0
 #define ALIGN_UP(x, a) (((x) + (a) - 1) / (a) * (a))

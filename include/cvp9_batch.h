@@ -109,7 +109,7 @@ uint64_t    cvp9_batch_stream_bytes(uint32_t width, uint32_t height);
 int         cvp9_batch_open_stream(cvp9_batch_t *b, uint32_t width, uint32_t height);
 
 /* Take device and page-locked memory from the driver now for `nstreams`
- * streams of width x height (their frames, output ring and step buffers),
+ * streams of width x height (their frames, output areas and step buffers),
  * so that opening and decoding that many streams later allocates nothing
  * from the driver: pinning host memory costs about 0.4 ms per MB and
  * device allocations can wait for the device, both on a serving loop's
