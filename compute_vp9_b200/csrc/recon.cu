@@ -66,6 +66,8 @@ __constant__ uint8_t c_tx_type[10] = CVP9_INTRA_TX_TYPE_INIT;
  * (phase 0's 128 does not fit a byte: callers take the centre sample for
  * it, which is what its filter computes); uploaded by cvp9k_configure */
 __constant__ uint32_t c_subpel_pk[16][2];
+/* the four VP9 filters (c_subpel4) packed the same way, for the FULL profile */
+__constant__ uint32_t c_subpel4_pk[4][16][2];
 
 __device__ __forceinline__ const double *dct_basis(int txl)
 {
@@ -73,6 +75,22 @@ __device__ __forceinline__ const double *dct_basis(int txl)
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ uint32_t tap_round(int acc) { return (uint32_t)clampi((acc + 64) >> 7, 0, 255); }
+
+__device__ __forceinline__ int dp4a_su(uint32_t taps, uint32_t px, int c)
+{
+    int d;
+    asm("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(taps), "r"(px), "r"(c));
+    return d;
+}
+
+/* One 8-tap output from samples s0 (samples 0-3 of the window) and s1
+ * (4-7): phase 0 is the centre sample itself. */
+__device__ __forceinline__ uint32_t tap8(uint32_t ta, uint32_t tb, int phase, uint32_t s0, uint32_t s1)
+{
+    return phase ? tap_round(dp4a_su(tb, s1, dp4a_su(ta, s0, 0))) : (s0 >> 24);
+}
 
 /* t / d for 0 <= t < 4096 and 1 <= d <= 16 without an integer divide:
  * (t * ceil(2^16 / d)) >> 16 is exact in that range. */
@@ -511,21 +529,37 @@ __device__ void predict_intra_chunk(ReconSmem &s, const BlkS &b, int gbx, int gb
     }
 }
 
-/* Stage a (sw x sh) window of a reference plane starting at (x0, y0), every
- * sample clamped into [0, pw-1] x [0, ph-1], into st (row pitch sp). */
-__device__ __forceinline__ void stage_window(uint8_t *st, int sp, const uint8_t *__restrict__ plane,
-                                             int stride, int pw, int ph, int x0, int y0,
-                                             int sw, int sh, int lane)
-{
-    int xm = pw > 0 ? pw - 1 : 0, ym = ph > 0 ? ph - 1 : 0;
-    const int sx = lane & 15;                 /* windows are at most 16 wide */
-    if (sx >= sw) return;
-    const int xx = clampi(x0 + sx, 0, xm);
-    for (int sy = lane >> 4; sy < sh; sy += 2) {
-        int yy = clampi(y0 + sy, 0, ym);
-        st[sy * sp + sx] = __ldg(plane + (size_t)yy * stride + xx);
+/* Stage a (sw x sh) window of a reference plane starting at (x0, y0), at
+ * most 16 wide and 2*MAXI high, every sample clamped into [0, pw-1] x
+ * [0, ph-1], in two steps: every lane's loads first, then its shared-memory
+ * stores. (Loaded and stored one by one, each load waits for the store
+ * before it, which may alias: a round trip to L2 per row.) */
+template <int MAXI>
+struct WinRows {
+    uint32_t v[MAXI];
+    __device__ __forceinline__ void load(const uint8_t *__restrict__ plane, int stride, int pw, int ph,
+                                         int x0, int y0, int sw, int sh, int lane)
+    {
+        const int xm = pw > 0 ? pw - 1 : 0, ym = ph > 0 ? ph - 1 : 0;
+        const int sx = lane & 15;
+        const int xx = clampi(x0 + sx, 0, xm);
+#pragma unroll
+        for (int k = 0; k < MAXI; k++) {
+            const int sy = (lane >> 4) + 2 * k;
+            v[k] = (sx < sw && sy < sh) ? (uint32_t)__ldg(plane + (size_t)clampi(y0 + sy, 0, ym) * stride + xx) : 0u;
+        }
     }
-}
+    __device__ __forceinline__ void store(uint8_t *st, int sp, int sw, int sh, int lane) const
+    {
+        const int sx = lane & 15;
+        if (sx >= sw) return;
+#pragma unroll
+        for (int k = 0; k < MAXI; k++) {
+            const int sy = (lane >> 4) + 2 * k;
+            if (sy < sh) st[sy * sp + sx] = (uint8_t)v[k];
+        }
+    }
+};
 
 /* Geometry of one chunk's REFCPU bilinear prediction: integer positions and
  * fractions of the luma and chroma windows (vp9_reconstruct.c:94-131,
@@ -709,7 +743,19 @@ __device__ __forceinline__ void fill_chunk(ReconSmem &s, int v, int lx0, int ly0
  * bits before the vertical pass (vp9_mc.comp.glsl:61-110). F: the filter
  * (the regular one under SPEC). avg: round-average into the tile (the
  * second prediction of a FULL compound block). */
-__device__ void spec_inter_pass(ReconSmem &s, const cvp9_ref_t &R, int mvx, int mvy, const int (*F)[8], bool avg,
+/* One 8-tap output of a staged row (4-byte aligned in shared memory) at
+ * column c: samples c..c+7 as two words, two dp4a (tap8). The same value as
+ * the scalar sum: clamp((sum + 64) >> 7, 0, 255). */
+__device__ __forceinline__ uint32_t htap8(const uint8_t *row, int c, const uint32_t *pk, int phase)
+{
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(row) + (c >> 2);
+    const unsigned sh = 8u * (unsigned)(c & 3);
+    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+    return tap8(pk[0], pk[1], phase, __funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
+}
+
+__device__ void spec_inter_pass(ReconSmem &s, const cvp9_ref_t &R, int mvx, int mvy, const int (*F)[8],
+                                const uint32_t (*P)[2], bool avg,
                                 int sbx, int sby, int lx0, int ly0, int lw, int lh,
                                 int cx0, int cy0, int clw, int clh, int warp, int lane)
 {
@@ -732,27 +778,29 @@ __device__ void spec_inter_pass(ReconSmem &s, const cvp9_ref_t &R, int mvx, int 
         uint8_t *sv = st + 492;         /* 11 x 12 */
         uint8_t *hu = st + 624;         /* 11 x 4  */
         uint8_t *hv = st + 668;         /* 11 x 4  */
-        stage_window(sy_, 16, rp, rw, rw, rh, bx - 3, by - 3, lw + 7, lh + 7, lane);
-        stage_window(su, 12, ru, rcs, cw2, ch2, cbx - 3, cby - 3, clw + 7, clh + 7, lane);
-        stage_window(sv, 12, rv, rcs, cw2, ch2, cbx - 3, cby - 3, clw + 7, clh + 7, lane);
+        {
+            /* all three windows' reads in flight at once */
+            WinRows<8> wl;
+            WinRows<6> wu, wv;
+            wl.load(rp, rw, rw, rh, bx - 3, by - 3, lw + 7, lh + 7, lane);
+            wu.load(ru, rcs, cw2, ch2, cbx - 3, cby - 3, clw + 7, clh + 7, lane);
+            wv.load(rv, rcs, cw2, ch2, cbx - 3, cby - 3, clw + 7, clh + 7, lane);
+            wl.store(sy_, 16, lw + 7, lh + 7, lane);
+            wu.store(su, 12, clw + 7, clh + 7, lane);
+            wv.store(sv, 12, clw + 7, clh + 7, lane);
+        }
         __syncwarp();
         /* horizontal pass (rounded, clipped to 8 bits) */
         for (int i = lane; i < (lh + 7) * lw; i += 32) {
-            int r = i / lw, c = i - r * lw;
-            int acc = 0;
-#pragma unroll
-            for (int t = 0; t < 8; t++) acc += F[fx][t] * sy_[r * 16 + c + t];
-            hy[r * 8 + c] = (uint8_t)clampi((acc + 64) >> 7, 0, 255);
+            int r = lw == 8 ? i >> 3 : i / lw, c = i - r * lw;
+            hy[r * 8 + c] = (uint8_t)htap8(sy_ + r * 16, c, P[fx], fx);
         }
         for (int i = lane; i < 2 * (clh + 7) * clw; i += 32) {
             int pl = i >= (clh + 7) * clw;
             int j = pl ? i - (clh + 7) * clw : i;
-            int r = j / clw, c = j - r * clw;
+            int r = clw == 4 ? j >> 2 : j / clw, c = j - r * clw;
             const uint8_t *src = pl ? sv : su;
-            int acc = 0;
-#pragma unroll
-            for (int t = 0; t < 8; t++) acc += F[cfx][t] * src[r * 12 + c + t];
-            (pl ? hv : hu)[r * 4 + c] = (uint8_t)clampi((acc + 64) >> 7, 0, 255);
+            (pl ? hv : hu)[r * 4 + c] = (uint8_t)htap8(src + r * 12, c, P[cfx], cfx);
         }
         __syncwarp();
         for (int idx = lane; idx < 64; idx += 32) {
@@ -802,11 +850,12 @@ __device__ void spec_inter_chunk(ReconSmem &s, const BlkS &b, int sbx, int sby,
     const cvp9_ref_t &R = job.ref[job.ref_slot_of[clampi((int)b.ref0 - 1, 0, 2)] & 7];
     if (!R.plane) { fill_chunk(s, 128, lx0, ly0, lw, lh, cx0, cy0, clw, clh, lane); return; }
     const int (*F)[8] = job.full ? c_subpel4[job.interp_filter & 3] : c_subpel;
-    spec_inter_pass(s, R, b.mvx, b.mvy, F, false, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh, warp, lane);
+    const uint32_t (*P)[2] = job.full ? c_subpel4_pk[job.interp_filter & 3] : c_subpel_pk;
+    spec_inter_pass(s, R, b.mvx, b.mvy, F, P, false, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh, warp, lane);
     if (b.ref1) {
         const cvp9_ref_t &R1 = job.ref[job.ref_slot_of[clampi((int)b.ref1 - 1, 0, 2)] & 7];
         if (R1.plane)
-            spec_inter_pass(s, R1, b.mv1x, b.mv1y, F, true, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh,
+            spec_inter_pass(s, R1, b.mv1x, b.mv1y, F, P, true, sbx, sby, lx0, ly0, lw, lh, cx0, cy0, clw, clh,
                             warp, lane);
     }
 }
@@ -2780,7 +2829,6 @@ __device__ __forceinline__ void ld16c(const uint8_t *plane, int stride, int pw, 
 
 
 /* shader rounding of one 8-tap sum: (acc + 64) >> 7 clipped to 8 bits */
-__device__ __forceinline__ uint32_t tap_round(int acc) { return (uint32_t)clampi((acc + 64) >> 7, 0, 255); }
 
 /* bytes k..k+3 of o[] as one word (k a compile-time index) */
 __device__ __forceinline__ uint32_t win4(const uint32_t o[4], int k)
@@ -2789,19 +2837,7 @@ __device__ __forceinline__ uint32_t win4(const uint32_t o[4], int k)
 }
 
 /* c + the dot product of four signed taps with four unsigned samples */
-__device__ __forceinline__ int dp4a_su(uint32_t taps, uint32_t px, int c)
-{
-    int d;
-    asm("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(taps), "r"(px), "r"(c));
-    return d;
-}
 
-/* One 8-tap output from samples s0 (samples 0-3 of the window) and s1
- * (4-7): phase 0 is the centre sample itself. */
-__device__ __forceinline__ uint32_t tap8(uint32_t ta, uint32_t tb, int phase, uint32_t s0, uint32_t s1)
-{
-    return phase ? tap_round(dp4a_su(tb, s1, dp4a_su(ta, s0, 0))) : (s0 >> 24);
-}
 
 /* 4x4 byte transpose: rows a..d (one word of four columns each) to four
  * words, one column each (its bytes in row order) */
@@ -4508,6 +4544,25 @@ int cvp9k_configure(void)
                 pk[f][h] = w;
             }
         if (cudaMemcpyToSymbol(c_subpel_pk, pk, sizeof(pk)) != cudaSuccess) return -1;
+    }
+    {
+        static const int taps4[4][16][8] = { CVP9_SUBPEL_REGULAR_INIT, CVP9_SUBPEL_SMOOTH_INIT,
+                                             CVP9_SUBPEL_SHARP_INIT, CVP9_SUBPEL_BILINEAR_INIT };
+        uint32_t pk[4][16][2];
+        for (int k = 0; k < 4; k++)
+            for (int f = 0; f < 16; f++)
+                for (int h = 0; h < 2; h++) {
+                    uint32_t w = 0;
+                    for (int t = 0; t < 4; t++) {
+                        const int v = taps4[k][f][4 * h + t];
+                        /* phase 0 (the centre tap alone, 128) is not packed:
+                         * tap8 takes the centre sample for it */
+                        if (f && (v < -128 || v > 127)) return -1;
+                        w |= (uint32_t)(uint8_t)(int8_t)v << (8 * t);
+                    }
+                    pk[k][f][h] = w;
+                }
+        if (cudaMemcpyToSymbol(c_subpel4_pk, pk, sizeof(pk)) != cudaSuccess) return -1;
     }
     size_t smem = sizeof(ReconSmem);
     if (cudaFuncSetAttribute(k_recon<CVP9_ARITH_REFCPU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
