@@ -20,7 +20,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-HOST_C = ["backend_common.c", "cuda_backend.c", "batch.c", "pack.c"]
+HOST_C = ["backend_common.c", "cuda_backend.c", "batch.c", "pack.c", "hbd.c"]
 CUDA_SRC = ["recon.cu", "recon_static.cu"]
 
 

@@ -135,6 +135,21 @@ __device__ __forceinline__ wi operator-(wi a, wi b) { return wi((int)((unsigned)
 __device__ __forceinline__ wi operator-(wi a) { return wi((int)(0u - (unsigned)a.v)); }
 __device__ __forceinline__ wi operator*(wi a, int k) { return wi((int)((unsigned)a.v * (unsigned)k)); }
 __device__ __forceinline__ wi RS(wi x) { return wi(((int)((unsigned)x.v + 8192u)) >> 14); }
+__device__ __forceinline__ wi shr(wi x, int k) { return wi(x.v >> k); }
+
+/* 64-bit integer for the same butterflies at 10 bits (profile 2): products
+ * of the +-2^17 dequantised range and the Q14 multipliers need 64 bits. */
+struct wl {
+    long long v;
+    __device__ __forceinline__ wl() : v(0) {}
+    __device__ __forceinline__ wl(long long x) : v(x) {}
+};
+__device__ __forceinline__ wl operator+(wl a, wl b) { return wl(a.v + b.v); }
+__device__ __forceinline__ wl operator-(wl a, wl b) { return wl(a.v - b.v); }
+__device__ __forceinline__ wl operator-(wl a) { return wl(-a.v); }
+__device__ __forceinline__ wl operator*(wl a, int k) { return wl(a.v * (long long)k); }
+__device__ __forceinline__ wl RS(wl x) { return wl((x.v + 8192) >> 14); }
+__device__ __forceinline__ wl shr(wl x, int k) { return wl(x.v >> k); }
 
 /* cos(k*pi/64) in Q14 */
 enum : int {
@@ -148,16 +163,18 @@ enum : int {
 
 /* 1-D inverse DCTs, in place on x[0..N). Same stage structure and rounding
  * as vp9_idct.comp.glsl:47-649. */
-__device__ __forceinline__ void idct4(wi *x)
+template <class T>
+__device__ __forceinline__ void idct4(T *x)
 {
-    wi s0 = RS((x[0] + x[2]) * K16), s1 = RS((x[0] - x[2]) * K16);
-    wi s2 = RS(x[1] * K24 - x[3] * K8), s3 = RS(x[1] * K8 + x[3] * K24);
+    T s0 = RS((x[0] + x[2]) * K16), s1 = RS((x[0] - x[2]) * K16);
+    T s2 = RS(x[1] * K24 - x[3] * K8), s3 = RS(x[1] * K8 + x[3] * K24);
     x[0] = s0 + s3; x[1] = s1 + s2; x[2] = s1 - s2; x[3] = s0 - s3;
 }
 
-__device__ __forceinline__ void idct8(wi *x)
+template <class T>
+__device__ __forceinline__ void idct8(T *x)
 {
-    wi a[8], b[8];
+    T a[8], b[8];
     a[0] = x[0]; a[1] = x[2]; a[2] = x[4]; a[3] = x[6];
     a[4] = RS(x[1] * K28 - x[7] * K4); a[7] = RS(x[1] * K4 + x[7] * K28);
     a[5] = RS(x[5] * K12 - x[3] * K20); a[6] = RS(x[5] * K20 + x[3] * K12);
@@ -170,9 +187,10 @@ __device__ __forceinline__ void idct8(wi *x)
     for (int i = 0; i < 4; i++) { x[i] = a[i] + a[7 - i]; x[7 - i] = a[i] - a[7 - i]; }
 }
 
-__device__ __forceinline__ void idct16(wi *x)
+template <class T>
+__device__ __forceinline__ void idct16(T *x)
 {
-    wi a[16], b[16];
+    T a[16], b[16];
     a[0] = x[0]; a[1] = x[8]; a[2] = x[4]; a[3] = x[12]; a[4] = x[2]; a[5] = x[10];
     a[6] = x[6]; a[7] = x[14]; a[8] = x[1]; a[9] = x[9]; a[10] = x[5]; a[11] = x[13];
     a[12] = x[3]; a[13] = x[11]; a[14] = x[7]; a[15] = x[15];
@@ -209,9 +227,10 @@ __device__ __forceinline__ void idct16(wi *x)
     for (int i = 0; i < 8; i++) { x[i] = b[i] + b[15 - i]; x[15 - i] = b[i] - b[15 - i]; }
 }
 
-__device__ __forceinline__ void idct32(wi *x)
+template <class T>
+__device__ __forceinline__ void idct32(T *x)
 {
-    wi a[32], b[32];
+    T a[32], b[32];
     a[0] = x[0]; a[1] = x[16]; a[2] = x[8]; a[3] = x[24]; a[4] = x[4]; a[5] = x[20];
     a[6] = x[12]; a[7] = x[28]; a[8] = x[2]; a[9] = x[18]; a[10] = x[10]; a[11] = x[26];
     a[12] = x[6]; a[13] = x[22]; a[14] = x[14]; a[15] = x[30];
@@ -985,7 +1004,8 @@ __device__ __forceinline__ void refcpu_add_res(ReconSmem &s, int i, int px0, int
     }
 }
 
-__device__ __forceinline__ void idct_n(wi *x, int n)
+template <class T>
+__device__ __forceinline__ void idct_n(T *x, int n)
 {
     if (n == 4) idct4(x);
     else if (n == 8) idct8(x);
@@ -1045,25 +1065,28 @@ __device__ __forceinline__ void spec_row(ReconSmem &s, int i, const TxRef &t)
 enum : int { KS1 = 5283, KS2 = 9929, KS3 = 13377, KS4 = 15212 };
 
 /* 1-D inverse ADSTs in place, 32-bit wrap and Q14 rounding as the DCTs. */
-__device__ __forceinline__ void iadst4(wi *x)
+template <class T>
+__device__ __forceinline__ void iadst4(T *x)
 {
-    wi a = x[0] * KS1 + x[2] * KS4 + x[3] * KS2;
-    wi b = x[0] * KS2 - x[2] * KS1 - x[3] * KS4;
-    wi c = (x[0] - x[2] + x[3]) * KS3;
-    wi d = x[1] * KS3;
+    T a = x[0] * KS1 + x[2] * KS4 + x[3] * KS2;
+    T b = x[0] * KS2 - x[2] * KS1 - x[3] * KS4;
+    T c = (x[0] - x[2] + x[3]) * KS3;
+    T d = x[1] * KS3;
     x[0] = RS(a + d); x[1] = RS(b + d); x[2] = RS(c); x[3] = RS(a + b - d);
 }
 
-__device__ __forceinline__ void rot(wi x, wi y, int ca, int cb, wi &o0, wi &o1)
+template <class T>
+__device__ __forceinline__ void rot(T x, T y, int ca, int cb, T &o0, T &o1)
 {
     o0 = x * ca + y * cb;
     o1 = x * cb - y * ca;
 }
 
-__device__ __forceinline__ void iadst8(wi *in)
+template <class T>
+__device__ __forceinline__ void iadst8(T *in)
 {
-    wi x0 = in[7], x1 = in[0], x2 = in[5], x3 = in[2], x4 = in[3], x5 = in[4], x6 = in[1], x7 = in[6];
-    wi s0, s1, s2, s3, s4, s5, s6, s7;
+    T x0 = in[7], x1 = in[0], x2 = in[5], x3 = in[2], x4 = in[3], x5 = in[4], x6 = in[1], x7 = in[6];
+    T s0, s1, s2, s3, s4, s5, s6, s7;
     rot(x0, x1, K2, K30, s0, s1);
     rot(x2, x3, K10, K22, s2, s3);
     rot(x4, x5, K18, K14, s4, s5);
@@ -1078,14 +1101,15 @@ __device__ __forceinline__ void iadst8(wi *in)
     x4 = RS(s4 + s6); x5 = RS(s5 + s7); x6 = RS(s4 - s6); x7 = RS(s5 - s7);
     x2 = RS((s2 + s3) * K16);
     x3 = RS((s2 - s3) * K16);
-    wi y6 = RS((x6 + x7) * K16), y7 = RS((x6 - x7) * K16);
+    T y6 = RS((x6 + x7) * K16), y7 = RS((x6 - x7) * K16);
     in[0] = s0; in[1] = -x4; in[2] = y6; in[3] = -x2;
     in[4] = x3; in[5] = -y7; in[6] = x5; in[7] = -s1;
 }
 
-__device__ __forceinline__ void iadst16(wi *in)
+template <class T>
+__device__ __forceinline__ void iadst16(T *in)
 {
-    wi x[16], s[16];
+    T x[16], s[16];
     x[0] = in[15]; x[1] = in[0]; x[2] = in[13]; x[3] = in[2]; x[4] = in[11]; x[5] = in[4];
     x[6] = in[9]; x[7] = in[6]; x[8] = in[7]; x[9] = in[8]; x[10] = in[5]; x[11] = in[10];
     x[12] = in[3]; x[13] = in[12]; x[14] = in[1]; x[15] = in[14];
@@ -1132,10 +1156,10 @@ __device__ __forceinline__ void iadst16(wi *in)
         x[g + 6] = RS(s[g + 4] - s[g + 6]);
         x[g + 7] = RS(s[g + 5] - s[g + 7]);
     }
-    wi t2 = RS(-((x[2] + x[3]) * K16)), t3 = RS((x[2] - x[3]) * K16);
-    wi t6 = RS((x[6] + x[7]) * K16), t7 = RS((x[7] - x[6]) * K16);
-    wi t10 = RS((x[10] + x[11]) * K16), t11 = RS((x[11] - x[10]) * K16);
-    wi t14 = RS(-((x[14] + x[15]) * K16)), t15 = RS((x[14] - x[15]) * K16);
+    T t2 = RS(-((x[2] + x[3]) * K16)), t3 = RS((x[2] - x[3]) * K16);
+    T t6 = RS((x[6] + x[7]) * K16), t7 = RS((x[7] - x[6]) * K16);
+    T t10 = RS((x[10] + x[11]) * K16), t11 = RS((x[11] - x[10]) * K16);
+    T t14 = RS(-((x[14] + x[15]) * K16)), t15 = RS((x[14] - x[15]) * K16);
     in[0] = x[0];  in[1] = -x[8];  in[2] = x[12];  in[3] = -x[4];
     in[4] = t6;    in[5] = t14;    in[6] = t10;    in[7] = t2;
     in[8] = t3;    in[9] = t11;    in[10] = t15;   in[11] = t7;
@@ -1144,19 +1168,20 @@ __device__ __forceinline__ void iadst16(wi *in)
 
 /* 4-point inverse Walsh-Hadamard (lossless frames); the row pass first
  * undoes the quantiser step 4 with a shift. */
-__device__ __forceinline__ void iwht4(wi *x, bool rows)
+template <class T>
+__device__ __forceinline__ void iwht4(T *x, bool rows)
 {
-    wi a = x[0], c = x[1], d = x[2], b = x[3];
-    if (rows) { a = wi(a.v >> 2); c = wi(c.v >> 2); d = wi(d.v >> 2); b = wi(b.v >> 2); }
+    T a = x[0], c = x[1], d = x[2], b = x[3];
+    if (rows) { a = shr(a, 2); c = shr(c, 2); d = shr(d, 2); b = shr(b, 2); }
     a = a + c; d = d - b;
-    wi e = wi((a - d).v >> 1);
+    T e = shr(a - d, 1);
     b = e - b; c = e - c;
     a = a - b; d = d + c;
     x[0] = a; x[1] = b; x[2] = c; x[3] = d;
 }
 
-template <int N>
-__device__ __forceinline__ void itx1(wi *v, bool adst)
+template <int N, class T>
+__device__ __forceinline__ void itx1(T *v, bool adst)
 {
     if (N == 4 && adst) iadst4(v);
     else if (N == 8 && adst) iadst8(v);
@@ -1233,9 +1258,10 @@ __device__ __forceinline__ uint8_t &TP(ReconSmem &s, int p, int x, int y)
 #define FAVG3(a, b, c) (((a) + 2 * (b) + (c) + 2) >> 2)
 
 /* One sample of a VP9 intra predictor from the TX's edges: above[-1..2n-1]
- * (above[-1] the corner), left[0..n-1]. */
-__device__ __forceinline__ int full_pred(int mode, int r, int c, int n, const uint8_t *above, const uint8_t *left,
-                                         int dc)
+ * (above[-1] the corner), left[0..n-1]; MAXV: the largest sample value (TM
+ * clips to it). */
+template <int MAXV = 255, class E>
+__device__ __forceinline__ int full_pred(int mode, int r, int c, int n, const E *above, const E *left, int dc)
 {
     switch (mode) {
     case 1: return above[c];
@@ -1271,7 +1297,7 @@ __device__ __forceinline__ int full_pred(int mode, int r, int c, int n, const ui
         const int k = (r >> 1) + c;
         return (r & 1) ? FAVG3(above[k], above[k + 1], above[k + 2]) : FAVG2(above[k], above[k + 1]);
     }
-    case 9: return clampi((int)left[r] + (int)above[c] - (int)above[-1], 0, 255);
+    case 9: return clampi((int)left[r] + (int)above[c] - (int)above[-1], 0, MAXV);
     default: return dc;
     }
 }
@@ -4121,9 +4147,14 @@ __global__ void __launch_bounds__(256) k_lf_mimap(const cvp9_job_t *__restrict__
 struct LfThr { int lim, mblim, hev; };
 
 /* Filter across one edge: q0 at s[0], p0 at s[-st]; fs = widest filter
- * allowed there (4, 8 or 16), narrowed by the flatness tests. */
-__device__ __forceinline__ void lf_edge_full(uint8_t *s, int st, int fs, LfThr th)
+ * allowed there (4, 8 or 16), narrowed by the flatness tests. T, SH: the
+ * sample type and bit depth - 8; at 10 bits (profile 2) the flatness test
+ * compares against 1 << SH, the 4-tap filter clamps to the signed range of
+ * the bit depth around 128 << SH, and th arrives shifted by SH. */
+template <class T, int SH>
+__device__ __forceinline__ void lf_edge_full(T *s, int st, int fs, LfThr th)
 {
+    constexpr int kFlat = 1 << SH, kMid = 128 << SH;
     auto P = [&](int i) -> int { return s[(-i - 1) * st]; };
     auto Q = [&](int i) -> int { return s[i * st]; };
     const int p3 = P(3), p2 = P(2), p1 = P(1), p0 = P(0), q0 = Q(0), q1 = Q(1), q2 = Q(2), q3 = Q(3);
@@ -4131,13 +4162,13 @@ __device__ __forceinline__ void lf_edge_full(uint8_t *s, int st, int fs, LfThr t
                       abs(q1 - q0) <= th.lim && abs(q2 - q1) <= th.lim && abs(q3 - q2) <= th.lim &&
                       abs(p0 - q0) * 2 + abs(p1 - q1) / 2 <= th.mblim;
     if (!mask) return;
-    const bool flat = fs >= 8 && abs(p1 - p0) <= 1 && abs(q1 - q0) <= 1 && abs(p2 - p0) <= 1 &&
-                      abs(q2 - q0) <= 1 && abs(p3 - p0) <= 1 && abs(q3 - q0) <= 1;
+    const bool flat = fs >= 8 && abs(p1 - p0) <= kFlat && abs(q1 - q0) <= kFlat && abs(p2 - p0) <= kFlat &&
+                      abs(q2 - q0) <= kFlat && abs(p3 - p0) <= kFlat && abs(q3 - q0) <= kFlat;
     bool flat2 = false;
     if (fs == 16 && flat) {
         flat2 = true;
 #pragma unroll
-        for (int i = 4; i < 8; i++) flat2 &= abs(P(i) - p0) <= 1 && abs(Q(i) - q0) <= 1;
+        for (int i = 4; i < 8; i++) flat2 &= abs(P(i) - p0) <= kFlat && abs(Q(i) - q0) <= kFlat;
     }
     if (flat2) {
         int v[16], o[16];
@@ -4151,7 +4182,7 @@ __device__ __forceinline__ void lf_edge_full(uint8_t *s, int st, int fs, LfThr t
             o[k] = (acc + 8) >> 4;
         }
 #pragma unroll
-        for (int k = 1; k < 15; k++) s[(k - 8) * st] = (uint8_t)o[k];
+        for (int k = 1; k < 15; k++) s[(k - 8) * st] = (T)o[k];
     } else if (flat) {
         int v[8], o[8];
 #pragma unroll
@@ -4164,20 +4195,20 @@ __device__ __forceinline__ void lf_edge_full(uint8_t *s, int st, int fs, LfThr t
             o[k] = (acc + 4) >> 3;
         }
 #pragma unroll
-        for (int k = 1; k < 7; k++) s[(k - 4) * st] = (uint8_t)o[k];
+        for (int k = 1; k < 7; k++) s[(k - 4) * st] = (T)o[k];
     } else {
-        auto sc8 = [](int v) { return v < -128 ? -128 : (v > 127 ? 127 : v); };
-        const int ps1 = p1 - 128, ps0 = p0 - 128, qs0 = q0 - 128, qs1 = q1 - 128;
+        auto sc8 = [](int v) { return v < -kMid ? -kMid : (v > kMid - 1 ? kMid - 1 : v); };
+        const int ps1 = p1 - kMid, ps0 = p0 - kMid, qs0 = q0 - kMid, qs1 = q1 - kMid;
         const bool hev = abs(p1 - p0) > th.hev || abs(q1 - q0) > th.hev;
         int f = hev ? sc8(ps1 - qs1) : 0;
         f = sc8(f + 3 * (qs0 - ps0));
         const int f1 = sc8(f + 4) >> 3, f2 = sc8(f + 3) >> 3;
-        s[0] = (uint8_t)(sc8(qs0 - f1) + 128);
-        s[-st] = (uint8_t)(sc8(ps0 + f2) + 128);
+        s[0] = (T)(sc8(qs0 - f1) + kMid);
+        s[-st] = (T)(sc8(ps0 + f2) + kMid);
         if (!hev) {
             const int f3 = (f1 + 1) >> 1;
-            s[st] = (uint8_t)(sc8(qs1 - f3) + 128);
-            s[-2 * st] = (uint8_t)(sc8(ps1 + f3) + 128);
+            s[st] = (T)(sc8(qs1 - f3) + kMid);
+            s[-2 * st] = (T)(sc8(ps1 + f3) + kMid);
         }
     }
 }
@@ -4216,11 +4247,19 @@ __device__ bool wait_at_least(const unsigned *flag, unsigned v)
     return false;
 }
 
+/* 4 samples as one load or store: a 32-bit word of 8-bit samples, two of
+ * 16-bit ones. */
+template <class T> struct Quad;
+template <> struct Quad<uint8_t> { using type = unsigned int; };
+template <> struct Quad<uint16_t> { using type = uint2; };
+
+template <class T, int SH>
 __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ jobs, int njobs,
                                                 uint32_t n_tickets, uint32_t *counter)
 {
-    __shared__ __align__(16) uint8_t wy[kLfY * kLfY];
-    __shared__ __align__(16) uint8_t wc[2][kLfC * kLfC];
+    using Q4 = typename Quad<T>::type;
+    __shared__ __align__(16) T wy[kLfY * kLfY];
+    __shared__ __align__(16) T wc[2][kLfC * kLfC];
     __shared__ int s_ticket;
     const int tid = threadIdx.x;
     for (;;) {
@@ -4238,14 +4277,14 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
             int bil = level >> ((sharp > 0) + (sharp > 4));
             if (sharp > 0 && bil > 9 - sharp) bil = 9 - sharp;
             if (bil < 1) bil = 1;
-            th.lim = bil;
-            th.mblim = 2 * (level + 2) + bil;
-            th.hev = level >> 4;
+            th.lim = bil << SH;
+            th.mblim = (2 * (level + 2) + bil) << SH;
+            th.hev = (level >> 4) << SH;
         }
         const int W = job.W, H = job.H, CW = job.CW, CH = job.CH;
-        uint8_t *Y = job.out;
-        uint8_t *U = Y + (size_t)W * H;
-        uint8_t *V = U + (size_t)CW * CH;
+        T *Y = reinterpret_cast<T *>(job.out);
+        T *U = Y + (size_t)W * H;
+        T *V = U + (size_t)CW * CH;
         unsigned *prog_prev = row > 0 ? job.sb_range + 4 * (size_t)(row - 1) * job.sb_cols + 3 : nullptr;
         unsigned *prog = job.sb_range + 4 * (size_t)row * job.sb_cols + 3;
         for (int c = 0; c < job.sb_cols; c++) {
@@ -4261,8 +4300,8 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 const int r = i / (kLfY / 4), w4 = i - r * (kLfY / 4);
                 const int gy = Y0 - 8 + r, gx = X0 - 8 + 4 * w4;
                 if (gy >= 0 && gy < H && gx >= 0 && gx < W)
-                    *reinterpret_cast<uint32_t *>(&wy[r * kLfY + 4 * w4]) =
-                        __ldcg(reinterpret_cast<const unsigned int *>(Y + (size_t)gy * W + gx));
+                    *reinterpret_cast<Q4 *>(&wy[r * kLfY + 4 * w4]) =
+                        __ldcg(reinterpret_cast<const Q4 *>(Y + (size_t)gy * W + gx));
             }
             for (int i = tid; i < 2 * kLfC * (kLfC / 4); i += 128) {
                 const int pl = i >= kLfC * (kLfC / 4);
@@ -4270,8 +4309,8 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 const int r = k / (kLfC / 4), w4 = k - r * (kLfC / 4);
                 const int gy = YC - 8 + r, gx = XC - 8 + 4 * w4;
                 if (gy >= 0 && gy < CH && gx >= 0 && gx < CW)
-                    *reinterpret_cast<uint32_t *>(&wc[pl][r * kLfC + 4 * w4]) =
-                        __ldcg(reinterpret_cast<const unsigned int *>((pl ? V : U) + (size_t)gy * CW + gx));
+                    *reinterpret_cast<Q4 *>(&wc[pl][r * kLfC + 4 * w4]) =
+                        __ldcg(reinterpret_cast<const Q4 *>((pl ? V : U) + (size_t)gy * CW + gx));
             }
             __syncthreads();
             /* vertical edges: a thread per row (64 luma, 32 + 32 chroma) */
@@ -4280,13 +4319,13 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 const int r = p == 0 ? tid : (tid - 32 - 32 * p);
                 const int sz = p ? 32 : 64, pw = p ? CW : W, ph = p ? CH : H;
                 const int gy = (p ? YC : Y0) + r, gx0 = p ? XC : X0;
-                uint8_t *row_p = p == 0 ? &wy[(8 + r) * kLfY + 8] : &wc[p - 1][(8 + r) * kLfC + 8];
+                T *row_p = p == 0 ? &wy[(8 + r) * kLfY + 8] : &wc[p - 1][(8 + r) * kLfC + 8];
                 if (gy < ph)
                     for (int x = 0; x < sz && gx0 + x < pw; x += 8) {
                         bool inner;
                         const int fs = lf_unit_edge(job, p, (gx0 + x) >> 3, gy >> 3, 0, inner);
-                        if (fs) lf_edge_full(row_p + x, 1, fs, th);
-                        if (inner && gx0 + x + 4 < pw) lf_edge_full(row_p + x + 4, 1, 4, th);
+                        if (fs) lf_edge_full<T, SH>(row_p + x, 1, fs, th);
+                        if (inner && gx0 + x + 4 < pw) lf_edge_full<T, SH>(row_p + x + 4, 1, 4, th);
                     }
             }
             __syncthreads();
@@ -4297,13 +4336,13 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 const int sz = p ? 32 : 64, pw = p ? CW : W, ph = p ? CH : H;
                 const int gx = (p ? XC : X0) + x, gy0 = p ? YC : Y0;
                 const int pitch = p ? kLfC : kLfY;
-                uint8_t *col_p = p == 0 ? &wy[8 * kLfY + 8 + x] : &wc[p - 1][8 * kLfC + 8 + x];
+                T *col_p = p == 0 ? &wy[8 * kLfY + 8 + x] : &wc[p - 1][8 * kLfC + 8 + x];
                 if (gx < pw)
                     for (int y = 0; y < sz && gy0 + y < ph; y += 8) {
                         bool inner;
                         const int fs = lf_unit_edge(job, p, gx >> 3, (gy0 + y) >> 3, 1, inner);
-                        if (fs) lf_edge_full(col_p + y * pitch, pitch, fs, th);
-                        if (inner && gy0 + y + 4 < ph) lf_edge_full(col_p + (y + 4) * pitch, pitch, 4, th);
+                        if (fs) lf_edge_full<T, SH>(col_p + y * pitch, pitch, fs, th);
+                        if (inner && gy0 + y + 4 < ph) lf_edge_full<T, SH>(col_p + (y + 4) * pitch, pitch, 4, th);
                     }
             }
             __syncthreads();
@@ -4314,8 +4353,8 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 if (r < 8 && w4 < 2) continue;                  /* the corner: untouched */
                 const int gy = Y0 - 8 + r, gx = X0 - 8 + 4 * w4;
                 if (gy >= 0 && gy < H && gx >= 0 && gx < W)
-                    *reinterpret_cast<uint32_t *>(Y + (size_t)gy * W + gx) =
-                        *reinterpret_cast<const uint32_t *>(&wy[r * kLfY + 4 * w4]);
+                    *reinterpret_cast<Q4 *>(Y + (size_t)gy * W + gx) =
+                        *reinterpret_cast<const Q4 *>(&wy[r * kLfY + 4 * w4]);
             }
             for (int i = tid; i < 2 * kLfC * (kLfC / 4); i += 128) {
                 const int pl = i >= kLfC * (kLfC / 4);
@@ -4324,14 +4363,643 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 if (r < 8 && w4 < 2) continue;
                 const int gy = YC - 8 + r, gx = XC - 8 + 4 * w4;
                 if (gy >= 0 && gy < CH && gx >= 0 && gx < CW)
-                    *reinterpret_cast<uint32_t *>((pl ? V : U) + (size_t)gy * CW + gx) =
-                        *reinterpret_cast<const uint32_t *>(&wc[pl][r * kLfC + 4 * w4]);
+                    *reinterpret_cast<Q4 *>((pl ? V : U) + (size_t)gy * CW + gx) =
+                        *reinterpret_cast<const Q4 *>(&wc[pl][r * kLfC + 4 * w4]);
             }
             __syncthreads();
             if (tid == 0) {
                 __threadfence();
                 st_release(prog, (unsigned)(c + 1));
             }
+        }
+    }
+}
+
+/* ── Profile 2 (10-bit 4:2:0): k_hbd_recon ─────────────────────────────
+ *
+ * The FULL profile's reconstruction on 16-bit samples in [0, 1023]. The
+ * frame brings its coefficients dequantised, as int32 (coeffs32, the dense
+ * layout of coeffs; the 32x32 halving already applied): the butterflies run
+ * in 64-bit integers (wl) with 32-bit values between the row and the column
+ * pass, both 8-tap passes of a prediction round and clip to 10 bits, intra
+ * edges that are missing read 511 above and 513 on the left (512 for a DC
+ * with neither), and every residual add clips to [0, 1023]. The loop filter
+ * is k_lf_full<uint16_t, 2>.
+ *
+ * One CTA per superblock ticket (SB-diagonal order over the step's jobs,
+ * persistent, as k_recon). Its inter blocks do not depend on one another or
+ * on other superblocks, so they go first and together: prediction a thread
+ * per column strip of up to 8 rows, then a thread per TX row, then per TX
+ * column. The intra blocks follow in list order, one warp each, TX by TX
+ * (each TX predicted from the reconstructed samples around it). A
+ * superblock whose blocks overlap runs block by block in list order, so
+ * the later block wins as in the reference order. */
+namespace {
+
+constexpr int kHbdThreads = 256, kHbdWarps = kHbdThreads / 32;
+constexpr int kHbdMaxBlocks = 256, kHbdMaxTx = 384;
+constexpr int kHYP = 72, kHCP = 40;      /* tile pitches in samples; column -1 at index 3 */
+constexpr int kHbdMax = 1023, kHbdMid = 512;
+
+struct HbdBlk {
+    uint8_t  x, y;            /* local luma origin in the SB                 */
+    uint8_t  w, h;            /* coded size                                  */
+    uint8_t  cw, ch;          /* luma region (a sub-8x8 block's whole 8x8)
+                               * clamped to the frame                        */
+    uint8_t  ccw, cch;        /* chroma region, clamped                      */
+    uint8_t  txl, flags;      /* tx_size; 1 intra, 2 skip                    */
+    uint8_t  ymode, uvmode;
+    uint8_t  ref0, ref1;
+    int16_t  mvx, mvy, mv1x, mv1y;
+    uint32_t coeff;
+};
+
+struct HbdTx {
+    uint32_t coeff;
+    uint8_t  plane, txl, x, y;   /* plane-local tile position */
+};
+
+struct HbdSmem {
+    uint16_t ty[65 * kHYP];                /* luma tile, row 0 = the row above */
+    uint16_t tc[2][33 * kHCP];
+    int32_t  tmp[64 * 64 + 2 * 32 * 32];   /* row-pass output at tile positions */
+    HbdBlk   blk[kHbdMaxBlocks];
+    HbdTx    tx[kHbdMaxTx];
+    uint16_t tx_base[kHbdMaxTx + 1];       /* prefix over TXs of their sizes   */
+    uint16_t it_base[kHbdMaxBlocks + 1];   /* prefix over blocks of their items */
+    unsigned cell[256];                    /* claims of each 4x4 cell          */
+    uint8_t  txnz[kHbdMaxTx];
+    int32_t  edge[1 + 64 + 32];            /* intra: above[-1..2n-1], left     */
+    int      scan[kHbdWarps];
+    cvp9_job_t jc;
+    int      ticket, ntx;
+};
+
+__device__ __forceinline__ uint16_t &HT(HbdSmem &s, int p, int x, int y)
+{
+    return p == 0 ? s.ty[(y + 1) * kHYP + x + 4] : s.tc[p - 1][(y + 1) * kHCP + x + 4];
+}
+
+__device__ __forceinline__ int32_t *hbd_tmp(HbdSmem &s, int p, int x, int y)
+{
+    return p == 0 ? &s.tmp[y * 64 + x] : &s.tmp[4096 + (p - 1) * 1024 + y * 32 + x];
+}
+
+__device__ __forceinline__ long long clampll(long long v, long long lo, long long hi)
+{
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+/* Exclusive prefix of v over the CTA's threads (thread order); *total: the
+ * sum. Every thread calls it. */
+__device__ int hbd_scan(HbdSmem &s, int v, int *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s.scan[warp] = x;
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kHbdWarps; w++) {
+        const int t = s.scan[w];
+        off += w < warp ? t : 0;
+        tot += t;
+    }
+    *total = tot;
+    __syncthreads();
+    return off + x - v;
+}
+
+/* Largest k in [0, n) with base[k] <= v (base ascending, base[0] = 0). */
+__device__ __forceinline__ int hbd_find(const uint16_t *base, int n, int v)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+/* Prediction items of an inter block: a column strip of up to 8 rows of
+ * one plane. */
+__device__ __forceinline__ int hbd_pred_items(const HbdBlk &b)
+{
+    return (int)b.cw * (((int)b.ch + 7) >> 3) + 2 * (int)b.ccw * (((int)b.cch + 7) >> 3);
+}
+
+/* One column strip of one plane of an inter block: both 8-tap passes (the
+ * frame's filter), each rounded and clipped to 10 bits, every fetch clamped
+ * into the reference plane; a compound block averages its second
+ * prediction in with rounding. A missing first reference predicts 512. */
+__device__ void hbd_pred_strip(HbdSmem &s, const HbdBlk &b, int item, int sbx, int sby)
+{
+    const cvp9_job_t &job = s.jc;
+    const int nl = (int)b.cw * (((int)b.ch + 7) >> 3), nc = (int)b.ccw * (((int)b.cch + 7) >> 3);
+    int p, k;
+    if (item < nl) { p = 0; k = item; }
+    else { p = 1 + (item - nl >= nc); k = item - nl - (p - 1) * nc; }
+    const int cols = p ? b.ccw : b.cw, rows = p ? b.cch : b.ch;
+    const int grp = k / cols, c = k - grp * cols;
+    const int r0 = grp * 8, nr = min(8, rows - r0);
+    const int lx = (p ? (b.x >> 1) : b.x) + c, ly0 = (p ? (b.y >> 1) : b.y) + r0;
+    const int gx = (p ? (sbx >> 1) : sbx) + lx, gy0 = (p ? (sby >> 1) : sby) + ly0;
+    const int (*F)[8] = c_subpel4[job.interp_filter & 3];
+    int out[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = kHbdMid;
+    for (int q = 0; q < 2; q++) {
+        const int rf = q ? b.ref1 : b.ref0;
+        if (q == 1 && rf == 0) break;
+        const cvp9_ref_t &R = job.ref[job.ref_slot_of[clampi(rf - 1, 0, 2)] & 7];
+        if (!R.plane) break;
+        const uint16_t *rp = reinterpret_cast<const uint16_t *>(R.plane);
+        int pw = R.w, ph = R.h;
+        if (p) {
+            rp += (size_t)R.w * R.h;
+            pw = (R.w + 1) >> 1;
+            ph = (R.h + 1) >> 1;
+            if (p == 2) rp += (size_t)pw * ph;
+        }
+        const int mvx = q ? b.mv1x : b.mvx, mvy = q ? b.mv1y : b.mvy;
+        const int X = gx + (p ? (mvx >> 4) : (mvx >> 3)), Y0 = gy0 + (p ? (mvy >> 4) : (mvy >> 3));
+        const int fx = p ? (mvx & 15) : ((mvx & 7) << 1), fy = p ? (mvy & 15) : ((mvy & 7) << 1);
+        int cx[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) cx[t] = clampi(X + t - 3, 0, pw - 1);
+        int h[15];
+#pragma unroll
+        for (int j = 0; j < 15; j++) {
+            h[j] = 0;
+            if (j >= nr + 7) continue;
+            const uint16_t *row = rp + (size_t)clampi(Y0 - 3 + j, 0, ph - 1) * pw;
+            if (fx == 0) {
+                h[j] = __ldg(row + cx[3]);
+            } else {
+                int a = 0;
+#pragma unroll
+                for (int t = 0; t < 8; t++) a += F[fx][t] * (int)__ldg(row + cx[t]);
+                h[j] = clampi((a + 64) >> 7, 0, kHbdMax);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            int v = h[i + 3];
+            if (fy != 0) {
+                int a = 0;
+#pragma unroll
+                for (int t = 0; t < 8; t++) a += F[fy][t] * h[i + t];
+                v = clampi((a + 64) >> 7, 0, kHbdMax);
+            }
+            out[i] = q ? (out[i] + v + 1) >> 1 : v;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if (i < nr) HT(s, p, lx, ly0 + i) = (uint16_t)out[i];
+}
+
+/* The TX layout of one plane of a block (as plane_layout). */
+__device__ __forceinline__ void hbd_plane_layout(const HbdBlk &b, const cvp9_job_t &job, int gx, int gy, int p,
+                                                 int &tx, int &nx, int &ny, int &pbw)
+{
+    const int sub8 = b.w < 8 || b.h < 8;
+    const int ew = sub8 ? 8 : b.w, eh = sub8 ? 8 : b.h;
+    const int ss = p > 0;
+    int pw = ss ? ew / 2 : ew, ph = ss ? eh / 2 : eh;
+    pw = pw < 4 ? 4 : pw;
+    ph = ph < 4 ? 4 : ph;
+    tx = b.txl;
+    if (ss) { const int mt = max_tx_for(pw, ph); tx = sub8 ? 0 : (tx > mt ? mt : tx); }
+    const int t4 = 1 << tx;
+    const int o4x = ((gx >> 3) * 2) >> ss, o4y = ((gy >> 3) * 2) >> ss;
+    int mw = pw / 4, mh = ph / 4;
+    const int lim_w = ((job.mi_cols * 2) >> ss) - o4x, lim_h = ((job.mi_rows * 2) >> ss) - o4y;
+    if (mw > lim_w) mw = lim_w;
+    if (mh > lim_h) mh = lim_h;
+    nx = mw > 0 ? (mw + t4 - 1) / t4 : 0;
+    ny = mh > 0 ? (mh + t4 - 1) / t4 : 0;
+    pbw = pw;
+}
+
+/* Residual TXs of an inter block in coefficient order (planes, then raster),
+ * written from s.tx[at] when `at` >= 0; returns their count. The running
+ * offset stops at num_coeffs: a TX that does not fit and every later one of
+ * the block are dropped. */
+__device__ int hbd_block_txs(HbdSmem &s, const HbdBlk &b, int sbx, int sby, int at)
+{
+    if ((b.flags & 2) || b.txl > 3) return 0;
+    const cvp9_job_t &job = s.jc;
+    const int gx = sbx + b.x, gy = sby + b.y;
+    uint64_t off = b.coeff;
+    int n = 0;
+    for (int p = 0; p < 3; p++) {
+        int txl, nx, ny, pbw;
+        hbd_plane_layout(b, job, gx, gy, p, txl, nx, ny, pbw);
+        const int sz = 16 << (2 * txl), ts = 4 << txl;
+        const int ox = p ? (b.x >> 1) : b.x, oy = p ? (b.y >> 1) : b.y;
+        for (int ty = 0; ty < ny; ty++)
+            for (int tx = 0; tx < nx; tx++) {
+                if (off + (uint64_t)sz > (uint64_t)job.num_coeffs) { off = job.num_coeffs; continue; }
+                if (at >= 0 && at + n < kHbdMaxTx) {
+                    HbdTx &t = s.tx[at + n];
+                    t.coeff = (uint32_t)off;
+                    t.plane = (uint8_t)p;
+                    t.txl = (uint8_t)txl;
+                    t.x = (uint8_t)(ox + tx * ts);
+                    t.y = (uint8_t)(oy + ty * ts);
+                }
+                off += (uint64_t)sz;
+                n++;
+            }
+    }
+    return n;
+}
+
+/* Row pass of TX row i: the frame's dequantised coefficients through the
+ * 1-D inverse (DCT, ADST along the row when row_adst, WHT when lossless),
+ * 64-bit inside, 32-bit out into the temp rows. Returns whether the row had
+ * a nonzero coefficient. */
+template <int N>
+__device__ __forceinline__ bool hbd_row(HbdSmem &s, const int32_t *X, int i, int p, int px0, int py0,
+                                        bool lossless, bool row_adst)
+{
+    wl v[N];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const int c = __ldg(X + i * N + k);
+        any |= c != 0;
+        v[k] = wl(c);
+    }
+    if (any) {
+        if (N == 4 && lossless) iwht4(v, true);
+        else itx1<N>(v, row_adst);
+    }
+    int32_t *d = hbd_tmp(s, p, px0, py0 + i);
+#pragma unroll
+    for (int k = 0; k < N; k++) d[k] = any ? (int32_t)v[k].v : 0;
+    return any;
+}
+
+/* Column pass of TX column j: the 1-D inverse down the column (64-bit),
+ * rounding shift 4/5/6/6 (none after the WHT), add and clip to 10 bits. */
+template <int N>
+__device__ __forceinline__ void hbd_col(HbdSmem &s, int j, int p, int px0, int py0, bool lossless, bool col_adst)
+{
+    wl v[N];
+#pragma unroll
+    for (int k = 0; k < N; k++) v[k] = wl(*hbd_tmp(s, p, px0 + j, py0 + k));
+    const bool wht = N == 4 && lossless;
+    if (wht) iwht4(v, false);
+    else itx1<N>(v, col_adst);
+    const int sh = N == 4 ? 4 : (N == 8 ? 5 : 6);
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const long long r = wht ? v[k].v : (v[k].v + (1ll << (sh - 1))) >> sh;
+        uint16_t &px = HT(s, p, px0 + j, py0 + k);
+        px = (uint16_t)clampll((long long)px + r, 0, kHbdMax);
+    }
+}
+
+__device__ __forceinline__ void hbd_row_n(HbdSmem &s, int txl, const int32_t *X, int i, int p, int x, int y,
+                                          bool lossless, bool row_adst, bool &any)
+{
+    switch (txl) {
+    case 0: any = hbd_row<4>(s, X, i, p, x, y, lossless, row_adst); break;
+    case 1: any = hbd_row<8>(s, X, i, p, x, y, lossless, row_adst); break;
+    case 2: any = hbd_row<16>(s, X, i, p, x, y, lossless, row_adst); break;
+    default: any = hbd_row<32>(s, X, i, p, x, y, lossless, false); break;
+    }
+}
+
+__device__ __forceinline__ void hbd_col_n(HbdSmem &s, int txl, int j, int p, int x, int y, bool lossless,
+                                          bool col_adst)
+{
+    switch (txl) {
+    case 0: hbd_col<4>(s, j, p, x, y, lossless, col_adst); break;
+    case 1: hbd_col<8>(s, j, p, x, y, lossless, col_adst); break;
+    case 2: hbd_col<16>(s, j, p, x, y, lossless, col_adst); break;
+    default: hbd_col<32>(s, j, p, x, y, lossless, false); break;
+    }
+}
+
+/* Inter blocks [lo, hi) of the SB, whole CTA: predictions, then the TX rows,
+ * then the TX columns of their residuals. */
+__device__ void hbd_inter_blocks(HbdSmem &s, int lo, int hi, int nb, int sbx, int sby)
+{
+    const int tid = threadIdx.x;
+    const cvp9_job_t &job = s.jc;
+    const bool mine = tid >= lo && tid < hi && tid < nb && !(s.blk[tid].flags & 1);
+    int total;
+    /* 1. predictions */
+    int cnt = mine ? hbd_pred_items(s.blk[tid]) : 0;
+    int base = hbd_scan(s, cnt, &total);
+    if (tid < kHbdMaxBlocks) s.it_base[tid] = (uint16_t)min(base, 0xFFFF);
+    __syncthreads();
+    for (int it = tid; it < total; it += kHbdThreads) {
+        const int bi = hbd_find(s.it_base, nb, it);
+        hbd_pred_strip(s, s.blk[bi], it - s.it_base[bi], sbx, sby);
+    }
+    /* 2. the residual TXs, a thread per block listing its own */
+    cnt = mine ? hbd_block_txs(s, s.blk[tid], sbx, sby, -1) : 0;
+    base = hbd_scan(s, cnt, &total);
+    if (total > kHbdMaxTx) {
+        if (tid == 0) atomicOr(job.status, (unsigned)CVP9_JOB_TOO_MANY);
+        total = kHbdMaxTx;
+    }
+    if (mine && cnt) hbd_block_txs(s, s.blk[tid], sbx, sby, base);
+    __syncthreads();
+    const int ntx = total;
+    /* prefix over TXs of their edge length (their rows, and columns), two
+     * consecutive TXs a thread */
+    {
+        const int t0 = 2 * tid, t1 = 2 * tid + 1;
+        const int a = t0 < ntx ? 4 << s.tx[t0].txl : 0, c = t1 < ntx ? 4 << s.tx[t1].txl : 0;
+        int nrow_all;
+        const int b0 = hbd_scan(s, a + c, &nrow_all);
+        if (t0 <= ntx) s.tx_base[t0] = (uint16_t)b0;
+        if (t1 <= ntx) s.tx_base[t1] = (uint16_t)(b0 + a);
+        if (t0 < ntx) s.txnz[t0] = 0;
+        if (t1 < ntx) s.txnz[t1] = 0;
+    }
+    if (ntx > 0) {
+        __syncthreads();
+        const int nrow = s.tx_base[ntx];
+        for (int it = tid; it < nrow; it += kHbdThreads) {
+            const int t = hbd_find(s.tx_base, ntx, it);
+            const HbdTx &x = s.tx[t];
+            bool any;
+            hbd_row_n(s, x.txl, job.coeffs32 + x.coeff, it - s.tx_base[t], x.plane, x.x, x.y, job.lossless, false,
+                      any);
+            if (any) s.txnz[t] = 1;
+        }
+        __syncthreads();
+        for (int it = tid; it < nrow; it += kHbdThreads) {
+            const int t = hbd_find(s.tx_base, ntx, it);
+            const HbdTx &x = s.tx[t];
+            if (s.txnz[t]) hbd_col_n(s, x.txl, it - s.tx_base[t], x.plane, x.x, x.y, job.lossless, false);
+        }
+    }
+    __syncthreads();
+}
+
+/* Intra prediction of one n x n TX of plane p (tile position lx, ly; plane
+ * position X0, Y0 in a pw x ph plane) by one warp, the FULL edge rules at 10
+ * bits: 511 above and 513 on the left when unavailable, above-right only for
+ * a 4x4 TX with have_right, samples past the plane's edge repeating the
+ * last one inside. */
+__device__ void hbd_intra_tx(HbdSmem &s, int p, int lx, int ly, int X0, int Y0, int pw, int ph, int n, int mode,
+                             bool have_top, bool have_left, bool have_right, int lane)
+{
+    int32_t *above = s.edge + 1, *left = s.edge + 65;
+    if (have_top) {
+        const int want = n + ((n == 4 && have_right) ? 4 : 0);
+        const int cnt = min(want, pw - X0);
+        for (int i = lane; i < 2 * n; i += 32) above[i] = HT(s, p, lx + (i < cnt ? i : cnt - 1), ly - 1);
+        if (lane == 0) above[-1] = have_left ? HT(s, p, lx - 1, ly - 1) : kHbdMid + 1;
+    } else {
+        for (int i = lane; i < 2 * n + 1; i += 32) s.edge[i] = kHbdMid - 1;
+    }
+    for (int i = lane; i < n; i += 32) left[i] = have_left ? HT(s, p, lx - 1, ly + min(i, ph - 1 - Y0)) : kHbdMid + 1;
+    __syncwarp();
+    int dc = kHbdMid;
+    if (mode == 0) {
+        const unsigned sa = __reduce_add_sync(0xffffffffu, lane < n ? (unsigned)above[lane] : 0u);
+        const unsigned sl = __reduce_add_sync(0xffffffffu, lane < n ? (unsigned)left[lane] : 0u);
+        if (have_top && have_left) dc = (int)((sa + sl + (unsigned)n) / (unsigned)(2 * n));
+        else if (have_top) dc = (int)((sa + (unsigned)n / 2) / (unsigned)n);
+        else if (have_left) dc = (int)((sl + (unsigned)n / 2) / (unsigned)n);
+    }
+    const int lg = n == 4 ? 2 : n == 8 ? 3 : n == 16 ? 4 : 5;
+    for (int idx = lane; idx < n * n; idx += 32) {
+        const int r = idx >> lg, c = idx & (n - 1);
+        HT(s, p, lx + c, ly + r) = (uint16_t)full_pred<kHbdMax>(mode, r, c, n, above, left, dc);
+    }
+    __syncwarp();
+}
+
+/* One intra block by warp 0: each plane's TXs in raster order, each
+ * predicted and given its residual before the next. */
+__device__ void hbd_intra_block(HbdSmem &s, const HbdBlk &b, int sbx, int sby, int lane)
+{
+    const cvp9_job_t &job = s.jc;
+    const int gx = sbx + b.x, gy = sby + b.y;
+    const int mi_col = gx >> 3, mi_row = gy >> 3;
+    const bool left_ok = mi_col > full_tile_start(mi_col, job.mi_cols, job.log2_tile_cols);
+    const bool resid = !(b.flags & 2) && b.txl <= 3;
+    uint64_t off = b.coeff;
+    for (int p = 0; p < 3; p++) {
+        int txl, nx, ny, pbw;
+        hbd_plane_layout(b, job, gx, gy, p, txl, nx, ny, pbw);
+        const int n = 4 << txl, sz = n * n;
+        const int mode = p ? (b.uvmode > 9 ? 0 : b.uvmode) : (b.ymode > 9 ? 0 : b.ymode);
+        const int tx_type = (p == 0 && !job.lossless && txl < 3 && b.ymode < 10) ? c_tx_type[b.ymode] : 0;
+        const int pw = p ? job.CW : job.W, ph = p ? job.CH : job.H;
+        const int ox = p ? (b.x >> 1) : b.x, oy = p ? (b.y >> 1) : b.y;
+        const int gox = p ? (gx >> 1) : gx, goy = p ? (gy >> 1) : gy;
+        for (int ty = 0; ty < ny; ty++)
+            for (int tx = 0; tx < nx; tx++) {
+                const int lx = ox + tx * n, ly = oy + ty * n;
+                hbd_intra_tx(s, p, lx, ly, gox + tx * n, goy + ty * n, pw, ph, n, mode, ty > 0 || mi_row > 0,
+                             tx > 0 || left_ok, (tx + 1) * n < pbw, lane);
+                if (!resid) continue;
+                if (off + (uint64_t)sz > (uint64_t)job.num_coeffs) { off = job.num_coeffs; continue; }
+                const int32_t *X = job.coeffs32 + off;
+                off += (uint64_t)sz;
+                bool any = false;
+                if (lane < n) hbd_row_n(s, txl, X, lane, p, lx, ly, job.lossless, tx_type == 2 || tx_type == 3, any);
+                any = __any_sync(0xffffffffu, any);
+                __syncwarp();
+                if (any && lane < n) hbd_col_n(s, txl, lane, p, lx, ly, job.lossless, tx_type == 1 || tx_type == 3);
+                __syncwarp();
+            }
+    }
+}
+
+} /* namespace */
+
+__global__ void __launch_bounds__(kHbdThreads, 2) k_hbd_recon(const cvp9_job_t *__restrict__ jobs,
+                                                              const uint32_t *__restrict__ tickets,
+                                                              uint32_t n_tickets, uint32_t *ticket_counter)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    HbdSmem &s = *reinterpret_cast<HbdSmem *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const cvp9_job_t &job = s.jc;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s.ticket = (int)atomicAdd(ticket_counter, 1u);
+        __syncthreads();
+        const int ticket = s.ticket;
+        if (ticket >= (int)n_tickets) return;
+        const uint32_t code = tickets[ticket];
+        const cvp9_job_t *gj = jobs + (code >> 20);
+        {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(gj);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&s.jc);
+            for (int i = tid; i < (int)(sizeof(cvp9_job_t) / 4); i += kHbdThreads) dst[i] = src[i];
+        }
+        const int sb = (int)(code & 0xFFFFFu);
+        const int g_sb_cols = gj->sb_cols;
+        const int sbr = sb / g_sb_cols, sbc = sb - sbr * g_sb_cols;
+        const int sbx = sbc * 64, sby = sbr * 64;
+        const uint32_t *rg = gj->sb_range + 4 * sb;
+        const uint32_t start = rg[0], end = rg[1], groups = rg[2];
+        const bool layout_bad = (*(volatile uint32_t *)gj->status & CVP9_JOB_BAD_BLOCK) != 0;
+        const bool bad = groups > 1 || end < start || end > gj->num_blocks ||
+                         (groups && end - start > (uint32_t)kHbdMaxBlocks);
+        int nb = (groups && !bad && !layout_bad) ? (int)(end - start) : 0;
+        /* the tile at 512, no cell claimed */
+        for (int i = tid; i < 65 * kHYP; i += kHbdThreads) s.ty[i] = kHbdMid;
+        for (int i = tid; i < 2 * 33 * kHCP; i += kHbdThreads) (&s.tc[0][0])[i] = kHbdMid;
+        for (int i = tid; i < 256; i += kHbdThreads) s.cell[i] = 0;
+        __syncthreads();
+
+        /* 1. blocks (each inside this SB, 4-aligned, 4..64 px, tx_size <= 3,
+         * sub-8x8 ones on the 8x8 grid), and the 4x4 cells they write */
+        bool my_intra = false, my_bad = false;
+        if (tid < nb) {
+            const vp9_macroblock_info_t g = job.blocks[start + tid];
+            const int lx = (int)g.x - sbx, ly = (int)g.y - sby;
+            const bool sub8 = g.width < 8 || g.height < 8;
+            const int bw = sub8 ? 8 : g.width, bh = sub8 ? 8 : g.height;
+            /* ... and a transform no larger than the block */
+            my_bad = lx < 0 || ly < 0 || (lx & 3) || (ly & 3) || (g.width & 3) || (g.height & 3) || g.width < 4 ||
+                     g.height < 4 || lx + g.width > 64 || ly + g.height > 64 || g.x >= job.W || g.y >= job.H ||
+                     g.tx_size > 3 || (sub8 && ((lx & 7) || (ly & 7))) || (4 << g.tx_size) > min(bw, bh);
+            HbdBlk b;
+            b.x = (uint8_t)(my_bad ? 0 : lx);
+            b.y = (uint8_t)(my_bad ? 0 : ly);
+            b.w = g.width;
+            b.h = g.height;
+            b.cw = (uint8_t)max(0, min(bw, job.W - (int)g.x));
+            b.ch = (uint8_t)max(0, min(bh, job.H - (int)g.y));
+            b.ccw = (uint8_t)max(0, min(max(bw / 2, 4), job.CW - (int)g.x / 2));
+            b.cch = (uint8_t)max(0, min(max(bh / 2, 4), job.CH - (int)g.y / 2));
+            b.txl = g.tx_size;
+            b.flags = (uint8_t)((g.is_intra ? 1 : 0) | (g.skip ? 2 : 0));
+            b.ymode = g.y_mode;
+            b.uvmode = g.uv_mode;
+            b.ref0 = g.ref_frame[0];
+            b.ref1 = g.is_intra ? 0 : g.ref_frame[1];
+            b.mvx = g.mv[0][0];
+            b.mvy = g.mv[0][1];
+            b.mv1x = g.mv[1][0];
+            b.mv1y = g.mv[1][1];
+            b.coeff = g.coeff_offset;
+            s.blk[tid] = b;
+            my_intra = g.is_intra != 0;
+        }
+        if (__syncthreads_or(my_bad)) {
+            if (tid == 0) atomicOr(job.status, (unsigned)CVP9_JOB_BAD_BLOCK);
+            nb = 0;
+            my_intra = false;
+        }
+        if (tid < nb) {
+            /* cells of the luma region a block writes (a sub-8x8 block its 8x8) */
+            const HbdBlk &b = s.blk[tid];
+            for (int cy = b.y >> 2; cy < min(16, (b.y + b.ch + 3) >> 2); cy++)
+                for (int cx = b.x >> 2; cx < min(16, (b.x + b.cw + 3) >> 2); cx++) atomicAdd(&s.cell[cy * 16 + cx], 1u);
+        }
+        __syncthreads();
+        bool my_over = false;
+        for (int i = tid; i < 256; i += kHbdThreads) my_over |= s.cell[i] > 1;
+        const bool overlap = __syncthreads_or(my_over) != 0;
+        const bool any_intra = __syncthreads_or(my_intra) != 0;
+
+        /* 2. intra blocks read the neighbour SBs' samples: wait for them,
+         * then load the row above (x = -1..63) and the column to the left */
+        if (any_intra) {
+            if (tid == 0) {
+                bool ok = true;
+                if (sbc > 0) ok &= wait_flag(job.sb_done + sb - 1, job.epoch);
+                if (sbr > 0) ok &= wait_flag(job.sb_done + sb - job.sb_cols, job.epoch);
+                if (sbr > 0 && sbc > 0) ok &= wait_flag(job.sb_done + sb - job.sb_cols - 1, job.epoch);
+                if (!ok) atomicOr(job.status, (unsigned)CVP9_JOB_TIMEOUT);
+            }
+            __syncthreads();
+            const uint16_t *Y = reinterpret_cast<const uint16_t *>(job.out);
+            const uint16_t *U = Y + (size_t)job.W * job.H;
+            const uint16_t *V = U + (size_t)job.CW * job.CH;
+            if (sby > 0) {
+                for (int i = tid - 1; i < 64; i += kHbdThreads) {
+                    const int gx = sbx + i;
+                    if (gx >= 0 && gx < job.W) HT(s, 0, i, -1) = __ldcg(Y + (size_t)(sby - 1) * job.W + gx);
+                }
+                for (int i = tid - 1; i < 32; i += kHbdThreads) {
+                    const int gx = (sbx >> 1) + i;
+                    if (gx >= 0 && gx < job.CW) {
+                        HT(s, 1, i, -1) = __ldcg(U + (size_t)((sby >> 1) - 1) * job.CW + gx);
+                        HT(s, 2, i, -1) = __ldcg(V + (size_t)((sby >> 1) - 1) * job.CW + gx);
+                    }
+                }
+            }
+            if (sbx > 0) {
+                for (int i = tid; i < 64; i += kHbdThreads) {
+                    const int gy = sby + i;
+                    if (gy < job.H) HT(s, 0, -1, i) = __ldcg(Y + (size_t)gy * job.W + sbx - 1);
+                }
+                for (int i = tid; i < 32; i += kHbdThreads) {
+                    const int gy = (sby >> 1) + i;
+                    if (gy < job.CH) {
+                        HT(s, 1, -1, i) = __ldcg(U + (size_t)gy * job.CW + (sbx >> 1) - 1);
+                        HT(s, 2, -1, i) = __ldcg(V + (size_t)gy * job.CW + (sbx >> 1) - 1);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        /* 3. reconstruct: inter blocks together, then intra blocks in order;
+         * overlapping blocks one by one in list order */
+        if (!overlap) {
+            hbd_inter_blocks(s, 0, nb, nb, sbx, sby);
+            if (any_intra)
+                for (int i = 0; i < nb; i++) {
+                    if (!(s.blk[i].flags & 1)) continue;
+                    if (warp == 0) hbd_intra_block(s, s.blk[i], sbx, sby, lane);
+                    __syncthreads();
+                }
+        } else {
+            for (int i = 0; i < nb; i++) {
+                if (s.blk[i].flags & 1) {
+                    if (warp == 0) hbd_intra_block(s, s.blk[i], sbx, sby, lane);
+                    __syncthreads();
+                } else {
+                    hbd_inter_blocks(s, i, i + 1, nb, sbx, sby);
+                }
+            }
+        }
+
+        /* 4. write the tile (clipped to the frame) and release the SB */
+        {
+            uint16_t *Y = reinterpret_cast<uint16_t *>(job.out);
+            uint16_t *U = Y + (size_t)job.W * job.H;
+            uint16_t *V = U + (size_t)job.CW * job.CH;
+            const int vw = min(64, job.W - sbx), vh = min(64, job.H - sby);
+            for (int i = tid; i < 64 * 64; i += kHbdThreads) {
+                const int r = i >> 6, c = i & 63;
+                if (r < vh && c < vw) Y[(size_t)(sby + r) * job.W + sbx + c] = HT(s, 0, c, r);
+            }
+            const int cvw = min(32, job.CW - (sbx >> 1)), cvh = min(32, job.CH - (sby >> 1));
+            for (int i = tid; i < 2 * 32 * 32; i += kHbdThreads) {
+                const int p = i >> 10, k = i & 1023, r = k >> 5, c = k & 31;
+                if (r < cvh && c < cvw) (p ? V : U)[(size_t)((sby >> 1) + r) * job.CW + (sbx >> 1) + c] = HT(s, 1 + p, c, r);
+            }
+        }
+        if (tid == 0 && bad)
+            atomicOr(job.status, (unsigned)CVP9_JOB_BAD_ORDER |
+                                 ((groups && end >= start && end - start > (uint32_t)kHbdMaxBlocks) ? (unsigned)CVP9_JOB_TOO_MANY : 0u));
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(job.sb_done + sb, job.epoch);
         }
     }
 }
@@ -4574,6 +5242,9 @@ int cvp9k_configure(void)
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_REFCPU, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_SPEC, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_inter<CVP9_ARITH_SPEC, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (cudaFuncSetAttribute(k_hbd_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(HbdSmem)) != cudaSuccess)
+        return -1;
+    cudaFuncSetAttribute(k_hbd_recon, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     /* Load every kernel the launcher can pick now. With lazy module loading
      * (the CUDA 12 default) a kernel's code is loaded at its first launch,
      * which stalls the device for tens of milliseconds; the tuner's first
@@ -4591,13 +5262,13 @@ int cvp9k_configure(void)
         (const void *)k_resid<CVP9_ARITH_REFCPU, kResidMinB, false>,
         (const void *)k_resid<CVP9_ARITH_REFCPU, kResid8MinB, true, 1>,
         (const void *)k_resid<CVP9_ARITH_REFCPU, kResidMinB, true, 2>,
-        (const void *)k_lf_full, (const void *)k_nv12_pack,
+        (const void *)k_lf_full<uint8_t, 0>, (const void *)k_nv12_pack,
         (const void *)k_loopfilter<CVP9_ARITH_SPEC, 32>, (const void *)k_loopfilter<CVP9_ARITH_REFCPU, 32>,
         (const void *)k_loopfilter<CVP9_ARITH_SPEC, 64>, (const void *)k_loopfilter<CVP9_ARITH_REFCPU, 64>,
         (const void *)k_lf_strip<CVP9_ARITH_SPEC>, (const void *)k_lf_strip<CVP9_ARITH_REFCPU>,
         (const void *)k_lf_flat_h, (const void *)k_lf_flat_v,
         (const void *)k_gather_luma, (const void *)k_scatter_coeffs, (const void *)k_unpack_coeffs,
-        (const void *)k_collect,
+        (const void *)k_collect, (const void *)k_hbd_recon, (const void *)k_lf_full<uint16_t, 2>,
     };
     for (size_t i = 0; i < sizeof(fns) / sizeof(fns[0]); i++) {
         cudaFuncAttributes fa;
@@ -4606,10 +5277,17 @@ int cvp9k_configure(void)
     return 0;
 }
 
+int cvp9k_hbd_ctas_per_sm(void)
+{
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_hbd_recon, kHbdThreads, sizeof(HbdSmem)) == cudaSuccess
+        ? n : -1;
+}
+
 int cvp9k_lf_full_ctas_per_sm(void)
 {
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lf_full, 128, 0) == cudaSuccess ? n : -1;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lf_full<uint8_t, 0>, 128, 0) == cudaSuccess ? n : -1;
 }
 
 int cvp9k_recon_ctas_per_sm(int arith)
@@ -4636,6 +5314,30 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
     if (e != cudaSuccess) return (int)e;
     const bool capturing = cap == cudaStreamCaptureStatusActive;
     if ((e = mark(L->ev[0], st, capturing)) != cudaSuccess) return (int)e;
+    if (L->hbd) {
+        /* profile 2: scan, mode-info map, k_hbd_recon, the 10-bit VP9 filter */
+        if (L->max_blocks > 0) {
+            dim3 g((unsigned)((L->max_blocks + 255) / 256), (unsigned)L->njobs);
+            k_scan_blocks<<<g, 256, 0, st>>>(L->jobs);
+            k_lf_mimap<<<g, 256, 0, st>>>(L->jobs);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+        if ((e = mark(L->ev[1], st, capturing)) != cudaSuccess) return (int)e;
+        if (L->n_tickets > 0) {
+            int grid = L->recon_ctas > 0 ? L->recon_ctas : (int)L->n_tickets;
+            if (grid > (int)L->n_tickets) grid = (int)L->n_tickets;
+            k_hbd_recon<<<grid, kHbdThreads, sizeof(HbdSmem), st>>>(L->jobs, L->tickets, L->n_tickets,
+                                                                    L->ticket_counter);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+        if ((e = mark(L->ev[2], st, capturing)) != cudaSuccess) return (int)e;
+        if (L->lf_tickets > 0 && L->lf_counter) {
+            const int grid = L->lf_ctas > 0 && L->lf_ctas < (int)L->lf_tickets ? L->lf_ctas : (int)L->lf_tickets;
+            k_lf_full<uint16_t, 2><<<grid, 128, 0, st>>>(L->jobs, L->njobs, L->lf_tickets, L->lf_counter);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+        return (int)mark(L->ev[3], st, capturing);
+    }
     if (L->max_blocks > 0 || L->scan_ctas > 0) {
         int gx = L->scan_ctas > 0 ? L->scan_ctas : (L->max_blocks + 255) / 256;
         dim3 g((unsigned)gx, (unsigned)L->njobs);
@@ -4709,7 +5411,7 @@ int cvp9k_launch_frame(const cvp9k_launch_t *L, cudaStream_t st)
     if (L->full) {
         if (L->lf_tickets > 0 && L->lf_counter) {
             const int grid = L->lf_ctas > 0 && L->lf_ctas < (int)L->lf_tickets ? L->lf_ctas : (int)L->lf_tickets;
-            k_lf_full<<<grid, 128, 0, st>>>(L->jobs, L->njobs, L->lf_tickets, L->lf_counter);
+            k_lf_full<uint8_t, 0><<<grid, 128, 0, st>>>(L->jobs, L->njobs, L->lf_tickets, L->lf_counter);
         }
         if (L->full_nv12_max_px > 0) {
             long long n = L->full_nv12_max_px;

@@ -77,6 +77,10 @@ typedef struct {
     uint8_t *dl;                    /* the step's contiguous output staging
                                      * (device): k_collect copies `out` here;
                                      * NULL: no download                           */
+    /* profile 2 (10-bit, k_hbd_recon): out and the reference planes hold
+     * uint16 samples in the same I420 layout; coeffs32 the dequantised
+     * coefficients (num_coeffs of them, the dense layout of coeffs) */
+    const int32_t *coeffs32;
 } cvp9_job_t;
 
 #ifdef __cplusplus

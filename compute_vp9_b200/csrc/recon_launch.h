@@ -48,6 +48,10 @@ typedef struct {
     uint32_t         lf_tickets;   /* njobs * (most superblock rows of a job)    */
     int              lf_ctas;      /* grid of k_lf_full                          */
     int              full_nv12_max_px;  /* > 0: largest W*H of a job with a target */
+    /* Profile 2 (10-bit): jobs with coeffs32 and 16-bit planes through
+     * k_scan_blocks, k_lf_mimap, k_hbd_recon (tickets, recon_ctas) and
+     * k_lf_full<uint16_t> (lf_* as for FULL); nothing else runs. */
+    int              hbd;
     cudaEvent_t      ev[4];        /* optional: before scan, recon, filter; after */
 } cvp9k_launch_t;
 
@@ -57,6 +61,8 @@ int    cvp9k_configure(void);
 int    cvp9k_recon_ctas_per_sm(int arith);
 /* CTAs of k_lf_full (128 threads, static shared memory) resident per SM. */
 int    cvp9k_lf_full_ctas_per_sm(void);
+/* CTAs of k_hbd_recon resident per SM. */
+int    cvp9k_hbd_ctas_per_sm(void);
 /* REFCPU upload of the coefficients the reconstruction reads — each block's
  * luma TXs — straight from page-locked host memory into jobs[j].coeffs, for
  * every job with coeffs_src set; adds the bytes moved to *bytes (device).

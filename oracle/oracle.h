@@ -121,6 +121,29 @@ void             oracle_stream_destroy(oracle_stream_t *s);
 int              oracle_stream_decode(oracle_stream_t *s, const vp9_parsed_frame_t *pf,
                                       uint8_t *out_i420);
 
+/* ── Profile 2 (10-bit, oracle_hbd.c): frames of uint16 samples held in
+ * oracle_frame_t (plane pointers cast), coefficients dequantised int32 ── */
+
+int  oracle_hbd_reconstruct(const vp9_parsed_frame_t *pf, const int32_t *coeffs,
+                            const oracle_frame_t *const pool[8], oracle_frame_t *out);
+/* one 1-D inverse (DCT, or ADST for n < 32 when adst), 64-bit */
+void oracle_hbd_itx1d(int n, int adst, const int64_t *in, int64_t *out);
+/* residual of one n x n TX (tx_type as oracle_full_itx2d) */
+void oracle_hbd_itx2d(const int32_t *in, int64_t *out, int n, int tx_type, int lossless);
+void oracle_hbd_mc_block(const uint16_t *ref0, const uint16_t *ref1, int rw, int rh, int rstride,
+                         uint16_t *dst, int dw, int dh, int dstride, int x, int y, int bw, int bh,
+                         int mv0x, int mv0y, int mv1x, int mv1y, int compound, int filter, int chroma);
+void oracle_hbd_intra_tx(uint16_t *plane, int pw, int ph, int stride, int x0, int y0, int n,
+                         int mode, int have_top, int have_left, int have_right);
+
+typedef struct oracle_hbd_stream oracle_hbd_stream_t;
+oracle_hbd_stream_t *oracle_hbd_stream_create(void);
+void                 oracle_hbd_stream_destroy(oracle_hbd_stream_t *s);
+/* One frame and the pool update (refresh_frame_flags, 0 meaning slot 0);
+ * the frame (w*h + 2*cw*ch samples) to out_i420 when non-NULL. */
+int                  oracle_hbd_stream_decode(oracle_hbd_stream_t *s, const vp9_parsed_frame_t *pf,
+                                              const int32_t *coeffs, uint16_t *out_i420);
+
 /* 8-bit DC/AC quantiser lookups (src/decoder/vp9_dequant.h:12-75). */
 int oracle_dc_quant(int qindex);
 int oracle_ac_quant(int qindex);

@@ -62,6 +62,21 @@ def oracle_lib():
         lib.oracle_full_mc_block.restype = None
         lib.oracle_full_intra_tx.argtypes = [C.c_void_p] + [C.c_int] * 10
         lib.oracle_full_intra_tx.restype = None
+        lib.oracle_hbd_stream_create.restype = C.c_void_p
+        lib.oracle_hbd_stream_destroy.argtypes = [C.c_void_p]
+        lib.oracle_hbd_stream_destroy.restype = None
+        lib.oracle_hbd_stream_decode.argtypes = [C.c_void_p, C.POINTER(ParsedFrame), C.c_void_p, C.c_void_p]
+        lib.oracle_hbd_itx1d.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        lib.oracle_hbd_itx1d.restype = None
+        lib.oracle_hbd_itx2d.argtypes = [C.c_void_p, C.c_void_p] + [C.c_int] * 3
+        lib.oracle_hbd_itx2d.restype = None
+        lib.oracle_hbd_intra_tx.argtypes = [C.c_void_p] + [C.c_int] * 10
+        lib.oracle_hbd_intra_tx.restype = None
+        lib.oracle_hbd_mc_block.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p] + \
+            [C.c_int] * 14
+        lib.oracle_hbd_mc_block.restype = None
+        lib.oracle_idct1d.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        lib.oracle_idct1d.restype = None
         lib.oracle_dc_quant.argtypes = [C.c_int]
         lib.oracle_ac_quant.argtypes = [C.c_int]
         _orc = lib
@@ -216,4 +231,68 @@ def full_mc_block(ref0, ref1, dst_shape, x, y, bw, bh, mv0, mv1=(0, 0), compound
     oracle_lib().oracle_full_mc_block(r0.ctypes.data, r1.ctypes.data, r0.shape[1], r0.shape[0], r0.shape[1],
                                       d.ctypes.data, d.shape[1], d.shape[0], d.shape[1], x, y, bw, bh,
                                       mv0[0], mv0[1], mv1[0], mv1[1], compound, filt, chroma)
+    return d
+
+
+class HbdOracleStream:
+    """The 10-bit restatement (oracle_hbd.c) + its reference pool."""
+
+    def __init__(self):
+        self._lib = oracle_lib()
+        self._h = self._lib.oracle_hbd_stream_create()
+
+    def decode(self, pf, coeffs32):
+        w, h = pf.contents.hdr.width, pf.contents.hdr.height
+        out = np.empty(_i420_size(w, h), np.uint16)
+        c = np.ascontiguousarray(coeffs32, np.int32)
+        if not self._lib.oracle_hbd_stream_decode(self._h, pf, c.ctypes.data, out.ctypes.data):
+            raise RuntimeError("oracle 10-bit decode failed")
+        return out
+
+    def close(self):
+        if self._h:
+            self._lib.oracle_hbd_stream_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def hbd_itx1d(vec, adst=0):
+    x = np.ascontiguousarray(vec, np.int64)
+    out = np.empty_like(x)
+    oracle_lib().oracle_hbd_itx1d(len(x), adst, x.ctypes.data, out.ctypes.data)
+    return out
+
+
+def idct1d(vec):
+    """The shader profiles' 32-bit 1-D inverse DCT (oracle_spec.c)."""
+    x = np.ascontiguousarray(vec, np.int32)
+    out = np.empty_like(x)
+    oracle_lib().oracle_idct1d(len(x), x.ctypes.data, out.ctypes.data)
+    return out
+
+
+def hbd_itx2d(coeffs, tx_type=0, lossless=0):
+    n = coeffs.shape[0]
+    x = np.ascontiguousarray(coeffs, np.int32)
+    out = np.empty((n, n), np.int64)
+    oracle_lib().oracle_hbd_itx2d(x.ctypes.data, out.ctypes.data, n, tx_type, lossless)
+    return out
+
+
+def hbd_intra_tx(plane, x0, y0, n, mode, have_top, have_left, have_right):
+    p = np.ascontiguousarray(plane, np.uint16).copy()
+    h, w = p.shape
+    oracle_lib().oracle_hbd_intra_tx(p.ctypes.data, w, h, w, x0, y0, n, mode, have_top, have_left, have_right)
+    return p
+
+
+def hbd_mc_block(ref0, ref1, dst_shape, x, y, bw, bh, mv0, mv1=(0, 0), compound=0, filt=0, chroma=0):
+    r0 = np.ascontiguousarray(ref0, np.uint16)
+    r1 = np.ascontiguousarray(ref1 if ref1 is not None else ref0, np.uint16)
+    d = np.zeros(dst_shape, np.uint16)
+    oracle_lib().oracle_hbd_mc_block(r0.ctypes.data, r1.ctypes.data, r0.shape[1], r0.shape[0], r0.shape[1],
+                                     d.ctypes.data, d.shape[1], d.shape[0], d.shape[1], x, y, bw, bh,
+                                     mv0[0], mv0[1], mv1[0], mv1[1], compound, filt, chroma)
     return d

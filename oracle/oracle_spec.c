@@ -36,305 +36,11 @@ enum {
 
 /* ── 1-D inverse DCTs (vp9_idct.comp.glsl:47-649) ──────────────────────── */
 
-static void idct4(const int *in, int *out)
-{
-    int s0 = RS((in[0] + in[2]) * C16);
-    int s1 = RS((in[0] - in[2]) * C16);
-    int s2 = RS(in[1] * C24 - in[3] * C8);
-    int s3 = RS(in[1] * C8 + in[3] * C24);
-    out[0] = s0 + s3;
-    out[1] = s1 + s2;
-    out[2] = s1 - s2;
-    out[3] = s0 - s3;
-}
-
-static void idct8(const int *in, int *out)
-{
-    int a[8], b[8];
-    a[0] = in[0]; a[1] = in[2]; a[2] = in[4]; a[3] = in[6];
-    a[4] = RS(in[1] * C28 - in[7] * C4);
-    a[7] = RS(in[1] * C4 + in[7] * C28);
-    a[5] = RS(in[5] * C12 - in[3] * C20);
-    a[6] = RS(in[5] * C20 + in[3] * C12);
-
-    b[0] = RS((a[0] + a[2]) * C16);
-    b[1] = RS((a[0] - a[2]) * C16);
-    b[2] = RS(a[1] * C24 - a[3] * C8);
-    b[3] = RS(a[1] * C8 + a[3] * C24);
-    b[4] = a[4] + a[5];
-    b[5] = a[4] - a[5];
-    b[6] = -a[6] + a[7];
-    b[7] = a[6] + a[7];
-
-    a[0] = b[0] + b[3];
-    a[1] = b[1] + b[2];
-    a[2] = b[1] - b[2];
-    a[3] = b[0] - b[3];
-    a[4] = b[4];
-    a[5] = RS((b[6] - b[5]) * C16);
-    a[6] = RS((b[5] + b[6]) * C16);
-    a[7] = b[7];
-
-    for (int i = 0; i < 4; i++) {
-        out[i] = a[i] + a[7 - i];
-        out[7 - i] = a[i] - a[7 - i];
-    }
-}
-
-static void idct16(const int *in, int *out)
-{
-    int a[16], b[16];
-    /* even/odd reordering of the inputs */
-    static const int perm[16] = { 0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15 };
-    for (int i = 0; i < 16; i++) a[i] = in[perm[i]];
-
-    for (int i = 0; i < 8; i++) b[i] = a[i];
-    b[8]  = RS(a[8] * C30 - a[15] * C2);
-    b[15] = RS(a[8] * C2 + a[15] * C30);
-    b[9]  = RS(a[9] * C14 - a[14] * C18);
-    b[14] = RS(a[9] * C18 + a[14] * C14);
-    b[10] = RS(a[10] * C22 - a[13] * C10);
-    b[13] = RS(a[10] * C10 + a[13] * C22);
-    b[11] = RS(a[11] * C6 - a[12] * C26);
-    b[12] = RS(a[11] * C26 + a[12] * C6);
-
-    for (int i = 0; i < 4; i++) a[i] = b[i];
-    a[4] = RS(b[4] * C28 - b[7] * C4);
-    a[7] = RS(b[4] * C4 + b[7] * C28);
-    a[5] = RS(b[5] * C12 - b[6] * C20);
-    a[6] = RS(b[5] * C20 + b[6] * C12);
-    a[8]  = b[8] + b[9];
-    a[9]  = b[8] - b[9];
-    a[10] = -b[10] + b[11];
-    a[11] = b[10] + b[11];
-    a[12] = b[12] + b[13];
-    a[13] = b[12] - b[13];
-    a[14] = -b[14] + b[15];
-    a[15] = b[14] + b[15];
-
-    b[0] = RS((a[0] + a[1]) * C16);
-    b[1] = RS((a[0] - a[1]) * C16);
-    b[2] = RS(a[2] * C24 - a[3] * C8);
-    b[3] = RS(a[2] * C8 + a[3] * C24);
-    b[4] = a[4] + a[5];
-    b[5] = a[4] - a[5];
-    b[6] = -a[6] + a[7];
-    b[7] = a[6] + a[7];
-    b[8] = a[8];
-    b[15] = a[15];
-    b[9]  = RS(-a[9] * C8 + a[14] * C24);
-    b[14] = RS(a[9] * C24 + a[14] * C8);
-    b[10] = RS(-a[10] * C24 - a[13] * C8);
-    b[13] = RS(-a[10] * C8 + a[13] * C24);
-    b[11] = a[11];
-    b[12] = a[12];
-
-    a[0] = b[0] + b[3];
-    a[1] = b[1] + b[2];
-    a[2] = b[1] - b[2];
-    a[3] = b[0] - b[3];
-    a[4] = b[4];
-    a[5] = RS((b[6] - b[5]) * C16);
-    a[6] = RS((b[5] + b[6]) * C16);
-    a[7] = b[7];
-    a[8]  = b[8] + b[11];
-    a[9]  = b[9] + b[10];
-    a[10] = b[9] - b[10];
-    a[11] = b[8] - b[11];
-    a[12] = -b[12] + b[15];
-    a[13] = -b[13] + b[14];
-    a[14] = b[13] + b[14];
-    a[15] = b[12] + b[15];
-
-    for (int i = 0; i < 4; i++) {
-        b[i] = a[i] + a[7 - i];
-        b[7 - i] = a[i] - a[7 - i];
-    }
-    b[8] = a[8];
-    b[9] = a[9];
-    b[10] = RS((-a[10] + a[13]) * C16);
-    b[13] = RS((a[10] + a[13]) * C16);
-    b[11] = RS((-a[11] + a[12]) * C16);
-    b[12] = RS((a[11] + a[12]) * C16);
-    b[14] = a[14];
-    b[15] = a[15];
-
-    for (int i = 0; i < 8; i++) {
-        out[i] = b[i] + b[15 - i];
-        out[15 - i] = b[i] - b[15 - i];
-    }
-}
-
-static void idct32(const int *in, int *out)
-{
-    int a[32], b[32];
-    /* stage 1: even inputs in bit-reversed order, odd inputs rotated */
-    static const int perm[16] = { 0, 16, 8, 24, 4, 20, 12, 28, 2, 18, 10, 26, 6, 22, 14, 30 };
-    for (int i = 0; i < 16; i++) a[i] = in[perm[i]];
-    a[16] = RS(in[1] * C31 - in[31] * C1);
-    a[31] = RS(in[1] * C1 + in[31] * C31);
-    a[17] = RS(in[17] * C15 - in[15] * C17);
-    a[30] = RS(in[17] * C17 + in[15] * C15);
-    a[18] = RS(in[9] * C23 - in[23] * C9);
-    a[29] = RS(in[9] * C9 + in[23] * C23);
-    a[19] = RS(in[25] * C7 - in[7] * C25);
-    a[28] = RS(in[25] * C25 + in[7] * C7);
-    a[20] = RS(in[5] * C27 - in[27] * C5);
-    a[27] = RS(in[5] * C5 + in[27] * C27);
-    a[21] = RS(in[21] * C11 - in[11] * C21);
-    a[26] = RS(in[21] * C21 + in[11] * C11);
-    a[22] = RS(in[13] * C19 - in[19] * C13);
-    a[25] = RS(in[13] * C13 + in[19] * C19);
-    a[23] = RS(in[29] * C3 - in[3] * C29);
-    a[24] = RS(in[29] * C29 + in[3] * C3);
-
-    /* stage 2 */
-    for (int i = 0; i < 8; i++) b[i] = a[i];
-    b[8]  = RS(a[8] * C30 - a[15] * C2);
-    b[15] = RS(a[8] * C2 + a[15] * C30);
-    b[9]  = RS(a[9] * C14 - a[14] * C18);
-    b[14] = RS(a[9] * C18 + a[14] * C14);
-    b[10] = RS(a[10] * C22 - a[13] * C10);
-    b[13] = RS(a[10] * C10 + a[13] * C22);
-    b[11] = RS(a[11] * C6 - a[12] * C26);
-    b[12] = RS(a[11] * C26 + a[12] * C6);
-    for (int i = 16; i < 32; i += 4) {
-        b[i]     = a[i] + a[i + 1];
-        b[i + 1] = a[i] - a[i + 1];
-        b[i + 2] = -a[i + 2] + a[i + 3];
-        b[i + 3] = a[i + 2] + a[i + 3];
-    }
-
-    /* stage 3 */
-    for (int i = 0; i < 4; i++) a[i] = b[i];
-    a[4] = RS(b[4] * C28 - b[7] * C4);
-    a[7] = RS(b[4] * C4 + b[7] * C28);
-    a[5] = RS(b[5] * C12 - b[6] * C20);
-    a[6] = RS(b[5] * C20 + b[6] * C12);
-    for (int i = 8; i < 16; i += 4) {
-        a[i]     = b[i] + b[i + 1];
-        a[i + 1] = b[i] - b[i + 1];
-        a[i + 2] = -b[i + 2] + b[i + 3];
-        a[i + 3] = b[i + 2] + b[i + 3];
-    }
-    a[16] = b[16];
-    a[31] = b[31];
-    a[17] = RS(-b[17] * C4 + b[30] * C28);
-    a[30] = RS(b[17] * C28 + b[30] * C4);
-    a[18] = RS(-b[18] * C28 - b[29] * C4);
-    a[29] = RS(-b[18] * C4 + b[29] * C28);
-    a[19] = b[19];
-    a[20] = b[20];
-    a[21] = RS(-b[21] * C20 + b[26] * C12);
-    a[26] = RS(b[21] * C12 + b[26] * C20);
-    a[22] = RS(-b[22] * C12 - b[25] * C20);
-    a[25] = RS(-b[22] * C20 + b[25] * C12);
-    a[23] = b[23];
-    a[24] = b[24];
-    a[27] = b[27];
-    a[28] = b[28];
-
-    /* stage 4 */
-    b[0] = RS((a[0] + a[1]) * C16);
-    b[1] = RS((a[0] - a[1]) * C16);
-    b[2] = RS(a[2] * C24 - a[3] * C8);
-    b[3] = RS(a[2] * C8 + a[3] * C24);
-    b[4] = a[4] + a[5];
-    b[5] = a[4] - a[5];
-    b[6] = -a[6] + a[7];
-    b[7] = a[6] + a[7];
-    b[8] = a[8];
-    b[15] = a[15];
-    b[9]  = RS(-a[9] * C8 + a[14] * C24);
-    b[14] = RS(a[9] * C24 + a[14] * C8);
-    b[10] = RS(-a[10] * C24 - a[13] * C8);
-    b[13] = RS(-a[10] * C8 + a[13] * C24);
-    b[11] = a[11];
-    b[12] = a[12];
-    for (int i = 16; i < 32; i += 8) {
-        b[i]     = a[i] + a[i + 3];
-        b[i + 1] = a[i + 1] + a[i + 2];
-        b[i + 2] = a[i + 1] - a[i + 2];
-        b[i + 3] = a[i] - a[i + 3];
-        b[i + 4] = -a[i + 4] + a[i + 7];
-        b[i + 5] = -a[i + 5] + a[i + 6];
-        b[i + 6] = a[i + 5] + a[i + 6];
-        b[i + 7] = a[i + 4] + a[i + 7];
-    }
-
-    /* stage 5 */
-    a[0] = b[0] + b[3];
-    a[1] = b[1] + b[2];
-    a[2] = b[1] - b[2];
-    a[3] = b[0] - b[3];
-    a[4] = b[4];
-    a[5] = RS((b[6] - b[5]) * C16);
-    a[6] = RS((b[5] + b[6]) * C16);
-    a[7] = b[7];
-    a[8]  = b[8] + b[11];
-    a[9]  = b[9] + b[10];
-    a[10] = b[9] - b[10];
-    a[11] = b[8] - b[11];
-    a[12] = -b[12] + b[15];
-    a[13] = -b[13] + b[14];
-    a[14] = b[13] + b[14];
-    a[15] = b[12] + b[15];
-    a[16] = b[16];
-    a[17] = b[17];
-    a[18] = RS(-b[18] * C8 + b[29] * C24);
-    a[29] = RS(b[18] * C24 + b[29] * C8);
-    a[19] = RS(-b[19] * C8 + b[28] * C24);
-    a[28] = RS(b[19] * C24 + b[28] * C8);
-    a[20] = RS(-b[20] * C24 - b[27] * C8);
-    a[27] = RS(-b[20] * C8 + b[27] * C24);
-    a[21] = RS(-b[21] * C24 - b[26] * C8);
-    a[26] = RS(-b[21] * C8 + b[26] * C24);
-    a[22] = b[22];
-    a[23] = b[23];
-    a[24] = b[24];
-    a[25] = b[25];
-    a[30] = b[30];
-    a[31] = b[31];
-
-    /* stage 6 */
-    for (int i = 0; i < 4; i++) {
-        b[i] = a[i] + a[7 - i];
-        b[7 - i] = a[i] - a[7 - i];
-    }
-    b[8] = a[8];
-    b[9] = a[9];
-    b[10] = RS((-a[10] + a[13]) * C16);
-    b[13] = RS((a[10] + a[13]) * C16);
-    b[11] = RS((-a[11] + a[12]) * C16);
-    b[12] = RS((a[11] + a[12]) * C16);
-    b[14] = a[14];
-    b[15] = a[15];
-    for (int i = 0; i < 4; i++) {
-        b[16 + i] = a[16 + i] + a[23 - i];
-        b[23 - i] = a[16 + i] - a[23 - i];
-        b[24 + i] = -a[24 + i] + a[31 - i];
-        b[31 - i] = a[24 + i] + a[31 - i];
-    }
-
-    /* stage 7 */
-    for (int i = 0; i < 8; i++) {
-        a[i] = b[i] + b[15 - i];
-        a[15 - i] = b[i] - b[15 - i];
-    }
-    for (int i = 16; i < 20; i++) a[i] = b[i];
-    for (int i = 0; i < 4; i++) {
-        int lo = 20 + i, hi = 27 - i;
-        a[lo] = RS((-b[lo] + b[hi]) * C16);
-        a[hi] = RS((b[lo] + b[hi]) * C16);
-    }
-    for (int i = 28; i < 32; i++) a[i] = b[i];
-
-    /* final stage */
-    for (int i = 0; i < 16; i++) {
-        out[i] = a[i] + a[31 - i];
-        out[31 - i] = a[i] - a[31 - i];
-    }
-}
+#define TXI int
+#define TXN(name) name
+#include "oracle_txfm_dct.inc"
+#undef TXI
+#undef TXN
 
 void oracle_idct1d(int n, const int *in, int *out)
 {

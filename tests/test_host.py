@@ -26,8 +26,10 @@ def _declared_functions(header):
 
 def test_library_exports_every_declared_function():
     lib = P.cuda_lib()
-    declared = _declared_functions("cuda_backend.h") + _declared_functions("cvp9_batch.h")
+    declared = (_declared_functions("cuda_backend.h") + _declared_functions("cvp9_batch.h") +
+                _declared_functions("cvp9_hbd.h"))
     assert "cuda_decode_frame" in declared and "cvp9_batch_submit" in declared
+    assert "cvp9_hbd_submit" in declared
     assert "cuda_reconstruct_noalloc" in declared
     missing = [n for n in declared if not hasattr(lib, n)]
     assert not missing, missing
