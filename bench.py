@@ -26,6 +26,8 @@ e2e          the same K steps through cvp9_batch_submit with the parsed
              own compiled reconstruction.
 value_spec   the same steps in the shader arithmetic; value_full the VP9
              (FULL) profile on mixed block/TX/filter content.
+value_hbd    profile 2 (10-bit): 16 x 3840x2160 streams of the 10-bit
+             config's content through the cvp9_hbd engine, GOP 120.
 Single-stream figures come from the plain per-stream path on stream 0.
 Each rank decodes its own 64 streams (weak scaling, no data-path collective).
 """
@@ -61,6 +63,8 @@ def parse():
     ap.add_argument("--arith", default="refcpu", choices=["refcpu", "spec", "full"])
     ap.add_argument("--no-spec", action="store_true", help="skip the shader-arithmetic leg")
     ap.add_argument("--no-full", action="store_true", help="skip the VP9 (FULL) leg")
+    ap.add_argument("--no-hbd", action="store_true", help="skip the profile 2 (10-bit) leg")
+    ap.add_argument("--hbd-streams", type=int, default=16)
     ap.add_argument("--no-capacity", action="store_true", help="skip the serving capacity sweeps")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-single", action="store_true", help="skip the single-stream leg")
@@ -69,7 +73,7 @@ def parse():
     ap.add_argument("--no-parity", action="store_true", help="skip the bit-exactness check of the e2e run")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the second batched run on mixed block/TX-size content")
-    ap.add_argument("--leg", default=None, choices=["gop", "inter", "key", "mixed", "link"],
+    ap.add_argument("--leg", default=None, choices=["gop", "inter", "key", "mixed", "link", "hbd"],
                     help="run one device-resident leg alone and print its timing (profiler captures); "
                          "mixed = the mixed block/TX-size content, GOP 60; link = the PCIe copy probe "
                          "(each direction alone and both at once, as single copies and as the "
@@ -623,6 +627,181 @@ def leg_roofline(wl, r, steps, warmup, peak):
     return {"recon_ms": recon_ms, "alg_bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak}
 
 
+# ── profile 2 (10-bit) ───────────────────────────────────────────────────────
+
+HBD_GOP = 120
+HBD_DISTINCT = 3
+# the 10-bit config's content: 3840x2160, 32x32 TX on half the blocks, 10%
+# coefficients dequantised up to +-2^17, +-256 px MVs, the sharp filter,
+# LAST/GOLDEN/ALTREF, loop-filter level per frame
+HBD_CONTENT = dict(gop=HBD_GOP, tx_weights=[10, 15, 25, 50], density_min=0.10, density_max=0.10,
+                   mv_range_px=256, interp_filter=2, nrefs=3, lf_level=-1, intra_in_inter=0.0)
+HBD_STEP = 288      # dequantiser step of the synthetic levels: |level| <= 512 -> +-2^17
+
+
+class HbdWorkload:
+    """S streams x HBD_DISTINCT 10-bit frames (a key frame, then inter frames
+    cycled), block records and int32 coefficients in one pinned host arena
+    and one device copy."""
+
+    def __init__(self, streams, w, h, seeds):
+        import numpy as np
+        import torch
+        from compute_vp9_b200 import BlockInfo, ParsedFrame, Synth, synth_config
+        from compute_vp9_b200.hbd import dequantise10
+        self.S, self.w, self.h = streams, w, h
+        per_stream = []
+        for s in range(streams):
+            syn = Synth(synth_config(2, w, h, seed=seeds[s], **HBD_CONTENT))
+            per = []
+            for f in range(HBD_DISTINCT):
+                pfp = syn.frame(f)
+                pfp.contents.hdr.bit_depth = 10
+                pfp.contents.hdr.profile = 2
+                pf = pfp.contents
+                blocks = np.ctypeslib.as_array(C.cast(pf.blocks, C.POINTER(C.c_uint8)),
+                                               shape=(pf.num_blocks * 32,)).copy()
+                c32 = dequantise10(pfp, HBD_STEP)
+                hdr = ParsedFrame()
+                C.memmove(C.byref(hdr), C.byref(pf), C.sizeof(ParsedFrame))
+                per.append((hdr, blocks, c32))
+            syn.close()
+            per_stream.append(per)
+        total, offs = 0, []
+        for per in per_stream:
+            o = []
+            for hdr, blocks, c32 in per:
+                ob = total
+                total += (blocks.nbytes + 255) // 256 * 256
+                oc = total
+                total += (c32.nbytes + 255) // 256 * 256
+                o.append((ob, oc))
+            offs.append(o)
+        self.host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        hv = self.host.numpy()
+        for per, o in zip(per_stream, offs):
+            for (hdr, blocks, c32), (ob, oc) in zip(per, o):
+                hv[ob:ob + blocks.nbytes] = blocks
+                hv[oc:oc + c32.nbytes] = c32.view(np.uint8)
+        self.dev = torch.empty(total, dtype=torch.uint8, device="cuda")
+        self.dev.copy_(self.host)
+        torch.cuda.synchronize()
+        hb, db = self.host.data_ptr(), self.dev.data_ptr()
+        self.frames = []        # [s][f] -> (pf host, pf device, coeffs host, coeffs device)
+        self.nnz, self.nblocks = [], []
+        for per, o in zip(per_stream, offs):
+            row, nz, nb = [], [], []
+            for (hdr, blocks, c32), (ob, oc) in zip(per, o):
+                ph, pd = ParsedFrame(), ParsedFrame()
+                for dst, base in ((ph, hb), (pd, db)):
+                    C.memmove(C.byref(dst), C.byref(hdr), C.sizeof(ParsedFrame))
+                    dst.blocks = C.cast(C.c_void_p(base + ob), C.POINTER(BlockInfo))
+                    dst.coeffs = None
+                row.append((ph, pd, hb + oc, db + oc))
+                nz.append(int(np.count_nonzero(c32)))
+                nb.append(hdr.num_blocks)
+            self.frames.append(row)
+            self.nnz.append(nz)
+            self.nblocks.append(nb)
+        self.c32 = [[c for (_, _, c) in per] for per in per_stream]
+
+    @staticmethod
+    def frame_of(t):
+        t %= HBD_GOP
+        return 0 if t == 0 else 1 + (t - 1) % (HBD_DISTINCT - 1)
+
+    def step(self, t, device):
+        f = self.frame_of(t)
+        return [(C.pointer(self.frames[s][f][1 if device else 0]), self.frames[s][f][3 if device else 2])
+                for s in range(self.S)]
+
+    def alg_bytes(self, t):
+        """One step's algorithmic bytes: the 16-bit frame written (3*W*H), the
+        reference read on inter frames (3*W*H), 4 bytes per nonzero
+        dequantised coefficient, 32 per block record."""
+        f = self.frame_of(t)
+        px = self.w * self.h
+        return sum(3 * px * (2 if f else 1) + 4 * self.nnz[s][f] + 32 * self.nblocks[s][f] for s in range(self.S))
+
+
+def run_hbd(wl, steps, warmup, device_inputs):
+    """W warm-up steps, then K timed steps t = 0..K-1 of the GOP schedule
+    (a key frame at t = 0), one step in flight: the engine completes each
+    step inside the next submit. Device time = the sum of each step's CUDA
+    event span (upload of jobs/inputs, kernels, download)."""
+    from compute_vp9_b200.hbd import HBD_DEVICE_INPUTS, HBD_NO_OUTPUT, HbdEngine
+    eng = HbdEngine()
+    sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
+    flags = (HBD_DEVICE_INPUTS | HBD_NO_OUTPUT) if device_inputs else 0
+    for t in range(warmup):
+        assert eng.submit(sids, wl.step(t, device_inputs), flags=flags) == 0
+    assert eng.wait() == 0
+    dev_ms, parts, recon, alg = 0.0, [0.0] * 5, [], []
+    t0 = time.perf_counter()
+    for t in range(steps):
+        assert eng.submit(sids, wl.step(t, device_inputs), flags=flags) == 0
+        assert eng.wait() == 0
+        ms = eng.step_times()
+        dev_ms += sum(ms)
+        parts = [a + b for a, b in zip(parts, ms)]
+        recon.append(ms[2])
+        alg.append(wl.alg_bytes(t))
+    wall = (time.perf_counter() - t0) * 1000.0
+    eng.close()
+    return {"ms": dev_ms, "wall_ms": wall, "parts": [p / steps for p in parts], "recon": recon, "alg": alg}
+
+
+def hbd_parity(streams=2, frames=3, seed0=1000):
+    """Fresh 10-bit streams of the same content, every frame downloaded and
+    compared with the 10-bit restatement (oracle/oracle_hbd.c)."""
+    import numpy as np
+    from compute_vp9_b200.hbd import HbdEngine, hbd_frames
+    from oracle.oracle_py import HbdOracleStream
+    eng = HbdEngine()
+    sids = [eng.open_stream(3840, 2160) for _ in range(streams)]
+    gens = [hbd_frames(2, 3840, 2160, frames, seed=seed0 + s, step=HBD_STEP, **HBD_CONTENT) for s in range(streams)]
+    orcs = [HbdOracleStream() for _ in range(streams)]
+    bad = 0
+    for f in range(frames):
+        fr = [next(g) for g in gens]
+        want = [o.decode(pf, c) for o, (pf, c) in zip(orcs, fr)]
+        assert eng.submit(sids, [(pf, c.ctypes.data) for pf, c in fr]) == 0
+        assert eng.wait() == 0
+        bad += sum(0 if np.array_equal(eng.get_frame(sid), w) else 1 for sid, w in zip(sids, want))
+    eng.close()
+    return {"streams_checked": streams, "frames_each": frames, "frames_mismatched": bad,
+            "bit_exact": bad == 0, "against": "oracle/oracle_hbd.c (10-bit restatement, unpinned)"}
+
+
+def hbd_leg(args, rank, peak, parity=True):
+    seeds = [rank * args.hbd_streams + s for s in range(args.hbd_streams)]
+    wl = HbdWorkload(args.hbd_streams, 3840, 2160, seeds)
+    steps = max(args.steps, HBD_GOP) if not args.leg else args.steps
+    R = run_hbd(wl, steps, args.warmup, True)
+    E = run_hbd(wl, min(steps, 30), args.warmup, False)
+    px = wl.S * wl.w * wl.h
+    recon_ms = statistics.mean(R["recon"][1:])        # inter steps
+    alg = statistics.mean(R["alg"][1:])
+    out = {"workload": "%d x 3840x2160 10-bit 4:2:0 streams, TX 4x4..32x32 weighted 10/15/25/50, 10%% "
+                       "coefficients dequantised up to +-2^17, +-256 px MVs, sharp filter, LAST/GOLDEN/ALTREF, "
+                       "a key frame every %d steps; %d timed steps from a key frame" % (wl.S, HBD_GOP, steps),
+           "value": px * steps / (R["ms"] / 1000.0) / 1e6, "unit": UNIT, "ms_per_step": R["ms"] / steps,
+           "wall_ms_per_step": R["wall_ms"] / steps,
+           "device_ms_per_step": dict(zip(("upload", "scan", "recon", "filter", "download"), R["parts"])),
+           "e2e": {"value": px * min(steps, 30) / (E["ms"] / 1000.0) / 1e6, "unit": UNIT,
+                   "ms_per_step": E["ms"] / min(steps, 30),
+                   "device_ms_per_step": dict(zip(("upload", "scan", "recon", "filter", "download"), E["parts"])),
+                   "what": "cvp9_hbd_submit from page-locked host arrays (block records + dense int32 "
+                           "coefficients up, every 16-bit frame down), timed on the engine's CUDA events"},
+           "roofline": {"bound": "hbm", "kernel": "k_hbd_recon (inter steps)", "achieved": alg / (recon_ms / 1e3) / 1e9,
+                        "peak": peak, "unit": "GB/s", "frac": alg / (recon_ms / 1e3) / 1e9 / peak,
+                        "alg_bytes_per_launch": alg, "launch_ms": recon_ms},
+           "dtype": "u16 samples, int64 butterflies"}
+    if parity:
+        out["parity"] = hbd_parity()
+    return out
+
+
 def link_probe(local):
     """PCIe host<->device throughput on this GPU: H2D alone, D2H alone and
     both at once on two streams, for one large copy per direction and for
@@ -716,6 +895,17 @@ def main():
     if args.leg == "link":
         if rank == 0:
             link_probe(local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.leg == "hbd":
+        import torch
+        torch.cuda.set_device(local)
+        os.environ.setdefault("CVP9_CUDA_DEVICE", str(local))
+        r = hbd_leg(args, rank, read_peaks()[0], parity=False)
+        if rank == 0:
+            print(json.dumps(r), flush=True)
         if ws > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -877,6 +1067,7 @@ def main():
                                       "filters, per-TX directional intra + ADST, the VP9 loop filter); "
                                       "parity against its from-spec restatement (unpinned)"}
             del wl2
+        value_hbd = None if args.no_hbd else hbd_leg(args, rank, peak)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
@@ -930,6 +1121,7 @@ def main():
             "value_spec": value_spec,
             "value_mixed_content": mixed,
             "value_full": value_full,
+            "value_hbd": value_hbd,
             "single_stream": single,
             "serving": serving,
             "serving_capacity": capacity,

@@ -70,6 +70,7 @@ def _run(engine, cases, together=True, seed=11):
             assert engine.wait() == CVP9_OK
         for (name, w, h, frames, sid, gen, orc), want in zip(live, wants):
             got = engine.get_frame(sid)
+            assert got.max() > got.min()            # real content, not a flat fill
             _check(got, want, w, h, "%s frame %d" % (name, f))
             got_all[(name, f)] = got
     for s in streams:
