@@ -4824,7 +4824,7 @@ __device__ void hbd_intra_block(HbdSmem &s, const HbdBlk &b, int sbx, int sby, i
 
 } /* namespace */
 
-__global__ void __launch_bounds__(kHbdThreads, 2) k_hbd_recon(const cvp9_job_t *__restrict__ jobs,
+__global__ void __launch_bounds__(kHbdThreads, 3) k_hbd_recon(const cvp9_job_t *__restrict__ jobs,
                                                               const uint32_t *__restrict__ tickets,
                                                               uint32_t n_tickets, uint32_t *ticket_counter)
 {
