@@ -703,7 +703,30 @@ class HbdWorkload:
             self.frames.append(row)
             self.nnz.append(nz)
             self.nblocks.append(nb)
-        self.c32 = [[c for (_, _, c) in per] for per in per_stream]
+        # the nonzero coefficients as (index, value) lists, in pinned memory
+        # (what a parser emitting them as it decodes tokens would hand over)
+        lists, total = [], 0
+        for per in per_stream:
+            row = []
+            for hdr, blocks, c32 in per:
+                pos = np.nonzero(c32[:hdr.num_coeffs])[0].astype(np.uint32)
+                row.append((pos, c32[pos].astype(np.int32)))
+                total += 2 * ((pos.nbytes + 255) // 256 * 256)
+            lists.append(row)
+        self.sparse = torch.empty(max(total, 1), dtype=torch.uint8, pin_memory=True)
+        sv, sb, off = self.sparse.numpy(), self.sparse.data_ptr(), 0
+        self.lists = []
+        for row in lists:
+            lr = []
+            for pos, val in row:
+                op = off
+                sv[op:op + pos.nbytes] = pos.view(np.uint8)
+                off += (pos.nbytes + 255) // 256 * 256
+                ov = off
+                sv[ov:ov + val.nbytes] = val.view(np.uint8)
+                off += (val.nbytes + 255) // 256 * 256
+                lr.append((pos.size, sb + op, sb + ov))
+            self.lists.append(lr)
 
     @staticmethod
     def frame_of(t):
@@ -715,6 +738,10 @@ class HbdWorkload:
         return [(C.pointer(self.frames[s][f][1 if device else 0]), self.frames[s][f][3 if device else 2])
                 for s in range(self.S)]
 
+    def step_lists(self, t):
+        f = self.frame_of(t)
+        return [C.pointer(self.frames[s][f][0]) for s in range(self.S)], [self.lists[s][f] for s in range(self.S)]
+
     def alg_bytes(self, t):
         """One step's algorithmic bytes: the 16-bit frame written (3*W*H), the
         reference read on inter frames (3*W*H), 4 bytes per nonzero
@@ -724,7 +751,7 @@ class HbdWorkload:
         return sum(3 * px * (2 if f else 1) + 4 * self.nnz[s][f] + 32 * self.nblocks[s][f] for s in range(self.S))
 
 
-def run_hbd(wl, steps, warmup, device_inputs):
+def run_hbd(wl, steps, warmup, device_inputs, sparse=False):
     """W warm-up steps, then K timed steps t = 0..K-1 of the GOP schedule
     (a key frame at t = 0), one step in flight: the engine completes each
     step inside the next submit. Device time = the sum of each step's CUDA
@@ -733,13 +760,19 @@ def run_hbd(wl, steps, warmup, device_inputs):
     eng = HbdEngine()
     sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
     flags = (HBD_DEVICE_INPUTS | HBD_NO_OUTPUT) if device_inputs else 0
+
+    def submit(t):
+        if sparse:
+            pfs, lists = wl.step_lists(t)
+            return eng.submit_sparse(sids, pfs, lists, flags=flags)
+        return eng.submit(sids, wl.step(t, device_inputs), flags=flags)
     for t in range(warmup):
-        assert eng.submit(sids, wl.step(t, device_inputs), flags=flags) == 0
+        assert submit(t) == 0
     assert eng.wait() == 0
     dev_ms, parts, recon, alg = 0.0, [0.0] * 5, [], []
     t0 = time.perf_counter()
     for t in range(steps):
-        assert eng.submit(sids, wl.step(t, device_inputs), flags=flags) == 0
+        assert submit(t) == 0
         assert eng.wait() == 0
         ms = eng.step_times()
         dev_ms += sum(ms)
@@ -749,6 +782,37 @@ def run_hbd(wl, steps, warmup, device_inputs):
     wall = (time.perf_counter() - t0) * 1000.0
     eng.close()
     return {"ms": dev_ms, "wall_ms": wall, "parts": [p / steps for p in parts], "recon": recon, "alg": alg}
+
+
+def hbd_live(wl, steps=60, fps=30.0):
+    """The streams served live: every 1/fps s one frame of each is due (a
+    step through cvp9_hbd_submit_sparse from host memory, frames
+    downloaded); latency = due time -> the step's frames in host memory
+    (host clock)."""
+    from compute_vp9_b200.hbd import HbdEngine
+    eng = HbdEngine()
+    sids = [eng.open_stream(wl.w, wl.h) for _ in range(wl.S)]
+    for t in range(3):
+        pfs, lists = wl.step_lists(t)
+        assert eng.submit_sparse(sids, pfs, lists) == 0
+    assert eng.wait() == 0
+    lat = []
+    t0 = time.perf_counter() + 0.05
+    for t in range(steps):
+        due = t0 + t / fps
+        now = time.perf_counter()
+        if now < due:
+            time.sleep(due - now)
+        pfs, lists = wl.step_lists(t)
+        assert eng.submit_sparse(sids, pfs, lists) == 0
+        assert eng.wait() == 0
+        lat.append((time.perf_counter() - due) * 1000.0)
+    eng.close()
+    s = sorted(lat)
+    return {"streams": wl.S, "fps": fps, "steps": steps, "p50_ms": statistics.median(s),
+            "p99_ms": s[min(len(s) - 1, int(0.99 * len(s)))], "offered": wl.S * wl.w * wl.h * fps / 1e6,
+            "unit": UNIT, "what": "every stream live at 30 fps, one step per frame period, inputs as "
+                                  "(index, value) lists from host memory, frames downloaded"}
 
 
 def hbd_parity(streams=2, frames=3, seed0=1000):
@@ -779,6 +843,7 @@ def hbd_leg(args, rank, peak, parity=True):
     steps = max(args.steps, HBD_GOP) if not args.leg else args.steps
     R = run_hbd(wl, steps, args.warmup, True)
     E = run_hbd(wl, min(steps, 30), args.warmup, False)
+    Es = run_hbd(wl, min(steps, 30), args.warmup, False, sparse=True)
     px = wl.S * wl.w * wl.h
     recon_ms = statistics.mean(R["recon"][1:])        # inter steps
     alg = statistics.mean(R["alg"][1:])
@@ -793,10 +858,17 @@ def hbd_leg(args, rank, peak, parity=True):
                    "device_ms_per_step": dict(zip(("upload", "scan", "recon", "filter", "download"), E["parts"])),
                    "what": "cvp9_hbd_submit from page-locked host arrays (block records + dense int32 "
                            "coefficients up, every 16-bit frame down), timed on the engine's CUDA events"},
+           "e2e_sparse_input": {"value": px * min(steps, 30) / (Es["ms"] / 1000.0) / 1e6, "unit": UNIT,
+                                "ms_per_step": Es["ms"] / min(steps, 30),
+                                "device_ms_per_step": dict(zip(("upload", "scan", "recon", "filter", "download"),
+                                                               Es["parts"])),
+                                "what": "as e2e, the coefficients as (index, value) lists through "
+                                        "cvp9_hbd_submit_sparse (8 bytes per nonzero coefficient up)"},
            "roofline": {"bound": "hbm", "kernel": "k_hbd_recon (inter steps)", "achieved": alg / (recon_ms / 1e3) / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": alg / (recon_ms / 1e3) / 1e9 / peak,
                         "alg_bytes_per_launch": alg, "launch_ms": recon_ms},
            "dtype": "u16 samples, int64 butterflies"}
+    out["live"] = hbd_live(wl)
     if parity:
         out["parity"] = hbd_parity()
     return out

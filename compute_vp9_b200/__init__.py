@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = [
     "cvp9_batch_tune_entry", "cvp9_batch_submit_sparse", "cvp9_pack_bound_words",
     "cvp9_pack_coeffs",
     "cvp9_hbd_create", "cvp9_hbd_destroy", "cvp9_hbd_open_stream", "cvp9_hbd_close_stream",
-    "cvp9_hbd_submit", "cvp9_hbd_wait", "cvp9_hbd_get_frame", "cvp9_hbd_step_times",
+    "cvp9_hbd_submit", "cvp9_hbd_submit_sparse", "cvp9_hbd_wait", "cvp9_hbd_get_frame", "cvp9_hbd_step_times",
 ]
 
 

@@ -220,8 +220,8 @@ int cvp9_hbd_wait(cvp9_hbd_t *h)
     return rc;
 }
 
-int cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_t *frames,
-                    const int64_t *pts, unsigned flags)
+static int submit_step(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_t *frames,
+                       const cvp9_hbd_coeff_list_t *lists, const int64_t *pts, unsigned flags)
 {
     if (!h || n <= 0 || n > 1024 || !sids || !frames) return CVP9_ERR_INVALID_DATA;
     cudaSetDevice(h->device);
@@ -235,17 +235,25 @@ int cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_
         int c = frame_check(&h->s[sid], pf);
         if (c != CVP9_OK) return c;
         if (pf->num_blocks && !pf->blocks) return CVP9_ERR_INVALID_DATA;
-        if (pf->num_coeffs && !frames[i].coeffs) return CVP9_ERR_INVALID_DATA;
+        if (!lists && pf->num_coeffs && !frames[i].coeffs) return CVP9_ERR_INVALID_DATA;
+        if (lists && lists[i].n && (!lists[i].pos || !lists[i].val)) return CVP9_ERR_INVALID_DATA;
     }
     /* step buffers */
     size_t in_bytes = 0;
     size_t ntk = 0;
     int max_blocks = 0, max_sb_rows = 0;
+    uint32_t max_n = 0;
     for (int i = 0; i < n; i++) {
         const vp9_parsed_frame_t *pf = frames[i].pf;
         if (!(flags & CVP9_HBD_DEVICE_INPUTS))
             in_bytes += (((size_t)pf->num_blocks * sizeof(vp9_macroblock_info_t) + 255) & ~(size_t)255) +
                         (((size_t)pf->num_coeffs * 4 + 255) & ~(size_t)255);
+        if (lists) {
+            /* the lists, and the dense array they are scattered into */
+            in_bytes += 2 * (((size_t)lists[i].n * 4 + 255) & ~(size_t)255);
+            if (flags & CVP9_HBD_DEVICE_INPUTS) in_bytes += ((size_t)pf->num_coeffs * 4 + 255) & ~(size_t)255;
+            if (lists[i].n > max_n) max_n = lists[i].n;
+        }
         const hbd_stream_t *s = &h->s[sids[i]];
         ntk += (size_t)s->n_sb;
         if ((int)pf->num_blocks > max_blocks) max_blocks = (int)pf->num_blocks;
@@ -308,10 +316,34 @@ int cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_
             at += (cb + 255) & ~(size_t)255;
             if (bb && cudaMemcpyAsync(db, pf->blocks, bb, cudaMemcpyHostToDevice, h->st) != cudaSuccess)
                 return CVP9_ERR_GPU;
-            if (cb && cudaMemcpyAsync(dc, frames[i].coeffs, cb, cudaMemcpyHostToDevice, h->st) != cudaSuccess)
+            if (!lists && cb &&
+                cudaMemcpyAsync(dc, frames[i].coeffs, cb, cudaMemcpyHostToDevice, h->st) != cudaSuccess)
                 return CVP9_ERR_GPU;
             blocks = (const vp9_macroblock_info_t *)db;
             coeffs = (const int32_t *)dc;
+        }
+        if (lists) {
+            const size_t cb = (size_t)pf->num_coeffs * 4, lb = (size_t)lists[i].n * 4;
+            uint8_t *dc = (uint8_t *)coeffs;
+            if (flags & CVP9_HBD_DEVICE_INPUTS) {
+                dc = h->d_in + at;
+                at += (cb + 255) & ~(size_t)255;
+                coeffs = (const int32_t *)dc;
+            }
+            uint8_t *dp = h->d_in + at;
+            at += (lb + 255) & ~(size_t)255;
+            uint8_t *dv = h->d_in + at;
+            at += (lb + 255) & ~(size_t)255;
+            const int dev = (flags & CVP9_HBD_DEVICE_INPUTS) != 0;
+            if ((cb && cudaMemsetAsync(dc, 0, cb, h->st) != cudaSuccess) ||
+                (lb && cudaMemcpyAsync(dp, lists[i].pos, lb, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                       h->st) != cudaSuccess) ||
+                (lb && cudaMemcpyAsync(dv, lists[i].val, lb, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                       h->st) != cudaSuccess))
+                return CVP9_ERR_GPU;
+            job->sp_pos = (const uint32_t *)dp;
+            job->sp_val32 = (const int32_t *)dv;
+            job->sp_n = lists[i].n;
         }
         job->blocks = blocks;
         job->coeffs = NULL;
@@ -362,6 +394,7 @@ int cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_
         cudaMemcpyAsync(h->d_tickets, h->h_tickets, (size_t)nt * 4, cudaMemcpyHostToDevice, h->st) != cudaSuccess ||
         cudaMemsetAsync(h->d_words, 0, (size_t)(n + 2) * 4, h->st) != cudaSuccess)
         return CVP9_ERR_GPU;
+    if (lists && cvp9k_launch_scatter(h->d_jobs, n, max_n, h->st) != 0) return CVP9_ERR_GPU;
 
     cvp9k_launch_t L;
     memset(&L, 0, sizeof(L));
@@ -397,6 +430,19 @@ int cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_
     h->pending_n = n;
     h->step_flags = (int)flags;
     return CVP9_OK;
+}
+
+int cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_t *frames,
+                    const int64_t *pts, unsigned flags)
+{
+    return submit_step(h, n, sids, frames, NULL, pts, flags);
+}
+
+int cvp9_hbd_submit_sparse(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_t *frames,
+                           const cvp9_hbd_coeff_list_t *lists, const int64_t *pts, unsigned flags)
+{
+    if (!lists) return CVP9_ERR_INVALID_DATA;
+    return submit_step(h, n, sids, frames, lists, pts, flags);
 }
 
 int cvp9_hbd_get_frame(cvp9_hbd_t *h, int sid, cvp9_hbd_frame_info_t *info)

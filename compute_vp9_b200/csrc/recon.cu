@@ -5075,6 +5075,15 @@ __global__ void __launch_bounds__(256) k_scatter_coeffs(const cvp9_job_t *__rest
 {
     const cvp9_job_t &job = jobs[blockIdx.y];
     const uint32_t n = job.sp_n;
+    if (job.sp_val32) {
+        /* profile 2: int32 dequantised values into coeffs32 */
+        int32_t *dst = const_cast<int32_t *>(job.coeffs32);
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+            const uint32_t p = job.sp_pos[k];
+            if (p < job.num_coeffs) dst[p] = job.sp_val32[k];
+        }
+        return;
+    }
     int16_t *dst = const_cast<int16_t *>(job.coeffs);
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t p = job.sp_pos[k];

@@ -81,6 +81,7 @@ typedef struct {
      * uint16 samples in the same I420 layout; coeffs32 the dequantised
      * coefficients (num_coeffs of them, the dense layout of coeffs) */
     const int32_t *coeffs32;
+    const int32_t *sp_val32;        /* sparse upload of coeffs32 (with sp_pos, sp_n) */
 } cvp9_job_t;
 
 #ifdef __cplusplus

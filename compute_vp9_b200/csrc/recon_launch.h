@@ -71,7 +71,8 @@ int    cvp9k_launch_gather(const cvp9_job_t *jobs, int njobs, int max_blocks, ui
                            cudaStream_t stream);
 
 /* Sparse coefficient upload: jobs[j].coeffs[sp_pos[k]] = sp_val[k] for
- * every job with sp_n > 0 (indices past num_coeffs are ignored). */
+ * every job with sp_n > 0 (indices past num_coeffs are ignored); jobs with
+ * sp_val32 set write coeffs32[sp_pos[k]] = sp_val32[k] instead. */
 int    cvp9k_launch_scatter(const cvp9_job_t *jobs, int njobs, uint32_t max_n, cudaStream_t stream);
 
 /* Packed coefficient upload: every job with `packed` set gets its dense

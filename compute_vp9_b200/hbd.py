@@ -21,6 +21,10 @@ class HbdFrame(C.Structure):
     _fields_ = [("pf", C.POINTER(ParsedFrame)), ("coeffs", C.c_void_p)]
 
 
+class HbdCoeffList(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("pos", C.c_void_p), ("val", C.c_void_p)]
+
+
 class HbdFrameInfo(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32),
                 ("stride_y", C.c_uint32), ("stride_uv", C.c_uint32),
@@ -43,6 +47,8 @@ def _lib():
         lib.cvp9_hbd_close_stream.argtypes = [vp, C.c_int]
         lib.cvp9_hbd_submit.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(HbdFrame),
                                         C.POINTER(C.c_int64), C.c_uint]
+        lib.cvp9_hbd_submit_sparse.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(HbdFrame),
+                                               C.POINTER(HbdCoeffList), C.POINTER(C.c_int64), C.c_uint]
         lib.cvp9_hbd_wait.argtypes = [vp]
         lib.cvp9_hbd_get_frame.argtypes = [vp, C.c_int, C.POINTER(HbdFrameInfo)]
         lib.cvp9_hbd_step_times.argtypes = [vp, C.POINTER(C.c_float)]
@@ -83,6 +89,18 @@ class HbdEngine:
             f[i].coeffs = co
         p = (C.c_int64 * n)(*(pts if pts is not None else range(n)))
         return self._lib.cvp9_hbd_submit(self._h, n, s, f, p, flags)
+
+    def submit_sparse(self, sids, pfs, lists, pts=None, flags=0):
+        """pfs: parsed-frame pointers; lists: [(n, pos address, val address)]."""
+        n = len(sids)
+        s = (C.c_int * n)(*sids)
+        f = (HbdFrame * n)()
+        ls = (HbdCoeffList * n)()
+        for i, pf in enumerate(pfs):
+            f[i].pf = pf
+            ls[i].n, ls[i].pos, ls[i].val = lists[i]
+        p = (C.c_int64 * n)(*(pts if pts is not None else range(n)))
+        return self._lib.cvp9_hbd_submit_sparse(self._h, n, s, f, ls, p, flags)
 
     def wait(self):
         return self._lib.cvp9_hbd_wait(self._h)

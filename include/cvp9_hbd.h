@@ -72,6 +72,19 @@ int  cvp9_hbd_close_stream(cvp9_hbd_t *h, int sid);
 /* One frame of each of n distinct streams through one launch chain. */
 int  cvp9_hbd_submit(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_t *frames,
                      const int64_t *pts, unsigned flags);
+/* The same with each frame's coefficients as (index, value) lists: the
+ * nonzero dequantised coefficients, indices into the dense layout,
+ * distinct. The engine zeroes the dense array on the device and scatters
+ * the lists into it, so the frames are those of cvp9_hbd_submit; 8 bytes per
+ * nonzero coefficient cross the bus instead of 4 per coefficient. frames[i]
+ * .coeffs is not read. */
+typedef struct {
+    uint32_t        n;
+    const uint32_t *pos;
+    const int32_t  *val;
+} cvp9_hbd_coeff_list_t;
+int  cvp9_hbd_submit_sparse(cvp9_hbd_t *h, int n, const int *sids, const cvp9_hbd_frame_t *frames,
+                            const cvp9_hbd_coeff_list_t *lists, const int64_t *pts, unsigned flags);
 /* Wait for the last step; CVP9_OK, CVP9_ERR_INVALID_DATA (a frame's blocks
  * were outside the supported domain; that frame is not delivered) or
  * CVP9_ERR_GPU. */

@@ -95,6 +95,33 @@ def test_hbd_alone_equals_in_the_mix():
         assert np.array_equal(alone[k], mixed[k]), k
 
 
+def test_hbd_sparse_lists_equal_dense_arrays():
+    """(index, value) lists scattered on the device give the frames of the
+    dense int32 arrays."""
+    e = HbdEngine()
+    cases = {k: CASES[k] for k in ("mixed", "tiles_sharp_full_range", "big_tx_smooth")}
+    dense = _run(e, cases, together=True, seed=6)
+    sids, gens, nf = [], [], []
+    for name, (preset, w, h, frames, step, ov) in cases.items():
+        sids.append(e.open_stream(w, h))
+        gens.append(hbd_frames(preset, w, h, frames, seed=6, step=step, **ov))
+        nf.append(frames)
+    for f in range(max(nf)):
+        live = [i for i in range(len(sids)) if f < nf[i]]
+        pfs, lists, keep = [], [], []
+        for i in live:
+            pf, c32 = next(gens[i])
+            pos = np.nonzero(c32[:pf.contents.num_coeffs])[0].astype(np.uint32)
+            val = c32[pos].astype(np.int32)
+            keep += [pos, val]
+            pfs.append(pf)
+            lists.append((pos.size, pos.ctypes.data, val.ctypes.data))
+        assert e.submit_sparse([sids[i] for i in live], pfs, lists) == CVP9_OK
+        assert e.wait() == CVP9_OK
+        for i in live:
+            assert np.array_equal(e.get_frame(sids[i]), dense[(list(cases)[i], f)]), (list(cases)[i], f)
+
+
 def test_hbd_4k_config_content():
     e = HbdEngine()
     _run(e, {"c4_2160p": (2, 3840, 2160, 2, 288, C4)}, seed=1)
@@ -103,7 +130,8 @@ def test_hbd_4k_config_content():
 def test_hbd_rejects_what_it_does_not_take():
     e = HbdEngine()
     sid = e.open_stream(64, 64)
-    (pf, c32), = list(hbd_frames(2, 64, 64, 1, seed=2))
+    gen = hbd_frames(2, 64, 64, 1, seed=2)
+    pf, c32 = next(gen)      # the generator owns the frame: keep it alive
     pf.contents.hdr.bit_depth = 8
     assert e.submit([sid], [(pf, c32.ctypes.data)]) == CVP9_ERR_UNSUPPORTED
     pf.contents.hdr.bit_depth = 10

@@ -112,7 +112,8 @@ def test_mc_clips_to_10_bits_and_phase_zero_copies():
 
 
 def test_flat_key_frame_stays_at_512():
-    (pf, c32), = list(hbd_frames(2, 128, 64, 1, seed=3, gop=1, intra_in_inter=0.0))
+    gen = hbd_frames(2, 128, 64, 1, seed=3, gop=1, intra_in_inter=0.0)
+    pf, c32 = next(gen)      # the generator owns the frame: keep it alive
     c32[:] = 0
     out = O.HbdOracleStream().decode(pf, c32)
     # DC blocks from 512 edges, no residual, LF sees no edge step
@@ -136,7 +137,8 @@ def test_sequence_decodes_in_range(step):
 
 
 def test_rejects_8bit_headers():
-    (pf, c32), = list(hbd_frames(2, 64, 64, 1, seed=1))
+    gen = hbd_frames(2, 64, 64, 1, seed=1)
+    pf, c32 = next(gen)      # the generator owns the frame: keep it alive
     pf.contents.hdr.bit_depth = 8
     with pytest.raises(RuntimeError):
         O.HbdOracleStream().decode(pf, c32)
