@@ -4390,10 +4390,11 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
  * persistent, as k_recon). Its inter blocks do not depend on one another or
  * on other superblocks, so they go first and together: prediction a thread
  * per column strip of up to 8 rows, then a thread per TX row, then per TX
- * column. The intra blocks follow in list order, one warp each, TX by TX
- * (each TX predicted from the reconstructed samples around it). A
- * superblock whose blocks overlap runs block by block in list order, so
- * the later block wins as in the reference order. */
+ * column. The intra blocks follow by dependency level, the blocks of a
+ * level on different warps, each block TX by TX (each TX predicted from the
+ * reconstructed samples around it). A superblock whose blocks overlap, or
+ * whose intra blocks read samples of blocks later in the list, runs block by
+ * block in list order, so every sample is what the list order makes it. */
 namespace {
 
 constexpr int kHbdThreads = 256, kHbdWarps = kHbdThreads / 32;
@@ -4428,11 +4429,13 @@ struct HbdSmem {
     uint16_t tx_base[kHbdMaxTx + 1];       /* prefix over TXs of their sizes   */
     uint16_t it_base[kHbdMaxBlocks + 1];   /* prefix over blocks of their items */
     unsigned cell[256];                    /* claims of each 4x4 cell          */
+    uint8_t  owner[256];                   /* the block claiming it (one claim) */
+    uint8_t  lvl[kHbdMaxBlocks];           /* intra blocks: dependency level   */
     uint8_t  txnz[kHbdMaxTx];
-    int32_t  edge[1 + 64 + 32];            /* intra: above[-1..2n-1], left     */
+    int32_t  edge[kHbdWarps][1 + 64 + 32]; /* intra, per warp: above[-1..2n-1], left */
     int      scan[kHbdWarps];
     cvp9_job_t jc;
-    int      ticket, ntx;
+    int      ticket, ntx, nlev, order_bad;
 };
 
 __device__ __forceinline__ uint16_t &HT(HbdSmem &s, int p, int x, int y)
@@ -4755,16 +4758,17 @@ __device__ void hbd_inter_blocks(HbdSmem &s, int lo, int hi, int nb, int sbx, in
  * a 4x4 TX with have_right, samples past the plane's edge repeating the
  * last one inside. */
 __device__ void hbd_intra_tx(HbdSmem &s, int p, int lx, int ly, int X0, int Y0, int pw, int ph, int n, int mode,
-                             bool have_top, bool have_left, bool have_right, int lane)
+                             bool have_top, bool have_left, bool have_right, int lane, int warp)
 {
-    int32_t *above = s.edge + 1, *left = s.edge + 65;
+    int32_t *edge = s.edge[warp];
+    int32_t *above = edge + 1, *left = edge + 65;
     if (have_top) {
         const int want = n + ((n == 4 && have_right) ? 4 : 0);
         const int cnt = min(want, pw - X0);
         for (int i = lane; i < 2 * n; i += 32) above[i] = HT(s, p, lx + (i < cnt ? i : cnt - 1), ly - 1);
         if (lane == 0) above[-1] = have_left ? HT(s, p, lx - 1, ly - 1) : kHbdMid + 1;
     } else {
-        for (int i = lane; i < 2 * n + 1; i += 32) s.edge[i] = kHbdMid - 1;
+        for (int i = lane; i < 2 * n + 1; i += 32) edge[i] = kHbdMid - 1;
     }
     for (int i = lane; i < n; i += 32) left[i] = have_left ? HT(s, p, lx - 1, ly + min(i, ph - 1 - Y0)) : kHbdMid + 1;
     __syncwarp();
@@ -4784,9 +4788,9 @@ __device__ void hbd_intra_tx(HbdSmem &s, int p, int lx, int ly, int X0, int Y0, 
     __syncwarp();
 }
 
-/* One intra block by warp 0: each plane's TXs in raster order, each
+/* One intra block by one warp: each plane's TXs in raster order, each
  * predicted and given its residual before the next. */
-__device__ void hbd_intra_block(HbdSmem &s, const HbdBlk &b, int sbx, int sby, int lane)
+__device__ void hbd_intra_block(HbdSmem &s, const HbdBlk &b, int sbx, int sby, int lane, int warp)
 {
     const cvp9_job_t &job = s.jc;
     const int gx = sbx + b.x, gy = sby + b.y;
@@ -4807,7 +4811,7 @@ __device__ void hbd_intra_block(HbdSmem &s, const HbdBlk &b, int sbx, int sby, i
             for (int tx = 0; tx < nx; tx++) {
                 const int lx = ox + tx * n, ly = oy + ty * n;
                 hbd_intra_tx(s, p, lx, ly, gox + tx * n, goy + ty * n, pw, ph, n, mode, ty > 0 || mi_row > 0,
-                             tx > 0 || left_ok, (tx + 1) * n < pbw, lane);
+                             tx > 0 || left_ok, (tx + 1) * n < pbw, lane, warp);
                 if (!resid) continue;
                 if (off + (uint64_t)sz > (uint64_t)job.num_coeffs) { off = job.num_coeffs; continue; }
                 const int32_t *X = job.coeffs32 + off;
@@ -4905,13 +4909,50 @@ __global__ void __launch_bounds__(kHbdThreads, 3) k_hbd_recon(const cvp9_job_t *
             /* cells of the luma region a block writes (a sub-8x8 block its 8x8) */
             const HbdBlk &b = s.blk[tid];
             for (int cy = b.y >> 2; cy < min(16, (b.y + b.ch + 3) >> 2); cy++)
-                for (int cx = b.x >> 2; cx < min(16, (b.x + b.cw + 3) >> 2); cx++) atomicAdd(&s.cell[cy * 16 + cx], 1u);
+                for (int cx = b.x >> 2; cx < min(16, (b.x + b.cw + 3) >> 2); cx++) {
+                    atomicAdd(&s.cell[cy * 16 + cx], 1u);
+                    s.owner[cy * 16 + cx] = (uint8_t)tid;
+                }
         }
         __syncthreads();
         bool my_over = false;
         for (int i = tid; i < 256; i += kHbdThreads) my_over |= s.cell[i] > 1;
-        const bool overlap = __syncthreads_or(my_over) != 0;
+        bool overlap = __syncthreads_or(my_over) != 0;
         const bool any_intra = __syncthreads_or(my_intra) != 0;
+        if (any_intra && !overlap) {
+            /* dependency levels of the intra blocks: 1 + the deepest intra
+             * block owning a sample of the row above, the column to the
+             * left or the corner (inter blocks, reconstructed first, count
+             * 0). A block reading samples of a block later in the list runs
+             * the superblock in list order instead. */
+            if (tid == 0) {
+                int nlev = 0, bad = 0;
+                for (int i = 0; i < nb; i++) {
+                    const HbdBlk &b = s.blk[i];
+                    s.lvl[i] = 0;
+                    if (!(b.flags & 1)) continue;
+                    int lv = 0;
+                    const int cx0 = b.x >> 2, cy0 = b.y >> 2;
+                    const int cx1 = (b.x + b.cw - 1) >> 2, cy1 = (b.y + b.ch - 1) >> 2;
+                    auto dep = [&](int cx, int cy) {
+                        if (cx < 0 || cy < 0 || cx > 15 || cy > 15) return;
+                        const int c = cy * 16 + cx;
+                        if (!s.cell[c]) return;
+                        const int j = s.owner[c];
+                        if (j > i) bad = 1;
+                        else if (j < i) lv = max(lv, (int)s.lvl[j]);
+                    };
+                    for (int cx = cx0 - 1; cx <= cx1; cx++) dep(cx, cy0 - 1);
+                    for (int cy = cy0; cy <= cy1; cy++) dep(cx0 - 1, cy);
+                    s.lvl[i] = (uint8_t)(lv + 1);
+                    nlev = max(nlev, lv + 1);
+                }
+                s.nlev = nlev;
+                s.order_bad = bad;
+            }
+            __syncthreads();
+            overlap = s.order_bad != 0;
+        }
 
         /* 2. intra blocks read the neighbour SBs' samples: wait for them,
          * then load the row above (x = -1..63) and the column to the left */
@@ -4960,16 +5001,20 @@ __global__ void __launch_bounds__(kHbdThreads, 3) k_hbd_recon(const cvp9_job_t *
          * overlapping blocks one by one in list order */
         if (!overlap) {
             hbd_inter_blocks(s, 0, nb, nb, sbx, sby);
-            if (any_intra)
+            /* intra blocks level by level, the blocks of a level one warp each */
+            const int nlev = any_intra ? s.nlev : 0;
+            for (int L = 1; L <= nlev; L++) {
+                int k = 0;
                 for (int i = 0; i < nb; i++) {
-                    if (!(s.blk[i].flags & 1)) continue;
-                    if (warp == 0) hbd_intra_block(s, s.blk[i], sbx, sby, lane);
-                    __syncthreads();
+                    if (s.lvl[i] != L) continue;
+                    if (k++ % kHbdWarps == warp) hbd_intra_block(s, s.blk[i], sbx, sby, lane, warp);
                 }
+                __syncthreads();
+            }
         } else {
             for (int i = 0; i < nb; i++) {
                 if (s.blk[i].flags & 1) {
-                    if (warp == 0) hbd_intra_block(s, s.blk[i], sbx, sby, lane);
+                    if (warp == 0) hbd_intra_block(s, s.blk[i], sbx, sby, lane, warp);
                     __syncthreads();
                 } else {
                     hbd_inter_blocks(s, i, i + 1, nb, sbx, sby);
