@@ -122,6 +122,44 @@ def test_hbd_sparse_lists_equal_dense_arrays():
             assert np.array_equal(e.get_frame(sids[i]), dense[(list(cases)[i], f)]), (list(cases)[i], f)
 
 
+def test_hbd_blocks_out_of_decode_order():
+    """The blocks of every superblock listed in reverse: intra blocks then
+    read samples of blocks that come later in the list, so those
+    superblocks run block by block in list order; the frames must still be
+    the list-order oracle's."""
+    import ctypes as C
+    from compute_vp9_b200 import BlockInfo
+    e = HbdEngine()
+    sid = e.open_stream(256, 128)
+    orc = HbdOracleStream()
+    gen = hbd_frames(2, 256, 128, 3, seed=8, step=16, gop=3, intra_in_inter=0.4, all_intra_modes=1)
+    for f in range(3):
+        pf, c32 = next(gen)
+        p = pf.contents
+        nb = p.num_blocks
+        raw = np.ctypeslib.as_array(C.cast(p.blocks, C.POINTER(C.c_uint8)), shape=(nb * 32,)).reshape(nb, 32)
+        x = raw[:, 0].astype(int) | (raw[:, 1].astype(int) << 8)
+        y = raw[:, 2].astype(int) | (raw[:, 3].astype(int) << 8)
+        sb = (y >> 6) * 1000 + (x >> 6)
+        order, i = [], 0
+        while i < nb:
+            j = i
+            while j < nb and sb[j] == sb[i]:
+                j += 1
+            order += list(range(j - 1, i - 1, -1))
+            i = j
+        rev = np.ascontiguousarray(raw[order])
+        orig = C.cast(p.blocks, C.c_void_p).value       # the address (a field read aliases the struct)
+        p.blocks = C.cast(C.c_void_p(rev.ctypes.data), C.POINTER(BlockInfo))
+        try:
+            want = orc.decode(pf, c32)
+            assert e.submit([sid], [(pf, c32.ctypes.data)]) == CVP9_OK
+            assert e.wait() == CVP9_OK
+            _check(e.get_frame(sid), want, 256, 128, "reversed frame %d" % f)
+        finally:
+            p.blocks = C.cast(C.c_void_p(orig), C.POINTER(BlockInfo))   # the generator writes the next frame there
+
+
 def test_hbd_4k_config_content():
     e = HbdEngine()
     _run(e, {"c4_2160p": (2, 3840, 2160, 2, 288, C4)}, seed=1)
