@@ -997,6 +997,14 @@ def main():
     import torch
     torch.cuda.set_device(local)
     os.environ.setdefault("CVP9_CUDA_DEVICE", str(local))
+    if ws > 1:
+        # the legs rank 0 runs alone while the other ranks wait at a barrier
+        # (CPU baseline, single stream, serving and its sweeps, the mixed,
+        # FULL and 10-bit legs) are measured at N = 1; at N > 1 every rank
+        # runs the timed legs only, which keeps the wait well inside the
+        # process group's timeout
+        args.no_cpu = args.no_single = args.no_serve = args.no_capacity = True
+        args.no_mixed = args.no_full = args.no_hbd = True
     from compute_vp9_b200 import ARITH_FULL, ARITH_REFCPU, ARITH_SPEC
     from oracle.oracle_py import FULL, REFCPU, SPEC
     arith = {"spec": ARITH_SPEC, "full": ARITH_FULL}.get(args.arith, ARITH_REFCPU)
