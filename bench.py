@@ -703,6 +703,9 @@ class HbdWorkload:
             self.frames.append(row)
             self.nnz.append(nz)
             self.nblocks.append(nb)
+        # the int32 coefficients as views of the pinned arena (the CPU leg)
+        self.c32 = [[hv[oc:oc + c32.nbytes].view(np.int32) for (_, _, c32), (ob, oc) in zip(per, o)]
+                    for per, o in zip(per_stream, offs)]
         # the nonzero coefficients as (index, value) lists, in pinned memory
         # (what a parser emitting them as it decodes tokens would hand over)
         lists, total = [], 0
@@ -815,6 +818,34 @@ def hbd_live(wl, steps=60, fps=30.0):
                                   "(index, value) lists from host memory, frames downloaded"}
 
 
+def hbd_cpu(wl, threads):
+    """The 10-bit restatement (oracle/oracle_hbd.c; the reference has no 10-bit
+    path) on host cores, one stream per thread: its key frame untimed, then
+    one inter frame each, timed from the moment every thread has its key
+    frame. Returns (Mpx/s, threads, sample)."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.oracle_py import HbdOracleStream
+    threads = max(1, min(threads, wl.S))
+    ready = threading.Barrier(threads)
+
+    def work(s):
+        o = HbdOracleStream()
+        o.decode(C.pointer(wl.frames[s][0][0]), wl.c32[s][0])
+        ready.wait()
+        t0 = time.perf_counter()
+        o.decode(C.pointer(wl.frames[s][1][0]), wl.c32[s][1])
+        t1 = time.perf_counter()
+        o.close()
+        return t0, t1
+    with ThreadPoolExecutor(threads) as ex:
+        spans = list(ex.map(work, range(threads)))
+    wall = max(t1 for _, t1 in spans) - min(t0 for t0, _ in spans)
+    return (threads * wl.w * wl.h / wall / 1e6, threads,
+            "%d streams x 1 inter frame of %dx%d 10-bit (one stream per thread, key frame untimed)"
+            % (threads, wl.w, wl.h))
+
+
 def hbd_parity(streams=2, frames=3, seed0=1000):
     """Fresh 10-bit streams of the same content, every frame downloaded and
     compared with the 10-bit restatement (oracle/oracle_hbd.c)."""
@@ -870,6 +901,8 @@ def hbd_leg(args, rank, peak, parity=True):
            "dtype": "u16 samples, int64 butterflies"}
     out["live"] = hbd_live(wl)
     if parity:
+        v, th, sample = hbd_cpu(wl, host_cores())
+        out["cpu_port"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port", "sample": sample}
         out["parity"] = hbd_parity()
     return out
 
