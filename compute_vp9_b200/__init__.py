@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = [
     "cvp9_pack_coeffs",
     "cvp9_hbd_create", "cvp9_hbd_destroy", "cvp9_hbd_open_stream", "cvp9_hbd_close_stream",
     "cvp9_hbd_submit", "cvp9_hbd_submit_sparse", "cvp9_hbd_wait", "cvp9_hbd_get_frame", "cvp9_hbd_step_times",
+    "cvp9_hbd_timer_start", "cvp9_hbd_timer_stop",
 ]
 
 

@@ -52,6 +52,8 @@ def _lib():
         lib.cvp9_hbd_wait.argtypes = [vp]
         lib.cvp9_hbd_get_frame.argtypes = [vp, C.c_int, C.POINTER(HbdFrameInfo)]
         lib.cvp9_hbd_step_times.argtypes = [vp, C.POINTER(C.c_float)]
+        lib.cvp9_hbd_timer_start.argtypes = [vp]
+        lib.cvp9_hbd_timer_stop.argtypes = [vp, C.POINTER(C.c_float)]
         _bound = True
     return lib
 
@@ -118,6 +120,16 @@ class HbdEngine:
         ms = (C.c_float * 5)()
         self._lib.cvp9_hbd_step_times(self._h, ms)
         return list(ms)
+
+    def timer_start(self):
+        return self._lib.cvp9_hbd_timer_start(self._h)
+
+    def timer_stop(self):
+        ms = C.c_float()
+        rc = self._lib.cvp9_hbd_timer_stop(self._h, C.byref(ms))
+        if rc != CVP9_OK:
+            raise Cvp9Error(rc, "cvp9_hbd_timer_stop")
+        return ms.value
 
     def close(self):
         if self._h:

@@ -28,10 +28,12 @@
  *
  * Lifetime: host inputs are read while cvp9_hbd_submit runs (arrays in
  * page-locked memory until the step completes); with CVP9_HBD_DEVICE_INPUTS
- * the block records and coefficients are device pointers. A frame's planes
- * from cvp9_hbd_get_frame stay valid until the stream's next step is
- * submitted. One step is in flight at a time: submit completes the
- * previous step first.
+ * the block records and coefficients are device pointers. Two steps are in
+ * flight at most: a submit completes the step two before it first, so the
+ * upload of one step, the kernels of the one before and the download of
+ * the one before that overlap. cvp9_hbd_get_frame completes every step in
+ * flight and returns the stream's latest frame; its planes stay valid until
+ * the stream's second next step is submitted.
  */
 #ifndef CVP9_HBD_H
 #define CVP9_HBD_H
@@ -92,8 +94,13 @@ int  cvp9_hbd_wait(cvp9_hbd_t *h);
 /* The stream's most recent delivered frame (host planes). */
 int  cvp9_hbd_get_frame(cvp9_hbd_t *h, int sid, cvp9_hbd_frame_info_t *info);
 /* Device times of the last completed step in ms: upload, scan, recon,
- * loop filter, download. */
+ * loop filter, download (with steps in flight the spans overlap the
+ * neighbouring steps'). */
 int  cvp9_hbd_step_times(cvp9_hbd_t *h, float ms[5]);
+/* Device time from timer_start (recorded behind all queued work) to
+ * timer_stop (behind the last submitted step's download), in ms. */
+int  cvp9_hbd_timer_start(cvp9_hbd_t *h);
+int  cvp9_hbd_timer_stop(cvp9_hbd_t *h, float *ms);
 
 #ifdef __cplusplus
 }

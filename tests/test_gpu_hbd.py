@@ -160,6 +160,39 @@ def test_hbd_blocks_out_of_decode_order():
             p.blocks = C.cast(C.c_void_p(orig), C.POINTER(BlockInfo))   # the generator writes the next frame there
 
 
+def test_hbd_two_steps_in_flight():
+    """Steps submitted back to back (two in flight: the next step's upload
+    and the previous one's download around the kernels) give the frames of
+    steps waited for one at a time; dense and sparse submits mixed."""
+    e = HbdEngine()
+    cases = {k: CASES[k] for k in ("mixed", "small_tx_lf63")}
+    sids, gens, orcs = [], [], []
+    for name, (preset, w, h, frames, step, ov) in cases.items():
+        sids.append(e.open_stream(w, h))
+        gens.append(hbd_frames(preset, w, h, 4, seed=13, step=step, **ov))
+        orcs.append(HbdOracleStream())
+    keep = []
+    for f in range(4):
+        fr = [next(g) for g in gens]
+        want = [o.decode(pf, c) for o, (pf, c) in zip(orcs, fr)]
+        if f % 2:
+            lists = []
+            for pf, c in fr:
+                pos = np.nonzero(c[:pf.contents.num_coeffs])[0].astype(np.uint32)
+                val = c[pos].astype(np.int32)
+                keep += [pos, val, c]
+                lists.append((pos.size, pos.ctypes.data, val.ctypes.data))
+            assert e.submit_sparse(sids, [pf for pf, _ in fr], lists) == CVP9_OK
+        else:
+            keep += [c for _, c in fr]
+            assert e.submit(sids, [(pf, c.ctypes.data) for pf, c in fr]) == CVP9_OK
+        if f % 2:
+            # two steps in flight: check the second, which read the first
+            for sid, w, (name, (preset, ww, hh, *_)) in zip(sids, want, cases.items()):
+                _check(e.get_frame(sid), w, ww, hh, "%s frame %d" % (name, f))
+            assert e.wait() == CVP9_OK
+
+
 def test_hbd_4k_config_content():
     e = HbdEngine()
     _run(e, {"c4_2160p": (2, 3840, 2160, 2, 288, C4)}, seed=1)
