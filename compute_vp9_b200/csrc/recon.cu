@@ -4216,10 +4216,11 @@ __device__ __forceinline__ void lf_edge_full(T *s, int st, int fs, LfThr th)
 /* Filter size of the edge on the left (dir 0) or top (dir 1) of 8x8 unit
  * (ux, uy) of a plane, 0 for none; inner: the 4x4 edge 4 samples in is
  * filtered too. Chroma units take the block at their top-left MI. */
-__device__ __forceinline__ int lf_unit_edge(const cvp9_job_t &job, int plane, int ux, int uy, int dir, bool &inner)
+/* e: the mode-info word of the unit's top-left MI (k_lf_mimap). */
+__device__ __forceinline__ int lf_unit_edge(const cvp9_job_t &job, int plane, int ux, int uy, int dir, bool &inner,
+                                            uint32_t e)
 {
     const int ss = plane > 0;
-    const uint32_t e = job.mi_map[(size_t)(uy << ss) * job.mi_cols + (ux << ss)];
     const uint32_t info = (e >> 16) == (job.epoch & 0xFFFFu) ? (e & 0xFFFFu) : 0u;
     const int tx = ss ? (int)((info >> 2) & 3u) : (int)(info & 3u);
     const bool skipi = (info >> 4) & 1u;
@@ -4260,6 +4261,7 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
     using Q4 = typename Quad<T>::type;
     __shared__ __align__(16) T wy[kLfY * kLfY];
     __shared__ __align__(16) T wc[2][kLfC * kLfC];
+    __shared__ uint32_t mi_s[64];          /* the superblock's 8x8 mode-info words */
     __shared__ int s_ticket;
     const int tid = threadIdx.x;
     for (;;) {
@@ -4294,6 +4296,11 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
             }
             __syncthreads();
             const int X0 = c * 64, Y0 = row * 64, XC = c * 32, YC = row * 32;
+            /* the superblock's mode info, once: each edge decision reads it */
+            if (tid < 64) {
+                const int mr = row * 8 + (tid >> 3), mc = c * 8 + (tid & 7);
+                mi_s[tid] = (mr < job.mi_rows && mc < job.mi_cols) ? job.mi_map[(size_t)mr * job.mi_cols + mc] : 0u;
+            }
             /* load the windows (4-byte words: W and the window origins are
              * multiples of 8, so every word is inside one row) */
             for (int i = tid; i < kLfY * (kLfY / 4); i += 128) {
@@ -4323,7 +4330,9 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 if (gy < ph)
                     for (int x = 0; x < sz && gx0 + x < pw; x += 8) {
                         bool inner;
-                        const int fs = lf_unit_edge(job, p, (gx0 + x) >> 3, gy >> 3, 0, inner);
+                        const int ux = (gx0 + x) >> 3, uy = gy >> 3, ss = p > 0;
+                        const int fs = lf_unit_edge(job, p, ux, uy, 0, inner,
+                                                    mi_s[((uy << ss) - row * 8) * 8 + (ux << ss) - c * 8]);
                         if (fs) lf_edge_full<T, SH>(row_p + x, 1, fs, th);
                         if (inner && gx0 + x + 4 < pw) lf_edge_full<T, SH>(row_p + x + 4, 1, 4, th);
                     }
@@ -4340,7 +4349,9 @@ __global__ void __launch_bounds__(128) k_lf_full(const cvp9_job_t *__restrict__ 
                 if (gx < pw)
                     for (int y = 0; y < sz && gy0 + y < ph; y += 8) {
                         bool inner;
-                        const int fs = lf_unit_edge(job, p, gx >> 3, (gy0 + y) >> 3, 1, inner);
+                        const int ux = gx >> 3, uy = (gy0 + y) >> 3, ss = p > 0;
+                        const int fs = lf_unit_edge(job, p, ux, uy, 1, inner,
+                                                    mi_s[((uy << ss) - row * 8) * 8 + (ux << ss) - c * 8]);
                         if (fs) lf_edge_full<T, SH>(col_p + y * pitch, pitch, fs, th);
                         if (inner && gy0 + y + 4 < ph) lf_edge_full<T, SH>(col_p + (y + 4) * pitch, pitch, 4, th);
                     }
