@@ -1154,7 +1154,7 @@ def main():
             cpu = {"value": v, "unit": UNIT, "cores": cthreads, "kind": kind, "sample": sample}
         launches_per_step = int(R["stats"].kernel_launches)
         lat = E["lat"]
-        # configs[1]-style content (blocks 8-64, TX 4x4-32x32 weighted
+        # the 1080p GOP-60 stream's content (blocks 8-64, TX 4x4-32x32 weighted
         # 30/30/25/15, 2-20% coefficients, +-128 px MVs over LAST/GOLDEN/
         # ALTREF, filters uniform over regular/smooth/sharp, GOP 60): REFCPU
         # and the VP9 (FULL) profile

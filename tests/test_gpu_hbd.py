@@ -29,7 +29,7 @@ CASES = {
                                      "all_intra_modes": 1, "intra_in_inter": 0.3}),
 }
 
-# configs[4]-shaped content: 3840x2160, 32x32 TX on half the blocks, 10%
+# the 10-bit 2160p workload's content: 32x32 TX on half the blocks, 10%
 # coefficients, +-256 px MVs, the sharp filter, three references, dequantised
 # values up to +-2^17
 C4 = dict(gop=120, tx_weights=[10, 15, 25, 50], density_min=0.10, density_max=0.10, mv_range_px=256,
