@@ -33,7 +33,9 @@
  * upload of one step, the kernels of the one before and the download of
  * the one before that overlap. cvp9_hbd_get_frame completes every step in
  * flight and returns the stream's latest frame; its planes stay valid until
- * the stream's second next step is submitted.
+ * the stream's second next step is submitted. An engine is used from one
+ * thread at a time (as a reference decoder context is); separate engines
+ * are independent.
  */
 #ifndef CVP9_HBD_H
 #define CVP9_HBD_H

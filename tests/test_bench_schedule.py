@@ -29,3 +29,10 @@ def test_synthetic_key_frames_refresh_every_slot():
         syn = Synth(synth_config(preset, 128, 64, 3, gop=5))
         assert syn.frame(0).contents.hdr.refresh_frame_flags == 0xFF
         assert syn.frame(5).contents.hdr.refresh_frame_flags == 0xFF
+
+
+def test_10bit_schedule_has_one_key_step_per_gop():
+    frames = [bench.HbdWorkload.frame_of(t) for t in range(bench.HBD_GOP)]
+    assert frames[0] == 0 and frames.count(0) == 1     # the timed 120 steps start at a key frame
+    assert set(frames[1:]) == set(range(1, bench.HBD_DISTINCT))
+    assert bench.HbdWorkload.frame_of(bench.HBD_GOP) == 0
